@@ -1,0 +1,287 @@
+/*
+ * tealeaf_b200_2d.h -- C ABI of the B200 (sm_100a) TeaLeaf 2D kernel suite.
+ *
+ * libtealeaf_b200_2d.so is a drop-in kernel suite for the unchanged TeaLeaf
+ * 2D host (main.c, diffuse.c, drivers/, chunk.c built with -DNO_MPI). It
+ * exports the 23 functions of the reference kernel interface with the same
+ * names, argument meaning and accumulate/synchronous result semantics
+ * (2d/kernel_interface.h:13-71), the optional diffuse_overload hook
+ * (2d/application.h:9-11), and a few additional entry points marked "new"
+ * below.
+ *
+ * The Chunk / Settings / State structs below restate the reference layouts
+ * field for field (2d/chunk.h:10-79, 2d/settings.h:69-150) so the library
+ * reads the host's structs at the host's offsets; a test compares every
+ * offset against the reference headers. FieldBufferType and ChunkExtension
+ * are the suite's own choice (tealeaf_b200/suite/2d/chunk_extension.h):
+ * field buffers are device pointers the host never dereferences.
+ *
+ * Result semantics (2d/drivers/cg_driver.c:35,72,88): every double* result
+ * is ACCUMULATED (*out += value) and valid when the call returns.
+ * Error semantics: by default a CUDA or argument error prints a message and
+ * calls exit(1), as the reference die() does (2d/shared.c:97-111);
+ * tl2d_set_error_mode(TL_ERRMODE_RECORD) makes calls record the error and
+ * return instead (read it with tl2d_get_error).
+ */
+#ifndef TEALEAF_B200_2D_H
+#define TEALEAF_B200_2D_H
+
+#include <stdbool.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- suite-owned extension point (same text as suite/2d/chunk_extension.h) */
+#ifndef TL_B200_CHUNK_EXTENSION_2D
+#define TL_B200_CHUNK_EXTENSION_2D
+typedef double* FieldBufferType;
+struct TlSuite2D;
+typedef struct ChunkExtension
+{
+    struct TlSuite2D* suite;
+} ChunkExtension;
+#endif
+
+/* ---- constants shared with the host (2d/shared.h:22-43) ------------------ */
+#define TL_NUM_FIELDS 6
+#define TL_CHUNK_LEFT 0
+#define TL_CHUNK_RIGHT 1
+#define TL_CHUNK_BOTTOM 2
+#define TL_CHUNK_TOP 3
+#define TL_EXTERNAL_FACE (-1)
+#define TL_FIELD_DENSITY 0
+#define TL_FIELD_ENERGY0 1
+#define TL_FIELD_ENERGY1 2
+#define TL_FIELD_U 3
+#define TL_FIELD_P 4
+#define TL_FIELD_SD 5
+#define TL_CONDUCTIVITY 1
+#define TL_RECIP_CONDUCTIVITY 2
+#define TL_CG_ITERS_FOR_EIGENVALUES 20
+#define TL_ERROR_SWITCH_MAX 1.0
+/* Solver enum values (2d/settings.h:50-56) and Geometry (2d/settings.h:131-136). */
+#define TL_JACOBI_SOLVER 0
+#define TL_CG_SOLVER 1
+#define TL_CHEBY_SOLVER 2
+#define TL_PPCG_SOLVER 3
+#define TL_GEOM_RECTANGULAR 0
+#define TL_GEOM_CIRCULAR 1
+#define TL_GEOM_POINT 2
+
+/* ---- host structs: layout restated from 2d/settings.h:69-128 ------------- */
+struct Profile;
+
+typedef struct Settings
+{
+    struct Profile* kernel_profile;
+    struct Profile* application_profile;
+    struct Profile* wallclock_profile;
+    FILE* tea_out_fp;
+    int rank;
+    int end_step;
+    int presteps;
+    int max_iters;
+    int coefficient;
+    int ppcg_inner_steps;
+    int summary_frequency;
+    int halo_depth;
+    int num_states;
+    int num_chunks;
+    int num_chunks_per_rank;
+    int num_ranks;
+    bool* fields_to_exchange;   /* host bool[TL_NUM_FIELDS] */
+    bool is_offload;
+    bool error_switch;
+    bool check_result;
+    bool preconditioner;
+    double eps;
+    double dt_init;
+    double end_time;
+    double eps_lim;
+    char* tea_in_filename;
+    char* tea_out_filename;
+    char* test_problem_filename;
+    int solver;                 /* enum Solver */
+    char* solver_name;
+    int kernel_language;        /* enum Kernel_Language */
+    int grid_x_cells;
+    int grid_y_cells;
+    double grid_x_min;
+    double grid_y_min;
+    double grid_x_max;
+    double grid_y_max;
+    double dx;
+    double dy;
+} Settings;
+
+/* 2d/settings.h:139-150 */
+typedef struct State
+{
+    bool defined;
+    double density;
+    double energy;
+    double x_min;
+    double y_min;
+    double x_max;
+    double y_max;
+    double radius;
+    int geometry;               /* enum Geometry */
+} State;
+
+/* 2d/chunk.h:10-79 */
+typedef struct Chunk
+{
+    double dt_init;
+    int* neighbours;            /* host int[4] */
+    double* left_send;
+    double* left_recv;
+    double* right_send;
+    double* right_recv;
+    double* top_send;
+    double* top_recv;
+    double* bottom_send;
+    double* bottom_recv;
+    int left;
+    int right;
+    int bottom;
+    int top;
+    int x;                      /* cells incl. halo: x_cells + 2*halo_depth */
+    int y;
+    FieldBufferType density0;
+    FieldBufferType density;
+    FieldBufferType energy0;
+    FieldBufferType energy;
+    FieldBufferType u;
+    FieldBufferType u0;
+    FieldBufferType p;
+    FieldBufferType r;
+    FieldBufferType mi;
+    FieldBufferType w;
+    FieldBufferType kx;
+    FieldBufferType ky;
+    FieldBufferType sd;
+    FieldBufferType cell_x;
+    FieldBufferType cell_y;
+    FieldBufferType cell_dx;
+    FieldBufferType cell_dy;
+    FieldBufferType vertex_dx;
+    FieldBufferType vertex_dy;
+    FieldBufferType vertex_x;
+    FieldBufferType vertex_y;
+    FieldBufferType volume;
+    FieldBufferType x_area;
+    FieldBufferType y_area;
+    double theta;
+    double eigmin;
+    double eigmax;
+    double* cg_alphas;          /* host arrays of max_iters (drivers write them) */
+    double* cg_betas;
+    double* cheby_alphas;
+    double* cheby_betas;
+    struct ChunkExtension* ext;
+} Chunk;
+
+/* ---- reference kernel interface (2d/kernel_interface.h:13-71) ------------ */
+/* Initialisation kernels */
+void run_set_chunk_data(Chunk* chunk, Settings* settings);                 /* :13 */
+void run_set_chunk_state(Chunk* chunk, Settings* settings, State* states); /* :15 */
+void run_kernel_initialise(Chunk* chunk, Settings* settings);              /* :17 */
+void run_kernel_finalise(Chunk* chunk, Settings* settings);                /* :19 */
+/* Solver-wide kernels */
+void run_local_halos(Chunk* chunk, Settings* settings, int depth);         /* :23 */
+void run_pack_or_unpack(Chunk* chunk, Settings* settings, int depth,       /* :25 */
+        int face, bool pack, FieldBufferType field, double* buffer);
+void run_store_energy(Chunk* chunk, Settings* settings);                   /* :28 */
+void run_field_summary(Chunk* chunk, Settings* settings,                   /* :30 */
+        double* vol, double* mass, double* ie, double* temp);
+/* CG solver kernels */
+void run_cg_init(Chunk* chunk, Settings* settings,                         /* :35 */
+        double rx, double ry, double* rro);
+void run_cg_calc_w(Chunk* chunk, Settings* settings, double* pw);          /* :38 */
+void run_cg_calc_ur(Chunk* chunk, Settings* settings,                      /* :40 */
+        double alpha, double* rrn);
+void run_cg_calc_p(Chunk* chunk, Settings* settings, double beta);         /* :42 */
+/* Chebyshev solver kernels */
+void run_cheby_init(Chunk* chunk, Settings* settings);                     /* :46 */
+void run_cheby_iterate(Chunk* chunk, Settings* settings,                   /* :48 */
+        double alpha, double beta);
+/* Jacobi solver kernels */
+void run_jacobi_init(Chunk* chunk, Settings* settings, double rx, double ry); /* :52 */
+void run_jacobi_iterate(Chunk* chunk, Settings* settings, double* error);  /* :54 */
+/* PPCG solver kernels */
+void run_ppcg_init(Chunk* chunk, Settings* settings);                      /* :58 */
+void run_ppcg_inner_iteration(Chunk* chunk, Settings* settings,            /* :60 */
+        double alpha, double beta);
+/* Shared solver kernels */
+void run_copy_u(Chunk* chunk, Settings* settings);                         /* :64 */
+void run_calculate_residual(Chunk* chunk, Settings* settings);             /* :66 */
+void run_calculate_2norm(Chunk* chunk, Settings* settings,                 /* :68 */
+        FieldBufferType buffer, double* norm);
+void run_finalise(Chunk* chunk, Settings* settings);                       /* :70 */
+
+/* ---- optional host hook (2d/application.h:9-11, 2d/main.c:32-36) -------- */
+/* Device-resident replacement of diffuse() (2d/diffuse.c:10-19): runs every
+ * timestep with the solver loops kept on the GPU (scalars alpha/beta/rro
+ * formed on the device, one host synchronisation per batch of iterations)
+ * and finishes with the host's field_summary_driver(…, true) when the host
+ * provides it. */
+void diffuse_overload(Chunk* chunk, Settings* settings);
+
+/* ---- new entry points (no reference counterpart) ------------------------- */
+#define TL_ERRMODE_EXIT 0
+#define TL_ERRMODE_RECORD 1
+/* Error behaviour: TL_ERRMODE_EXIT (default, like die()) or TL_ERRMODE_RECORD. */
+void tl2d_set_error_mode(int mode);
+/* Returns the first recorded error code (0: none) and its message; clears it. */
+int tl2d_get_error(char* msg, int msg_len);
+/* The cudaStream_t every kernel of this chunk is issued on (as void*). */
+void* tl2d_stream(Chunk* chunk);
+
+/* Field ids for the host-buffer staging calls. */
+#define TL2D_DENSITY0 0
+#define TL2D_DENSITY 1
+#define TL2D_ENERGY0 2
+#define TL2D_ENERGY 3
+#define TL2D_U 4
+#define TL2D_U0 5
+#define TL2D_P 6
+#define TL2D_R 7
+#define TL2D_MI 8
+#define TL2D_W 9
+#define TL2D_KX 10
+#define TL2D_KY 11
+#define TL2D_SD 12
+#define TL2D_VOLUME 13
+#define TL2D_NUM_IDS 14
+/* Copies a full x*y field between a host buffer and the chunk (blocking;
+ * pinned host memory gives full PCIe/NVLink-C2C bandwidth). */
+void tl2d_upload_field(Chunk* chunk, Settings* settings, int field_id,
+        const double* host, long long count);
+void tl2d_download_field(Chunk* chunk, Settings* settings, int field_id,
+        double* host, long long count);
+
+/* Per-timestep statistics of the device-resident driver. */
+typedef struct TlStepStats
+{
+    int cg_iters;       /* CG iterations (CG solver, or presteps of Cheby/PPCG) */
+    int cheby_iters;
+    int ppcg_iters;     /* outer PPCG iterations */
+    int jacobi_iters;
+    int est_iters;      /* Chebyshev estimate */
+    int total_iters;    /* loop trips of the solver loop (tt at exit) */
+    double error;
+    double eigmin;
+    double eigmax;
+    double exact_error; /* ||u0 - A u||^2 after the solve (check_result) */
+} TlStepStats;
+
+/* One timestep of solve() (2d/diffuse.c:22-80) on the device-resident path. */
+void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEALEAF_B200_2D_H */
