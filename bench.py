@@ -1,0 +1,365 @@
+"""Benchmark: TeaLeaf 2D FP64 drop-in on B200 (solver iterations/s, HBM GB/s).
+
+Workload (default): the 4096^2 drop-in case -- 8 seeded rectangles + 4
+circles on [0,10]^2, reciprocal-density conductivity, CG to eps 1e-15,
+dt 0.004 (tealeaf_b200.problems.dropin_2d). A "step" is one implicit
+timestep (solve(), 2d/diffuse.c:22-80) of that problem.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--size 4096] [--solver cg|cheby|ppcg]
+
+B200 arm: value = solver iterations/s of the whole job (replicas on N GPUs,
+no data-path collective: the path does not shard, DESIGN.md "replicas only"),
+with the fields resident in HBM. e2e = the same metric through the
+reference-facing C ABI (run_* driven by the host mirror) with the inputs
+copied from pinned host buffers each step and the energy field copied back.
+Reference arm (--impl reference): the reference omp3 CPU program on this
+host's cores, bounded samples of the same workload (each step capped at a
+fixed iteration count).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+# Compulsory bytes per interior cell of each kernel (each operand read or
+# written once): w=Ap reads p,kx,ky writes w; u/r update reads u,p,r,w writes
+# u,r; p update reads p,r writes p; ...
+KERNEL_BYTES_PER_CELL = {
+    "k_cg_calc_w": 32, "k_cg_calc_ur": 48, "k_cg_calc_p": 24,
+    "k_cheby_sweep": 64, "k_add_p": 24, "k_ppcg_inner_a": 56, "k_ppcg_inner_b": 24,
+    "k_norm2": 8, "k_residual": 40,
+}
+# Algorithmic bytes of one CG iteration per interior cell (12 FP64 streams:
+# sweep 1 r,p,kx,ky -> p,w; sweep 2 u,p,r,w -> u,r).
+CG_BYTES_PER_CELL_ITER = 96
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(tea_in: str, steps: int, cap: int, threads: int):
+    """Reference omp3 program (stock flags) on this host: per-step (iterations, seconds)."""
+    from oracle.oracle import run_reference  # checker/baseline only
+    res = run_reference(tea_in, dims=2, suite="omp3", threads=threads, fast=True, max_iters=cap)
+    out = []
+    for s in res[:steps]:
+        it = sum(s.iterations.values())
+        out.append((it, s.seconds))
+    return out
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def bench_reference(args, rank, world):
+    from tealeaf_b200 import problems
+    if rank != 0:
+        return None
+    prob = problems.dropin_2d(args.size, seed=2, steps=args.warmup + args.steps, solver=args.solver)
+    threads = host_threads()
+    t0 = time.time()
+    samples = cpu_reference_sample(prob.tea_in(), args.warmup + args.steps, args.cpu_cap, threads)
+    timed = samples[args.warmup:]
+    iters = sum(i for i, _ in timed)
+    secs = sum(t for _, t in timed)
+    value = iters / secs if secs > 0 else 0.0
+    cells = args.size * args.size
+    line = {
+        "metric": "solver_iterations_per_s", "value": value, "unit": "iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(1, len(timed)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded tea.in generator)", "impl": "reference",
+        "config": {"workload": "dropin_2d_%d_%s" % (args.size, args.solver), "cells": cells,
+                   "solver": args.solver, "eps": 1e-15, "dt": 0.004, "parallelism": "replicas"},
+        "cells_iterations_per_s": value * cells,
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
+                         "sample": "reference omp3 (oracle/_ref/harness2d_omp3_fast, OMP_NUM_THREADS=%d), "
+                                   "%d timesteps capped at %d CG iterations each"
+                                   % (threads, len(timed), args.cpu_cap)},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(time.time() - t0, 2),
+    }
+    return line
+
+
+def bench_b200(args, rank, world, local_rank):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from tealeaf_b200 import abi, problems
+    from tealeaf_b200.host import Host
+
+    torch.cuda.set_device(local_rank)
+    lib = abi.load(2)
+    lib.tl2d_set_device(local_rank)
+    prob = problems.dropin_2d(args.size, seed=2, steps=args.warmup + args.steps + 8, solver=args.solver)
+    h = Host(prob.tea_in(), dims=2)
+    stream = torch.cuda.ExternalStream(h.lib.tl2d_stream(C.byref(h.chunk)))
+    cells = args.size * args.size
+    interior_launch_cells = cells
+
+    tt = 0
+    for _ in range(args.warmup):
+        h.solve(tt)
+        tt += 1
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    h.lib.tl2d_profile_reset(C.byref(h.chunk))
+    h.lib.tl2d_profile_enable(C.byref(h.chunk), 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = 0
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        e0.record(stream)
+        for _ in range(args.steps):
+            r = h.solve(tt)
+            iters += sum(r.iterations.values())
+            tt += 1
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    # per-kernel device time inside the timed region
+    prof = {}
+    idx = 0
+    name = C.create_string_buffer(128)
+    calls, kms = C.c_longlong(), C.c_double()
+    while h.lib.tl2d_profile_read(C.byref(h.chunk), idx, name, 128, C.byref(calls), C.byref(kms)):
+        if calls.value:
+            prof[name.value.decode()] = (calls.value, kms.value)
+        idx += 1
+    h.lib.tl2d_profile_enable(C.byref(h.chunk), 0)
+    launches = sum(c for c, _ in prof.values())
+
+    # whole-job aggregate: max device time over ranks, iterations summed
+    t = torch.tensor([ms, float(iters)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, iters_all = mx[0].item(), sm[1].item()
+    else:
+        ms_max, iters_all = ms, float(iters)
+    value = iters_all / (ms_max / 1000.0)
+
+    # e2e through the C ABI with host buffers: upload the step's inputs from
+    # pinned host memory, solve, read the energy field and summary back.
+    init = Host(prob.tea_in(), dims=2)
+    dens_h = torch.from_numpy(init.download("density")).pin_memory()
+    en_h = torch.from_numpy(init.download("energy")).pin_memory()
+    init.finalise()
+    out_h = torch.empty_like(en_h).pin_memory()
+    n = dens_h.numel()
+    e2e_iters = 0
+    e2 = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
+    nsteps_e2e = max(1, min(args.steps, args.e2e_steps))
+    fn_up, fn_down = h.lib.tl2d_upload_field, h.lib.tl2d_download_field
+    torch.cuda.synchronize()
+    e2[0].record(stream)
+    for _ in range(nsteps_e2e):
+        fn_up(C.byref(h.chunk), C.byref(h.settings), 1, C.c_void_p(dens_h.data_ptr()), n)
+        fn_up(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(en_h.data_ptr()), n)
+        r = h.solve(0)
+        fn_down(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(out_h.data_ptr()), n)
+        abi.check(h.lib, 2)
+        e2e_iters += sum(r.iterations.values())
+    e2[1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2[0].elapsed_time(e2[1])
+    te = torch.tensor([e2e_ms, float(e2e_iters)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = te.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = te.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        e2e_ms_max, e2e_iters_all = mx[0].item(), sm[1].item()
+    else:
+        e2e_ms_max, e2e_iters_all = e2e_ms, float(e2e_iters)
+    h.finalise()
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    # dominant kernel of the timed region
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roofline = None
+    if dom:
+        kname, (kcalls, kms_tot) = dom
+        base = kname.split("<")[0]
+        bpc = KERNEL_BYTES_PER_CELL.get(base)
+        if bpc:
+            avg_s = kms_tot / kcalls / 1000.0
+            achieved = bpc * interior_launch_cells / avg_s / 1e9
+            roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_per_launch(kname, cells),
+                        "bytes_per_launch": bpc * interior_launch_cells, "avg_launch_ms": kms_tot / kcalls,
+                        "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                        else "fallback 6650 GB/s"}
+    total_kernel_ms = sum(v[1] for v in prof.values())
+    eff_gbs = CG_BYTES_PER_CELL_ITER * cells * value / max(1, world) / 1e9
+    line = {
+        "metric": "solver_iterations_per_s", "value": value, "unit": "iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded tea.in generator, dropin_2d seed 2)",
+        "config": {"workload": "dropin_2d_%d_%s" % (args.size, args.solver), "cells": cells,
+                   "solver": args.solver, "eps": 1e-15, "dt": 0.004, "parallelism": "replicas",
+                   "l2": "no flush: working set %.2f GB > 126 MB L2" % (8 * (args.size + 4) ** 2 * 8 / 1e9),
+                   "driver": "host mirror over run_* (synchronous reductions)"},
+        "cells_iterations_per_s": value * cells,
+        "hbm_effective_gbs_per_gpu": eff_gbs,
+        "hbm_effective_frac_per_gpu": eff_gbs / peak,
+        "roofline": roofline,
+        "kernels": {k: {"calls": c, "ms": round(m, 3), "share": round(m / total_kernel_ms, 4)}
+                    for k, (c, m) in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_iters_all / (e2e_ms_max / 1000.0), "unit": "iter/s",
+                "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8 + 32,
+                "steps": nsteps_e2e, "path": "run_* C ABI + tl2d_upload/download_field, pinned host buffers"},
+        "clocks": sampler.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = host_threads()
+            samples = cpu_reference_sample(prob.tea_in(), 2, args.cpu_cap, threads)
+            it_s = sum(i for i, _ in samples) / sum(t for _, t in samples)
+            line["cpu_baseline"] = {"value": it_s, "unit": "iter/s", "cores": threads, "kind": "reference",
+                                    "sample": "reference omp3 (stock flags) on this host, 2 timesteps of the "
+                                              "same workload capped at %d CG iterations each" % args.cpu_cap}
+        except Exception as exc:  # baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    return line
+
+
+def traffic_per_launch(kernel: str, cells: int):
+    """DRAM bytes per launch from the committed ncu summary (scaled per cell), if any."""
+    p = REPO / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        per_cell = d["bytes_per_cell"].get(kernel.split("<")[0])
+        return None if per_cell is None else per_cell * cells
+    except Exception:
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--solver", default="cg", choices=["cg", "cheby", "ppcg"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-cap", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = bench_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        line = bench_b200(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -33,6 +33,12 @@
 extern "C" {
 #endif
 
+/* Every function below is exported even when the library is built with
+ * hidden default visibility. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 /* ---- suite-owned extension point (same text as suite/2d/chunk_extension.h) */
 #ifndef TL_B200_CHUNK_EXTENSION_2D
 #define TL_B200_CHUNK_EXTENSION_2D
@@ -236,8 +242,18 @@ void diffuse_overload(Chunk* chunk, Settings* settings);
 void tl2d_set_error_mode(int mode);
 /* Returns the first recorded error code (0: none) and its message; clears it. */
 int tl2d_get_error(char* msg, int msg_len);
+/* Selects the CUDA device for the chunks initialised afterwards on this thread. */
+void tl2d_set_device(int device);
 /* The cudaStream_t every kernel of this chunk is issued on (as void*). */
 void* tl2d_stream(Chunk* chunk);
+
+/* Per-kernel device-time profile (CUDA events around every launch on the
+ * chunk's stream, resolved at the next synchronisation): enable/disable,
+ * reset, and read entry `index` (returns 0 past the last entry). */
+void tl2d_profile_enable(Chunk* chunk, int on);
+void tl2d_profile_reset(Chunk* chunk);
+int tl2d_profile_read(Chunk* chunk, int index, char* name, int name_len,
+        long long* calls, double* ms);
 
 /* Field ids for the host-buffer staging calls. */
 #define TL2D_DENSITY0 0
@@ -279,6 +295,10 @@ typedef struct TlStepStats
 
 /* One timestep of solve() (2d/diffuse.c:22-80) on the device-resident path. */
 void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stats);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

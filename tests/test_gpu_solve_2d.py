@@ -1,0 +1,69 @@
+"""Whole-solve parity of the 2D suite (B200 only).
+
+Two hosts drive the suite through the unchanged kernel interface:
+  * the Python mirror of the reference drivers (tealeaf_b200.host.Host);
+  * the reference's OWN C host and drivers, compiled from the reference
+    sources and linked with libtealeaf_b200_2d.so (oracle/_ref/harness2d_b200).
+Both are compared with the golden fixtures produced by the reference omp3
+program: per-step iteration counts exactly, field summaries (vol, mass, ie,
+temp) within 1e-12 relative.
+"""
+import json
+
+import pytest
+
+from oracle.oracle import harness_path, run_reference
+from tealeaf_b200.host import Host
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def golden(golden_dir):
+    return {c["name"]: c for c in json.loads((golden_dir / "ref_runs.json").read_text())}
+
+
+def compare(steps, gold, rtol=RTOL):
+    assert len(steps) == len(gold["steps"])
+    for n, (s, g) in enumerate(zip(steps, gold["steps"])):
+        assert s.iterations == g["iterations"], "step %d" % (n + 1)
+        for a, b in zip(s.summary, g["summary"]):
+            assert a == pytest.approx(float(b), rel=rtol), "step %d" % (n + 1)
+
+
+CASES_2D = ["shipped_2d_64_1", "odd_2d_97x61_cg", "odd_2d_97x61_cheby", "odd_2d_97x61_ppcg",
+            "odd_2d_97x61_jacobi", "plain_2d_512_cg", "plain_2d_512_cheby"]
+
+
+@pytest.mark.parametrize("name", CASES_2D)
+def test_python_host_matches_reference(name, golden_dir):
+    g = golden(golden_dir)[name]
+    h = Host(g["tea_in"], dims=2)
+    try:
+        steps = h.run()
+    finally:
+        h.finalise()
+    compare(steps, g)
+
+
+@pytest.mark.parametrize("name", ["shipped_2d_64_1", "odd_2d_97x61_cg", "odd_2d_97x61_cheby",
+                                  "odd_2d_97x61_ppcg", "plain_2d_512_cg"])
+def test_reference_host_binary_dropin(name, golden_dir):
+    """The unchanged reference C host + drivers, linked with the B200 library."""
+    if not harness_path(2, "b200").exists():
+        pytest.skip("oracle/_ref/harness2d_b200 not built")
+    g = golden(golden_dir)[name]
+    steps = run_reference(g["tea_in"], dims=2, suite="b200")
+    compare(steps, g)
+
+
+def test_known_answer_shipped_64(golden_dir):
+    """The reference's own known answer (2d/tea.problems: 64 64 1) at its 1e-5 tolerance."""
+    g = golden(golden_dir)["shipped_2d_64_1"]
+    h = Host(g["tea_in"], dims=2)
+    try:
+        temp = h.run()[-1].summary[3]
+    finally:
+        h.finalise()
+    assert abs(100.0 * (temp / g["tea_problems"]) - 100.0) < 0.001
