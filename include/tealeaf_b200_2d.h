@@ -293,6 +293,25 @@ typedef struct TlStepStats
     double exact_error; /* ||u0 - A u||^2 after the solve (check_result) */
 } TlStepStats;
 
+/* Allocation-free 2-norm: no counterpart in the reference. Adds the sum of
+ * squares of the interior of `field` (a device array of x*y values, halo
+ * included, index k + j*x) to the device double *norm_dev, like
+ * run_calculate_2norm does for a host double, with the same launch shape and
+ * summation order. For callers that cannot allocate device memory, or cannot
+ * take the device-wide synchronisation a cudaMalloc/cudaFree implies (e.g. a
+ * host whose memory is held by its own pool allocator): the reduction scratch
+ * is a static device array of 65536 block partials (about 512 KiB) that every
+ * GPU loading the library holds until exit, so this call allocates nothing.
+ * Interiors needing more than 65536 blocks of 128 x 8 cells (beyond about
+ * 8192 x 8192) are rejected with an error before any launch. Asynchronous on
+ * `stream` (a cudaStream_t, NULL for the default stream). The first call on
+ * a device looks up the array's address (cudaGetSymbolAddress) and caches it;
+ * make that first call before any stream capture. All calls share the one
+ * array: calls that overlap on the GPU race and must be serialised. Returns 0,
+ * or an error code with the message available from tl2d_get_error. */
+int tl2d_calculate_2norm_noalloc(const double* field, int x, int y, int halo_depth,
+        double* norm_dev, void* stream);
+
 /* One timestep of solve() (2d/diffuse.c:22-80) on the device-resident path. */
 void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stats);
 
