@@ -1,0 +1,534 @@
+// driver2d.cu -- device-resident timestep for the 2D suite.
+//
+// tl2d_solve_step runs one solve() (2d/diffuse.c:22-80) with the solver loops
+// of 2d/drivers/{cg,cheby,ppcg,jacobi}_driver.c kept on the GPU: the scalars
+// (alpha = rro/pw, beta = rrn/rro, the Chebyshev/PPCG coefficients by trip),
+// the stop test and the CG-to-Chebyshev/PPCG switch are evaluated by the last
+// block of each reduction, and the host only launches trips in batches and
+// looks at a mapped "done" word once per batch. Everything the host needs on
+// the way is computed on the host exactly as the reference drivers do: the
+// Lanczos eigenvalue bounds (tridiagonal QL), the Chebyshev tables and the
+// iteration estimate (single-precision logf/roundf, as cheby_driver.c:146-160).
+//
+// The fused sweeps of kernels2d.cuh do the CG iteration in 96 B/cell, a
+// Chebyshev trip in 56-72 B/cell and a PPCG inner step in 64 B/cell. Memory
+// ends each solve in the state the reference leaves it in: pending updates
+// and halo reflections are closed at the end of every phase, following the
+// reference's halo flags (e.g. the halo of u is not refreshed during PPCG).
+//
+// diffuse_overload (2d/application.h:9-11) runs every timestep this way.
+#include "suite2d_impl.hpp"
+
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+using namespace tl2d;
+
+extern "C" void print_and_log(Settings* settings, const char* format, ...) __attribute__((weak));
+extern "C" void field_summary_driver(Chunk* chunks, Settings* settings, bool is_solve_finished) __attribute__((weak));
+
+namespace {
+
+constexpr int kBatch = 16;   // solver-loop trips launched between looks at the done word
+
+// -------------------------------------------------------------- host maths --
+
+// Eigenvalues of a symmetric tridiagonal matrix, implicit QL with shifts
+// (published "tqli"; the reference adapts it, 2d/drivers/eigenvalue_driver.c:71-121).
+bool tridiag_ql(std::vector<double>& d, std::vector<double>& e)
+{
+    const int n = (int)d.size();
+    for (int i = 0; i < n - 1; ++i) e[i] = e[i + 1];
+    e[n - 1] = 0.0;
+    for (int l = 0; l < n; ++l) {
+        int sweeps = 0, m;
+        for (;;) {
+            for (m = l; m < n - 1; ++m) {
+                const double dd = fabs(d[m]) + fabs(d[m + 1]);
+                if (fabs(e[m]) + dd == dd) break;
+            }
+            if (m == l) break;
+            if (sweeps++ == 30) return false;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = sqrt((g * g) + 1.0);
+            g = d[m] - d[l] + e[l] / (g + (g < 0 ? -fabs(r) : fabs(r)));
+            double s = 1.0, c = 1.0, p = 0.0;
+            for (int i = m - 1; i >= l; --i) {
+                const double f = s * e[i];
+                const double b = c * e[i];
+                r = sqrt(f * f + g * g);
+                e[i + 1] = r;
+                if (r == 0.0) {
+                    d[i + 1] -= p;
+                    e[m] = 0.0;
+                    continue;
+                }
+                s = f / r;
+                c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * s + 2.0 * c * b;
+                p = s * r;
+                d[i + 1] = g + p;
+                g = c * r - b;
+            }
+            d[l] = d[l] - p;
+            e[l] = g;
+            e[m] = 0.0;
+        }
+    }
+    return true;
+}
+
+// eigenvalue_driver_initialise (2d/drivers/eigenvalue_driver.c:11-67)
+bool eigen_bounds(Chunk* chunk, int n)
+{
+    std::vector<double> d(n > 0 ? n : 1, 0.0), e(n > 0 ? n : 1, 0.0);
+    for (int i = 0; i < n; ++i) {
+        d[i] = 1.0 / chunk->cg_alphas[i];
+        if (i > 0) d[i] += chunk->cg_betas[i - 1] / chunk->cg_alphas[i - 1];
+        if (i < n - 1) e[i + 1] = sqrt(chunk->cg_betas[i]) / chunk->cg_alphas[i];
+    }
+    if (!tridiag_ql(d, e)) {
+        tl::fail(30, "Too many iterations in TQLI routine");
+        return false;
+    }
+    double lo = DBL_MAX, hi = DBL_MIN;
+    for (int i = 0; i < n; ++i) {
+        lo = d[i] < lo ? d[i] : lo;
+        hi = d[i] > hi ? d[i] : hi;
+    }
+    if (lo < 0.0 || hi < 0.0) {
+        tl::fail(31, "Calculated negative eigenvalues.");
+        return false;
+    }
+    chunk->eigmin = lo * 0.95;
+    chunk->eigmax = hi * 1.05;
+    return true;
+}
+
+// cheby_coef_driver (2d/drivers/cheby_driver.c:163-183)
+void cheby_coefs(Chunk* chunk, int count)
+{
+    chunk->theta = (chunk->eigmax + chunk->eigmin) / 2.0;
+    const double delta = (chunk->eigmax - chunk->eigmin) / 2.0;
+    const double sigma = chunk->theta / delta;
+    double rho_old = 1.0 / sigma;
+    for (int i = 0; i < count; ++i) {
+        const double rho_new = 1.0 / (2.0 * sigma - rho_old);
+        chunk->cheby_alphas[i] = rho_new * rho_old;
+        chunk->cheby_betas[i] = 2.0 * rho_new / delta;
+        rho_old = rho_new;
+    }
+}
+
+// cheby_calc_est_iterations (2d/drivers/cheby_driver.c:146-160)
+int cheby_est(const Chunk* chunk, double error, double bb)
+{
+    const double cn = chunk->eigmax / chunk->eigmin;
+    const double it_alpha = DBL_EPSILON * bb / (4.0 * error);
+    const double gamm = (sqrt(cn) - 1.0) / (sqrt(cn) + 1.0);
+    return (int)roundf(logf(it_alpha) / (2.0 * logf(gamm)));
+}
+
+// ------------------------------------------------------------- the driver --
+
+struct Run {
+    TlSuite2D* s;
+    Chunk* chunk;
+    Settings* settings;
+    DevParams prm;
+    Faces fc;
+    dim3 gi;
+    DevState host_state;   // last copy read back
+
+    const int* done() const { return &s->d_state->done; }
+
+    DevState read_state()
+    {
+        TL_CUDA(cudaMemcpyAsync(&host_state, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+        if (s->prof.on) s->prof.resolve();
+        return host_state;
+    }
+    void write_state(const DevState& st)
+    {
+        host_state = st;
+        s->h_mirror[0] = st.done;
+        s->h_mirror[1] = st.trip;
+        s->h_mirror[2] = st.reason;
+        TL_CUDA(cudaMemcpyAsync(s->d_state, &host_state, sizeof(DevState), cudaMemcpyHostToDevice, s->stream));
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+    }
+
+    // Launches trips through `launch_trip(t)` in batches, looking at the done
+    // word of the previous batch while the current one runs; returns when the
+    // loop has ended (state read back).
+    template <typename F>
+    DevState loop(int first_trip, F&& launch_trip)
+    {
+        cudaEvent_t ev[2];
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+        int t = first_trip, batch = 0;
+        bool pending_prev = false;
+        while (t < prm.max_iters && !tl::failed()) {
+            const int end = std::min(prm.max_iters, t + kBatch);
+            for (; t < end; ++t) launch_trip(t);
+            cudaEventRecord(ev[batch & 1], s->stream);
+            if (pending_prev) {
+                cudaEventSynchronize(ev[(batch + 1) & 1]);
+                if (*(volatile int*)&s->h_mirror[0]) break;
+            }
+            pending_prev = true;
+            ++batch;
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        return read_state();
+    }
+
+    // ------------------------------------------------------------- CG phase
+    // Trips `from`.. of cg_main_step_driver (2d/drivers/cg_driver.c:65-124)
+    // until the loop ends; `fresh`: the first trip follows cg_init (nothing
+    // pending). Closes the phase: last p update and the halo of u and p.
+    DevState cg_phase(int from, bool fresh)
+    {
+        double* buf[2] = {chunk->p, s->alt[ALT_P]};
+        FinCgW fin_w{s->d_state, s->d_cg_alphas};
+        FinCgUr fin_ur{s->d_state, s->d_cg_betas, prm, s->d_mirror};
+        const Scalar beta{0.0, &s->d_state->beta}, alpha{0.0, &s->d_state->alpha};
+        // parity of the current p buffer: trip t (t > from or !fresh) writes buf[(t - from + base) & 1]
+        int cur = 0;
+        auto trip = [&](int t) {
+            if (fresh && t == from) {
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gi, BX, 0, s->stream>>>(
+                              s->g, fc, beta, buf[cur], buf[cur], chunk->r, chunk->w, chunk->kx, chunk->ky,
+                              s->rs, done(), fin_w)));
+            } else {
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gi, BX, 0, s->stream>>>(
+                              s->g, fc, beta, buf[cur], buf[cur ^ 1], chunk->r, chunk->w, chunk->kx,
+                              chunk->ky, s->rs, done(), fin_w)));
+                cur ^= 1;
+            }
+            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<true><<<gi, BX, 0, s->stream>>>(
+                          s->g, fc, 1, alpha, chunk->u, buf[cur], chunk->r, chunk->w, s->rs, done(), fin_ur)));
+        };
+        DevState st = loop(from, trip);
+        // Trips from..st.trip-1 ran; the fused ones flipped the current buffer.
+        const int ran = st.trip - from;
+        const int flips = fresh ? std::max(0, ran - 1) : ran;
+        double* pcur = buf[flips & 1];
+        if (pcur != chunk->p) swap_alt(s, chunk, ALT_P);
+        TL_LAUNCH(s, "k_cg_close", (k_cg_close<<<gi, BX, 0, s->stream>>>(s->g, fc, beta, 1, chunk->p, chunk->r,
+                                                                           chunk->u)));
+        // host copies of the CG coefficients (the reference drivers keep them on the host)
+        if (st.trip > 0) {
+            TL_CUDA(cudaMemcpyAsync(chunk->cg_alphas, s->d_cg_alphas, sizeof(double) * st.trip,
+                                    cudaMemcpyDeviceToHost, s->stream));
+            TL_CUDA(cudaMemcpyAsync(chunk->cg_betas, s->d_cg_betas, sizeof(double) * st.trip,
+                                    cudaMemcpyDeviceToHost, s->stream));
+        }
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+        return st;
+    }
+
+    double norm(const double* b)
+    {
+        TL_LAUNCH(s, "k_norm2", k_norm2<<<gi, BX, 0, s->stream>>>(s->g, b, s->rs));
+        double o = 0.0;
+        fetch(s, 1, &o);
+        return o;
+    }
+
+    void copy(double* dst, const double* src)
+    {
+        TL_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)s->g.x * s->g.y, cudaMemcpyDeviceToDevice,
+                                s->stream));
+    }
+
+    // --------------------------------------------------------- Chebyshev
+    // 2d/drivers/cheby_driver.c:11-143 after the switch at trip `tt`.
+    DevState cheby_phase(int tt, TlStepStats* stats)
+    {
+        if (!eigen_bounds(chunk, tt)) return host_state;
+        const int count = prm.max_iters - tt;
+        cheby_coefs(chunk, count);
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, chunk->cheby_alphas, sizeof(double) * count,
+                                cudaMemcpyHostToDevice, s->stream));
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, chunk->cheby_betas, sizeof(double) * count,
+                                cudaMemcpyHostToDevice, s->stream));
+        const double bb = norm(chunk->u0);
+        // cheby_init (cheby.c:26-54) without its final u += p, which the next trip folds in
+        TL_LAUNCH(s, "k_cheby_sweep<init>",
+                  k_cheby_sweep<true><<<gi, BX, 0, s->stream>>>(s->g, 0.0, 0.0, chunk->theta, chunk->u, chunk->u0,
+                                                               chunk->p, chunk->r, chunk->w, chunk->kx, chunk->ky));
+        copy(s->alt[ALT_U], chunk->u);
+        copy(s->alt[ALT_P], chunk->p);
+        DevState st = host_state;
+        st.nch = 1;
+        st.est = 0;
+        st.done = 0;
+        st.reason = 0;
+        write_state(st);
+        double* ub[2] = {chunk->u, s->alt[ALT_U]};
+        double* pb[2] = {chunk->p, s->alt[ALT_P]};
+        ChebyCoef coef{0.0, 0.0, s->d_cheby_alphas, s->d_cheby_betas, s->d_state};
+        DevParams pc = prm;
+        pc.switch_enabled = 0;   // already switched
+        int cur = 0;
+        auto trip = [&](int t, int force) {
+            FinChebyTrip fin{s->d_state, pc, s->d_mirror, force};
+            TL_LAUNCH(s, "k_cheby_trip", (k_cheby_trip<true, true><<<gi, BX, 0, s->stream>>>(
+                          s->g, fc, coef, force, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->u0, chunk->w,
+                          chunk->r, chunk->kx, chunk->ky, s->rs, done(), fin, pc)));
+            cur ^= 1;
+            (void)t;
+        };
+        // first Chebyshev trip: always takes the norm, then the estimate
+        trip(tt, 1);
+        st = read_state();
+        const double error = s->h_out[0];
+        const int est = cheby_est(chunk, error, bb);
+        if (stats) stats->est_iters = est;
+        if (!st.done) {
+            st.est = est;
+            write_state(st);
+            st = loop(tt + 1, [&](int t) { trip(t, 0); });
+        }
+        const int trips = st.nch - 1;           // Chebyshev trips run
+        if (ub[trips & 1] != chunk->u) swap_alt(s, chunk, ALT_U);
+        if (pb[trips & 1] != chunk->p) swap_alt(s, chunk, ALT_P);
+        TL_LAUNCH(s, "k_add_p_close", k_add_p_close<<<gi, BX, 0, s->stream>>>(s->g, fc, chunk->u, chunk->p));
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+        if (stats) stats->cheby_iters = trips;
+        return st;
+    }
+
+    // --------------------------------------------------------------- PPCG
+    // 2d/drivers/ppcg_driver.c:10-189 after the switch at trip `tt`.
+    DevState ppcg_phase(int tt, TlStepStats* stats)
+    {
+        if (!eigen_bounds(chunk, tt)) return host_state;
+        const int ni = settings->ppcg_inner_steps;
+        cheby_coefs(chunk, ni);
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, chunk->cheby_alphas, sizeof(double) * ni,
+                                cudaMemcpyHostToDevice, s->stream));
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, chunk->cheby_betas, sizeof(double) * ni, cudaMemcpyHostToDevice,
+                                s->stream));
+        // ppcg_init_driver: r = u0 - A u (the halo of p is already in place)
+        TL_LAUNCH(s, "k_residual", k_residual<<<gi, BX, 0, s->stream>>>(s->g, chunk->u, chunk->u0, chunk->r,
+                                                                          chunk->kx, chunk->ky));
+        copy(s->alt[ALT_R], chunk->r);
+        copy(s->alt[ALT_SD], chunk->sd);
+        DevState st = host_state;
+        st.done = 0;
+        st.reason = 0;
+        st.nch = 0;
+        write_state(st);
+        double* pb[2] = {chunk->p, s->alt[ALT_P]};
+        double* rb[2] = {chunk->r, s->alt[ALT_R]};
+        double* sb[2] = {chunk->sd, s->alt[ALT_SD]};
+        int pc = 0, rc = 0, sc = 0;
+        const Scalar beta{0.0, &s->d_state->beta}, alpha{0.0, &s->d_state->alpha};
+        const PpcgCoef coef{0.0, 0.0, s->d_cheby_alphas, s->d_cheby_betas};
+        DevParams pp_prm = prm;
+        pp_prm.switch_enabled = 0;   // already switched
+        FinPpcgW fin_w{s->d_state};
+        FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
+        auto trip = [&](int t) {
+            if (t == tt) {
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gi, BX, 0, s->stream>>>(
+                              s->g, fc, beta, pb[pc], pb[pc], rb[rc], chunk->w, chunk->kx, chunk->ky, s->rs,
+                              done(), fin_w)));
+            } else {
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gi, BX, 0, s->stream>>>(
+                              s->g, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->w, chunk->kx, chunk->ky, s->rs,
+                              done(), fin_w)));
+                pc ^= 1;
+            }
+            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<false><<<gi, BX, 0, s->stream>>>(
+                          s->g, fc, 1, alpha, chunk->u, pb[pc], rb[rc], chunk->w, s->rs, done(), tl::NoFinish())));
+            for (int pp = 0; pp < ni; ++pp) {
+                const bool last = pp == ni - 1;
+                if (pp == 0 && last)
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<1, true><<<gi, BX, 0, s->stream>>>(
+                                  s->g, fc, chunk->theta, coef, 0, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1], chunk->u,
+                                  chunk->kx, chunk->ky, s->rs, done(), fin_n)));
+                else if (pp == 0)
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<1, false><<<gi, BX, 0, s->stream>>>(
+                                  s->g, fc, chunk->theta, coef, 0, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1], chunk->u,
+                                  chunk->kx, chunk->ky, s->rs, done(), tl::NoFinish())));
+                else if (last)
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<2, true><<<gi, BX, 0, s->stream>>>(
+                                  s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1],
+                                  chunk->u, chunk->kx, chunk->ky, s->rs, done(), fin_n)));
+                else
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<2, false><<<gi, BX, 0, s->stream>>>(
+                                  s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1],
+                                  chunk->u, chunk->kx, chunk->ky, s->rs, done(), tl::NoFinish())));
+                sc ^= 1;
+                rc ^= 1;
+            }
+        };
+        st = loop(tt, trip);
+        const int outer = st.nch;               // PPCG trips run
+        const int pflips = std::max(0, outer - 1);
+        const int rflips = outer * ni;
+        if (pb[pflips & 1] != chunk->p) swap_alt(s, chunk, ALT_P);
+        if (rb[rflips & 1] != chunk->r) swap_alt(s, chunk, ALT_R);
+        if (sb[rflips & 1] != chunk->sd) swap_alt(s, chunk, ALT_SD);
+        // close: the last sd update of the last inner step, the last p update
+        // and the halo of p (the halo of u is not refreshed during PPCG).
+        if (outer > 0) {
+            TL_LAUNCH(s, "k_ppcg_inner_b",
+                      k_ppcg_inner_b<<<gi, BX, 0, s->stream>>>(s->g, chunk->cheby_alphas[ni - 1],
+                                                               chunk->cheby_betas[ni - 1], chunk->sd, chunk->r));
+            TL_LAUNCH(s, "k_cg_close", (k_cg_close<<<gi, BX, 0, s->stream>>>(s->g, fc, beta, 1, chunk->p, chunk->r,
+                                                                               nullptr)));
+        }
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+        if (stats) stats->ppcg_iters = outer;
+        return st;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stats)
+{
+    if (tl::failed()) return;
+    TlSuite2D* s = suite_of(chunk);
+    if (!s) return;
+    if (settings->max_iters > s->table_len) {
+        tl::fail(32, "max_iters %d exceeds the %d the chunk was initialised with", settings->max_iters, s->table_len);
+        return;
+    }
+    if (settings->num_chunks_per_rank != 1) {
+        tl::fail(34, "the device-resident driver solves one chunk per rank (num_chunks_per_rank=%d)",
+                 settings->num_chunks_per_rank);
+        return;
+    }
+    flush(s, chunk);
+    TlStepStats local{};
+    TlStepStats* st_out = stats ? stats : &local;
+    *st_out = TlStepStats{};
+    Run R{s, chunk, settings, {}, faces_of(chunk), interior_grid(s->g), {}};
+    R.prm.eps = settings->eps;
+    R.prm.eps_lim = settings->eps_lim;
+    R.prm.max_iters = settings->max_iters;
+    R.prm.presteps = settings->presteps;
+    R.prm.error_switch = settings->error_switch ? 1 : 0;
+    R.prm.switch_enabled = (settings->solver == TL_CHEBY_SOLVER || settings->solver == TL_PPCG_SOLVER) ? 1 : 0;
+    R.prm.dims3 = 0;
+    bool* flags = settings->fields_to_exchange;
+
+    // solve(): dt, rx, ry (2d/diffuse.c:28-35)
+    const double dt = chunk->dt_init < settings->dt_init ? chunk->dt_init : settings->dt_init;
+    const double rx = dt / (settings->dx * settings->dx);
+    const double ry = dt / (settings->dy * settings->dy);
+    // halo of energy and density, depth 2 (2d/diffuse.c:38-41)
+    int h2[TL_NUM_FIELDS] = {0};
+    h2[TL_FIELD_ENERGY1] = h2[TL_FIELD_DENSITY] = 2;
+    for (int f = 0; f < TL_NUM_FIELDS; ++f) s->pend.halo[f] = h2[f];
+    flush(s, chunk);
+
+    double error = 1e10;
+    DevState st{};
+    if (settings->solver == TL_JACOBI_SOLVER) {
+        tl::fail(33, "the device-resident driver runs CG, Chebyshev and PPCG; drive Jacobi through run_*");
+        return;
+    }
+    // cg_init_driver: cg_init, halo(u, p) depth 1, copy_u (2d/drivers/cg_driver.c:30-62)
+    if (settings->coefficient != TL_CONDUCTIVITY && settings->coefficient != TL_RECIP_CONDUCTIVITY) {
+        tl::fail(7, "Coefficient %d is not valid.", settings->coefficient);
+        return;
+    }
+    TL_LAUNCH(s, "k_cg_init", k_cg_init<<<full_grid(s->g), FB, 0, s->stream>>>(
+                                  s->g, settings->coefficient, rx, ry, chunk->density, chunk->energy, chunk->u,
+                                  chunk->p, s->alt[ALT_P], chunk->r, chunk->w, chunk->kx, chunk->ky, s->rs,
+                                  FinCgInit{s->d_state, s->d_mirror}));
+    int h1[TL_NUM_FIELDS] = {0};
+    h1[TL_FIELD_U] = h1[TL_FIELD_P] = 1;
+    for (int f = 0; f < TL_NUM_FIELDS; ++f) s->pend.halo[f] = h1[f];
+    flush(s, chunk);
+    TL_LAUNCH(s, "k_copy_u", k_copy_u<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->u0, chunk->u));
+    R.read_state();
+
+    st = R.cg_phase(0, true);
+    error = st.error;
+    if (st.reason == 2 && settings->solver == TL_CHEBY_SOLVER) {
+        const int tt_sw = st.trip;
+        st = R.cheby_phase(tt_sw, st_out);
+        st_out->cg_iters = tt_sw;
+        error = st.error;
+        for (int f = 0; f < TL_NUM_FIELDS; ++f) flags[f] = false;
+        flags[TL_FIELD_U] = true;
+    } else if (st.reason == 2 && settings->solver == TL_PPCG_SOLVER) {
+        const int tt_sw = st.trip;
+        st = R.ppcg_phase(tt_sw, st_out);
+        st_out->cg_iters = tt_sw;
+        error = st.error;
+        for (int f = 0; f < TL_NUM_FIELDS; ++f) flags[f] = false;
+        flags[TL_FIELD_P] = true;
+    } else {
+        // converged or capped during CG
+        st_out->cg_iters = st.reason == 1 ? st.trip - 1 : st.trip;
+        for (int f = 0; f < TL_NUM_FIELDS; ++f) flags[f] = false;
+        flags[TL_FIELD_U] = flags[TL_FIELD_P] = true;
+    }
+    if (tl::failed()) return;
+    // the reference's printed iteration count is the loop index at exit
+    const int tt_exit = st.reason == 1 ? st.trip - 1 : st.trip;
+    st_out->total_iters = tt_exit;
+    if (settings->solver == TL_CHEBY_SOLVER && st_out->cheby_iters) st_out->cg_iters = tt_exit - st_out->cheby_iters + 1;
+    if (settings->solver == TL_PPCG_SOLVER && st_out->ppcg_iters) st_out->cg_iters = tt_exit - st_out->ppcg_iters + 1;
+    st_out->error = error;
+    st_out->eigmin = chunk->eigmin;
+    st_out->eigmax = chunk->eigmax;
+
+    // solve_finished_driver (2d/drivers/solve_finished_driver.c:7-43)
+    if (settings->check_result) {
+        TL_LAUNCH(s, "k_residual", k_residual<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->u, chunk->u0, chunk->r,
+                                                                            chunk->kx, chunk->ky));
+        st_out->exact_error = R.norm(chunk->r);
+    }
+    TL_LAUNCH(s, "k_finalise", k_finalise<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->energy, chunk->density, chunk->u));
+    flags[TL_FIELD_ENERGY1] = true;
+    for (int f = 0; f < TL_NUM_FIELDS; ++f) s->pend.halo[f] = flags[f] ? 1 : 0;
+    flush(s, chunk);
+    TL_CUDA(cudaStreamSynchronize(s->stream));
+
+    if (print_and_log && settings->tea_out_fp) {
+        if (settings->solver == TL_CG_SOLVER) {
+            print_and_log(settings, "CG: \t\t\t%d iterations\n", st_out->cg_iters);
+        } else if (settings->solver == TL_CHEBY_SOLVER) {
+            print_and_log(settings, "CG: \t\t\t%d iterations\n", st_out->cg_iters);
+            print_and_log(settings, "Cheby: \t\t\t%d iterations (%d estimated)\n", st_out->cheby_iters,
+                          st_out->est_iters);
+        } else {
+            print_and_log(settings, "CG: \t\t\t%d iterations\n", st_out->cg_iters);
+            print_and_log(settings, "PPCG: \t\t\t%d iterations (%d inner iterations per)\n", st_out->ppcg_iters,
+                          settings->ppcg_inner_steps);
+        }
+    }
+    (void)tt;
+}
+
+// 2d/application.h:9-11: replaces diffuse() (2d/diffuse.c:10-19).
+void diffuse_overload(Chunk* chunks, Settings* settings)
+{
+    if (print_and_log && settings->tea_out_fp)
+        print_and_log(settings, "This implementation overloads the diffuse function.\n");
+    for (int tt = 0; tt < settings->end_step && !tl::failed(); ++tt) {
+        if (print_and_log && settings->tea_out_fp) print_and_log(settings, "\nTimestep %d\n", tt + 1);
+        for (int cc = 0; cc < settings->num_chunks_per_rank; ++cc) tl2d_solve_step(&chunks[cc], settings, tt, nullptr);
+        if (settings->summary_frequency > 0 && tt % settings->summary_frequency == 0 && field_summary_driver)
+            field_summary_driver(chunks, settings, false);
+    }
+    if (field_summary_driver) field_summary_driver(chunks, settings, true);
+}
+
+}  // extern "C"

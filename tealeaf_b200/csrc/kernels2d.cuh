@@ -1,0 +1,948 @@
+// kernels2d.cuh -- device kernels of the 2D suite (included by suite2d.cu
+// and driver2d.cu; every kernel has internal linkage in each includer).
+//
+// Kernel shapes: interior sweeps run one thread per column (BX = 128 columns
+// per block, one warp = 256 contiguous bytes per load) and walk ROWS rows down
+// the column, carrying the vertical neighbours of the stencil in registers,
+// so each field is read from DRAM once per sweep. Reductions are fused into
+// the sweep that produces their operands and finished by one last-block pass
+// (common.cuh).
+//
+// Floating point: includers are compiled with -fmad=false so each + - * / is
+// one IEEE operation in the reference's expression order.
+#pragma once
+
+#include "common.cuh"
+#include "tealeaf_b200_2d.h"
+using tl::ReduceSlots;
+
+// Types have external linkage (identical in every includer); kernels are
+// static, so each includer has its own copies.
+namespace tl2d {
+
+constexpr int BX = 128;   // threads (columns) per block of an interior sweep
+constexpr int ROWS = 8;   // rows per thread of an interior sweep
+constexpr int FB = 256;   // threads per block of full-array kernels
+
+struct Geo {
+    int x, y, hd;
+};
+
+// ----------------------------------------------------------------- kernels
+
+__device__ __forceinline__ double coef_w(int coefficient, double density)
+{
+    return coefficient == TL_CONDUCTIVITY ? density : 1.0 / density;
+}
+
+__device__ __forceinline__ double face(double r, double wa, double wb)
+{
+    return r * (wa + wb) / (2.0 * wa * wb);
+}
+
+// 5-point operator in the reference operand order (2d/shared.h:49-54):
+// c = centre, l/r = x-1/x+1, d/u = y-1/y+1; kxc = kx[i], kxr = kx[i+1],
+// kyc = ky[i], kyu = ky[i+x].
+__device__ __forceinline__ double smvp(double kxc, double kxr, double kyc, double kyu,
+                                       double c, double l, double r, double d, double u)
+{
+    return (1.0 + (kxr + kxc) + (kyu + kyc)) * c - (kxr * r + kxc * l) - (kyu * u + kyc * d);
+}
+
+__device__ __forceinline__ int block_id() { return blockIdx.x + blockIdx.y * gridDim.x; }
+__device__ __forceinline__ int block_count() { return gridDim.x * gridDim.y; }
+
+// Column-strip coordinates of an interior sweep.
+struct Strip {
+    int k, j0, j1;
+    bool active;
+    __device__ Strip(const Geo& g)
+    {
+        k = g.hd + blockIdx.x * BX + threadIdx.x;
+        j0 = g.hd + blockIdx.y * ROWS;
+        j1 = min(j0 + ROWS, g.y - g.hd);
+        active = k < g.x - g.hd;
+    }
+};
+
+// w = A p and pw = sum(w*p)   (cg.c:88-113)
+static __global__ void __launch_bounds__(BX) k_cg_calc_w(Geo g, const double* __restrict__ p, double* __restrict__ w,
+                                                  const double* __restrict__ kx, const double* __restrict__ ky,
+                                                  ReduceSlots rs)
+{
+    Strip s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const int x = g.x;
+        long i = s.k + (long)s.j0 * x;
+        double pd = p[i - x], pc = p[i], kyc = ky[i];
+#pragma unroll 4
+        for (int j = s.j0; j < s.j1; ++j, i += x) {
+            const double pu = p[i + x], kyu = ky[i + x];
+            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, pc, p[i - 1], p[i + 1], pd, pu);
+            w[i] = v;
+            acc[0] += v * pc;
+            pd = pc;
+            pc = pu;
+            kyc = kyu;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count());
+}
+
+// u += alpha p; r -= alpha w; rrn = sum(r*r)   (cg.c:116-143)
+static __global__ void __launch_bounds__(BX) k_cg_calc_ur(Geo g, double alpha, double* __restrict__ u,
+                                                   const double* __restrict__ p, double* __restrict__ r,
+                                                   const double* __restrict__ w, ReduceSlots rs)
+{
+    Strip s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+        for (int j = s.j0; j < s.j1; ++j, i += g.x) {
+            u[i] += alpha * p[i];
+            const double rn = r[i] - alpha * w[i];
+            r[i] = rn;
+            acc[0] += rn * rn;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count());
+}
+
+// p = beta p + r   (cg.c:146-164)
+static __global__ void __launch_bounds__(BX) k_cg_calc_p(Geo g, double beta, double* __restrict__ p,
+                                                  const double* __restrict__ r)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) p[i] = beta * p[i] + r[i];
+}
+
+// Chebyshev sweep (cheby.c:26-85): w = A u; r = u0 - w;
+// p = r/theta (INIT) or alpha p + beta r. u itself is updated by k_add_p.
+template <bool INIT>
+static __global__ void __launch_bounds__(BX) k_cheby_sweep(Geo g, double alpha, double beta, double theta,
+                                                    const double* __restrict__ u, const double* __restrict__ u0,
+                                                    double* __restrict__ p, double* __restrict__ r,
+                                                    double* __restrict__ w, const double* __restrict__ kx,
+                                                    const double* __restrict__ ky)
+{
+    Strip s(g);
+    if (!s.active) return;
+    const int x = g.x;
+    long i = s.k + (long)s.j0 * x;
+    double ud = u[i - x], uc = u[i], kyc = ky[i];
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += x) {
+        const double uu = u[i + x], kyu = ky[i + x];
+        const double v = smvp(kx[i], kx[i + 1], kyc, kyu, uc, u[i - 1], u[i + 1], ud, uu);
+        w[i] = v;
+        const double rr = u0[i] - v;
+        r[i] = rr;
+        p[i] = INIT ? rr / theta : alpha * p[i] + beta * rr;
+        ud = uc;
+        uc = uu;
+        kyc = kyu;
+    }
+}
+
+// u += p on the interior (cheby_calc_u, cheby.c:8-24)
+static __global__ void __launch_bounds__(BX) k_add_p(Geo g, double* __restrict__ u, const double* __restrict__ p)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) u[i] += p[i];
+}
+
+// sd = r / theta   (ppcg.c:9-26)
+static __global__ void __launch_bounds__(BX) k_ppcg_init(Geo g, double theta, const double* __restrict__ r,
+                                                  double* __restrict__ sd)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) sd[i] = r[i] / theta;
+}
+
+// r -= A sd; u += sd   (ppcg.c:41-50)
+static __global__ void __launch_bounds__(BX) k_ppcg_inner_a(Geo g, double* __restrict__ u, double* __restrict__ r,
+                                                     const double* __restrict__ kx, const double* __restrict__ ky,
+                                                     const double* __restrict__ sd)
+{
+    Strip s(g);
+    if (!s.active) return;
+    const int x = g.x;
+    long i = s.k + (long)s.j0 * x;
+    double sdd = sd[i - x], sdc = sd[i], kyc = ky[i];
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += x) {
+        const double sdu = sd[i + x], kyu = ky[i + x];
+        const double v = smvp(kx[i], kx[i + 1], kyc, kyu, sdc, sd[i - 1], sd[i + 1], sdd, sdu);
+        r[i] -= v;
+        u[i] += sdc;
+        sdd = sdc;
+        sdc = sdu;
+        kyc = kyu;
+    }
+}
+
+// sd = alpha sd + beta r   (ppcg.c:52-60)
+static __global__ void __launch_bounds__(BX) k_ppcg_inner_b(Geo g, double alpha, double beta, double* __restrict__ sd,
+                                                     const double* __restrict__ r)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) sd[i] = alpha * sd[i] + beta * r[i];
+}
+
+// u0 = u on the interior   (solver_methods.c:9-25)
+static __global__ void __launch_bounds__(BX) k_copy_u(Geo g, double* __restrict__ u0, const double* __restrict__ u)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) u0[i] = u[i];
+}
+
+// r = u0 - A u   (solver_methods.c:28-48)
+static __global__ void __launch_bounds__(BX) k_residual(Geo g, const double* __restrict__ u, const double* __restrict__ u0,
+                                                 double* __restrict__ r, const double* __restrict__ kx,
+                                                 const double* __restrict__ ky)
+{
+    Strip s(g);
+    if (!s.active) return;
+    const int x = g.x;
+    long i = s.k + (long)s.j0 * x;
+    double ud = u[i - x], uc = u[i], kyc = ky[i];
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += x) {
+        const double uu = u[i + x], kyu = ky[i + x];
+        r[i] = u0[i] - smvp(kx[i], kx[i + 1], kyc, kyu, uc, u[i - 1], u[i + 1], ud, uu);
+        ud = uc;
+        uc = uu;
+        kyc = kyu;
+    }
+}
+
+// sum(b*b) over the interior   (solver_methods.c:51-71)
+static __global__ void __launch_bounds__(BX) k_norm2(Geo g, const double* __restrict__ b, ReduceSlots rs)
+{
+    Strip s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+        for (int j = s.j0; j < s.j1; ++j, i += g.x) acc[0] += b[i] * b[i];
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count());
+}
+
+// energy = u / density   (solver_methods.c:74-90)
+static __global__ void __launch_bounds__(BX) k_finalise(Geo g, double* __restrict__ energy,
+                                                 const double* __restrict__ density, const double* __restrict__ u)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+#pragma unroll 4
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) energy[i] = u[i] / density[i];
+}
+
+// vol, mass, ie, temp   (field_summary.c:8-45)
+static __global__ void __launch_bounds__(BX) k_field_summary(Geo g, const double* __restrict__ volume,
+                                                      const double* __restrict__ density,
+                                                      const double* __restrict__ energy0,
+                                                      const double* __restrict__ u, ReduceSlots rs)
+{
+    Strip s(g);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (s.active) {
+        long i = s.k + (long)s.j0 * g.x;
+        for (int j = s.j0; j < s.j1; ++j, i += g.x) {
+            const double cv = volume[i];
+            const double cm = cv * density[i];
+            acc[0] += cv;
+            acc[1] += cm;
+            acc[2] += cm * energy0[i];
+            acc[3] += cm * u[i];
+        }
+    }
+    tl::grid_sum<4, BX>(acc, rs, block_id(), block_count());
+}
+
+// Jacobi sweep (jacobi.c:78-101): reads r (a copy of u), writes u, L1 change.
+static __global__ void __launch_bounds__(BX) k_jacobi_iterate(Geo g, const double* __restrict__ kx,
+                                                       const double* __restrict__ ky,
+                                                       const double* __restrict__ u0, double* __restrict__ u,
+                                                       const double* __restrict__ r, ReduceSlots rs)
+{
+    Strip s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const int x = g.x;
+        long i = s.k + (long)s.j0 * x;
+        for (int j = s.j0; j < s.j1; ++j, i += x) {
+            const double kxc = kx[i], kxr = kx[i + 1], kyc = ky[i], kyu = ky[i + x];
+            const double v = (u0[i] + (kxr * r[i + 1] + kxc * r[i - 1]) + (kyu * r[i + x] + kyc * r[i - x]))
+                           / (1.0 + (kxc + kxr) + (kyc + kyu));
+            u[i] = v;
+            acc[0] += fabs(v - r[i]);
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count());
+}
+
+// ---- full-array kernels (thread per cell) --------------------------------
+
+// cg_init fused (cg.c:9-85), p written to both p buffers: u = e*rho everywhere; face coefficients on
+// [hd, n-1); w = A u, r = u - w, p = r on the interior with rro = sum(r*p);
+// p = r = 0 elsewhere and w = conductivity on the rest of [1, n-1).
+// Coefficients and neighbour values are recomputed from density/energy with
+// the reference expressions, so they equal the stored ones bit for bit.
+template <typename Finish>
+static __global__ void __launch_bounds__(FB) k_cg_init(Geo g, int coefficient, double rx, double ry,
+                                                const double* __restrict__ density,
+                                                const double* __restrict__ energy, double* __restrict__ u,
+                                                double* __restrict__ p, double* __restrict__ p2,
+                                                double* __restrict__ r,
+                                                double* __restrict__ w, double* __restrict__ kx,
+                                                double* __restrict__ ky, ReduceSlots rs, Finish fin)
+{
+    const int x = g.x, y = g.y, hd = g.hd;
+    const int k = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * (FB / 32) + (threadIdx.x >> 5);
+    double acc[1] = {0.0};
+    if (k < x && j < y) {
+        const long i = k + (long)j * x;
+        const double rho = density[i];
+        const double uc = energy[i] * rho;
+        u[i] = uc;
+        const bool interior = k >= hd && k < x - hd && j >= hd && j < y - hd;
+        const bool ring = k >= 1 && k < x - 1 && j >= 1 && j < y - 1;
+        const bool kzone = k >= hd && k < x - 1 && j >= hd && j < y - 1;
+        double wc = 0.0;
+        if (ring) wc = coef_w(coefficient, rho);
+        double kxc = 0.0, kyc = 0.0;
+        if (kzone) {
+            kxc = face(rx, coef_w(coefficient, density[i - 1]), wc);
+            kyc = face(ry, coef_w(coefficient, density[i - x]), wc);
+            kx[i] = kxc;
+            ky[i] = kyc;
+        }
+        if (interior) {
+            // kx[i+1] / ky[i+x] are computed only inside [hd, n-1); with a one-cell
+            // halo the last column/row keeps whatever the array held (cg.c:56-62).
+            const double kxr = (k + 1 < x - 1) ? face(rx, wc, coef_w(coefficient, density[i + 1])) : kx[i + 1];
+            const double kyu = (j + 1 < y - 1) ? face(ry, wc, coef_w(coefficient, density[i + x])) : ky[i + x];
+            const double ul = energy[i - 1] * density[i - 1];
+            const double ur = energy[i + 1] * density[i + 1];
+            const double ud = energy[i - x] * density[i - x];
+            const double uu = energy[i + x] * density[i + x];
+            const double v = smvp(kxc, kxr, kyc, kyu, uc, ul, ur, ud, uu);
+            w[i] = v;
+            const double rr = uc - v;
+            r[i] = rr;
+            p[i] = rr;
+            if (p2) p2[i] = rr;
+            acc[0] = rr * rr;
+        } else {
+            p[i] = 0.0;
+            if (p2) p2[i] = 0.0;
+            r[i] = 0.0;
+            if (ring) w[i] = wc;
+        }
+    }
+    tl::grid_sum<1, FB>(acc, rs, block_id(), block_count(), fin);
+}
+
+// jacobi_init (jacobi.c:10-57): u0 = u = e*rho on [1, n-1); kx, ky on [hd, n-1).
+static __global__ void __launch_bounds__(FB) k_jacobi_init(Geo g, int coefficient, double rx, double ry,
+                                                    const double* __restrict__ density,
+                                                    const double* __restrict__ energy, double* __restrict__ u0,
+                                                    double* __restrict__ u, double* __restrict__ kx,
+                                                    double* __restrict__ ky)
+{
+    const int x = g.x, y = g.y, hd = g.hd;
+    const int k = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * (FB / 32) + (threadIdx.x >> 5);
+    if (k >= x || j >= y) return;
+    const long i = k + (long)j * x;
+    if (k >= 1 && k < x - 1 && j >= 1 && j < y - 1) {
+        const double t = energy[i] * density[i];
+        u0[i] = t;
+        u[i] = t;
+    }
+    if (k >= hd && k < x - 1 && j >= hd && j < y - 1) {
+        const double c = coef_w(coefficient, density[i]);
+        const double l = coef_w(coefficient, density[i - 1]);
+        const double d = coef_w(coefficient, density[i - x]);
+        kx[i] = rx * (l + c) / (2.0 * l * c);
+        ky[i] = ry * (d + c) / (2.0 * d * c);
+    }
+}
+
+// set_chunk_data (set_chunk_data.c:10-53): vertices, cell centres, volumes, areas.
+static __global__ void k_set_chunk_data_axes(int x, int y, int hd, double x_min, double y_min, double dx, double dy,
+                                      double* vertex_x, double* vertex_y, double* cell_x, double* cell_y)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t <= x) vertex_x[t] = x_min + dx * (double)(t - hd);
+    if (t <= y) vertex_y[t] = y_min + dy * (double)(t - hd);
+    if (t < x) cell_x[t] = 0.5 * ((x_min + dx * (double)(t - hd)) + (x_min + dx * (double)(t + 1 - hd)));
+    if (t < y) cell_y[t] = 0.5 * ((y_min + dy * (double)(t - hd)) + (y_min + dy * (double)(t + 1 - hd)));
+}
+
+static __global__ void k_set_chunk_data_cells(long n, double dx, double dy, double* volume, double* x_area,
+                                       double* y_area)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        volume[i] = dx * dy;
+        x_area[i] = dy;
+        y_area[i] = dx;
+    }
+}
+
+// set_chunk_state (set_chunk_state.c:9-84): the last state that covers a cell wins.
+static __global__ void __launch_bounds__(FB) k_set_chunk_state(Geo g, const double* __restrict__ vertex_x,
+                                                        const double* __restrict__ vertex_y,
+                                                        const double* __restrict__ cell_x,
+                                                        const double* __restrict__ cell_y,
+                                                        double* __restrict__ density, double* __restrict__ energy0,
+                                                        double* __restrict__ u, int num_states,
+                                                        const State* __restrict__ states)
+{
+    const int x = g.x, y = g.y;
+    const int k = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int j = blockIdx.y * (FB / 32) + (threadIdx.x >> 5);
+    if (k >= x || j >= y) return;
+    const long i = k + (long)j * x;
+    double e = states[0].energy, d = states[0].density;
+    for (int s = 1; s < num_states; ++s) {
+        const State st = states[s];
+        bool hit = false;
+        if (st.geometry == TL_GEOM_RECTANGULAR) {
+            hit = vertex_x[k + 1] >= st.x_min && vertex_x[k] < st.x_max && vertex_y[j + 1] >= st.y_min &&
+                  vertex_y[j] < st.y_max;
+        } else if (st.geometry == TL_GEOM_CIRCULAR) {
+            const double ax = cell_x[k] - st.x_min, ay = cell_y[j] - st.y_min;
+            hit = sqrt(ax * ax + ay * ay) <= st.radius;
+        } else if (st.geometry == TL_GEOM_POINT) {
+            hit = vertex_x[k] == st.x_min && vertex_y[j] == st.y_min;
+        }
+        if (hit) {
+            e = st.energy;
+            d = st.density;
+        }
+    }
+    energy0[i] = e;
+    density[i] = d;
+    if (k >= 1 && k < x - 1 && j >= 1 && j < y - 1) u[i] = e * d;
+}
+
+// Reflective halo update of up to six fields (local_halos.c:21-149): for each
+// external face, copy `depth` interior layers outwards, interior span only.
+struct HaloArgs {
+    double* f[TL_NUM_FIELDS];
+    int nf;
+    int ext[4];  // left, right, bottom, top are external
+};
+
+static __global__ void k_local_halos(Geo g, int depth, HaloArgs a)
+{
+    const int x = g.x, y = g.y, hd = g.hd;
+    const int ny = y - 2 * hd, nx = x - 2 * hd;
+    const long per_field = (long)depth * (2L * ny + 2L * nx);
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= per_field || blockIdx.y >= (unsigned)a.nf) return;
+    double* f = a.f[blockIdx.y];
+    long q = t;
+    const int d = (int)(q % depth);
+    q /= depth;
+    if (q < ny) {  // left
+        if (!a.ext[0]) return;
+        const long row = (long)(hd + q) * x;
+        f[row + (hd - d - 1)] = f[row + (hd + d)];
+        return;
+    }
+    q -= ny;
+    if (q < ny) {  // right
+        if (!a.ext[1]) return;
+        const long row = (long)(hd + q) * x;
+        f[row + (x - hd + d)] = f[row + (x - hd - 1 - d)];
+        return;
+    }
+    q -= ny;
+    if (q < nx) {  // bottom
+        if (!a.ext[2]) return;
+        const long kk = hd + q;
+        f[kk + (long)(hd - d - 1) * x] = f[kk + (long)(hd + d) * x];
+        return;
+    }
+    q -= nx;
+    if (q < nx) {  // top
+        if (!a.ext[3]) return;
+        const long kk = hd + q;
+        f[kk + (long)(y - hd + d) * x] = f[kk + (long)(y - hd - 1 - d) * x];
+    }
+}
+
+// MPI face buffers (pack_halos.c:4-207): pack copies a face of the field into
+// a contiguous staging buffer, unpack scatters the buffer into the halo.
+static __global__ void k_pack(Geo g, int depth, int face, int pack, double* __restrict__ field, double* __restrict__ buf)
+{
+    const int x = g.x, y = g.y, hd = g.hd;
+    const int nx = x - 2 * hd, ny = y - 2 * hd;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long fi, bi;
+    if (face == TL_CHUNK_LEFT || face == TL_CHUNK_RIGHT) {
+        if (t >= (long)ny * depth) return;
+        const int jj = hd + (int)(t / depth), c = (int)(t % depth);
+        int kk;
+        if (face == TL_CHUNK_LEFT) kk = pack ? hd + c : hd - depth + c;
+        else kk = pack ? x - hd - depth + c : x - hd + c;
+        fi = (long)jj * x + kk;
+        bi = c + (long)(jj - hd) * depth;
+    } else {
+        if (t >= (long)nx * depth) return;
+        const int kk = hd + (int)(t % nx), c = (int)(t / nx);
+        int jj;
+        if (face == TL_CHUNK_BOTTOM) jj = pack ? hd + c : hd - depth + c;
+        else jj = pack ? y - hd - depth + c : y - hd + c;
+        fi = (long)jj * x + kk;
+        bi = (kk - hd) + (long)c * nx;
+    }
+    if (pack) buf[bi] = field[fi];
+    else field[fi] = buf[bi];
+}
+
+
+// ===================================================================
+// Fused kernels: each absorbs the operations the reference performs between
+// two sweeps (the p update of the previous CG step, the reflective halo of
+// the stencil operand, the "u += p" of the previous Chebyshev step, the sd
+// update of the previous PPCG inner step), so one pass over memory does what
+// the reference does in two or three. Values that the reference would read
+// from a freshly reflected halo are taken from the mirrored interior cell
+// directly, and the reflected values are also written to the halo cells, so
+// memory ends in the state the reference leaves it in.
+// ===================================================================
+
+// Scalar operand: a host value, or a device location (device-resident driver).
+struct Scalar {
+    double v;
+    const double* dev;
+    __device__ __forceinline__ double get() const { return dev ? *dev : v; }
+};
+
+// External faces whose depth-1 halo is reflected (left, right, bottom, top).
+struct Faces {
+    int l, r, b, t;
+};
+
+// Control block of the device-resident solver loops (device memory).
+struct DevState {
+    double rro, pw, rrn, alpha, beta, error;
+    double theta;
+    int trip;     // completed trips of the solver loop (the reference's tt)
+    int done;     // the loop has ended
+    int reason;   // 1 converged, 2 switch to Chebyshev/PPCG, 3 max_iters
+    int nch;      // Chebyshev trips done (next coefficient index)
+    int est;      // Chebyshev iteration estimate
+    int pad;
+};
+
+// Read-only parameters of a solve.
+struct DevParams {
+    double eps, eps_lim;
+    int max_iters, presteps, error_switch, switch_enabled, dims3;
+};
+
+// Stop test of the solver loops: 2D tests the error itself, 3D its square
+// root (3d/drivers/cg_solver_driver.c:24-25); the switch from CG to
+// Chebyshev/PPCG is evaluated for the next trip (2d/drivers/cheby_driver.c:30-32).
+__device__ __forceinline__ void end_of_trip(DevState* st, const DevParams& prm, double error, int* host_mirror)
+{
+    const double e = prm.dims3 ? sqrt(error) : error;
+    st->error = e;
+    const int tt = st->trip;
+    st->trip = tt + 1;
+    int reason = 0;
+    if (fabs(e) < prm.eps) reason = 1;
+    else if (tt + 1 >= prm.max_iters) reason = 3;
+    else if (prm.switch_enabled) {
+        const bool sw = prm.error_switch ? (e < prm.eps_lim) && (tt + 1 > TL_CG_ITERS_FOR_EIGENVALUES)
+                                         : (tt + 1 > prm.presteps) && (e < TL_ERROR_SWITCH_MAX);
+        if (sw) reason = 2;
+    }
+    if (reason) {
+        st->done = 1;
+        st->reason = reason;
+    }
+    if (host_mirror) {
+        host_mirror[0] = st->done;
+        host_mirror[1] = st->trip;
+        host_mirror[2] = st->reason;
+    }
+}
+
+// Finishers (thread 0 of the last block, with the grid totals).
+struct FinCgInit {         // rro of cg_init_driver (cg_driver.c:30-62) starts the loop state
+    DevState* st;
+    int* host_mirror;
+    __device__ void operator()(const double* t) const
+    {
+        st->rro = t[0];
+        st->trip = 0;
+        st->done = 0;
+        st->reason = 0;
+        st->nch = 0;
+        st->error = 1e10;
+        if (host_mirror) {
+            host_mirror[0] = 0;
+            host_mirror[1] = 0;
+            host_mirror[2] = 0;
+        }
+    }
+};
+
+struct FinCgW {            // alpha = rro / pw; cg_alphas[tt] = alpha  (cg_driver.c:87-93)
+    DevState* st;
+    double* cg_alphas;
+    __device__ void operator()(const double* t) const
+    {
+        st->pw = t[0];
+        const double a = st->rro / t[0];
+        st->alpha = a;
+        if (cg_alphas) cg_alphas[st->trip] = a;
+    }
+};
+
+struct FinCgUr {           // beta = rrn / rro; rro = error = rrn  (cg_driver.c:104-123)
+    DevState* st;
+    double* cg_betas;
+    DevParams prm;
+    int* host_mirror;
+    __device__ void operator()(const double* t) const
+    {
+        const double rrn = t[0];
+        const double b = rrn / st->rro;
+        st->beta = b;
+        cg_betas[st->trip] = b;
+        st->rro = rrn;
+        st->rrn = rrn;
+        end_of_trip(st, prm, rrn, host_mirror);
+    }
+};
+
+__device__ __forceinline__ bool gate_closed(const int* done) { return done && *(volatile const int*)done; }
+
+// Halo store of value v of interior cell (k, j) into the mirrored cells of
+// the external faces closer than `depth` (local_halos.c:66-149 pattern).
+__device__ __forceinline__ void reflect_store(double* f, const Geo& g, const Faces& fc, int depth, int k, int j,
+                                             double v)
+{
+    const long row = (long)j * g.x;
+    if (fc.l && k - g.hd < depth) f[row + (2 * g.hd - 1 - k)] = v;
+    if (fc.r && (g.x - g.hd - 1 - k) < depth) f[row + (2 * (g.x - g.hd) - 1 - k)] = v;
+    if (fc.b && j - g.hd < depth) f[(long)(2 * g.hd - 1 - j) * g.x + k] = v;
+    if (fc.t && (g.y - g.hd - 1 - j) < depth) f[(long)(2 * (g.y - g.hd) - 1 - j) * g.x + k] = v;
+}
+
+// CG sweep 1: [p = beta p + r] (FUSE_P, cg.c:146-164) ; depth-1 reflective
+// halo of p (REFLECT) ; w = A p ; pw = sum(w*p)  (cg.c:88-113).
+// p is read from p_in and the updated p written to p_out (a second buffer:
+// neighbours still read the old p); with REFLECT the halo of p_out is written.
+template <bool FUSE_P, bool REFLECT, typename Finish>
+static __global__ void __launch_bounds__(BX) k_cg_w_fused(Geo g, Faces fc, Scalar beta, const double* __restrict__ p_in,
+                                                   double* __restrict__ p_out, const double* __restrict__ r,
+                                                   double* __restrict__ w, const double* __restrict__ kx,
+                                                   const double* __restrict__ ky, ReduceSlots rs,
+                                                   const int* __restrict__ done, Finish fin)
+{
+    if (gate_closed(done)) return;
+    Strip s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const double bt = FUSE_P ? beta.get() : 0.0;
+        const int x = g.x, k = s.k;
+        const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
+        auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
+        long i = k + (long)s.j0 * x;
+        double pc = cur(i);
+        double pd = (s.j0 == g.hd) ? ((REFLECT && fc.b) ? pc : p_in[i - x]) : cur(i - x);
+        double kyc = ky[i];
+        for (int j = s.j0; j < s.j1; ++j, i += x) {
+            const bool at_t = j == g.y - g.hd - 1;
+            const double pu = at_t ? ((REFLECT && fc.t) ? pc : p_in[i + x]) : cur(i + x);
+            const double pl = at_l ? ((REFLECT && fc.l) ? pc : p_in[i - 1]) : cur(i - 1);
+            const double pr = at_r ? ((REFLECT && fc.r) ? pc : p_in[i + 1]) : cur(i + 1);
+            const double kyu = ky[i + x];
+            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, pc, pl, pr, pd, pu);
+            w[i] = v;
+            acc[0] += v * pc;
+            if (FUSE_P) p_out[i] = pc;
+            if (REFLECT) reflect_store(p_out, g, fc, 1, k, j, pc);
+            pd = pc;
+            pc = pu;
+            kyc = kyu;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
+// CG sweep 2: u += alpha p ; r -= alpha w ; rrn = sum(r*r) (cg.c:116-143),
+// first writing the pending reflective halo of u (HALO_U, depth udepth) from
+// the values u holds before the update.
+template <bool HALO_U, typename Finish>
+static __global__ void __launch_bounds__(BX) k_cg_ur_fused(Geo g, Faces fc, int udepth, Scalar alpha,
+                                                    double* __restrict__ u, const double* __restrict__ p,
+                                                    double* __restrict__ r, const double* __restrict__ w,
+                                                    ReduceSlots rs, const int* __restrict__ done, Finish fin)
+{
+    if (gate_closed(done)) return;
+    Strip s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const double a = alpha.get();
+        long i = s.k + (long)s.j0 * g.x;
+        for (int j = s.j0; j < s.j1; ++j, i += g.x) {
+            const double uo = u[i];
+            if (HALO_U) reflect_store(u, g, fc, udepth, s.k, j, uo);
+            u[i] = uo + a * p[i];
+            const double rn = r[i] - a * w[i];
+            r[i] = rn;
+            acc[0] += rn * rn;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
+// p = beta p + r in place, with the depth-1 halo of p (and of u unless u is
+// null) written from the final values (the end of a device-resident CG phase: the last trip's
+// calc_p and halo update, cg_driver.c:116-123 + halo_update_driver).
+static __global__ void __launch_bounds__(BX) k_cg_close(Geo g, Faces fc, Scalar beta, int apply_p, double* __restrict__ p,
+                                                 const double* __restrict__ r, double* __restrict__ u)
+{
+    Strip s(g);
+    if (!s.active) return;
+    const double bt = beta.get();
+    long i = s.k + (long)s.j0 * g.x;
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) {
+        const double pn = apply_p ? bt * p[i] + r[i] : p[i];
+        p[i] = pn;
+        reflect_store(p, g, fc, 1, s.k, j, pn);
+        if (u) reflect_store(u, g, fc, 1, s.k, j, u[i]);
+    }
+}
+
+// --------------------------------------------------------- Chebyshev ----
+// Chebyshev coefficients of the current trip: host values, or the device
+// tables indexed by the trip counter.
+struct ChebyCoef {
+    double alpha, beta;
+    const double* alphas;   // device tables (device-resident driver) or null
+    const double* betas;
+    const DevState* st;
+    __device__ __forceinline__ void get(double& a, double& b) const
+    {
+        if (alphas) {
+            const int n = st->nch;
+            a = alphas[n];
+            b = betas[n];
+        } else {
+            a = alpha;
+            b = beta;
+        }
+    }
+};
+
+struct FinChebyTrip {      // end of one Chebyshev trip of the device-resident loop
+    DevState* st;
+    DevParams prm;
+    int* host_mirror;
+    int force_norm;        // the first trip always takes the norm (cheby_driver.c:49-50)
+    __device__ void operator()(const double* t) const
+    {
+        const bool norm = force_norm || (st->nch >= st->est && ((st->trip + 1) % 10) == 0);
+        st->nch += 1;
+        end_of_trip(st, prm, norm ? t[0] : st->error, host_mirror);
+    }
+};
+
+// One Chebyshev trip (cheby.c:57-85) with the previous trip's u += p folded
+// in (ADD: u_n = u_{n-1} + p_{n-1}, read at the stencil points from u_in and
+// p_in): w = A u_n ; r = u0 - w ; p_n = alpha p_{n-1} + beta r. Writes u_n to
+// u_out and p_n to p_out (second buffers: neighbours read the old values),
+// w and r when `write_wr`, and reduces sum(r*r).
+template <bool ADD, bool REFLECT, typename Finish>
+static __global__ void __launch_bounds__(BX) k_cheby_trip(Geo g, Faces fc, ChebyCoef coef, int write_wr_always,
+                                                   const double* __restrict__ u_in, const double* __restrict__ p_in,
+                                                   double* __restrict__ u_out, double* __restrict__ p_out,
+                                                   const double* __restrict__ u0, double* __restrict__ w,
+                                                   double* __restrict__ r, const double* __restrict__ kx,
+                                                   const double* __restrict__ ky, ReduceSlots rs,
+                                                   const int* __restrict__ done, Finish fin, DevParams prm)
+{
+    if (gate_closed(done)) return;
+    Strip s(g);
+    double acc[1] = {0.0};
+    double a, b;
+    coef.get(a, b);
+    // w and r are only observable on the trips that take the norm, and on
+    // the last trip of the loop (their values stay in memory afterwards).
+    const bool wr = write_wr_always || !coef.st ||
+                    (coef.st->nch >= coef.st->est && ((coef.st->trip + 1) % 10) == 0) ||
+                    (coef.st->trip + 1 >= prm.max_iters);
+    if (s.active) {
+        const int x = g.x, k = s.k;
+        const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
+        auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
+        long i = k + (long)s.j0 * x;
+        double uc = cur(i);
+        double ud = (s.j0 == g.hd) ? ((REFLECT && fc.b) ? uc : u_in[i - x]) : cur(i - x);
+        double kyc = ky[i];
+        for (int j = s.j0; j < s.j1; ++j, i += x) {
+            const bool at_t = j == g.y - g.hd - 1;
+            const double uu = at_t ? ((REFLECT && fc.t) ? uc : u_in[i + x]) : cur(i + x);
+            const double ul = at_l ? ((REFLECT && fc.l) ? uc : u_in[i - 1]) : cur(i - 1);
+            const double ur = at_r ? ((REFLECT && fc.r) ? uc : u_in[i + 1]) : cur(i + 1);
+            const double kyu = ky[i + x];
+            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, uc, ul, ur, ud, uu);
+            const double rr = u0[i] - v;
+            const double pn = a * p_in[i] + b * rr;
+            if (wr) {
+                w[i] = v;
+                r[i] = rr;
+            }
+            acc[0] += rr * rr;
+            p_out[i] = pn;
+            if (ADD) u_out[i] = uc;
+            if (REFLECT) reflect_store(ADD ? u_out : const_cast<double*>(u_in), g, fc, 1, k, j, uc);
+            ud = uc;
+            uc = uu;
+            kyc = kyu;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
+// u += p in place with the depth-1 halo of u written from the final values
+// (closing the pending "u += p" of the last Chebyshev trip, cheby.c:8-24,
+// and the halo update that followed it).
+static __global__ void __launch_bounds__(BX) k_add_p_close(Geo g, Faces fc, double* __restrict__ u,
+                                                    const double* __restrict__ p)
+{
+    Strip s(g);
+    if (!s.active) return;
+    long i = s.k + (long)s.j0 * g.x;
+    for (int j = s.j0; j < s.j1; ++j, i += g.x) {
+        const double un = u[i] + p[i];
+        u[i] = un;
+        reflect_store(u, g, fc, 1, s.k, j, un);
+    }
+}
+
+// --------------------------------------------------------------- PPCG ----
+// PPCG inner-step coefficients: host values or device tables [pp].
+struct PpcgCoef {
+    double alpha, beta;
+    const double* alphas;
+    const double* betas;
+    __device__ __forceinline__ void get(int pp, double& a, double& b) const
+    {
+        if (alphas) {
+            a = alphas[pp];
+            b = betas[pp];
+        } else {
+            a = alpha;
+            b = beta;
+        }
+    }
+};
+
+// One PPCG inner step (ppcg.c:29-61) with the previous step's sd update folded
+// in: FOLD 0: sd = sd_in (as stored); FOLD 1: sd = r_in / theta (ppcg_init,
+// ppcg.c:9-26); FOLD 2: sd = a_prev sd_in + b_prev r_in. Then, with the
+// depth-1 reflective halo of sd: r = r_in - A sd ; u += sd. sd goes to
+// sd_out, r to r_out (second buffers: neighbours read the old values);
+// NORM reduces sum(r*r) of the new r.
+template <int FOLD, bool NORM, typename Finish>
+static __global__ void __launch_bounds__(BX) k_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef, int pp_prev,
+                                                  const double* __restrict__ sd_in, double* __restrict__ sd_out,
+                                                  const double* __restrict__ r_in, double* __restrict__ r_out,
+                                                  double* __restrict__ u, const double* __restrict__ kx,
+                                                  const double* __restrict__ ky, ReduceSlots rs,
+                                                  const int* __restrict__ done, Finish fin)
+{
+    if (gate_closed(done)) return;
+    Strip s(g);
+    double acc[1] = {0.0};
+    double a = 0.0, b = 0.0;
+    if (FOLD == 2) coef.get(pp_prev, a, b);
+    if (s.active) {
+        const int x = g.x, k = s.k;
+        const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
+        auto cur = [&](long idx) {
+            if (FOLD == 0) return sd_in[idx];
+            if (FOLD == 1) return r_in[idx] / theta;
+            return a * sd_in[idx] + b * r_in[idx];
+        };
+        long i = k + (long)s.j0 * x;
+        double sc = cur(i);
+        double sdn = (s.j0 == g.hd) ? (fc.b ? sc : sd_in[i - x]) : cur(i - x);
+        double kyc = ky[i];
+        for (int j = s.j0; j < s.j1; ++j, i += x) {
+            const bool at_t = j == g.y - g.hd - 1;
+            const double su = at_t ? (fc.t ? sc : sd_in[i + x]) : cur(i + x);
+            const double sl = at_l ? (fc.l ? sc : sd_in[i - 1]) : cur(i - 1);
+            const double sr = at_r ? (fc.r ? sc : sd_in[i + 1]) : cur(i + 1);
+            const double kyu = ky[i + x];
+            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, sc, sl, sr, sdn, su);
+            const double rn = r_in[i] - v;
+            r_out[i] = rn;
+            u[i] += sc;
+            sd_out[i] = sc;
+            reflect_store(sd_out, g, fc, 1, k, j, sc);
+            if (NORM) acc[0] += rn * rn;
+            sdn = sc;
+            sc = su;
+            kyc = kyu;
+        }
+    }
+    if (NORM) tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
+struct FinPpcgW {          // alpha = rro / pw  (ppcg_driver.c:100)
+    DevState* st;
+    __device__ void operator()(const double* t) const
+    {
+        st->pw = t[0];
+        st->alpha = st->rro / t[0];
+    }
+};
+
+struct FinPpcgNorm {       // beta = rrn / rro ; error = rro = rrn  (ppcg_driver.c:131-149)
+    DevState* st;
+    DevParams prm;
+    int* host_mirror;
+    __device__ void operator()(const double* t) const
+    {
+        const double rrn = t[0];
+        st->beta = rrn / st->rro;
+        st->rro = rrn;
+        st->rrn = rrn;
+        st->nch += 1;
+        end_of_trip(st, prm, rrn, host_mirror);
+    }
+};
+
+}  // namespace tl2d

@@ -1,0 +1,79 @@
+// suite2d_impl.hpp -- host-side state of one 2D chunk, shared by the
+// kernel-interface layer (suite2d.cu) and the device-resident driver
+// (driver2d.cu).
+#pragma once
+
+#include "kernels2d.cuh"
+
+#include <cuda_runtime.h>
+
+// Buffers that alternate between two slices (fused sweeps read the old values
+// at stencil neighbours while writing the new ones). The Chunk always points
+// at the current slice; the suite keeps the other.
+enum AltField { ALT_P = 0, ALT_U = 1, ALT_R = 2, ALT_SD = 3, ALT_COUNT = 4 };
+
+struct TlSuite2D {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    tl2d::Geo g{0, 0, 0};
+    void* slab = nullptr;
+    size_t slab_bytes = 0;
+    tl::ReduceSlots rs{};
+    double* h_out = nullptr;          // mapped pinned result slots
+    long partial_capacity = 0;        // doubles
+    State* d_states = nullptr;
+    int d_states_cap = 0;
+    double* d_comm = nullptr;         // pack/unpack staging
+    long d_comm_cap = 0;
+    double* alt[ALT_COUNT] = {nullptr, nullptr, nullptr, nullptr};
+    tl::Profiler prof;                // per-kernel device time (off by default)
+
+    // Operations the reference host requested that have not been run yet:
+    // a CG p update and reflective halo updates (depth per field, 0 = none).
+    // They are absorbed by the next sweep that can fuse them, or flushed.
+    struct {
+        bool calc_p = false;
+        double beta = 0.0;
+        int halo[TL_NUM_FIELDS] = {0, 0, 0, 0, 0, 0};
+    } pend;
+
+    // Device-resident driver state.
+    tl2d::DevState* d_state = nullptr;
+    int* h_mirror = nullptr;          // mapped: done, trip, reason
+    int* d_mirror = nullptr;          // device view of h_mirror
+    double* d_cg_alphas = nullptr;    // device coefficient tables [max_iters]
+    double* d_cg_betas = nullptr;
+    double* d_cheby_alphas = nullptr;
+    double* d_cheby_betas = nullptr;
+    int table_len = 0;
+};
+
+// Launch on the suite stream, bracketed by profiler events when enabled.
+#define TL_LAUNCH(s, name, ...)                \
+    do {                                       \
+        (s)->prof.begin((s)->stream, name);    \
+        __VA_ARGS__;                           \
+        (s)->prof.end((s)->stream);            \
+        TL_LAUNCHED(name);                     \
+    } while (0)
+
+namespace tl2d {
+
+TlSuite2D* suite_of(Chunk* chunk);
+inline dim3 interior_grid(const Geo& g)
+{
+    return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, ROWS));
+}
+inline dim3 full_grid(const Geo& g) { return dim3(tl::ceil_div(g.x, 32), tl::ceil_div(g.y, FB / 32)); }
+// Waits for the stream and returns the published sums.
+bool fetch(TlSuite2D* s, int n, double* out);
+// Runs every pending operation (p update, then halo updates).
+void flush(TlSuite2D* s, Chunk* chunk);
+// External faces of the chunk (neighbours == EXTERNAL_FACE).
+Faces faces_of(const Chunk* chunk);
+// The chunk's pointer to an alternating field, and the swap after a fused sweep.
+FieldBufferType* field_slot(Chunk* chunk, AltField f);
+void swap_alt(TlSuite2D* s, Chunk* chunk, AltField f);
+
+}  // namespace tl2d

@@ -468,6 +468,28 @@ class Host:
         res.summary = self.field_summary()
         return res
 
+    # -- device-resident timestep (tl2d_solve_step) ----------------------------------
+    def solve_device(self, tt: int) -> StepResult:
+        """One timestep with the solver loop kept on the GPU (same results as solve())."""
+        fn = getattr(self.lib, "tl%dd_solve_step" % self.dims)
+        stats = abi.StepStats()
+        fn(C.byref(self.chunk), C.byref(self.settings), tt, C.byref(stats))
+        abi.check(self.lib, self.dims)
+        res = StepResult(error=stats.error, exact_error=stats.exact_error, eigmin=stats.eigmin,
+                         eigmax=stats.eigmax, est_iterations=stats.est_iters)
+        s = self.cfg.solver
+        res.iterations["CG"] = stats.cg_iters
+        if s == CHEBY_SOLVER:
+            res.iterations["Cheby"] = stats.cheby_iters
+        elif s == PPCG_SOLVER:
+            res.iterations["PPCG"] = stats.ppcg_iters
+        res.summary = self.field_summary()
+        return res
+
+    def run_device(self, steps: Optional[int] = None) -> List[StepResult]:
+        n = self.cfg.end_step if steps is None else steps
+        return [self.solve_device(tt) for tt in range(n)]
+
     def run(self, steps: Optional[int] = None) -> List[StepResult]:
         n = self.cfg.end_step if steps is None else steps
         return [self.solve(tt) for tt in range(n)]
