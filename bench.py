@@ -8,11 +8,13 @@ timestep (solve(), 2d/diffuse.c:22-80) of that problem.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                   [--size 4096] [--solver cg|cheby|ppcg]
 
-B200 arm: value = solver iterations/s of the whole job (replicas on N GPUs,
-no data-path collective: the path does not shard, DESIGN.md "replicas only"),
-with the fields resident in HBM. e2e = the same metric through the
-reference-facing C ABI (run_* driven by the host mirror) with the inputs
-copied from pinned host buffers each step and the energy field copied back.
+B200 arm: value = solver iterations/s of the whole job (independent replicas
+on N GPUs: the path does not shard), fields resident in HBM, timesteps run by
+the device-resident solver loop (tl2d_solve_step). e2e = the same metric
+through the C ABI with the step's inputs copied from pinned host buffers and
+the energy field copied back every step; e2e_kernel_interface = the same,
+with the timestep driven through the run_* kernel interface the way the
+reference drivers call it.
 Reference arm (--impl reference): the reference omp3 CPU program on this
 host's cores, bounded samples of the same workload (each step capped at a
 fixed iteration count).
@@ -36,6 +38,10 @@ sys.path.insert(0, str(REPO))
 # written once): w=Ap reads p,kx,ky writes w; u/r update reads u,p,r,w writes
 # u,r; p update reads p,r writes p; ...
 KERNEL_BYTES_PER_CELL = {
+    "k_cg_w_fused": 48,      # reads p_old, r, kx, ky; writes p, w
+    "k_cg_ur_fused": 48,     # reads u, p, r, w; writes u, r
+    "k_cheby_trip": 56,      # reads u, p, u0, kx, ky; writes u, p (w, r only on norm trips)
+    "k_ppcg_step": 64,       # reads sd, r, kx, ky, u; writes sd, r, u
     "k_cg_calc_w": 32, "k_cg_calc_ur": 48, "k_cg_calc_p": 24,
     "k_cheby_sweep": 64, "k_add_p": 24, "k_ppcg_inner_a": 56, "k_ppcg_inner_b": 24,
     "k_norm2": 8, "k_residual": 40,
@@ -178,9 +184,10 @@ def bench_b200(args, rank, world, local_rank):
     cells = args.size * args.size
     interior_launch_cells = cells
 
+    step = h.solve_device if args.driver == "device" else h.solve
     tt = 0
     for _ in range(args.warmup):
-        h.solve(tt)
+        step(tt)
         tt += 1
     if world > 1:
         dist.barrier()
@@ -194,7 +201,7 @@ def bench_b200(args, rank, world, local_rank):
     with sampler:
         e0.record(stream)
         for _ in range(args.steps):
-            r = h.solve(tt)
+            r = step(tt)
             iters += sum(r.iterations.values())
             tt += 1
         e1.record(stream)
@@ -224,39 +231,42 @@ def bench_b200(args, rank, world, local_rank):
         ms_max, iters_all = ms, float(iters)
     value = iters_all / (ms_max / 1000.0)
 
-    # e2e through the C ABI with host buffers: upload the step's inputs from
-    # pinned host memory, solve, read the energy field and summary back.
+    # e2e through the C ABI with host buffers: every step uploads the step's
+    # inputs (density, energy) from pinned host memory, runs the timestep and
+    # reads the energy field and the field summary back.
     init = Host(prob.tea_in(), dims=2)
     dens_h = torch.from_numpy(init.download("density")).pin_memory()
     en_h = torch.from_numpy(init.download("energy")).pin_memory()
     init.finalise()
     out_h = torch.empty_like(en_h).pin_memory()
     n = dens_h.numel()
-    e2e_iters = 0
-    e2 = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
-    nsteps_e2e = max(1, min(args.steps, args.e2e_steps))
     fn_up, fn_down = h.lib.tl2d_upload_field, h.lib.tl2d_download_field
-    torch.cuda.synchronize()
-    e2[0].record(stream)
-    for _ in range(nsteps_e2e):
-        fn_up(C.byref(h.chunk), C.byref(h.settings), 1, C.c_void_p(dens_h.data_ptr()), n)
-        fn_up(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(en_h.data_ptr()), n)
-        r = h.solve(0)
-        fn_down(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(out_h.data_ptr()), n)
-        abi.check(h.lib, 2)
-        e2e_iters += sum(r.iterations.values())
-    e2[1].record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e2[0].elapsed_time(e2[1])
-    te = torch.tensor([e2e_ms, float(e2e_iters)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = te.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = te.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        e2e_ms_max, e2e_iters_all = mx[0].item(), sm[1].item()
-    else:
-        e2e_ms_max, e2e_iters_all = e2e_ms, float(e2e_iters)
+    nsteps_e2e = max(1, min(args.steps, args.e2e_steps))
+
+    def e2e(step_fn):
+        its = 0
+        ev = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(nsteps_e2e):
+            fn_up(C.byref(h.chunk), C.byref(h.settings), 1, C.c_void_p(dens_h.data_ptr()), n)
+            fn_up(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(en_h.data_ptr()), n)
+            r = step_fn(0)
+            fn_down(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(out_h.data_ptr()), n)
+            abi.check(h.lib, 2)
+            its += sum(r.iterations.values())
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        t2 = torch.tensor([ev[0].elapsed_time(ev[1]), float(its)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            mx, sm = t2.clone(), t2.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+            return sm[1].item() / (mx[0].item() / 1000.0)
+        return t2[1].item() / (t2[0].item() / 1000.0)
+
+    e2e_device = e2e(h.solve_device)
+    e2e_kernel_interface = e2e(h.solve) if args.e2e_kernel_interface else None
     h.finalise()
 
     if rank != 0:
@@ -287,7 +297,8 @@ def bench_b200(args, rank, world, local_rank):
         "config": {"workload": "dropin_2d_%d_%s" % (args.size, args.solver), "cells": cells,
                    "solver": args.solver, "eps": 1e-15, "dt": 0.004, "parallelism": "replicas",
                    "l2": "no flush: working set %.2f GB > 126 MB L2" % (8 * (args.size + 4) ** 2 * 8 / 1e9),
-                   "driver": "host mirror over run_* (synchronous reductions)"},
+                   "driver": "device-resident solver loop (tl2d_solve_step)" if args.driver == "device"
+                   else "host mirror of the reference drivers over run_*"},
         "cells_iterations_per_s": value * cells,
         "hbm_effective_gbs_per_gpu": eff_gbs,
         "hbm_effective_frac_per_gpu": eff_gbs / peak,
@@ -295,9 +306,14 @@ def bench_b200(args, rank, world, local_rank):
         "kernels": {k: {"calls": c, "ms": round(m, 3), "share": round(m / total_kernel_ms, 4)}
                     for k, (c, m) in sorted(prof.items(), key=lambda kv: -kv[1][1])},
         "gpu_launches": launches,
-        "e2e": {"value": e2e_iters_all / (e2e_ms_max / 1000.0), "unit": "iter/s",
-                "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8 + 32,
-                "steps": nsteps_e2e, "path": "run_* C ABI + tl2d_upload/download_field, pinned host buffers"},
+        "e2e": {"value": e2e_device, "unit": "iter/s",
+                "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8 + 32, "steps": nsteps_e2e,
+                "path": "C ABI: tl2d_upload_field (pinned host) -> tl2d_solve_step -> run_field_summary "
+                        "-> tl2d_download_field"},
+        "e2e_kernel_interface": None if e2e_kernel_interface is None else {
+            "value": e2e_kernel_interface, "unit": "iter/s",
+            "path": "same, timestep driven through the run_* kernel interface by the host mirror of "
+                    "the reference drivers (two synchronous reductions per CG iteration)"},
         "clocks": sampler.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -337,6 +353,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-cap", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--driver", default="device", choices=["device", "run"])
+    ap.add_argument("--e2e-kernel-interface", type=int, default=1)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

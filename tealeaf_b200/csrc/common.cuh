@@ -187,12 +187,20 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;  // lane 0
 }
 
-// Block sum of N values; returns true in thread 0, which holds the sums in v.
+// Linear thread index of 1-, 2- or 3-D blocks (blockDim.x a multiple of 32
+// or the only dimension, so warps are contiguous runs of it).
+__device__ __forceinline__ int linear_tid()
+{
+    return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+
+// Block sum of N values; thread 0 holds the sums in v afterwards.
 template <int N, int BLOCK>
 __device__ __forceinline__ void block_sum(double (&v)[N], double (*smem)[BLOCK / kWarp])
 {
-    const int lane = threadIdx.x & (kWarp - 1);
-    const int warp = threadIdx.x / kWarp;
+    const int tid = linear_tid();
+    const int lane = tid & (kWarp - 1);
+    const int warp = tid / kWarp;
 #pragma unroll
     for (int r = 0; r < N; ++r) v[r] = warp_sum(v[r]);
     if (lane == 0) {
@@ -222,8 +230,9 @@ __device__ __forceinline__ void grid_sum(double (&v)[N], const ReduceSlots& s, i
 {
     __shared__ double smem[N][BLOCK / kWarp];
     __shared__ bool last;
+    const int tid = linear_tid();
     block_sum<N, BLOCK>(v, smem);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
 #pragma unroll
         for (int r = 0; r < N; ++r) s.partials[(long)bid * N + r] = v[r];
         __threadfence();
@@ -236,13 +245,13 @@ __device__ __forceinline__ void grid_sum(double (&v)[N], const ReduceSlots& s, i
     double t[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) t[r] = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += BLOCK) {
+    for (int b = tid; b < nblocks; b += BLOCK) {
 #pragma unroll
         for (int r = 0; r < N; ++r) t[r] += __ldcg(&s.partials[(long)b * N + r]);
     }
     __syncthreads();  // smem reuse
     block_sum<N, BLOCK>(t, smem);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
 #pragma unroll
         for (int r = 0; r < N; ++r) {
             s.out_dev[r] = t[r];

@@ -17,6 +17,7 @@
 // reference's halo flags (e.g. the halo of u is not refreshed during PPCG).
 //
 // diffuse_overload (2d/application.h:9-11) runs every timestep this way.
+#include "host_maths.hpp"
 #include "suite2d_impl.hpp"
 
 #include <cfloat>
@@ -24,6 +25,9 @@
 #include <vector>
 
 using namespace tl2d;
+using tl::cheby_coefs;
+using tl::cheby_est;
+using tl::eigen_bounds;
 
 extern "C" void print_and_log(Settings* settings, const char* format, ...) __attribute__((weak));
 extern "C" void field_summary_driver(Chunk* chunks, Settings* settings, bool is_solve_finished) __attribute__((weak));
@@ -31,105 +35,6 @@ extern "C" void field_summary_driver(Chunk* chunks, Settings* settings, bool is_
 namespace {
 
 constexpr int kBatch = 16;   // solver-loop trips launched between looks at the done word
-
-// -------------------------------------------------------------- host maths --
-
-// Eigenvalues of a symmetric tridiagonal matrix, implicit QL with shifts
-// (published "tqli"; the reference adapts it, 2d/drivers/eigenvalue_driver.c:71-121).
-bool tridiag_ql(std::vector<double>& d, std::vector<double>& e)
-{
-    const int n = (int)d.size();
-    for (int i = 0; i < n - 1; ++i) e[i] = e[i + 1];
-    e[n - 1] = 0.0;
-    for (int l = 0; l < n; ++l) {
-        int sweeps = 0, m;
-        for (;;) {
-            for (m = l; m < n - 1; ++m) {
-                const double dd = fabs(d[m]) + fabs(d[m + 1]);
-                if (fabs(e[m]) + dd == dd) break;
-            }
-            if (m == l) break;
-            if (sweeps++ == 30) return false;
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = sqrt((g * g) + 1.0);
-            g = d[m] - d[l] + e[l] / (g + (g < 0 ? -fabs(r) : fabs(r)));
-            double s = 1.0, c = 1.0, p = 0.0;
-            for (int i = m - 1; i >= l; --i) {
-                const double f = s * e[i];
-                const double b = c * e[i];
-                r = sqrt(f * f + g * g);
-                e[i + 1] = r;
-                if (r == 0.0) {
-                    d[i + 1] -= p;
-                    e[m] = 0.0;
-                    continue;
-                }
-                s = f / r;
-                c = g / r;
-                g = d[i + 1] - p;
-                r = (d[i] - g) * s + 2.0 * c * b;
-                p = s * r;
-                d[i + 1] = g + p;
-                g = c * r - b;
-            }
-            d[l] = d[l] - p;
-            e[l] = g;
-            e[m] = 0.0;
-        }
-    }
-    return true;
-}
-
-// eigenvalue_driver_initialise (2d/drivers/eigenvalue_driver.c:11-67)
-bool eigen_bounds(Chunk* chunk, int n)
-{
-    std::vector<double> d(n > 0 ? n : 1, 0.0), e(n > 0 ? n : 1, 0.0);
-    for (int i = 0; i < n; ++i) {
-        d[i] = 1.0 / chunk->cg_alphas[i];
-        if (i > 0) d[i] += chunk->cg_betas[i - 1] / chunk->cg_alphas[i - 1];
-        if (i < n - 1) e[i + 1] = sqrt(chunk->cg_betas[i]) / chunk->cg_alphas[i];
-    }
-    if (!tridiag_ql(d, e)) {
-        tl::fail(30, "Too many iterations in TQLI routine");
-        return false;
-    }
-    double lo = DBL_MAX, hi = DBL_MIN;
-    for (int i = 0; i < n; ++i) {
-        lo = d[i] < lo ? d[i] : lo;
-        hi = d[i] > hi ? d[i] : hi;
-    }
-    if (lo < 0.0 || hi < 0.0) {
-        tl::fail(31, "Calculated negative eigenvalues.");
-        return false;
-    }
-    chunk->eigmin = lo * 0.95;
-    chunk->eigmax = hi * 1.05;
-    return true;
-}
-
-// cheby_coef_driver (2d/drivers/cheby_driver.c:163-183)
-void cheby_coefs(Chunk* chunk, int count)
-{
-    chunk->theta = (chunk->eigmax + chunk->eigmin) / 2.0;
-    const double delta = (chunk->eigmax - chunk->eigmin) / 2.0;
-    const double sigma = chunk->theta / delta;
-    double rho_old = 1.0 / sigma;
-    for (int i = 0; i < count; ++i) {
-        const double rho_new = 1.0 / (2.0 * sigma - rho_old);
-        chunk->cheby_alphas[i] = rho_new * rho_old;
-        chunk->cheby_betas[i] = 2.0 * rho_new / delta;
-        rho_old = rho_new;
-    }
-}
-
-// cheby_calc_est_iterations (2d/drivers/cheby_driver.c:146-160)
-int cheby_est(const Chunk* chunk, double error, double bb)
-{
-    const double cn = chunk->eigmax / chunk->eigmin;
-    const double it_alpha = DBL_EPSILON * bb / (4.0 * error);
-    const double gamm = (sqrt(cn) - 1.0) / (sqrt(cn) + 1.0);
-    return (int)roundf(logf(it_alpha) / (2.0 * logf(gamm)));
-}
 
 // ------------------------------------------------------------- the driver --
 
@@ -393,6 +298,52 @@ struct Run {
     }
 };
 
+// solve_finished_driver (2d/drivers/solve_finished_driver.c:7-43)
+void solve_finished(Run& R, TlStepStats* st_out)
+{
+    TlSuite2D* s = R.s;
+    Chunk* chunk = R.chunk;
+    Settings* settings = R.settings;
+    bool* flags = settings->fields_to_exchange;
+    flush(s, chunk);
+    if (settings->check_result) {
+        TL_LAUNCH(s, "k_residual", k_residual<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->u, chunk->u0, chunk->r,
+                                                                            chunk->kx, chunk->ky));
+        st_out->exact_error = R.norm(chunk->r);
+    }
+    TL_LAUNCH(s, "k_finalise", k_finalise<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->energy, chunk->density, chunk->u));
+    flags[TL_FIELD_ENERGY1] = true;
+    for (int f = 0; f < TL_NUM_FIELDS; ++f) s->pend.halo[f] = flags[f] ? 1 : 0;
+    flush(s, chunk);
+    TL_CUDA(cudaStreamSynchronize(s->stream));
+}
+
+// jacobi_driver (2d/drivers/jacobi_driver.c:7-83), driven from the host
+// through the suite's own kernel-interface entry points (Jacobi is not a
+// performance path; its stop test needs a host round trip every trip).
+double jacobi_loop(Chunk* chunk, Settings* settings, double rx, double ry, int* iters)
+{
+    bool* flags = settings->fields_to_exchange;
+    run_jacobi_init(chunk, settings, rx, ry);
+    run_copy_u(chunk, settings);
+    for (int f = 0; f < TL_NUM_FIELDS; ++f) flags[f] = false;
+    flags[TL_FIELD_U] = true;
+    double error = 1e10;
+    int tt;
+    for (tt = 0; tt < settings->max_iters && !tl::failed(); ++tt) {
+        run_jacobi_iterate(chunk, settings, &error);
+        if (tt % 50 == 0) {
+            run_local_halos(chunk, settings, 1);
+            run_calculate_residual(chunk, settings);
+            run_calculate_2norm(chunk, settings, chunk->r, &error);
+        }
+        run_local_halos(chunk, settings, 1);
+        if (fabs(error) < settings->eps) break;
+    }
+    *iters = tt;
+    return error;
+}
+
 }  // namespace
 
 extern "C" {
@@ -438,7 +389,13 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
     double error = 1e10;
     DevState st{};
     if (settings->solver == TL_JACOBI_SOLVER) {
-        tl::fail(33, "the device-resident driver runs CG, Chebyshev and PPCG; drive Jacobi through run_*");
+        int it = 0;
+        error = jacobi_loop(chunk, settings, rx, ry, &it);
+        st_out->jacobi_iters = it;
+        st_out->total_iters = it;
+        st_out->error = error;
+        solve_finished(R, st_out);
+        if (print_and_log && settings->tea_out_fp) print_and_log(settings, "Jacobi: \t\t%d iterations\n", it);
         return;
     }
     // cg_init_driver: cg_init, halo(u, p) depth 1, copy_u (2d/drivers/cg_driver.c:30-62)
@@ -483,23 +440,13 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
     // the reference's printed iteration count is the loop index at exit
     const int tt_exit = st.reason == 1 ? st.trip - 1 : st.trip;
     st_out->total_iters = tt_exit;
-    if (settings->solver == TL_CHEBY_SOLVER && st_out->cheby_iters) st_out->cg_iters = tt_exit - st_out->cheby_iters + 1;
-    if (settings->solver == TL_PPCG_SOLVER && st_out->ppcg_iters) st_out->cg_iters = tt_exit - st_out->ppcg_iters + 1;
+    if (settings->solver == TL_CHEBY_SOLVER) st_out->cg_iters = tt_exit - st_out->cheby_iters + 1;
+    if (settings->solver == TL_PPCG_SOLVER) st_out->cg_iters = tt_exit - st_out->ppcg_iters + 1;
     st_out->error = error;
     st_out->eigmin = chunk->eigmin;
     st_out->eigmax = chunk->eigmax;
 
-    // solve_finished_driver (2d/drivers/solve_finished_driver.c:7-43)
-    if (settings->check_result) {
-        TL_LAUNCH(s, "k_residual", k_residual<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->u, chunk->u0, chunk->r,
-                                                                            chunk->kx, chunk->ky));
-        st_out->exact_error = R.norm(chunk->r);
-    }
-    TL_LAUNCH(s, "k_finalise", k_finalise<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->energy, chunk->density, chunk->u));
-    flags[TL_FIELD_ENERGY1] = true;
-    for (int f = 0; f < TL_NUM_FIELDS; ++f) s->pend.halo[f] = flags[f] ? 1 : 0;
-    flush(s, chunk);
-    TL_CUDA(cudaStreamSynchronize(s->stream));
+    solve_finished(R, st_out);
 
     if (print_and_log && settings->tea_out_fp) {
         if (settings->solver == TL_CG_SOLVER) {

@@ -13,12 +13,26 @@
 #pragma once
 
 #include "common.cuh"
+#include "solver_common.cuh"
 #include "tealeaf_b200_2d.h"
 using tl::ReduceSlots;
 
 // Types have external linkage (identical in every includer); kernels are
 // static, so each includer has its own copies.
 namespace tl2d {
+
+using tl::ChebyCoef;
+using tl::DevParams;
+using tl::DevState;
+using tl::FinCgInit;
+using tl::FinCgUr;
+using tl::FinCgW;
+using tl::FinChebyTrip;
+using tl::FinPpcgNorm;
+using tl::FinPpcgW;
+using tl::gate_closed;
+using tl::PpcgCoef;
+using tl::Scalar;
 
 constexpr int BX = 128;   // threads (columns) per block of an interior sweep
 constexpr int ROWS = 8;   // rows per thread of an interior sweep
@@ -525,6 +539,11 @@ static __global__ void k_pack(Geo g, int depth, int face, int pack, double* __re
 }
 
 
+// External faces whose depth-1 halo is reflected (left, right, bottom, top).
+struct Faces {
+    int l, r, b, t;
+};
+
 // ===================================================================
 // Fused kernels: each absorbs the operations the reference performs between
 // two sweeps (the p update of the previous CG step, the reflective halo of
@@ -536,114 +555,6 @@ static __global__ void k_pack(Geo g, int depth, int face, int pack, double* __re
 // memory ends in the state the reference leaves it in.
 // ===================================================================
 
-// Scalar operand: a host value, or a device location (device-resident driver).
-struct Scalar {
-    double v;
-    const double* dev;
-    __device__ __forceinline__ double get() const { return dev ? *dev : v; }
-};
-
-// External faces whose depth-1 halo is reflected (left, right, bottom, top).
-struct Faces {
-    int l, r, b, t;
-};
-
-// Control block of the device-resident solver loops (device memory).
-struct DevState {
-    double rro, pw, rrn, alpha, beta, error;
-    double theta;
-    int trip;     // completed trips of the solver loop (the reference's tt)
-    int done;     // the loop has ended
-    int reason;   // 1 converged, 2 switch to Chebyshev/PPCG, 3 max_iters
-    int nch;      // Chebyshev trips done (next coefficient index)
-    int est;      // Chebyshev iteration estimate
-    int pad;
-};
-
-// Read-only parameters of a solve.
-struct DevParams {
-    double eps, eps_lim;
-    int max_iters, presteps, error_switch, switch_enabled, dims3;
-};
-
-// Stop test of the solver loops: 2D tests the error itself, 3D its square
-// root (3d/drivers/cg_solver_driver.c:24-25); the switch from CG to
-// Chebyshev/PPCG is evaluated for the next trip (2d/drivers/cheby_driver.c:30-32).
-__device__ __forceinline__ void end_of_trip(DevState* st, const DevParams& prm, double error, int* host_mirror)
-{
-    const double e = prm.dims3 ? sqrt(error) : error;
-    st->error = e;
-    const int tt = st->trip;
-    st->trip = tt + 1;
-    int reason = 0;
-    if (fabs(e) < prm.eps) reason = 1;
-    else if (tt + 1 >= prm.max_iters) reason = 3;
-    else if (prm.switch_enabled) {
-        const bool sw = prm.error_switch ? (e < prm.eps_lim) && (tt + 1 > TL_CG_ITERS_FOR_EIGENVALUES)
-                                         : (tt + 1 > prm.presteps) && (e < TL_ERROR_SWITCH_MAX);
-        if (sw) reason = 2;
-    }
-    if (reason) {
-        st->done = 1;
-        st->reason = reason;
-    }
-    if (host_mirror) {
-        host_mirror[0] = st->done;
-        host_mirror[1] = st->trip;
-        host_mirror[2] = st->reason;
-    }
-}
-
-// Finishers (thread 0 of the last block, with the grid totals).
-struct FinCgInit {         // rro of cg_init_driver (cg_driver.c:30-62) starts the loop state
-    DevState* st;
-    int* host_mirror;
-    __device__ void operator()(const double* t) const
-    {
-        st->rro = t[0];
-        st->trip = 0;
-        st->done = 0;
-        st->reason = 0;
-        st->nch = 0;
-        st->error = 1e10;
-        if (host_mirror) {
-            host_mirror[0] = 0;
-            host_mirror[1] = 0;
-            host_mirror[2] = 0;
-        }
-    }
-};
-
-struct FinCgW {            // alpha = rro / pw; cg_alphas[tt] = alpha  (cg_driver.c:87-93)
-    DevState* st;
-    double* cg_alphas;
-    __device__ void operator()(const double* t) const
-    {
-        st->pw = t[0];
-        const double a = st->rro / t[0];
-        st->alpha = a;
-        if (cg_alphas) cg_alphas[st->trip] = a;
-    }
-};
-
-struct FinCgUr {           // beta = rrn / rro; rro = error = rrn  (cg_driver.c:104-123)
-    DevState* st;
-    double* cg_betas;
-    DevParams prm;
-    int* host_mirror;
-    __device__ void operator()(const double* t) const
-    {
-        const double rrn = t[0];
-        const double b = rrn / st->rro;
-        st->beta = b;
-        cg_betas[st->trip] = b;
-        st->rro = rrn;
-        st->rrn = rrn;
-        end_of_trip(st, prm, rrn, host_mirror);
-    }
-};
-
-__device__ __forceinline__ bool gate_closed(const int* done) { return done && *(volatile const int*)done; }
 
 // Halo store of value v of interior cell (k, j) into the mirrored cells of
 // the external faces closer than `depth` (local_halos.c:66-149 pattern).
@@ -745,38 +656,6 @@ static __global__ void __launch_bounds__(BX) k_cg_close(Geo g, Faces fc, Scalar 
 }
 
 // --------------------------------------------------------- Chebyshev ----
-// Chebyshev coefficients of the current trip: host values, or the device
-// tables indexed by the trip counter.
-struct ChebyCoef {
-    double alpha, beta;
-    const double* alphas;   // device tables (device-resident driver) or null
-    const double* betas;
-    const DevState* st;
-    __device__ __forceinline__ void get(double& a, double& b) const
-    {
-        if (alphas) {
-            const int n = st->nch;
-            a = alphas[n];
-            b = betas[n];
-        } else {
-            a = alpha;
-            b = beta;
-        }
-    }
-};
-
-struct FinChebyTrip {      // end of one Chebyshev trip of the device-resident loop
-    DevState* st;
-    DevParams prm;
-    int* host_mirror;
-    int force_norm;        // the first trip always takes the norm (cheby_driver.c:49-50)
-    __device__ void operator()(const double* t) const
-    {
-        const bool norm = force_norm || (st->nch >= st->est && ((st->trip + 1) % 10) == 0);
-        st->nch += 1;
-        end_of_trip(st, prm, norm ? t[0] : st->error, host_mirror);
-    }
-};
 
 // One Chebyshev trip (cheby.c:57-85) with the previous trip's u += p folded
 // in (ADD: u_n = u_{n-1} + p_{n-1}, read at the stencil points from u_in and
@@ -852,22 +731,6 @@ static __global__ void __launch_bounds__(BX) k_add_p_close(Geo g, Faces fc, doub
 }
 
 // --------------------------------------------------------------- PPCG ----
-// PPCG inner-step coefficients: host values or device tables [pp].
-struct PpcgCoef {
-    double alpha, beta;
-    const double* alphas;
-    const double* betas;
-    __device__ __forceinline__ void get(int pp, double& a, double& b) const
-    {
-        if (alphas) {
-            a = alphas[pp];
-            b = betas[pp];
-        } else {
-            a = alpha;
-            b = beta;
-        }
-    }
-};
 
 // One PPCG inner step (ppcg.c:29-61) with the previous step's sd update folded
 // in: FOLD 0: sd = sd_in (as stored); FOLD 1: sd = r_in / theta (ppcg_init,
@@ -921,28 +784,5 @@ static __global__ void __launch_bounds__(BX) k_ppcg_step(Geo g, Faces fc, double
     if (NORM) tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
-struct FinPpcgW {          // alpha = rro / pw  (ppcg_driver.c:100)
-    DevState* st;
-    __device__ void operator()(const double* t) const
-    {
-        st->pw = t[0];
-        st->alpha = st->rro / t[0];
-    }
-};
-
-struct FinPpcgNorm {       // beta = rrn / rro ; error = rro = rrn  (ppcg_driver.c:131-149)
-    DevState* st;
-    DevParams prm;
-    int* host_mirror;
-    __device__ void operator()(const double* t) const
-    {
-        const double rrn = t[0];
-        st->beta = rrn / st->rro;
-        st->rro = rrn;
-        st->rrn = rrn;
-        st->nch += 1;
-        end_of_trip(st, prm, rrn, host_mirror);
-    }
-};
 
 }  // namespace tl2d

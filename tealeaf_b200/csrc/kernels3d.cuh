@@ -1,0 +1,670 @@
+// kernels3d.cuh -- device kernels of the 3D suite (included by suite3d.cu
+// and driver3d.cu; kernels are static in each includer).
+//
+// Interior sweeps: blocks of 32 (x) x 4 (y) threads, each thread walking
+// ZR cells up a z-pencil with the z-neighbours of the 7-point stencil carried
+// in registers; x-neighbours come from the same warp's lines (L1) and
+// y-neighbours from the neighbouring warps of the block (L1/L2), so each
+// field streams from DRAM once per sweep. Index k + j*x + i*x*y, halo
+// included (3d/shared.h:52-58). Includers are compiled with -fmad=false.
+#pragma once
+
+#include "common.cuh"
+#include "solver_common.cuh"
+#include "tealeaf_b200_3d.h"
+
+using tl::ReduceSlots;
+
+namespace tl3d {
+
+using tl::ChebyCoef;
+using tl::DevParams;
+using tl::DevState;
+using tl::FinCgInit;
+using tl::FinCgUr;
+using tl::FinCgW;
+using tl::FinChebyTrip;
+using tl::FinPpcgNorm;
+using tl::FinPpcgW;
+using tl::gate_closed;
+using tl::PpcgCoef;
+using tl::Scalar;
+
+constexpr int BX = 32;   // x threads per block of an interior sweep
+constexpr int BY = 4;    // y threads per block
+constexpr int ZR = 8;    // z cells per thread
+constexpr int NT = BX * BY;
+constexpr int FBX = 32, FBY = 8;   // full-array kernels
+
+struct Geo {
+    int x, y, z, hd;
+    __host__ __device__ long xy() const { return (long)x * y; }
+};
+
+// External faces whose depth-1 halo is reflected.
+struct Faces {
+    int l, r, b, t, k, f;   // left, right, bottom, top, back, front
+};
+
+__device__ __forceinline__ double coef_w(int coefficient, double density)
+{
+    return coefficient == TL3_CONDUCTIVITY ? density : 1.0 / density;
+}
+
+__device__ __forceinline__ double face(double r, double wa, double wb) { return r * (wa + wb) / (2.0 * wa * wb); }
+
+// 7-point operator in the reference operand order (3d/shared.h:52-58).
+__device__ __forceinline__ double smvp(double kxc, double kxr, double kyc, double kyu, double kzc, double kzf,
+                                       double c, double l, double r, double d, double u, double b, double f)
+{
+    return (1.0 + (kxr + kxc) + (kyu + kyc) + (kzf + kzc)) * c - (kxr * r + kxc * l) - (kyu * u + kyc * d) -
+           (kzf * f + kzc * b);
+}
+
+__device__ __forceinline__ int block_id() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+__device__ __forceinline__ int block_count() { return gridDim.x * gridDim.y * gridDim.z; }
+
+struct Pencil {
+    int k, j, i0, i1;
+    bool active;
+    __device__ Pencil(const Geo& g)
+    {
+        k = g.hd + blockIdx.x * BX + threadIdx.x;
+        j = g.hd + blockIdx.y * BY + threadIdx.y;
+        i0 = g.hd + blockIdx.z * ZR;
+        i1 = min(i0 + ZR, g.z - g.hd);
+        active = k < g.x - g.hd && j < g.y - g.hd;
+    }
+};
+
+__device__ __forceinline__ void reflect_store(double* f, const Geo& g, const Faces& fc, int depth, int k, int j,
+                                             int i, double v)
+{
+    const long xy = g.xy();
+    const long base = (long)i * xy + (long)j * g.x;
+    if (fc.l && k - g.hd < depth) f[base + (2 * g.hd - 1 - k)] = v;
+    if (fc.r && (g.x - g.hd - 1 - k) < depth) f[base + (2 * (g.x - g.hd) - 1 - k)] = v;
+    if (fc.b && j - g.hd < depth) f[(long)i * xy + (long)(2 * g.hd - 1 - j) * g.x + k] = v;
+    if (fc.t && (g.y - g.hd - 1 - j) < depth) f[(long)i * xy + (long)(2 * (g.y - g.hd) - 1 - j) * g.x + k] = v;
+    if (fc.k && i - g.hd < depth) f[(long)(2 * g.hd - 1 - i) * xy + (long)j * g.x + k] = v;
+    if (fc.f && (g.z - g.hd - 1 - i) < depth) f[(long)(2 * (g.z - g.hd) - 1 - i) * xy + (long)j * g.x + k] = v;
+}
+
+// Generic stencil walker: CUR(idx) gives the operand value at an interior
+// cell; halo neighbours come from `raw` (memory) unless REFLECT mirrors them
+// on an external face. Calls body(i, centre, smvp) for every cell.
+template <bool REFLECT, typename Cur, typename Body>
+__device__ __forceinline__ void walk(const Geo& g, const Faces& fc, const Pencil& s, const double* __restrict__ raw,
+                                     const double* __restrict__ kx, const double* __restrict__ ky,
+                                     const double* __restrict__ kz, Cur cur, Body body)
+{
+    const int x = g.x, k = s.k, j = s.j;
+    const long xy = g.xy();
+    const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
+    const bool at_b = j == g.hd, at_t = j == g.y - g.hd - 1;
+    long i = k + (long)j * x + (long)s.i0 * xy;
+    double c = cur(i);
+    double bk = (s.i0 == g.hd) ? ((REFLECT && fc.k) ? c : raw[i - xy]) : cur(i - xy);
+    double kzc = kz[i];
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+        const bool at_f = ii == g.z - g.hd - 1;
+        const double fr = at_f ? ((REFLECT && fc.f) ? c : raw[i + xy]) : cur(i + xy);
+        const double l = at_l ? ((REFLECT && fc.l) ? c : raw[i - 1]) : cur(i - 1);
+        const double r = at_r ? ((REFLECT && fc.r) ? c : raw[i + 1]) : cur(i + 1);
+        const double d = at_b ? ((REFLECT && fc.b) ? c : raw[i - x]) : cur(i - x);
+        const double u = at_t ? ((REFLECT && fc.t) ? c : raw[i + x]) : cur(i + x);
+        const double kzf = kz[i + xy];
+        const double v = smvp(kx[i], kx[i + 1], ky[i], ky[i + x], kzc, kzf, c, l, r, d, u, bk, fr);
+        body(ii, i, c, v);
+        bk = c;
+        c = fr;
+        kzc = kzf;
+    }
+}
+
+// ------------------------------------------------------ CG (cg_solver.c) --
+
+// [p = beta p + r] ; depth-1 reflective halo of p ; w = A p ; pw = sum(w p)
+// (3d/c_kernels/omp3/cg_solver.c:105-193).
+template <bool FUSE_P, bool REFLECT, typename Finish>
+static __global__ void __launch_bounds__(NT) k3_cg_w(Geo g, Faces fc, Scalar beta, const double* __restrict__ p_in,
+                                                    double* __restrict__ p_out, const double* __restrict__ r,
+                                                    double* __restrict__ w, const double* __restrict__ kx,
+                                                    const double* __restrict__ ky, const double* __restrict__ kz,
+                                                    ReduceSlots rs, const int* __restrict__ done, Finish fin)
+{
+    if (gate_closed(done)) return;
+    Pencil s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const double bt = FUSE_P ? beta.get() : 0.0;
+        auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
+        walk<REFLECT>(g, fc, s, p_in, kx, ky, kz, cur, [&](int ii, long i, double c, double v) {
+            w[i] = v;
+            acc[0] += v * c;
+            if (FUSE_P) p_out[i] = c;
+            if (REFLECT) reflect_store(p_out, g, fc, 1, s.k, s.j, ii, c);
+        });
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+}
+
+// u += alpha p ; r -= alpha w ; rrn = sum(r r), after writing the pending
+// halo of u from its old values (HALO_U).
+template <bool HALO_U, typename Finish>
+static __global__ void __launch_bounds__(NT) k3_cg_ur(Geo g, Faces fc, int udepth, Scalar alpha, double* __restrict__ u,
+                                                     const double* __restrict__ p, double* __restrict__ r,
+                                                     const double* __restrict__ w, ReduceSlots rs,
+                                                     const int* __restrict__ done, Finish fin)
+{
+    if (gate_closed(done)) return;
+    Pencil s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const double a = alpha.get();
+        const long xy = g.xy();
+        long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+        for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+            const double uo = u[i];
+            if (HALO_U) reflect_store(u, g, fc, udepth, s.k, s.j, ii, uo);
+            u[i] = uo + a * p[i];
+            const double rn = r[i] - a * w[i];
+            r[i] = rn;
+            acc[0] += rn * rn;
+        }
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+}
+
+// p = beta p + r (APPLY_P) and the depth-1 halos of p and (unless null) u.
+static __global__ void __launch_bounds__(NT) k3_cg_close(Geo g, Faces fc, Scalar beta, int apply_p,
+                                                        double* __restrict__ p, const double* __restrict__ r,
+                                                        double* __restrict__ u)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    const double bt = beta.get();
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+        const double pn = apply_p ? bt * p[i] + r[i] : p[i];
+        p[i] = pn;
+        reflect_store(p, g, fc, 1, s.k, s.j, ii, pn);
+        if (u) reflect_store(u, g, fc, 1, s.k, s.j, ii, u[i]);
+    }
+}
+
+// Chebyshev trip (3d/c_kernels/omp3/cheby_solver.c:62-99) with the previous
+// trip's u += p folded in (ADD), or the init sweep (INIT: p = r / theta).
+template <bool ADD, bool REFLECT, bool INIT, typename Finish>
+static __global__ void __launch_bounds__(NT) k3_cheby_trip(Geo g, Faces fc, ChebyCoef coef, double theta,
+                                                          int write_wr_always, const double* __restrict__ u_in,
+                                                          const double* __restrict__ p_in, double* __restrict__ u_out,
+                                                          double* __restrict__ p_out, const double* __restrict__ u0,
+                                                          double* __restrict__ w, double* __restrict__ r,
+                                                          const double* __restrict__ kx, const double* __restrict__ ky,
+                                                          const double* __restrict__ kz, ReduceSlots rs,
+                                                          const int* __restrict__ done, Finish fin, DevParams prm)
+{
+    if (gate_closed(done)) return;
+    Pencil s(g);
+    double acc[1] = {0.0};
+    double a = 0.0, b = 0.0;
+    if (!INIT) coef.get(a, b);
+    const bool wr = INIT || write_wr_always || !coef.st ||
+                    (coef.st->nch >= coef.st->est && ((coef.st->trip + 1) % 10) == 0) ||
+                    (coef.st->trip + 1 >= prm.max_iters);
+    if (s.active) {
+        auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
+        walk<REFLECT>(g, fc, s, u_in, kx, ky, kz, cur, [&](int ii, long i, double c, double v) {
+            const double rr = u0[i] - v;
+            const double pn = INIT ? rr / theta : a * p_in[i] + b * rr;
+            if (wr) {
+                w[i] = v;
+                r[i] = rr;
+            }
+            acc[0] += rr * rr;
+            p_out[i] = pn;
+            if (ADD) u_out[i] = c;
+            if (REFLECT) reflect_store(ADD ? u_out : const_cast<double*>(u_in), g, fc, 1, s.k, s.j, ii, c);
+        });
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+}
+
+// u += p with the depth-1 halo of u written from the final values (APPLY),
+// or u += p on the interior only (cheby_calc_u, cheby_solver.c:8-24).
+template <bool CLOSE>
+static __global__ void __launch_bounds__(NT) k3_add_p(Geo g, Faces fc, double* __restrict__ u,
+                                                     const double* __restrict__ p)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+        const double un = u[i] + p[i];
+        u[i] = un;
+        if (CLOSE) reflect_store(u, g, fc, 1, s.k, s.j, ii, un);
+    }
+}
+
+// PPCG inner step (3d/c_kernels/omp3/ppcg_solver.c:29-73) with the previous
+// step's sd update folded in (FOLD 1: sd = r/theta; FOLD 2: a sd + b r).
+template <int FOLD, bool NORM, typename Finish>
+static __global__ void __launch_bounds__(NT) k3_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef, int pp_prev,
+                                                         const double* __restrict__ sd_in, double* __restrict__ sd_out,
+                                                         const double* __restrict__ r_in, double* __restrict__ r_out,
+                                                         double* __restrict__ u, const double* __restrict__ kx,
+                                                         const double* __restrict__ ky, const double* __restrict__ kz,
+                                                         ReduceSlots rs, const int* __restrict__ done, Finish fin)
+{
+    if (gate_closed(done)) return;
+    Pencil s(g);
+    double acc[1] = {0.0};
+    double a = 0.0, b = 0.0;
+    if (FOLD == 2) coef.get(pp_prev, a, b);
+    if (s.active) {
+        auto cur = [&](long idx) {
+            if (FOLD == 0) return sd_in[idx];
+            if (FOLD == 1) return r_in[idx] / theta;
+            return a * sd_in[idx] + b * r_in[idx];
+        };
+        walk<true>(g, fc, s, sd_in, kx, ky, kz, cur, [&](int ii, long i, double c, double v) {
+            const double rn = r_in[i] - v;
+            r_out[i] = rn;
+            u[i] += c;
+            sd_out[i] = c;
+            reflect_store(sd_out, g, fc, 1, s.k, s.j, ii, c);
+            if (NORM) acc[0] += rn * rn;
+        });
+    }
+    if (NORM) tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+}
+
+// sd = alpha sd + beta r (the second loop of ppcg_inner_iteration)
+static __global__ void __launch_bounds__(NT) k3_ppcg_sd(Geo g, double alpha, double beta, double* __restrict__ sd,
+                                                       const double* __restrict__ r)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) sd[i] = alpha * sd[i] + beta * r[i];
+}
+
+// r -= A sd ; u += sd (the first loop of ppcg_inner_iteration, halo as stored)
+static __global__ void __launch_bounds__(NT) k3_ppcg_inner_a(Geo g, double* __restrict__ u, double* __restrict__ r,
+                                                            const double* __restrict__ kx, const double* __restrict__ ky,
+                                                            const double* __restrict__ kz, const double* __restrict__ sd)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    Faces none{0, 0, 0, 0, 0, 0};
+    walk<false>(g, none, s, sd, kx, ky, kz, [&](long idx) { return sd[idx]; },
+                [&](int, long i, double c, double v) {
+                    r[i] -= v;
+                    u[i] += c;
+                });
+}
+
+// ------------------------------------------------- shared solver methods --
+
+static __global__ void __launch_bounds__(NT) k3_ppcg_init(Geo g, double theta, const double* __restrict__ r,
+                                                         double* __restrict__ sd)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) sd[i] = r[i] / theta;
+}
+
+static __global__ void __launch_bounds__(NT) k3_copy_u(Geo g, double* __restrict__ u0, const double* __restrict__ u)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) u0[i] = u[i];
+}
+
+static __global__ void __launch_bounds__(NT) k3_residual(Geo g, const double* __restrict__ u,
+                                                        const double* __restrict__ u0, double* __restrict__ r,
+                                                        const double* __restrict__ kx, const double* __restrict__ ky,
+                                                        const double* __restrict__ kz)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    Faces none{0, 0, 0, 0, 0, 0};
+    walk<false>(g, none, s, u, kx, ky, kz, [&](long idx) { return u[idx]; },
+                [&](int, long i, double, double v) { r[i] = u0[i] - v; });
+}
+
+static __global__ void __launch_bounds__(NT) k3_norm2(Geo g, const double* __restrict__ b, ReduceSlots rs)
+{
+    Pencil s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const long xy = g.xy();
+        long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+        for (int ii = s.i0; ii < s.i1; ++ii, i += xy) acc[0] += b[i] * b[i];
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count());
+}
+
+static __global__ void __launch_bounds__(NT) k3_finalise(Geo g, double* __restrict__ energy,
+                                                        const double* __restrict__ density, const double* __restrict__ u)
+{
+    Pencil s(g);
+    if (!s.active) return;
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) energy[i] = u[i] / density[i];
+}
+
+static __global__ void __launch_bounds__(NT) k3_field_summary(Geo g, const double* __restrict__ volume,
+                                                             const double* __restrict__ density,
+                                                             const double* __restrict__ energy0,
+                                                             const double* __restrict__ u, ReduceSlots rs)
+{
+    Pencil s(g);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (s.active) {
+        const long xy = g.xy();
+        long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+        for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+            const double cv = volume[i];
+            const double cm = cv * density[i];
+            acc[0] += cv;
+            acc[1] += cm;
+            acc[2] += cm * energy0[i];
+            acc[3] += cm * u[i];
+        }
+    }
+    tl::grid_sum<4, NT>(acc, rs, block_id(), block_count());
+}
+
+// Jacobi sweep (3d/c_kernels/omp3/jacobi_solver.c:69-115), r holds the old u.
+static __global__ void __launch_bounds__(NT) k3_jacobi_iterate(Geo g, const double* __restrict__ kx,
+                                                              const double* __restrict__ ky,
+                                                              const double* __restrict__ kz,
+                                                              const double* __restrict__ u0, double* __restrict__ u,
+                                                              const double* __restrict__ r, ReduceSlots rs)
+{
+    Pencil s(g);
+    double acc[1] = {0.0};
+    if (s.active) {
+        const int x = g.x;
+        const long xy = g.xy();
+        long i = s.k + (long)s.j * x + (long)s.i0 * xy;
+        for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+            const double v = (u0[i] + (kx[i + 1] * r[i + 1] + kx[i] * r[i - 1]) +
+                              (ky[i + x] * r[i + x] + ky[i] * r[i - x]) + (kz[i + xy] * r[i + xy] + kz[i] * r[i - xy])) /
+                             (1.0 + (kx[i] + kx[i + 1]) + (ky[i] + ky[i + x]) + (kz[i] + kz[i + xy]));
+            u[i] = v;
+            acc[0] += fabs(v - r[i]);
+        }
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count());
+}
+
+// ------------------------------------------------- full-array kernels ----
+
+struct Cell {
+    int k, j, i;
+    bool in;
+    __device__ Cell(const Geo& g)
+    {
+        k = blockIdx.x * FBX + threadIdx.x;
+        j = blockIdx.y * FBY + threadIdx.y;
+        i = blockIdx.z;
+        in = k < g.x && j < g.y;
+    }
+};
+
+// cg_solver_init fused (3d/c_kernels/omp3/cg_solver.c:9-102), p written to
+// both p buffers; coefficients and neighbour values recomputed with the
+// reference expressions.
+template <typename Finish>
+static __global__ void __launch_bounds__(FBX* FBY) k3_cg_init(Geo g, int coefficient, double rx, double ry, double rz,
+                                                             const double* __restrict__ density,
+                                                             const double* __restrict__ energy, double* __restrict__ u,
+                                                             double* __restrict__ p, double* __restrict__ p2,
+                                                             double* __restrict__ r, double* __restrict__ w,
+                                                             double* __restrict__ kx, double* __restrict__ ky,
+                                                             double* __restrict__ kz, ReduceSlots rs, Finish fin)
+{
+    const Cell c(g);
+    const int x = g.x, y = g.y, z = g.z, hd = g.hd;
+    const long xy = g.xy();
+    double acc[1] = {0.0};
+    if (c.in) {
+        const int k = c.k, j = c.j, ii = c.i;
+        const long i = k + (long)j * x + (long)ii * xy;
+        const double rho = density[i];
+        const double uc = energy[i] * rho;
+        u[i] = uc;
+        const bool interior = k >= hd && k < x - hd && j >= hd && j < y - hd && ii >= hd && ii < z - hd;
+        const bool ring = k >= 1 && k < x - 1 && j >= 1 && j < y - 1 && ii >= 1 && ii < z - 1;
+        const bool kzone = k >= hd && k < x - 1 && j >= hd && j < y - 1 && ii >= hd && ii < z - 1;
+        double wc = 0.0;
+        if (ring) wc = coef_w(coefficient, rho);
+        double kxc = 0.0, kyc = 0.0, kzc = 0.0;
+        if (kzone) {
+            kxc = face(rx, coef_w(coefficient, density[i - 1]), wc);
+            kyc = face(ry, coef_w(coefficient, density[i - x]), wc);
+            kzc = face(rz, coef_w(coefficient, density[i - xy]), wc);
+            kx[i] = kxc;
+            ky[i] = kyc;
+            kz[i] = kzc;
+        }
+        if (interior) {
+            const double kxr = (k + 1 < x - 1) ? face(rx, wc, coef_w(coefficient, density[i + 1])) : kx[i + 1];
+            const double kyu = (j + 1 < y - 1) ? face(ry, wc, coef_w(coefficient, density[i + x])) : ky[i + x];
+            const double kzf = (ii + 1 < z - 1) ? face(rz, wc, coef_w(coefficient, density[i + xy])) : kz[i + xy];
+            const double v = smvp(kxc, kxr, kyc, kyu, kzc, kzf, uc, energy[i - 1] * density[i - 1],
+                                  energy[i + 1] * density[i + 1], energy[i - x] * density[i - x],
+                                  energy[i + x] * density[i + x], energy[i - xy] * density[i - xy],
+                                  energy[i + xy] * density[i + xy]);
+            w[i] = v;
+            const double rr = uc - v;
+            r[i] = rr;
+            p[i] = rr;
+            if (p2) p2[i] = rr;
+            acc[0] = rr * rr;
+        } else {
+            p[i] = 0.0;
+            if (p2) p2[i] = 0.0;
+            r[i] = 0.0;
+            if (ring) w[i] = wc;
+        }
+    }
+    tl::grid_sum<1, FBX * FBY>(acc, rs, block_id(), block_count(), fin);
+}
+
+// jacobi_solver_init (3d/c_kernels/omp3/jacobi_solver.c:9-66)
+static __global__ void __launch_bounds__(FBX* FBY) k3_jacobi_init(Geo g, int coefficient, double rx, double ry,
+                                                                 double rz, const double* __restrict__ density,
+                                                                 const double* __restrict__ energy,
+                                                                 double* __restrict__ u0, double* __restrict__ u,
+                                                                 double* __restrict__ kx, double* __restrict__ ky,
+                                                                 double* __restrict__ kz)
+{
+    const Cell c(g);
+    if (!c.in) return;
+    const int x = g.x, y = g.y, z = g.z, hd = g.hd, k = c.k, j = c.j, ii = c.i;
+    const long xy = g.xy();
+    const long i = k + (long)j * x + (long)ii * xy;
+    if (k >= 1 && k < x - 1 && j >= 1 && j < y - 1 && ii >= 1 && ii < z - 1) {
+        const double t = energy[i] * density[i];
+        u0[i] = t;
+        u[i] = t;
+    }
+    if (k >= hd && k < x - 1 && j >= hd && j < y - 1 && ii >= hd && ii < z - 1) {
+        const double cc = coef_w(coefficient, density[i]);
+        const double l = coef_w(coefficient, density[i - 1]);
+        const double d = coef_w(coefficient, density[i - x]);
+        const double b = coef_w(coefficient, density[i - xy]);
+        kx[i] = rx * (l + cc) / (2.0 * l * cc);
+        ky[i] = ry * (d + cc) / (2.0 * d * cc);
+        kz[i] = rz * (b + cc) / (2.0 * b * cc);
+    }
+}
+
+// set_chunk_data (3d/c_kernels/omp3/set_chunk_data.c:8-74)
+static __global__ void k3_set_chunk_data_axes(Geo g, double x_min, double y_min, double z_min, double dx, double dy,
+                                             double dz, double* vx, double* vy, double* vz, double* cx, double* cy,
+                                             double* cz)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int hd = g.hd;
+    if (t <= g.x) vx[t] = x_min + dx * (double)(t - hd);
+    if (t <= g.y) vy[t] = y_min + dy * (double)(t - hd);
+    if (t <= g.z) vz[t] = z_min + dz * (double)(t - hd);
+    if (t < g.x) cx[t] = 0.5 * ((x_min + dx * (double)(t - hd)) + (x_min + dx * (double)(t + 1 - hd)));
+    if (t < g.y) cy[t] = 0.5 * ((y_min + dy * (double)(t - hd)) + (y_min + dy * (double)(t + 1 - hd)));
+    if (t < g.z) cz[t] = 0.5 * ((z_min + dz * (double)(t - hd)) + (z_min + dz * (double)(t + 1 - hd)));
+}
+
+static __global__ void k3_set_chunk_data_cells(long n, double dx, double dy, double dz, double* volume,
+                                              double* x_area, double* y_area, double* z_area)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        volume[i] = dx * dy * dz;
+        x_area[i] = dy * dz;
+        y_area[i] = dx * dz;
+        z_area[i] = dx * dy;
+    }
+}
+
+// set_chunk_state (3d/c_kernels/omp3/set_chunk_state.c:9-98): last state wins.
+static __global__ void __launch_bounds__(FBX* FBY) k3_set_chunk_state(Geo g, const double* __restrict__ vx,
+                                                                     const double* __restrict__ vy,
+                                                                     const double* __restrict__ vz,
+                                                                     const double* __restrict__ cx,
+                                                                     const double* __restrict__ cy,
+                                                                     const double* __restrict__ cz,
+                                                                     double* __restrict__ density,
+                                                                     double* __restrict__ energy0,
+                                                                     double* __restrict__ u, int num_states,
+                                                                     const State* __restrict__ states)
+{
+    const Cell c(g);
+    if (!c.in) return;
+    const int k = c.k, j = c.j, ii = c.i;
+    const long i = k + (long)j * g.x + (long)ii * g.xy();
+    double e = states[0].energy, d = states[0].density;
+    for (int s = 1; s < num_states; ++s) {
+        const State st = states[s];
+        bool hit = false;
+        if (st.geometry == TL3_GEOM_CUBOID) {
+            hit = vx[k + 1] >= st.x_min && vx[k] < st.x_max && vy[j + 1] >= st.y_min && vy[j] < st.y_max &&
+                  vz[ii + 1] >= st.z_min && vz[ii] < st.z_max;
+        } else if (st.geometry == TL3_GEOM_SPHERICAL) {
+            const double ax = cx[k] - st.x_min, ay = cy[j] - st.y_min, az = cz[ii] - st.z_min;
+            hit = sqrt(ax * ax + ay * ay + az * az) <= st.radius;
+        } else if (st.geometry == TL3_GEOM_POINT) {
+            hit = vx[k] == st.x_min && vy[j] == st.y_min && vz[ii] == st.z_min;
+        }
+        if (hit) {
+            e = st.energy;
+            d = st.density;
+        }
+    }
+    energy0[i] = e;
+    density[i] = d;
+    if (k >= 1 && k < g.x - 1 && j >= 1 && j < g.y - 1 && ii >= 1 && ii < g.z - 1) u[i] = e * d;
+}
+
+// Reflective halo update of up to six fields (3d/c_kernels/omp3/local_halos.c).
+struct HaloArgs3 {
+    double* f[TL3_NUM_FIELDS];
+    int nf;
+    int ext[6];
+};
+
+static __global__ void k3_local_halos(Geo g, int depth, HaloArgs3 a)
+{
+    const int x = g.x, y = g.y, z = g.z, hd = g.hd;
+    const long nx = x - 2 * hd, ny = y - 2 * hd, nz = z - 2 * hd;
+    const long xy = g.xy();
+    const long lr = nz * ny * depth, tb = nz * nx * depth, fb = ny * nx * depth;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (blockIdx.y >= (unsigned)a.nf || t >= 2 * (lr + tb + fb)) return;
+    double* f = a.f[blockIdx.y];
+    long q = t;
+    int face;
+    if (q < 2 * lr) face = (int)(q / lr), q %= lr;
+    else if ((q -= 2 * lr) < 2 * tb) face = 2 + (int)(q / tb), q %= tb;
+    else q -= 2 * tb, face = 4 + (int)(q / fb), q %= fb;
+    if (!a.ext[face]) return;
+    const int d = (int)(q % depth);
+    q /= depth;
+    if (face < 2) {           // left / right: q over (ii, jj)
+        const int jj = hd + (int)(q % ny), ii = hd + (int)(q / ny);
+        const long base = (long)ii * xy + (long)jj * x;
+        if (face == 0) f[base + (hd - d - 1)] = f[base + (hd + d)];
+        else f[base + (x - hd + d)] = f[base + (x - hd - 1 - d)];
+    } else if (face < 4) {    // bottom / top: q over (ii, kk)
+        const int kk = hd + (int)(q % nx), ii = hd + (int)(q / nx);
+        const long base = (long)ii * xy + kk;
+        if (face == 2) f[base + (long)(hd - d - 1) * x] = f[base + (long)(hd + d) * x];
+        else f[base + (long)(y - hd + d) * x] = f[base + (long)(y - hd - 1 - d) * x];
+    } else {                  // back / front: q over (jj, kk)
+        const int kk = hd + (int)(q % nx), jj = hd + (int)(q / nx);
+        const long base = (long)jj * x + kk;
+        if (face == 4) f[base + (long)(hd - d - 1) * xy] = f[base + (long)(hd + d) * xy];
+        else f[base + (long)(z - hd + d) * xy] = f[base + (long)(z - hd - 1 - d) * xy];
+    }
+}
+
+// MPI face buffers (3d/c_kernels/omp3/pack_halos.c): pack/unpack one face.
+static __global__ void k3_pack(Geo g, int depth, int face, int pack, double* __restrict__ field,
+                               double* __restrict__ buf)
+{
+    const int x = g.x, y = g.y, z = g.z, hd = g.hd;
+    const long nx = x - 2 * hd, ny = y - 2 * hd, nz = z - 2 * hd;
+    const long xy = g.xy();
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long fi, bi;
+    if (face == TL3_CHUNK_LEFT || face == TL3_CHUNK_RIGHT) {
+        if (t >= nz * ny * depth) return;
+        const int c = (int)(t % depth), jj = hd + (int)((t / depth) % ny), ii = hd + (int)(t / (depth * ny));
+        int kk;
+        if (face == TL3_CHUNK_LEFT) kk = pack ? hd + c : hd - depth + c;
+        else kk = pack ? x - hd - depth + c : x - hd + c;
+        fi = (long)ii * xy + (long)jj * x + kk;
+        bi = c + (long)(jj - hd) * depth + (long)(ii - hd) * depth * ny;
+    } else if (face == TL3_CHUNK_BOTTOM || face == TL3_CHUNK_TOP) {
+        if (t >= nz * nx * depth) return;
+        const int kk = hd + (int)(t % nx), c = (int)((t / nx) % depth), ii = hd + (int)(t / (nx * depth));
+        int jj;
+        if (face == TL3_CHUNK_BOTTOM) jj = pack ? hd + c : hd - depth + c;
+        else jj = pack ? y - hd - depth + c : y - hd + c;
+        fi = (long)ii * xy + (long)jj * x + kk;
+        bi = (kk - hd) + (long)c * nx + (long)(ii - hd) * depth * nx;
+    } else {
+        if (t >= ny * nx * depth) return;
+        const int kk = hd + (int)(t % nx), jj = hd + (int)((t / nx) % ny), c = (int)(t / (nx * ny));
+        int ii;
+        if (face == TL3_CHUNK_BACK) ii = pack ? hd + c : hd - depth + c;
+        else ii = pack ? z - hd - depth + c : z - hd + c;
+        fi = (long)ii * xy + (long)jj * x + kk;
+        bi = (kk - hd) + (long)(jj - hd) * nx + (long)c * nx * ny;
+    }
+    if (pack) buf[bi] = field[fi];
+    else field[fi] = buf[bi];
+}
+
+// r = u over the full array (the first loop of jacobi_solver_iterate),
+// skipped once a device-resident loop has ended.
+static __global__ void k3_copy_full(long n, double* __restrict__ dst, const double* __restrict__ src,
+                                   const int* __restrict__ done)
+{
+    if (gate_closed(done)) return;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+}  // namespace tl3d
