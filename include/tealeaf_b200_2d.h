@@ -312,6 +312,12 @@ typedef struct TlStepStats
 int tl2d_calculate_2norm_noalloc(const double* field, int x, int y, int halo_depth,
         double* norm_dev, void* stream);
 
+/* The four field-summary totals from a parallel tree reduction: one sweep at
+ * full bandwidth instead of run_field_summary's serial reference order, so
+ * the last bits differ from the reference (accumulated like run_field_summary). */
+void tl2d_field_summary_fast(Chunk* chunk, Settings* settings,
+        double* vol, double* mass, double* ie, double* temp);
+
 /* One timestep of solve() (2d/diffuse.c:22-80) on the device-resident path. */
 void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stats);
 

@@ -286,6 +286,12 @@ typedef struct TlStepStats3
     double exact_error;
 } TlStepStats3;
 
+/* The four field-summary totals from a parallel tree reduction: one sweep at
+ * full bandwidth instead of run_field_summary's serial reference order, so
+ * the last bits differ from the reference (accumulated like run_field_summary). */
+void tl3d_field_summary_fast(Chunk* chunk, Settings* settings,
+        double* vol, double* mass, double* ie, double* temp);
+
 /* One timestep of solve() (3d/diffuse.c:21-81) on the device-resident path. */
 void tl3d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats3* stats);
 

@@ -44,7 +44,8 @@ struct Run {
     Settings* settings;
     DevParams prm;
     Faces fc;
-    dim3 gi;
+    dim3 gi;               // interior sweeps
+    dim3 gh;               // fused sweeps: interior + halo-duty block row
     DevState host_state;   // last copy read back
 
     const int* done() const { return &s->d_state->done; }
@@ -107,17 +108,17 @@ struct Run {
         int cur = 0;
         auto trip = [&](int t) {
             if (fresh && t == from) {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gi, BX, 0, s->stream>>>(
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gh, BX, 0, s->stream>>>(
                               s->g, fc, beta, buf[cur], buf[cur], chunk->r, chunk->w, chunk->kx, chunk->ky,
-                              s->rs, done(), fin_w)));
+                              nullptr, 0, s->rs, done(), fin_w)));
             } else {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gi, BX, 0, s->stream>>>(
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gh, BX, 0, s->stream>>>(
                               s->g, fc, beta, buf[cur], buf[cur ^ 1], chunk->r, chunk->w, chunk->kx,
-                              chunk->ky, s->rs, done(), fin_w)));
+                              chunk->ky, nullptr, 0, s->rs, done(), fin_w)));
                 cur ^= 1;
             }
-            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<true><<<gi, BX, 0, s->stream>>>(
-                          s->g, fc, 1, alpha, chunk->u, buf[cur], chunk->r, chunk->w, s->rs, done(), fin_ur)));
+            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
+                          s->g, alpha, chunk->u, buf[cur], chunk->r, chunk->w, s->rs, done(), fin_ur)));
         };
         DevState st = loop(from, trip);
         // Trips from..st.trip-1 ran; the fused ones flipped the current buffer.
@@ -184,7 +185,7 @@ struct Run {
         int cur = 0;
         auto trip = [&](int t, int force) {
             FinChebyTrip fin{s->d_state, pc, s->d_mirror, force};
-            TL_LAUNCH(s, "k_cheby_trip", (k_cheby_trip<true, true><<<gi, BX, 0, s->stream>>>(
+            TL_LAUNCH(s, "k_cheby_trip", (k_cheby_trip<true, true><<<gh, BX, 0, s->stream>>>(
                           s->g, fc, coef, force, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->u0, chunk->w,
                           chunk->r, chunk->kx, chunk->ky, s->rs, done(), fin, pc)));
             cur ^= 1;
@@ -243,33 +244,33 @@ struct Run {
         FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
         auto trip = [&](int t) {
             if (t == tt) {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gi, BX, 0, s->stream>>>(
-                              s->g, fc, beta, pb[pc], pb[pc], rb[rc], chunk->w, chunk->kx, chunk->ky, s->rs,
-                              done(), fin_w)));
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gh, BX, 0, s->stream>>>(
+                              s->g, fc, beta, pb[pc], pb[pc], rb[rc], chunk->w, chunk->kx, chunk->ky, nullptr, 0,
+                              s->rs, done(), fin_w)));
             } else {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gi, BX, 0, s->stream>>>(
-                              s->g, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->w, chunk->kx, chunk->ky, s->rs,
-                              done(), fin_w)));
+                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gh, BX, 0, s->stream>>>(
+                              s->g, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->w, chunk->kx, chunk->ky, nullptr,
+                              0, s->rs, done(), fin_w)));
                 pc ^= 1;
             }
-            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<false><<<gi, BX, 0, s->stream>>>(
-                          s->g, fc, 1, alpha, chunk->u, pb[pc], rb[rc], chunk->w, s->rs, done(), tl::NoFinish())));
+            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
+                          s->g, alpha, chunk->u, pb[pc], rb[rc], chunk->w, s->rs, done(), tl::NoFinish())));
             for (int pp = 0; pp < ni; ++pp) {
                 const bool last = pp == ni - 1;
                 if (pp == 0 && last)
-                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<1, true><<<gi, BX, 0, s->stream>>>(
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<1, true><<<gh, BX, 0, s->stream>>>(
                                   s->g, fc, chunk->theta, coef, 0, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1], chunk->u,
                                   chunk->kx, chunk->ky, s->rs, done(), fin_n)));
                 else if (pp == 0)
-                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<1, false><<<gi, BX, 0, s->stream>>>(
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<1, false><<<gh, BX, 0, s->stream>>>(
                                   s->g, fc, chunk->theta, coef, 0, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1], chunk->u,
                                   chunk->kx, chunk->ky, s->rs, done(), tl::NoFinish())));
                 else if (last)
-                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<2, true><<<gi, BX, 0, s->stream>>>(
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<2, true><<<gh, BX, 0, s->stream>>>(
                                   s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1],
                                   chunk->u, chunk->kx, chunk->ky, s->rs, done(), fin_n)));
                 else
-                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<2, false><<<gi, BX, 0, s->stream>>>(
+                    TL_LAUNCH(s, "k_ppcg_step", (k_ppcg_step<2, false><<<gh, BX, 0, s->stream>>>(
                                   s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1],
                                   chunk->u, chunk->kx, chunk->ky, s->rs, done(), tl::NoFinish())));
                 sc ^= 1;
@@ -366,7 +367,7 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
     TlStepStats local{};
     TlStepStats* st_out = stats ? stats : &local;
     *st_out = TlStepStats{};
-    Run R{s, chunk, settings, {}, faces_of(chunk), interior_grid(s->g), {}};
+    Run R{s, chunk, settings, {}, faces_of(chunk), interior_grid(s->g), fused_grid(s->g), {}};
     R.prm.eps = settings->eps;
     R.prm.eps_lim = settings->eps_lim;
     R.prm.max_iters = settings->max_iters;

@@ -31,6 +31,7 @@ struct Run3 {
     DevParams prm;
     Faces fc;
     dim3 gi, bl;
+    dim3 gh;   // fused sweeps: interior + halo-duty z-plane
     DevState host_state;
 
     const int* done() const { return &s->d_state->done; }
@@ -100,18 +101,17 @@ struct Run3 {
         int cur = 0;
         auto trip = [&](int t) {
             if (fresh && t == from) {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gi, bl, 0, s->stream>>>(
+                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gh, bl, 0, s->stream>>>(
                                s->g, fc, beta, buf[cur], buf[cur], chunk->vec_r, chunk->vec_w, chunk->vec_kx,
-                               chunk->vec_ky, chunk->vec_kz, s->rs, done(), fin_w)));
+                               chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
             } else {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gi, bl, 0, s->stream>>>(
+                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gh, bl, 0, s->stream>>>(
                                s->g, fc, beta, buf[cur], buf[cur ^ 1], chunk->vec_r, chunk->vec_w, chunk->vec_kx,
-                               chunk->vec_ky, chunk->vec_kz, s->rs, done(), fin_w)));
+                               chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
                 cur ^= 1;
             }
-            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<true><<<gi, bl, 0, s->stream>>>(
-                           s->g, fc, 1, alpha, chunk->vec_u, buf[cur], chunk->vec_r, chunk->vec_w, s->rs, done(),
-                           fin_ur)));
+            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(
+                           s->g, alpha, chunk->vec_u, buf[cur], chunk->vec_r, chunk->vec_w, s->rs, done(), fin_ur)));
         };
         DevState st = loop(from, trip);
         const int ran = st.trip - from;
@@ -144,7 +144,7 @@ struct Run3 {
         tl::DevParams pc = prm;
         pc.switch_enabled = 0;
         TL3_LAUNCH(s, "k3_cheby_trip<init>",
-                   (k3_cheby_trip<false, false, true><<<gi, bl, 0, s->stream>>>(
+                   (k3_cheby_trip<false, false, true><<<gh, bl, 0, s->stream>>>(
                        s->g, none, tl::ChebyCoef{0.0, 0.0, nullptr, nullptr, nullptr}, chunk->theta, 1, chunk->vec_u,
                        chunk->vec_p, chunk->vec_u, chunk->vec_p, chunk->vec_u0, chunk->vec_w, chunk->vec_r,
                        chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr, tl::NoFinish(), pc)));
@@ -162,7 +162,7 @@ struct Run3 {
         int cur = 0;
         auto trip = [&](int, int force) {
             tl::FinChebyTrip fin{s->d_state, pc, s->d_mirror, force};
-            TL3_LAUNCH(s, "k3_cheby_trip", (k3_cheby_trip<true, true, false><<<gi, bl, 0, s->stream>>>(
+            TL3_LAUNCH(s, "k3_cheby_trip", (k3_cheby_trip<true, true, false><<<gh, bl, 0, s->stream>>>(
                            s->g, fc, coef, 0.0, force, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->vec_u0,
                            chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(),
                            fin, pc)));
@@ -219,22 +219,21 @@ struct Run3 {
         tl::FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
         auto trip = [&](int t) {
             if (t == tt) {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gi, bl, 0, s->stream>>>(
+                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gh, bl, 0, s->stream>>>(
                                s->g, fc, beta, pb[pc], pb[pc], rb[rc], chunk->vec_w, chunk->vec_kx, chunk->vec_ky,
-                               chunk->vec_kz, s->rs, done(), fin_w)));
+                               chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
             } else {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gi, bl, 0, s->stream>>>(
+                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gh, bl, 0, s->stream>>>(
                                s->g, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->vec_w, chunk->vec_kx,
-                               chunk->vec_ky, chunk->vec_kz, s->rs, done(), fin_w)));
+                               chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
                 pc ^= 1;
             }
-            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<false><<<gi, bl, 0, s->stream>>>(
-                           s->g, fc, 1, alpha, chunk->vec_u, pb[pc], rb[rc], chunk->vec_w, s->rs, done(),
-                           tl::NoFinish())));
+            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(
+                           s->g, alpha, chunk->vec_u, pb[pc], rb[rc], chunk->vec_w, s->rs, done(), tl::NoFinish())));
             for (int pp = 0; pp < ni; ++pp) {
                 const bool last = pp == ni - 1;
 #define STEP3(FOLD, NORM, FIN)                                                                                    \
-    TL3_LAUNCH(s, "k3_ppcg_step", (k3_ppcg_step<FOLD, NORM><<<gi, bl, 0, s->stream>>>(                            \
+    TL3_LAUNCH(s, "k3_ppcg_step", (k3_ppcg_step<FOLD, NORM><<<gh, bl, 0, s->stream>>>(                            \
                                       s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1], \
                                       chunk->vec_u, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(),    \
                                       FIN)))
@@ -337,7 +336,7 @@ void tl3d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats3* sta
     TlStepStats3 local{};
     TlStepStats3* st_out = stats ? stats : &local;
     *st_out = TlStepStats3{};
-    Run3 R{s, chunk, settings, {}, faces_of(chunk), interior_grid(s->g), interior_block(), {}};
+    Run3 R{s, chunk, settings, {}, faces_of(chunk), interior_grid(s->g), interior_block(), fused_grid(s->g), {}};
     R.prm.eps = settings->eps;
     R.prm.eps_lim = settings->eps_lim;
     R.prm.max_iters = settings->max_iters;

@@ -34,8 +34,22 @@ using tl::gate_closed;
 using tl::PpcgCoef;
 using tl::Scalar;
 
+// Tuning of the fused sweeps: rows unrolled per thread and the minimum blocks
+// per SM the register allocation must allow (__launch_bounds__).
+#ifndef TL2D_UNROLL
+#define TL2D_UNROLL 4
+#endif
+#ifndef TL2D_MINB
+#define TL2D_MINB 16
+#endif
+#define TL2D_STR(x) #x
+#define TL2D_PRAGMA_UNROLL(n) _Pragma(TL2D_STR(unroll n))
+
 constexpr int BX = 128;   // threads (columns) per block of an interior sweep
-constexpr int ROWS = 8;   // rows per thread of an interior sweep
+#ifndef TL2D_ROWS
+#define TL2D_ROWS 8
+#endif
+constexpr int ROWS = TL2D_ROWS;   // rows per thread of an interior sweep
 constexpr int FB = 256;   // threads per block of full-array kernels
 
 struct Geo {
@@ -568,56 +582,122 @@ __device__ __forceinline__ void reflect_store(double* f, const Geo& g, const Fac
     if (fc.t && (g.y - g.hd - 1 - j) < depth) f[(long)(2 * (g.y - g.hd) - 1 - j) * g.x + k] = v;
 }
 
-// CG sweep 1: [p = beta p + r] (FUSE_P, cg.c:146-164) ; depth-1 reflective
-// halo of p (REFLECT) ; w = A p ; pw = sum(w*p)  (cg.c:88-113).
-// p is read from p_in and the updated p written to p_out (a second buffer:
-// neighbours still read the old p); with REFLECT the halo of p_out is written.
+// Halo duty: the extra block row of a fused sweep writes reflective halo
+// cells, so the row loop of the other blocks stays free of scattered stores.
+// For every external face and layer d < depth: dst[mirror] = val(source),
+// source = the interior cell d layers in (local_halos.c:66-149 pattern).
+// `val` must read only data the sweep does not modify.
+template <typename Val>
+__device__ __forceinline__ void halo_duty(const Geo& g, const Faces& fc, int depth, double* __restrict__ dst,
+                                          Val val)
+{
+    const int x = g.x, hd = g.hd;
+    const long nx = g.x - 2 * hd, ny = g.y - 2 * hd;
+    const long per = (long)depth * (2 * ny + 2 * nx);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
+        const int d = (int)(t % depth);
+        long q = t / depth;
+        if (q < ny) {
+            const long row = (long)(hd + q) * x;
+            if (fc.l) dst[row + (hd - 1 - d)] = val(row + (hd + d));
+        } else if ((q -= ny) < ny) {
+            const long row = (long)(hd + q) * x;
+            if (fc.r) dst[row + (x - hd + d)] = val(row + (x - hd - 1 - d));
+        } else if ((q -= ny) < nx) {
+            const long col = hd + q;
+            if (fc.b) dst[col + (long)(hd - 1 - d) * x] = val(col + (long)(hd + d) * x);
+        } else {
+            q -= nx;
+            const long col = hd + q;
+            if (fc.t) dst[col + (long)(g.y - hd + d) * x] = val(col + (long)(g.y - hd - 1 - d) * x);
+        }
+    }
+}
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Column-strip coordinates with the column clamped for lanes past the
+// interior (they load valid cells, feed the warp shuffles, store nothing).
+struct StripC {
+    int k, kk, j0, j1, lane;
+    bool active, at_l, at_r;
+    __device__ StripC(const Geo& g)
+    {
+        k = g.hd + blockIdx.x * BX + threadIdx.x;
+        active = k < g.x - g.hd;
+        kk = active ? k : g.x - g.hd - 1;
+        j0 = g.hd + blockIdx.y * ROWS;
+        j1 = min(j0 + ROWS, g.y - g.hd);
+        lane = threadIdx.x & 31;
+        at_l = kk == g.hd;
+        at_r = kk == g.x - g.hd - 1;
+    }
+};
+
+// CG sweep 1 (grid: interior blocks + one halo-duty block row):
+//   [p = beta p + r]   (FUSE_P; cg.c:146-164, the previous step's calc_p)
+//   w = A p ; pw = sum(w*p)   (cg.c:88-113)
+// With REFLECT the depth-1 reflective halo of p is taken from the mirrored
+// interior cell and written into p_out's halo; with u_halo the pending
+// reflective halo of u (depth uhd, u is not modified here) is written too.
+// p is read from p_in, the new p written to p_out (a second buffer, since
+// neighbours still read the old p; p_out == p_in when !FUSE_P).
 template <bool FUSE_P, bool REFLECT, typename Finish>
-static __global__ void __launch_bounds__(BX) k_cg_w_fused(Geo g, Faces fc, Scalar beta, const double* __restrict__ p_in,
-                                                   double* __restrict__ p_out, const double* __restrict__ r,
-                                                   double* __restrict__ w, const double* __restrict__ kx,
-                                                   const double* __restrict__ ky, ReduceSlots rs,
-                                                   const int* __restrict__ done, Finish fin)
+static __global__ void __launch_bounds__(BX, TL2D_MINB) k_cg_w_fused(Geo g, Faces fc, Scalar beta,
+                                                          const double* __restrict__ p_in, double* p_out,
+                                                          const double* __restrict__ r, double* __restrict__ w,
+                                                          const double* __restrict__ kx,
+                                                          const double* __restrict__ ky, double* u_halo, int uhd,
+                                                          ReduceSlots rs, const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
-    Strip s(g);
     double acc[1] = {0.0};
-    if (s.active) {
-        const double bt = FUSE_P ? beta.get() : 0.0;
-        const int x = g.x, k = s.k;
-        const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
-        auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
-        long i = k + (long)s.j0 * x;
+    const double bt = FUSE_P ? beta.get() : 0.0;
+    auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
+    if (blockIdx.y + 1 < gridDim.y) {
+        const StripC s(g);
+        const int x = g.x;
+        long i = s.kk + (long)s.j0 * x;
         double pc = cur(i);
         double pd = (s.j0 == g.hd) ? ((REFLECT && fc.b) ? pc : p_in[i - x]) : cur(i - x);
         double kyc = ky[i];
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
         for (int j = s.j0; j < s.j1; ++j, i += x) {
             const bool at_t = j == g.y - g.hd - 1;
             const double pu = at_t ? ((REFLECT && fc.t) ? pc : p_in[i + x]) : cur(i + x);
-            const double pl = at_l ? ((REFLECT && fc.l) ? pc : p_in[i - 1]) : cur(i - 1);
-            const double pr = at_r ? ((REFLECT && fc.r) ? pc : p_in[i + 1]) : cur(i + 1);
             const double kyu = ky[i + x];
-            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, pc, pl, pr, pd, pu);
-            w[i] = v;
-            acc[0] += v * pc;
-            if (FUSE_P) p_out[i] = pc;
-            if (REFLECT) reflect_store(p_out, g, fc, 1, k, j, pc);
+            const double kxc = kx[i];
+            double pl = __shfl_up_sync(kFull, pc, 1);
+            double pr = __shfl_down_sync(kFull, pc, 1);
+            double kxr = __shfl_down_sync(kFull, kxc, 1);
+            if (s.at_l) pl = (REFLECT && fc.l) ? pc : p_in[i - 1];
+            else if (s.lane == 0) pl = cur(i - 1);
+            if (s.at_r) pr = (REFLECT && fc.r) ? pc : p_in[i + 1];
+            else if (s.lane == 31) pr = cur(i + 1);
+            if (s.at_r || s.lane == 31) kxr = kx[i + 1];
+            const double v = smvp(kxc, kxr, kyc, kyu, pc, pl, pr, pd, pu);
+            if (s.active) {
+                w[i] = v;
+                acc[0] += v * pc;
+                if (FUSE_P) p_out[i] = pc;
+            }
             pd = pc;
             pc = pu;
             kyc = kyu;
         }
+    } else {
+        if (REFLECT) halo_duty(g, fc, 1, p_out, cur);
+        if (u_halo) halo_duty(g, fc, uhd, u_halo, [&](long idx) { return u_halo[idx]; });
     }
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
-// CG sweep 2: u += alpha p ; r -= alpha w ; rrn = sum(r*r) (cg.c:116-143),
-// first writing the pending reflective halo of u (HALO_U, depth udepth) from
-// the values u holds before the update.
-template <bool HALO_U, typename Finish>
-static __global__ void __launch_bounds__(BX) k_cg_ur_fused(Geo g, Faces fc, int udepth, Scalar alpha,
-                                                    double* __restrict__ u, const double* __restrict__ p,
-                                                    double* __restrict__ r, const double* __restrict__ w,
-                                                    ReduceSlots rs, const int* __restrict__ done, Finish fin)
+// CG sweep 2: u += alpha p ; r -= alpha w ; rrn = sum(r*r)  (cg.c:116-143)
+template <typename Finish>
+static __global__ void __launch_bounds__(BX, TL2D_MINB) k_cg_ur_fused(Geo g, Scalar alpha, double* __restrict__ u,
+                                                           const double* __restrict__ p, double* __restrict__ r,
+                                                           const double* __restrict__ w, ReduceSlots rs,
+                                                           const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
     Strip s(g);
@@ -625,10 +705,9 @@ static __global__ void __launch_bounds__(BX) k_cg_ur_fused(Geo g, Faces fc, int 
     if (s.active) {
         const double a = alpha.get();
         long i = s.k + (long)s.j0 * g.x;
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
         for (int j = s.j0; j < s.j1; ++j, i += g.x) {
-            const double uo = u[i];
-            if (HALO_U) reflect_store(u, g, fc, udepth, s.k, j, uo);
-            u[i] = uo + a * p[i];
+            u[i] += a * p[i];
             const double rn = r[i] - a * w[i];
             r[i] = rn;
             acc[0] += rn * rn;
@@ -661,18 +740,20 @@ static __global__ void __launch_bounds__(BX) k_cg_close(Geo g, Faces fc, Scalar 
 // in (ADD: u_n = u_{n-1} + p_{n-1}, read at the stencil points from u_in and
 // p_in): w = A u_n ; r = u0 - w ; p_n = alpha p_{n-1} + beta r. Writes u_n to
 // u_out and p_n to p_out (second buffers: neighbours read the old values),
-// w and r when `write_wr`, and reduces sum(r*r).
+// w and r when `write_wr` applies, and reduces sum(r*r). With REFLECT the
+// depth-1 halo of u_n is taken from the mirrored cells and written by the
+// halo-duty block row (grid: interior blocks + one row).
 template <bool ADD, bool REFLECT, typename Finish>
-static __global__ void __launch_bounds__(BX) k_cheby_trip(Geo g, Faces fc, ChebyCoef coef, int write_wr_always,
-                                                   const double* __restrict__ u_in, const double* __restrict__ p_in,
-                                                   double* __restrict__ u_out, double* __restrict__ p_out,
-                                                   const double* __restrict__ u0, double* __restrict__ w,
-                                                   double* __restrict__ r, const double* __restrict__ kx,
-                                                   const double* __restrict__ ky, ReduceSlots rs,
-                                                   const int* __restrict__ done, Finish fin, DevParams prm)
+static __global__ void __launch_bounds__(BX, TL2D_MINB) k_cheby_trip(Geo g, Faces fc, ChebyCoef coef, int write_wr_always,
+                                                          const double* __restrict__ u_in,
+                                                          const double* __restrict__ p_in, double* u_out,
+                                                          double* __restrict__ p_out, const double* __restrict__ u0,
+                                                          double* __restrict__ w, double* __restrict__ r,
+                                                          const double* __restrict__ kx,
+                                                          const double* __restrict__ ky, ReduceSlots rs,
+                                                          const int* __restrict__ done, Finish fin, DevParams prm)
 {
     if (gate_closed(done)) return;
-    Strip s(g);
     double acc[1] = {0.0};
     double a, b;
     coef.get(a, b);
@@ -681,35 +762,46 @@ static __global__ void __launch_bounds__(BX) k_cheby_trip(Geo g, Faces fc, Cheby
     const bool wr = write_wr_always || !coef.st ||
                     (coef.st->nch >= coef.st->est && ((coef.st->trip + 1) % 10) == 0) ||
                     (coef.st->trip + 1 >= prm.max_iters);
-    if (s.active) {
-        const int x = g.x, k = s.k;
-        const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
-        auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
-        long i = k + (long)s.j0 * x;
+    auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
+    if (blockIdx.y + 1 < gridDim.y) {
+        const StripC s(g);
+        const int x = g.x;
+        long i = s.kk + (long)s.j0 * x;
         double uc = cur(i);
         double ud = (s.j0 == g.hd) ? ((REFLECT && fc.b) ? uc : u_in[i - x]) : cur(i - x);
         double kyc = ky[i];
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
         for (int j = s.j0; j < s.j1; ++j, i += x) {
             const bool at_t = j == g.y - g.hd - 1;
             const double uu = at_t ? ((REFLECT && fc.t) ? uc : u_in[i + x]) : cur(i + x);
-            const double ul = at_l ? ((REFLECT && fc.l) ? uc : u_in[i - 1]) : cur(i - 1);
-            const double ur = at_r ? ((REFLECT && fc.r) ? uc : u_in[i + 1]) : cur(i + 1);
             const double kyu = ky[i + x];
-            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, uc, ul, ur, ud, uu);
+            const double kxc = kx[i];
+            double ul = __shfl_up_sync(kFull, uc, 1);
+            double ur = __shfl_down_sync(kFull, uc, 1);
+            double kxr = __shfl_down_sync(kFull, kxc, 1);
+            if (s.at_l) ul = (REFLECT && fc.l) ? uc : u_in[i - 1];
+            else if (s.lane == 0) ul = cur(i - 1);
+            if (s.at_r) ur = (REFLECT && fc.r) ? uc : u_in[i + 1];
+            else if (s.lane == 31) ur = cur(i + 1);
+            if (s.at_r || s.lane == 31) kxr = kx[i + 1];
+            const double v = smvp(kxc, kxr, kyc, kyu, uc, ul, ur, ud, uu);
             const double rr = u0[i] - v;
-            const double pn = a * p_in[i] + b * rr;
-            if (wr) {
-                w[i] = v;
-                r[i] = rr;
+            if (s.active) {
+                const double pn = a * p_in[i] + b * rr;
+                if (wr) {
+                    w[i] = v;
+                    r[i] = rr;
+                }
+                acc[0] += rr * rr;
+                p_out[i] = pn;
+                if (ADD) u_out[i] = uc;
             }
-            acc[0] += rr * rr;
-            p_out[i] = pn;
-            if (ADD) u_out[i] = uc;
-            if (REFLECT) reflect_store(ADD ? u_out : const_cast<double*>(u_in), g, fc, 1, k, j, uc);
             ud = uc;
             uc = uu;
             kyc = kyu;
         }
+    } else if (REFLECT) {
+        halo_duty(g, fc, 1, ADD ? u_out : const_cast<double*>(u_in), cur);
     }
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
@@ -736,53 +828,63 @@ static __global__ void __launch_bounds__(BX) k_add_p_close(Geo g, Faces fc, doub
 // in: FOLD 0: sd = sd_in (as stored); FOLD 1: sd = r_in / theta (ppcg_init,
 // ppcg.c:9-26); FOLD 2: sd = a_prev sd_in + b_prev r_in. Then, with the
 // depth-1 reflective halo of sd: r = r_in - A sd ; u += sd. sd goes to
-// sd_out, r to r_out (second buffers: neighbours read the old values);
-// NORM reduces sum(r*r) of the new r.
+// sd_out, r to r_out (second buffers: neighbours read the old values); the
+// halo-duty block row writes sd_out's halo; NORM reduces sum(r*r) of the new r.
 template <int FOLD, bool NORM, typename Finish>
-static __global__ void __launch_bounds__(BX) k_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef, int pp_prev,
-                                                  const double* __restrict__ sd_in, double* __restrict__ sd_out,
-                                                  const double* __restrict__ r_in, double* __restrict__ r_out,
-                                                  double* __restrict__ u, const double* __restrict__ kx,
-                                                  const double* __restrict__ ky, ReduceSlots rs,
-                                                  const int* __restrict__ done, Finish fin)
+static __global__ void __launch_bounds__(BX, TL2D_MINB) k_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef, int pp_prev,
+                                                         const double* __restrict__ sd_in,
+                                                         double* __restrict__ sd_out,
+                                                         const double* __restrict__ r_in, double* __restrict__ r_out,
+                                                         double* __restrict__ u, const double* __restrict__ kx,
+                                                         const double* __restrict__ ky, ReduceSlots rs,
+                                                         const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
-    Strip s(g);
     double acc[1] = {0.0};
     double a = 0.0, b = 0.0;
     if (FOLD == 2) coef.get(pp_prev, a, b);
-    if (s.active) {
-        const int x = g.x, k = s.k;
-        const bool at_l = k == g.hd, at_r = k == g.x - g.hd - 1;
-        auto cur = [&](long idx) {
-            if (FOLD == 0) return sd_in[idx];
-            if (FOLD == 1) return r_in[idx] / theta;
-            return a * sd_in[idx] + b * r_in[idx];
-        };
-        long i = k + (long)s.j0 * x;
+    auto cur = [&](long idx) {
+        if (FOLD == 0) return sd_in[idx];
+        if (FOLD == 1) return r_in[idx] / theta;
+        return a * sd_in[idx] + b * r_in[idx];
+    };
+    if (blockIdx.y + 1 < gridDim.y) {
+        const StripC s(g);
+        const int x = g.x;
+        long i = s.kk + (long)s.j0 * x;
         double sc = cur(i);
         double sdn = (s.j0 == g.hd) ? (fc.b ? sc : sd_in[i - x]) : cur(i - x);
         double kyc = ky[i];
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
         for (int j = s.j0; j < s.j1; ++j, i += x) {
             const bool at_t = j == g.y - g.hd - 1;
             const double su = at_t ? (fc.t ? sc : sd_in[i + x]) : cur(i + x);
-            const double sl = at_l ? (fc.l ? sc : sd_in[i - 1]) : cur(i - 1);
-            const double sr = at_r ? (fc.r ? sc : sd_in[i + 1]) : cur(i + 1);
             const double kyu = ky[i + x];
-            const double v = smvp(kx[i], kx[i + 1], kyc, kyu, sc, sl, sr, sdn, su);
-            const double rn = r_in[i] - v;
-            r_out[i] = rn;
-            u[i] += sc;
-            sd_out[i] = sc;
-            reflect_store(sd_out, g, fc, 1, k, j, sc);
-            if (NORM) acc[0] += rn * rn;
+            const double kxc = kx[i];
+            double sl = __shfl_up_sync(kFull, sc, 1);
+            double sr = __shfl_down_sync(kFull, sc, 1);
+            double kxr = __shfl_down_sync(kFull, kxc, 1);
+            if (s.at_l) sl = fc.l ? sc : sd_in[i - 1];
+            else if (s.lane == 0) sl = cur(i - 1);
+            if (s.at_r) sr = fc.r ? sc : sd_in[i + 1];
+            else if (s.lane == 31) sr = cur(i + 1);
+            if (s.at_r || s.lane == 31) kxr = kx[i + 1];
+            const double v = smvp(kxc, kxr, kyc, kyu, sc, sl, sr, sdn, su);
+            if (s.active) {
+                const double rn = r_in[i] - v;
+                r_out[i] = rn;
+                u[i] += sc;
+                sd_out[i] = sc;
+                if (NORM) acc[0] += rn * rn;
+            }
             sdn = sc;
             sc = su;
             kyc = kyu;
         }
+    } else {
+        halo_duty(g, fc, 1, sd_out, cur);
     }
     if (NORM) tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
-
 
 }  // namespace tl2d

@@ -30,7 +30,17 @@ using tl::gate_closed;
 using tl::PpcgCoef;
 using tl::Scalar;
 
-constexpr int BX = 32;   // x threads per block of an interior sweep
+#ifndef TL3D_UNROLL
+#define TL3D_UNROLL 4
+#endif
+#ifndef TL3D_MINB
+#define TL3D_MINB 16
+#endif
+#define TL3D_STR(x) #x
+#define TL3D_PRAGMA_UNROLL(n) _Pragma(TL3D_STR(unroll n))
+constexpr unsigned kFull3 = 0xffffffffu;
+
+constexpr int BX = 32;   // x threads per block of an interior sweep (one warp per y row)
 constexpr int BY = 4;    // y threads per block
 constexpr int ZR = 8;    // z cells per thread
 constexpr int NT = BX * BY;
@@ -76,6 +86,106 @@ struct Pencil {
         active = k < g.x - g.hd && j < g.y - g.hd;
     }
 };
+
+// Pencil with the cell clamped into the interior for lanes past it (they
+// load valid cells and feed the x-neighbour shuffles, but store nothing).
+struct PencilC {
+    int k, j, i0, i1, lane;
+    bool active, rowok, at_l, at_r, at_b, at_t;
+    __device__ PencilC(const Geo& g)
+    {
+        const int k0 = g.hd + blockIdx.x * BX + threadIdx.x;
+        const int j0 = g.hd + blockIdx.y * BY + threadIdx.y;
+        rowok = j0 < g.y - g.hd;
+        active = rowok && k0 < g.x - g.hd;
+        k = min(k0, g.x - g.hd - 1);
+        j = min(j0, g.y - g.hd - 1);
+        i0 = g.hd + blockIdx.z * ZR;
+        i1 = min(i0 + ZR, g.z - g.hd);
+        lane = threadIdx.x;
+        at_l = k == g.hd;
+        at_r = k == g.x - g.hd - 1;
+        at_b = j == g.hd;
+        at_t = j == g.y - g.hd - 1;
+    }
+};
+
+// Halo duty of the extra z-plane of blocks: reflective halo cells of the
+// external faces, dst[mirror] = val(source) for layers d < depth (3D
+// local_halos.c pattern). `val` reads only data the sweep does not modify.
+template <typename Val>
+__device__ __forceinline__ void halo_duty3(const Geo& g, const Faces& fc, int depth, double* __restrict__ dst, Val val)
+{
+    const int x = g.x, y = g.y, z = g.z, hd = g.hd;
+    const long nx = x - 2 * hd, ny = y - 2 * hd, nz = z - 2 * hd;
+    const long xy = g.xy();
+    const long lr = nz * ny * depth, tb = nz * nx * depth, fb = ny * nx * depth;
+    const long nthreads = (long)gridDim.x * gridDim.y * blockDim.x * blockDim.y;
+    const long t0 = ((long)blockIdx.y * gridDim.x + blockIdx.x) * (blockDim.x * blockDim.y) +
+                    threadIdx.y * blockDim.x + threadIdx.x;
+    for (long t = t0; t < 2 * (lr + tb + fb); t += nthreads) {
+        long q = t;
+        int face;
+        if (q < 2 * lr) face = (int)(q / lr), q %= lr;
+        else if ((q -= 2 * lr) < 2 * tb) face = 2 + (int)(q / tb), q %= tb;
+        else q -= 2 * tb, face = 4 + (int)(q / fb), q %= fb;
+        const int d = (int)(q % depth);
+        q /= depth;
+        if (face < 2) {
+            const int jj = hd + (int)(q % ny), ii = hd + (int)(q / ny);
+            const long base = (long)ii * xy + (long)jj * x;
+            if (face == 0 && fc.l) dst[base + (hd - 1 - d)] = val(base + (hd + d));
+            if (face == 1 && fc.r) dst[base + (x - hd + d)] = val(base + (x - hd - 1 - d));
+        } else if (face < 4) {
+            const int kk = hd + (int)(q % nx), ii = hd + (int)(q / nx);
+            const long base = (long)ii * xy + kk;
+            if (face == 2 && fc.b) dst[base + (long)(hd - 1 - d) * x] = val(base + (long)(hd + d) * x);
+            if (face == 3 && fc.t) dst[base + (long)(y - hd + d) * x] = val(base + (long)(y - hd - 1 - d) * x);
+        } else {
+            const int kk = hd + (int)(q % nx), jj = hd + (int)(q / nx);
+            const long base = (long)jj * x + kk;
+            if (face == 4 && fc.k) dst[base + (long)(hd - 1 - d) * xy] = val(base + (long)(hd + d) * xy);
+            if (face == 5 && fc.f) dst[base + (long)(z - hd + d) * xy] = val(base + (long)(z - hd - 1 - d) * xy);
+        }
+    }
+}
+
+// Fused stencil walker: like walk() but with x-neighbours from warp shuffles,
+// clamped lanes, and no halo stores. body(i, centre, smvp, active).
+template <bool REFLECT, typename Cur, typename Body>
+__device__ __forceinline__ void walkc(const Geo& g, const Faces& fc, const PencilC& s,
+                                      const double* __restrict__ raw, const double* __restrict__ kx,
+                                      const double* __restrict__ ky, const double* __restrict__ kz, Cur cur, Body body)
+{
+    const int x = g.x;
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * x + (long)s.i0 * xy;
+    double c = cur(i);
+    double bk = (s.i0 == g.hd) ? ((REFLECT && fc.k) ? c : raw[i - xy]) : cur(i - xy);
+    double kzc = kz[i];
+    TL3D_PRAGMA_UNROLL(TL3D_UNROLL)
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+        const bool at_f = ii == g.z - g.hd - 1;
+        const double fr = at_f ? ((REFLECT && fc.f) ? c : raw[i + xy]) : cur(i + xy);
+        const double kxc = kx[i];
+        double l = __shfl_up_sync(kFull3, c, 1);
+        double r = __shfl_down_sync(kFull3, c, 1);
+        double kxr = __shfl_down_sync(kFull3, kxc, 1);
+        if (s.at_l) l = (REFLECT && fc.l) ? c : raw[i - 1];
+        else if (s.lane == 0) l = cur(i - 1);
+        if (s.at_r) r = (REFLECT && fc.r) ? c : raw[i + 1];
+        else if (s.lane == 31) r = cur(i + 1);
+        if (s.at_r || s.lane == 31) kxr = kx[i + 1];
+        const double d = s.at_b ? ((REFLECT && fc.b) ? c : raw[i - x]) : cur(i - x);
+        const double u = s.at_t ? ((REFLECT && fc.t) ? c : raw[i + x]) : cur(i + x);
+        const double kzf = kz[i + xy];
+        const double v = smvp(kxc, kxr, ky[i], ky[i + x], kzc, kzf, c, l, r, d, u, bk, fr);
+        body(ii, i, c, v);
+        bk = c;
+        c = fr;
+        kzc = kzf;
+    }
+}
 
 __device__ __forceinline__ void reflect_store(double* f, const Geo& g, const Faces& fc, int depth, int k, int j,
                                              int i, double v)
@@ -125,37 +235,44 @@ __device__ __forceinline__ void walk(const Geo& g, const Faces& fc, const Pencil
 // ------------------------------------------------------ CG (cg_solver.c) --
 
 // [p = beta p + r] ; depth-1 reflective halo of p ; w = A p ; pw = sum(w p)
-// (3d/c_kernels/omp3/cg_solver.c:105-193).
+// (3d/c_kernels/omp3/cg_solver.c:105-193). Grid: interior blocks plus one
+// z-plane of halo-duty blocks (the reflected halo of p_out, and the pending
+// halo of u when u_halo is given; u is read-only here).
 template <bool FUSE_P, bool REFLECT, typename Finish>
-static __global__ void __launch_bounds__(NT) k3_cg_w(Geo g, Faces fc, Scalar beta, const double* __restrict__ p_in,
-                                                    double* __restrict__ p_out, const double* __restrict__ r,
-                                                    double* __restrict__ w, const double* __restrict__ kx,
-                                                    const double* __restrict__ ky, const double* __restrict__ kz,
-                                                    ReduceSlots rs, const int* __restrict__ done, Finish fin)
+static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_w(Geo g, Faces fc, Scalar beta,
+                                                               const double* __restrict__ p_in, double* p_out,
+                                                               const double* __restrict__ r, double* __restrict__ w,
+                                                               const double* __restrict__ kx,
+                                                               const double* __restrict__ ky,
+                                                               const double* __restrict__ kz, double* u_halo, int uhd,
+                                                               ReduceSlots rs, const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
-    Pencil s(g);
     double acc[1] = {0.0};
-    if (s.active) {
-        const double bt = FUSE_P ? beta.get() : 0.0;
-        auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
-        walk<REFLECT>(g, fc, s, p_in, kx, ky, kz, cur, [&](int ii, long i, double c, double v) {
-            w[i] = v;
-            acc[0] += v * c;
-            if (FUSE_P) p_out[i] = c;
-            if (REFLECT) reflect_store(p_out, g, fc, 1, s.k, s.j, ii, c);
+    const double bt = FUSE_P ? beta.get() : 0.0;
+    auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
+    if (blockIdx.z + 1 < gridDim.z) {
+        const PencilC s(g);
+        walkc<REFLECT>(g, fc, s, p_in, kx, ky, kz, cur, [&](int, long i, double c, double v) {
+            if (s.active) {
+                w[i] = v;
+                acc[0] += v * c;
+                if (FUSE_P) p_out[i] = c;
+            }
         });
+    } else {
+        if (REFLECT) halo_duty3(g, fc, 1, p_out, cur);
+        if (u_halo) halo_duty3(g, fc, uhd, u_halo, [&](long idx) { return u_halo[idx]; });
     }
     tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
 }
 
-// u += alpha p ; r -= alpha w ; rrn = sum(r r), after writing the pending
-// halo of u from its old values (HALO_U).
-template <bool HALO_U, typename Finish>
-static __global__ void __launch_bounds__(NT) k3_cg_ur(Geo g, Faces fc, int udepth, Scalar alpha, double* __restrict__ u,
-                                                     const double* __restrict__ p, double* __restrict__ r,
-                                                     const double* __restrict__ w, ReduceSlots rs,
-                                                     const int* __restrict__ done, Finish fin)
+// u += alpha p ; r -= alpha w ; rrn = sum(r r)  (cg_solver.c:134-160)
+template <typename Finish>
+static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_ur(Geo g, Scalar alpha, double* __restrict__ u,
+                                                                const double* __restrict__ p, double* __restrict__ r,
+                                                                const double* __restrict__ w, ReduceSlots rs,
+                                                                const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
     Pencil s(g);
@@ -164,10 +281,9 @@ static __global__ void __launch_bounds__(NT) k3_cg_ur(Geo g, Faces fc, int udept
         const double a = alpha.get();
         const long xy = g.xy();
         long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+        TL3D_PRAGMA_UNROLL(TL3D_UNROLL)
         for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
-            const double uo = u[i];
-            if (HALO_U) reflect_store(u, g, fc, udepth, s.k, s.j, ii, uo);
-            u[i] = uo + a * p[i];
+            u[i] += a * p[i];
             const double rn = r[i] - a * w[i];
             r[i] = rn;
             acc[0] += rn * rn;
@@ -196,38 +312,45 @@ static __global__ void __launch_bounds__(NT) k3_cg_close(Geo g, Faces fc, Scalar
 
 // Chebyshev trip (3d/c_kernels/omp3/cheby_solver.c:62-99) with the previous
 // trip's u += p folded in (ADD), or the init sweep (INIT: p = r / theta).
+// With REFLECT the halo-duty z-plane writes the reflected halo of u_n.
 template <bool ADD, bool REFLECT, bool INIT, typename Finish>
-static __global__ void __launch_bounds__(NT) k3_cheby_trip(Geo g, Faces fc, ChebyCoef coef, double theta,
-                                                          int write_wr_always, const double* __restrict__ u_in,
-                                                          const double* __restrict__ p_in, double* __restrict__ u_out,
-                                                          double* __restrict__ p_out, const double* __restrict__ u0,
-                                                          double* __restrict__ w, double* __restrict__ r,
-                                                          const double* __restrict__ kx, const double* __restrict__ ky,
-                                                          const double* __restrict__ kz, ReduceSlots rs,
-                                                          const int* __restrict__ done, Finish fin, DevParams prm)
+static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cheby_trip(Geo g, Faces fc, ChebyCoef coef, double theta,
+                                                                     int write_wr_always,
+                                                                     const double* __restrict__ u_in,
+                                                                     const double* __restrict__ p_in, double* u_out,
+                                                                     double* p_out, const double* __restrict__ u0,
+                                                                     double* __restrict__ w, double* __restrict__ r,
+                                                                     const double* __restrict__ kx,
+                                                                     const double* __restrict__ ky,
+                                                                     const double* __restrict__ kz, ReduceSlots rs,
+                                                                     const int* __restrict__ done, Finish fin,
+                                                                     DevParams prm)
 {
     if (gate_closed(done)) return;
-    Pencil s(g);
     double acc[1] = {0.0};
     double a = 0.0, b = 0.0;
     if (!INIT) coef.get(a, b);
     const bool wr = INIT || write_wr_always || !coef.st ||
                     (coef.st->nch >= coef.st->est && ((coef.st->trip + 1) % 10) == 0) ||
                     (coef.st->trip + 1 >= prm.max_iters);
-    if (s.active) {
-        auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
-        walk<REFLECT>(g, fc, s, u_in, kx, ky, kz, cur, [&](int ii, long i, double c, double v) {
-            const double rr = u0[i] - v;
-            const double pn = INIT ? rr / theta : a * p_in[i] + b * rr;
-            if (wr) {
-                w[i] = v;
-                r[i] = rr;
+    auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
+    if (blockIdx.z + 1 < gridDim.z) {
+        const PencilC s(g);
+        walkc<REFLECT>(g, fc, s, u_in, kx, ky, kz, cur, [&](int, long i, double c, double v) {
+            if (s.active) {
+                const double rr = u0[i] - v;
+                const double pn = INIT ? rr / theta : a * p_in[i] + b * rr;
+                if (wr) {
+                    w[i] = v;
+                    r[i] = rr;
+                }
+                acc[0] += rr * rr;
+                p_out[i] = pn;
+                if (ADD) u_out[i] = c;
             }
-            acc[0] += rr * rr;
-            p_out[i] = pn;
-            if (ADD) u_out[i] = c;
-            if (REFLECT) reflect_store(ADD ? u_out : const_cast<double*>(u_in), g, fc, 1, s.k, s.j, ii, c);
         });
+    } else if (REFLECT) {
+        halo_duty3(g, fc, 1, ADD ? u_out : const_cast<double*>(u_in), cur);
     }
     tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
 }
@@ -250,34 +373,42 @@ static __global__ void __launch_bounds__(NT) k3_add_p(Geo g, Faces fc, double* _
 }
 
 // PPCG inner step (3d/c_kernels/omp3/ppcg_solver.c:29-73) with the previous
-// step's sd update folded in (FOLD 1: sd = r/theta; FOLD 2: a sd + b r).
+// step's sd update folded in (FOLD 1: sd = r/theta; FOLD 2: a sd + b r); the
+// halo-duty z-plane writes the reflected halo of sd_out.
 template <int FOLD, bool NORM, typename Finish>
-static __global__ void __launch_bounds__(NT) k3_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef, int pp_prev,
-                                                         const double* __restrict__ sd_in, double* __restrict__ sd_out,
-                                                         const double* __restrict__ r_in, double* __restrict__ r_out,
-                                                         double* __restrict__ u, const double* __restrict__ kx,
-                                                         const double* __restrict__ ky, const double* __restrict__ kz,
-                                                         ReduceSlots rs, const int* __restrict__ done, Finish fin)
+static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef,
+                                                                    int pp_prev, const double* __restrict__ sd_in,
+                                                                    double* __restrict__ sd_out,
+                                                                    const double* __restrict__ r_in,
+                                                                    double* __restrict__ r_out,
+                                                                    double* __restrict__ u,
+                                                                    const double* __restrict__ kx,
+                                                                    const double* __restrict__ ky,
+                                                                    const double* __restrict__ kz, ReduceSlots rs,
+                                                                    const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
-    Pencil s(g);
     double acc[1] = {0.0};
     double a = 0.0, b = 0.0;
     if (FOLD == 2) coef.get(pp_prev, a, b);
-    if (s.active) {
-        auto cur = [&](long idx) {
-            if (FOLD == 0) return sd_in[idx];
-            if (FOLD == 1) return r_in[idx] / theta;
-            return a * sd_in[idx] + b * r_in[idx];
-        };
-        walk<true>(g, fc, s, sd_in, kx, ky, kz, cur, [&](int ii, long i, double c, double v) {
-            const double rn = r_in[i] - v;
-            r_out[i] = rn;
-            u[i] += c;
-            sd_out[i] = c;
-            reflect_store(sd_out, g, fc, 1, s.k, s.j, ii, c);
-            if (NORM) acc[0] += rn * rn;
+    auto cur = [&](long idx) {
+        if (FOLD == 0) return sd_in[idx];
+        if (FOLD == 1) return r_in[idx] / theta;
+        return a * sd_in[idx] + b * r_in[idx];
+    };
+    if (blockIdx.z + 1 < gridDim.z) {
+        const PencilC s(g);
+        walkc<true>(g, fc, s, sd_in, kx, ky, kz, cur, [&](int, long i, double c, double v) {
+            if (s.active) {
+                const double rn = r_in[i] - v;
+                r_out[i] = rn;
+                u[i] += c;
+                sd_out[i] = c;
+                if (NORM) acc[0] += rn * rn;
+            }
         });
+    } else {
+        halo_duty3(g, fc, 1, sd_out, cur);
     }
     if (NORM) tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
 }

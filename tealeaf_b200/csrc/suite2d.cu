@@ -206,7 +206,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     };
     s->table_len = (int)mi;
     // Reduction partials: one slot set per block of the largest reduction launch.
-    const dim3 gi = interior_grid(s->g), gf = full_grid(s->g);
+    const dim3 gi = fused_grid(s->g), gf = full_grid(s->g);
     const long blocks = std::max<long>((long)gi.x * gi.y, (long)gf.x * gf.y);
     s->partial_capacity = blocks * tl::kMaxSums;
 
@@ -364,8 +364,28 @@ void run_store_energy(Chunk* chunk, Settings* settings)
                             cudaMemcpyDeviceToDevice, s->stream));
 }
 
-// 2d/kernel_interface.h:30 (field_summary.c:8-45)
+// 2d/kernel_interface.h:30 (field_summary.c:8-45): the reference's serial
+// summation order, so the totals match its rounding.
 void run_field_summary(Chunk* chunk, Settings* settings, double* vol, double* mass, double* ie, double* temp)
+{
+    (void)settings;
+    TlSuite2D* s = ready(chunk);
+    if (!s) return;
+    TL_LAUNCH(s, "k_field_summary_ordered",
+              tl::k_field_summary_ordered<<<1, 32, 0, s->stream>>>(s->g.x, s->g.y, 1, s->g.hd, 0, chunk->volume,
+                                                                 chunk->density, chunk->energy0, chunk->u,
+                                                                 s->rs.out_dev, s->rs.out_host));
+    double o[4];
+    if (!fetch(s, 4, o)) return;
+    *vol += o[0];
+    *mass += o[1];
+    *ie += o[2];
+    *temp += o[3];
+}
+
+// New: the same four totals from a parallel tree reduction (one sweep at
+// full bandwidth; differs from the reference's serial order by rounding).
+void tl2d_field_summary_fast(Chunk* chunk, Settings* settings, double* vol, double* mass, double* ie, double* temp)
 {
     (void)settings;
     TlSuite2D* s = ready(chunk);
@@ -399,9 +419,10 @@ void run_cg_init(Chunk* chunk, Settings* settings, double rx, double ry, double*
     if (fetch(s, 1, &o)) *rro += o;
 }
 
-// 2d/kernel_interface.h:38 (cg.c:88-113). Absorbs a pending p update and a
-// pending depth-1 halo of p: one sweep reads old p and r, writes the new p
-// (to the second p buffer) with its reflected halo, w = A p and p.w.
+// 2d/kernel_interface.h:38 (cg.c:88-113). Absorbs a pending p update, a
+// pending depth-1 halo of p and a pending halo of u: one sweep reads old p
+// and r, writes the new p (to the second p buffer) with its reflected halo,
+// w = A p and p.w; the halo-duty block row writes the halos (u is read-only here).
 void run_cg_calc_w(Chunk* chunk, Settings* settings, double* pw)
 {
     (void)settings;
@@ -411,51 +432,42 @@ void run_cg_calc_w(Chunk* chunk, Settings* settings, double* pw)
     if (s->pend.halo[TL_FIELD_P] > 1) flush(s, chunk);
     const bool fuse = s->pend.calc_p;
     const bool refl = s->pend.halo[TL_FIELD_P] == 1;
+    const int ud = s->pend.halo[TL_FIELD_U];
+    double* u_halo = ud > 0 ? chunk->u : nullptr;
     const Faces fc = faces_of(chunk);
     const Scalar beta{s->pend.beta, nullptr};
-    const dim3 gr = interior_grid(s->g);
+    const dim3 gr = fused_grid(s->g);
     double* p_out = fuse ? s->alt[ALT_P] : chunk->p;
-    if (fuse && refl)
-        TL_LAUNCH(s, "k_cg_w_fused", k_cg_w_fused<true, true><<<gr, BX, 0, s->stream>>>(
-                      s->g, fc, beta, chunk->p, p_out, chunk->r, chunk->w, chunk->kx, chunk->ky, s->rs,
-                      nullptr, tl::NoFinish()));
-    else if (fuse)
-        TL_LAUNCH(s, "k_cg_w_fused", k_cg_w_fused<true, false><<<gr, BX, 0, s->stream>>>(
-                      s->g, fc, beta, chunk->p, p_out, chunk->r, chunk->w, chunk->kx, chunk->ky, s->rs,
-                      nullptr, tl::NoFinish()));
-    else if (refl)
-        TL_LAUNCH(s, "k_cg_w_fused", k_cg_w_fused<false, true><<<gr, BX, 0, s->stream>>>(
-                      s->g, fc, beta, chunk->p, p_out, chunk->r, chunk->w, chunk->kx, chunk->ky, s->rs,
-                      nullptr, tl::NoFinish()));
-    else
-        TL_LAUNCH(s, "k_cg_calc_w", k_cg_calc_w<<<gr, BX, 0, s->stream>>>(s->g, chunk->p, chunk->w, chunk->kx,
-                                                                          chunk->ky, s->rs));
+#define W2(F, R)                                                                                                    \
+    TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<F, R><<<gr, BX, 0, s->stream>>>(s->g, fc, beta, chunk->p, p_out,    \
+                                                                               chunk->r, chunk->w, chunk->kx,      \
+                                                                               chunk->ky, u_halo, ud, s->rs,       \
+                                                                               nullptr, tl::NoFinish())))
+    if (fuse && refl) W2(true, true);
+    else if (fuse) W2(true, false);
+    else if (refl) W2(false, true);
+    else W2(false, false);
+#undef W2
     if (fuse) swap_alt(s, chunk, ALT_P);
     s->pend.calc_p = false;
     s->pend.halo[TL_FIELD_P] = 0;
+    s->pend.halo[TL_FIELD_U] = 0;
     double o;
     if (fetch(s, 1, &o)) *pw += o;
 }
 
-// 2d/kernel_interface.h:40 (cg.c:116-143). Absorbs a pending halo of u (its
-// reflection is written from the values u holds before the update).
+// 2d/kernel_interface.h:40 (cg.c:116-143). A halo of u still pending here
+// (a host that did not call calc_w first) is run before u changes.
 void run_cg_calc_ur(Chunk* chunk, Settings* settings, double alpha, double* rrn)
 {
     (void)settings;
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
-    if (s->pend.calc_p) flush(s, chunk);
-    const int ud = s->pend.halo[TL_FIELD_U];
-    const Scalar a{alpha, nullptr};
-    if (ud > 0)
-        TL_LAUNCH(s, "k_cg_ur_fused", k_cg_ur_fused<true><<<interior_grid(s->g), BX, 0, s->stream>>>(
-                      s->g, faces_of(chunk), ud, a, chunk->u, chunk->p, chunk->r, chunk->w, s->rs, nullptr,
-                      tl::NoFinish()));
-    else
-        TL_LAUNCH(s, "k_cg_calc_ur", k_cg_calc_ur<<<interior_grid(s->g), BX, 0, s->stream>>>(
-                      s->g, alpha, chunk->u, chunk->p, chunk->r, chunk->w, s->rs));
-    s->pend.halo[TL_FIELD_U] = 0;
+    if (s->pend.calc_p || s->pend.halo[TL_FIELD_U]) flush(s, chunk);
+    TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<interior_grid(s->g), BX, 0, s->stream>>>(
+                                      s->g, Scalar{alpha, nullptr}, chunk->u, chunk->p, chunk->r, chunk->w, s->rs,
+                                      nullptr, tl::NoFinish())));
     double o;
     if (fetch(s, 1, &o)) *rrn += o;
 }

@@ -66,6 +66,13 @@ inline dim3 interior_grid(const Geo& g)
     return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, ROWS));
 }
 inline dim3 full_grid(const Geo& g) { return dim3(tl::ceil_div(g.x, 32), tl::ceil_div(g.y, FB / 32)); }
+// Interior grid plus the halo-duty block row of the fused sweeps.
+inline dim3 fused_grid(const Geo& g)
+{
+    dim3 d = interior_grid(g);
+    d.y += 1;
+    return d;
+}
 // Waits for the stream and returns the published sums.
 bool fetch(TlSuite2D* s, int n, double* out);
 // Runs every pending operation (p update, then halo updates).

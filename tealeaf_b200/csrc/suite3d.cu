@@ -197,7 +197,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
         {&s->d_cg_alphas, mi}, {&s->d_cg_betas, mi}, {&s->d_cheby_alphas, mi}, {&s->d_cheby_betas, mi},
     };
     s->table_len = (int)mi;
-    const dim3 gi = interior_grid(s->g), gf = full_grid(s->g);
+    const dim3 gi = fused_grid(s->g), gf = full_grid(s->g);
     const long blocks = std::max<long>((long)gi.x * gi.y * gi.z, (long)gf.x * gf.y * gf.z);
     s->partial_capacity = blocks * tl::kMaxSums;
     auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -347,8 +347,27 @@ void run_store_energy(Chunk* chunk, Settings* settings)
                             cudaMemcpyDeviceToDevice, s->stream));
 }
 
-// 3d/kernel_interface.h:24 (3d/c_kernels/omp3/field_summary.c:8-49)
+// 3d/kernel_interface.h:24 (3d/c_kernels/omp3/field_summary.c:8-49): the
+// reference's serial summation order.
 void run_field_summary(Chunk* chunk, Settings* settings, double* vol, double* mass, double* ie, double* temp)
+{
+    (void)settings;
+    TlSuite3D* s = ready(chunk);
+    if (!s) return;
+    TL3_LAUNCH(s, "k_field_summary_ordered",
+               tl::k_field_summary_ordered<<<1, 32, 0, s->stream>>>(s->g.x, s->g.y, s->g.z, s->g.hd, s->g.hd,
+                                                                  chunk->volume, chunk->density, chunk->energy0,
+                                                                  chunk->vec_u, s->rs.out_dev, s->rs.out_host));
+    double o[4];
+    if (!fetch(s, 4, o)) return;
+    *vol += o[0];
+    *mass += o[1];
+    *ie += o[2];
+    *temp += o[3];
+}
+
+// New: tree-reduced field summary (full bandwidth, different rounding).
+void tl3d_field_summary_fast(Chunk* chunk, Settings* settings, double* vol, double* mass, double* ie, double* temp)
 {
     (void)settings;
     TlSuite3D* s = ready(chunk);
@@ -383,7 +402,7 @@ void run_cg_solver_init(Chunk* chunk, Settings* settings, double rx, double ry, 
 }
 
 // 3d/kernel_interface.h:32 (cg_solver.c:105-131), absorbing a pending p
-// update and depth-1 halo of p.
+// update, a pending depth-1 halo of p and a pending halo of u.
 void run_cg_solver_calc_w(Chunk* chunk, Settings* settings, double* pw)
 {
     (void)settings;
@@ -393,15 +412,17 @@ void run_cg_solver_calc_w(Chunk* chunk, Settings* settings, double* pw)
     if (s->pend.halo[TL3_FIELD_P] > 1) flush(s, chunk);
     const bool fuse = s->pend.calc_p;
     const bool refl = s->pend.halo[TL3_FIELD_P] == 1;
+    const int ud = s->pend.halo[TL3_FIELD_U];
+    double* u_halo = ud > 0 ? chunk->vec_u : nullptr;
     const Faces fc = faces_of(chunk);
     const Scalar beta{s->pend.beta, nullptr};
-    const dim3 gr = interior_grid(s->g), bl = interior_block();
+    const dim3 gr = fused_grid(s->g), bl = interior_block();
     double* p_out = fuse ? s->alt[ALT3_P] : chunk->vec_p;
 #define W3(F, R)                                                                                                   \
     TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<F, R><<<gr, bl, 0, s->stream>>>(s->g, fc, beta, chunk->vec_p, p_out,         \
                                                                       chunk->vec_r, chunk->vec_w, chunk->vec_kx,   \
-                                                                      chunk->vec_ky, chunk->vec_kz, s->rs, nullptr, \
-                                                                      tl::NoFinish())))
+                                                                      chunk->vec_ky, chunk->vec_kz, u_halo, ud,    \
+                                                                      s->rs, nullptr, tl::NoFinish())))
     if (fuse && refl) W3(true, true);
     else if (fuse) W3(true, false);
     else if (refl) W3(false, true);
@@ -410,30 +431,23 @@ void run_cg_solver_calc_w(Chunk* chunk, Settings* settings, double* pw)
     if (fuse) swap_alt(s, chunk, ALT3_P);
     s->pend.calc_p = false;
     s->pend.halo[TL3_FIELD_P] = 0;
+    s->pend.halo[TL3_FIELD_U] = 0;
     double o;
     if (fetch(s, 1, &o)) *pw += o;
 }
 
-// 3d/kernel_interface.h:34 (cg_solver.c:134-160), absorbing a pending halo of u.
+// 3d/kernel_interface.h:34 (cg_solver.c:134-160); a halo of u still pending
+// here is run before u changes.
 void run_cg_solver_calc_ur(Chunk* chunk, Settings* settings, double alpha, double* rrn)
 {
     (void)settings;
     if (tl::failed()) return;
     TlSuite3D* s = suite_of(chunk);
     if (!s) return;
-    if (s->pend.calc_p) flush(s, chunk);
-    const int ud = s->pend.halo[TL3_FIELD_U];
-    const Scalar a{alpha, nullptr};
-    const dim3 gr = interior_grid(s->g), bl = interior_block();
-    if (ud > 0)
-        TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<true><<<gr, bl, 0, s->stream>>>(s->g, faces_of(chunk), ud, a, chunk->vec_u,
-                                                                          chunk->vec_p, chunk->vec_r, chunk->vec_w,
-                                                                          s->rs, nullptr, tl::NoFinish())));
-    else
-        TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<false><<<gr, bl, 0, s->stream>>>(s->g, faces_of(chunk), 0, a, chunk->vec_u,
-                                                                           chunk->vec_p, chunk->vec_r, chunk->vec_w,
-                                                                           s->rs, nullptr, tl::NoFinish())));
-    s->pend.halo[TL3_FIELD_U] = 0;
+    if (s->pend.calc_p || s->pend.halo[TL3_FIELD_U]) flush(s, chunk);
+    TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<interior_grid(s->g), interior_block(), 0, s->stream>>>(
+                                  s->g, Scalar{alpha, nullptr}, chunk->vec_u, chunk->vec_p, chunk->vec_r,
+                                  chunk->vec_w, s->rs, nullptr, tl::NoFinish())));
     double o;
     if (fetch(s, 1, &o)) *rrn += o;
 }
@@ -456,12 +470,12 @@ void run_cheby_solver_init(Chunk* chunk, Settings* settings)
     (void)settings;
     TlSuite3D* s = ready(chunk);
     if (!s) return;
-    const dim3 gr = interior_grid(s->g), bl = interior_block();
+    const dim3 gf = fused_grid(s->g), gr = interior_grid(s->g), bl = interior_block();
     const Faces none{0, 0, 0, 0, 0, 0};
     const tl::ChebyCoef coef{0.0, 0.0, nullptr, nullptr, nullptr};
     tl::DevParams prm{};
     TL3_LAUNCH(s, "k3_cheby_trip<init>",
-               (k3_cheby_trip<false, false, true><<<gr, bl, 0, s->stream>>>(
+               (k3_cheby_trip<false, false, true><<<gf, bl, 0, s->stream>>>(
                    s->g, none, coef, chunk->theta, 1, chunk->vec_u, chunk->vec_p, chunk->vec_u, chunk->vec_p,
                    chunk->vec_u0, chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs,
                    nullptr, tl::NoFinish(), prm)));
@@ -474,12 +488,12 @@ void run_cheby_solver_iterate(Chunk* chunk, Settings* settings, double alpha, do
     (void)settings;
     TlSuite3D* s = ready(chunk);
     if (!s) return;
-    const dim3 gr = interior_grid(s->g), bl = interior_block();
+    const dim3 gf = fused_grid(s->g), gr = interior_grid(s->g), bl = interior_block();
     const Faces none{0, 0, 0, 0, 0, 0};
     const tl::ChebyCoef coef{alpha, beta, nullptr, nullptr, nullptr};
     tl::DevParams prm{};
     TL3_LAUNCH(s, "k3_cheby_trip",
-               (k3_cheby_trip<false, false, false><<<gr, bl, 0, s->stream>>>(
+               (k3_cheby_trip<false, false, false><<<gf, bl, 0, s->stream>>>(
                    s->g, none, coef, 0.0, 1, chunk->vec_u, chunk->vec_p, chunk->vec_u, chunk->vec_p, chunk->vec_u0,
                    chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr,
                    tl::NoFinish(), prm)));

@@ -56,6 +56,13 @@ inline dim3 interior_grid(const Geo& g)
     return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, BY), tl::ceil_div(g.z - 2 * g.hd, ZR));
 }
 inline dim3 full_grid(const Geo& g) { return dim3(tl::ceil_div(g.x, FBX), tl::ceil_div(g.y, FBY), g.z); }
+// Interior grid plus the halo-duty z-plane of the fused sweeps.
+inline dim3 fused_grid(const Geo& g)
+{
+    dim3 d = interior_grid(g);
+    d.z += 1;
+    return d;
+}
 inline dim3 interior_block() { return dim3(BX, BY); }
 inline dim3 full_block() { return dim3(FBX, FBY); }
 bool fetch(TlSuite3D* s, int n, double* out);

@@ -469,8 +469,9 @@ class Host:
         return res
 
     # -- device-resident timestep (tl2d_solve_step) ----------------------------------
-    def solve_device(self, tt: int) -> StepResult:
-        """One timestep with the solver loop kept on the GPU (same results as solve())."""
+    def solve_device(self, tt: int, summary: bool = True) -> StepResult:
+        """One timestep with the solver loop kept on the GPU (same results as solve());
+        `summary` appends the field summary (vol, mass, ie, temp) to the result."""
         fn = getattr(self.lib, "tl%dd_solve_step" % self.dims)
         stats = abi.StepStats()
         fn(C.byref(self.chunk), C.byref(self.settings), tt, C.byref(stats))
@@ -483,7 +484,10 @@ class Host:
             res.iterations["Cheby"] = stats.cheby_iters
         elif s == PPCG_SOLVER:
             res.iterations["PPCG"] = stats.ppcg_iters
-        res.summary = self.field_summary()
+        elif s == JACOBI_SOLVER:
+            res.iterations = {"Jacobi": stats.jacobi_iters}
+        if summary:
+            res.summary = self.field_summary()
         return res
 
     def run_device(self, steps: Optional[int] = None) -> List[StepResult]:
