@@ -254,6 +254,9 @@ void tl2d_profile_enable(Chunk* chunk, int on);
 void tl2d_profile_reset(Chunk* chunk);
 int tl2d_profile_read(Chunk* chunk, int index, char* name, int name_len,
         long long* calls, double* ms);
+/* Kernel launches issued for this chunk since initialisation (counted
+ * whether or not the profile is enabled); -1 for an unknown chunk. */
+long long tl2d_launch_count(Chunk* chunk);
 
 /* Field ids for the host-buffer staging calls. */
 #define TL2D_DENSITY0 0

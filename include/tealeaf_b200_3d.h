@@ -249,6 +249,9 @@ void tl3d_profile_enable(Chunk* chunk, int on);
 void tl3d_profile_reset(Chunk* chunk);
 int tl3d_profile_read(Chunk* chunk, int index, char* name, int name_len,
         long long* calls, double* ms);
+/* Kernel launches issued for this chunk since initialisation (counted
+ * whether or not the profile is enabled); -1 for an unknown chunk. */
+long long tl3d_launch_count(Chunk* chunk);
 
 /* Field ids for the host-buffer staging calls (x*y*z values each). */
 #define TL3D_DENSITY0 0

@@ -174,6 +174,9 @@ def load(dims: int) -> C.CDLL:
     f = getattr(lib, pre + "profile_read")
     f.argtypes = [C.POINTER(chunk_t), _i, C.c_char_p, _i, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
     f.restype = _i
+    f = getattr(lib, pre + "launch_count")
+    f.argtypes = [C.POINTER(chunk_t)]
+    f.restype = C.c_longlong
     if hasattr(lib, pre + "calculate_2norm_noalloc"):
         f = getattr(lib, pre + "calculate_2norm_noalloc")
         f.argtypes = [_p, _i, _i, _i, _p, _p]

@@ -91,6 +91,7 @@ class Profiler {
 public:
     static constexpr int kMaxKernels = 64;
     bool on = false;
+    long long launches = 0;   // every launch, counted whether or not timing is on
     const char* names[kMaxKernels] = {nullptr};
     long calls[kMaxKernels] = {0};
     double ms[kMaxKernels] = {0.0};
@@ -108,6 +109,7 @@ public:
     }
     void begin(cudaStream_t st, const char* name)
     {
+        ++launches;
         if (!on) return;
         Pending p;
         p.id = id_of(name);

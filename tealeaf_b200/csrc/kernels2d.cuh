@@ -2,8 +2,9 @@
 // and driver2d.cu; every kernel has internal linkage in each includer).
 //
 // Kernel shapes: interior sweeps run one thread per column (BX = 128 columns
-// per block, one warp = 256 contiguous bytes per load) and walk ROWS rows down
-// the column, carrying the vertical neighbours of the stencil in registers,
+// per block, one warp = 256 contiguous bytes per load) and walk Geo::rows
+// rows (4-32, chosen per mesh so the grid fills the SMs) down the column,
+// carrying the vertical neighbours of the stencil in registers,
 // so each field is read from DRAM once per sweep. Reductions are fused into
 // the sweep that produces their operands and finished by one last-block pass
 // (common.cuh).
@@ -46,14 +47,12 @@ using tl::Scalar;
 #define TL2D_PRAGMA_UNROLL(n) _Pragma(TL2D_STR(unroll n))
 
 constexpr int BX = 128;   // threads (columns) per block of an interior sweep
-#ifndef TL2D_ROWS
-#define TL2D_ROWS 8
-#endif
-constexpr int ROWS = TL2D_ROWS;   // rows per thread of an interior sweep
+constexpr int ROWS = 8;   // default rows per thread of an interior sweep (Geo::rows)
 constexpr int FB = 256;   // threads per block of full-array kernels
 
 struct Geo {
     int x, y, hd;
+    int rows = ROWS;   // rows per thread of every interior sweep (chosen per chunk)
 };
 
 // ----------------------------------------------------------------- kernels
@@ -87,8 +86,8 @@ struct Strip {
     __device__ Strip(const Geo& g)
     {
         k = g.hd + blockIdx.x * BX + threadIdx.x;
-        j0 = g.hd + blockIdx.y * ROWS;
-        j1 = min(j0 + ROWS, g.y - g.hd);
+        j0 = g.hd + blockIdx.y * g.rows;
+        j1 = min(j0 + g.rows, g.y - g.hd);
         active = k < g.x - g.hd;
     }
 };
@@ -626,8 +625,8 @@ struct StripC {
         k = g.hd + blockIdx.x * BX + threadIdx.x;
         active = k < g.x - g.hd;
         kk = active ? k : g.x - g.hd - 1;
-        j0 = g.hd + blockIdx.y * ROWS;
-        j1 = min(j0 + ROWS, g.y - g.hd);
+        j0 = g.hd + blockIdx.y * g.rows;
+        j1 = min(j0 + g.rows, g.y - g.hd);
         lane = threadIdx.x & 31;
         at_l = kk == g.hd;
         at_r = kk == g.x - g.hd - 1;

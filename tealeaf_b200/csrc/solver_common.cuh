@@ -191,66 +191,86 @@ struct FinPpcgNorm {       // beta = rrn / rro ; error = rro = rrn  (ppcg_driver
 };
 
 // Field summary in the reference's summation order (2d field_summary.c:8-45,
-// 3d field_summary.c:8-49: one serial loop, x fastest, then y, then z). The
-// per-cell products are formed by all 32 lanes at once; the four running sums
-// are then advanced cell by cell in exactly the reference's order, so vol,
-// mass and ie come out bit-identical to the reference's, and temp differs
-// only by the solution itself. One warp; about 5 ns per cell. For 2D pass
-// z = 1, hdz = 0.
-static __global__ void __launch_bounds__(32) k_field_summary_ordered(int x, int y, int z, int hd, int hdz,
-                                                                    const double* __restrict__ volume,
-                                                                    const double* __restrict__ density,
-                                                                    const double* __restrict__ energy0,
-                                                                    const double* __restrict__ u,
-                                                                    double* out_dev, double* out_host)
+// 3d field_summary.c:8-49: one serial loop, x fastest, then y, then z), so
+// vol, mass and ie come out bit-identical to the reference's and temp
+// differs only by the solution itself. A serial sum cannot be reassociated,
+// so each of the four sums is one dependent chain of adds: warp w < 4 (lane
+// 0) advances sum w through a shared-memory tile of per-cell terms while
+// the producer warps form the next tile's terms (volume, volume * density,
+// mass * energy0, mass * u) from coalesced loads. One block; the chains'
+// add latency bounds it (a few ns per cell). For 2D pass z = 1, hdz = 0.
+constexpr int kSumTile = 1024;              // cells per tile
+constexpr int kSumProducers = 256;          // producer threads (8 warps)
+constexpr int kSumThreads = 128 + kSumProducers;
+constexpr size_t kSumSmem = 2 * 4 * kSumTile * sizeof(double);
+
+static __global__ void __launch_bounds__(kSumThreads) k_field_summary_ordered(int x, int y, int z, int hd, int hdz,
+                                                                             const double* __restrict__ volume,
+                                                                             const double* __restrict__ density,
+                                                                             const double* __restrict__ energy0,
+                                                                             const double* __restrict__ u,
+                                                                             double* out_dev, double* out_host)
 {
-    const int lane = threadIdx.x;
+    extern __shared__ double terms[];   // [2 buffers][4 sums][kSumTile]
+    const int nx = x - 2 * hd, ny = y - 2 * hd, nz = z - 2 * hdz;
+    const long n = (long)nx * ny * nz;
+    const long ntiles = (n + kSumTile - 1) / kSumTile;
     const long xy = (long)x * y;
-    double vol = 0.0, mass = 0.0, ie = 0.0, temp = 0.0;
-    for (int i = hdz; i < z - hdz; ++i) {
-        for (int j = hd; j < y - hd; ++j) {
-            const long row = (long)i * xy + (long)j * x;
-            for (int k0 = hd; k0 < x - hd; k0 += 32) {
-                const int k = k0 + lane;
-                double cv = 0.0, cm = 0.0, te = 0.0, tu = 0.0;
-                if (k < x - hd) {
-                    cv = volume[row + k];
-                    cm = cv * density[row + k];
-                    te = cm * energy0[row + k];
-                    tu = cm * u[row + k];
-                }
-                const int cnt = min(32, x - hd - k0);
-                if (cnt == 32) {
-#pragma unroll
-                    for (int l = 0; l < 32; ++l) {
-                        vol += __shfl_sync(0xffffffffu, cv, l);
-                        mass += __shfl_sync(0xffffffffu, cm, l);
-                        ie += __shfl_sync(0xffffffffu, te, l);
-                        temp += __shfl_sync(0xffffffffu, tu, l);
-                    }
-                } else {
-                    for (int l = 0; l < cnt; ++l) {
-                        vol += __shfl_sync(0xffffffffu, cv, l);
-                        mass += __shfl_sync(0xffffffffu, cm, l);
-                        ie += __shfl_sync(0xffffffffu, te, l);
-                        temp += __shfl_sync(0xffffffffu, tu, l);
-                    }
-                }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pt = (int)threadIdx.x - 128;   // producer thread id (< 0: a chain warp)
+
+    auto produce = [&](long t) {
+        double* dst = terms + (t & 1) * 4 * kSumTile;
+        const long base = t * kSumTile;
+        for (int m = pt; m < kSumTile; m += kSumProducers) {
+            const long c = base + m;
+            if (c >= n) break;
+            const long r = c / nx;
+            const long idx = (long)(hdz + r / ny) * xy + (long)(hd + r % ny) * x + (hd + c % nx);
+            const double cv = volume[idx];
+            const double cm = cv * density[idx];
+            dst[m] = cv;
+            dst[kSumTile + m] = cm;
+            dst[2 * kSumTile + m] = cm * energy0[idx];
+            dst[3 * kSumTile + m] = cm * u[idx];
+        }
+    };
+
+    double acc = 0.0;
+    if (pt >= 0 && ntiles > 0) produce(0);
+    __syncthreads();
+    for (long t = 0; t < ntiles; ++t) {
+        if (pt >= 0) {
+            if (t + 1 < ntiles) produce(t + 1);
+        } else if (lane == 0) {
+            const double* src = terms + (t & 1) * 4 * kSumTile + warp * kSumTile;
+            const int cnt = (int)min((long)kSumTile, n - t * kSumTile);
+            if (cnt == kSumTile) {
+#pragma unroll 16
+                for (int m = 0; m < kSumTile; ++m) acc += src[m];
+            } else {
+                for (int m = 0; m < cnt; ++m) acc += src[m];
             }
         }
+        __syncthreads();
     }
-    if (lane == 0) {
-        out_dev[0] = vol;
-        out_dev[1] = mass;
-        out_dev[2] = ie;
-        out_dev[3] = temp;
-        if (out_host) {
-            out_host[0] = vol;
-            out_host[1] = mass;
-            out_host[2] = ie;
-            out_host[3] = temp;
-        }
+    if (pt < 0 && lane == 0) {
+        out_dev[warp] = acc;
+        if (out_host) out_host[warp] = acc;
     }
+}
+
+// Launches k_field_summary_ordered on `st`, raising its dynamic shared
+// memory limit on the current device first (a summary is rare; the call is
+// repeated so every device a process uses is covered).
+static inline void launch_field_summary_ordered(cudaStream_t st, int x, int y, int z, int hd, int hdz,
+                                                const double* volume, const double* density,
+                                                const double* energy0, const double* u, double* out_dev,
+                                                double* out_host)
+{
+    cudaFuncSetAttribute(k_field_summary_ordered, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
+    k_field_summary_ordered<<<1, kSumThreads, kSumSmem, st>>>(x, y, z, hd, hdz, volume, density, energy0, u,
+                                                              out_dev, out_host);
 }
 
 }  // namespace tl

@@ -162,6 +162,12 @@ void tl2d_profile_reset(Chunk* chunk)
     if (s) s->prof.reset();
 }
 
+long long tl2d_launch_count(Chunk* chunk)
+{
+    TlSuite2D* s = suite_of(chunk);
+    return s ? s->prof.launches : -1;
+}
+
 int tl2d_profile_read(Chunk* chunk, int index, char* name, int name_len, long long* calls, double* ms)
 {
     TlSuite2D* s = suite_of(chunk);
@@ -189,6 +195,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     TL_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     if (!TL_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) return;
     s->g = Geo{chunk->x, chunk->y, settings->halo_depth};
+    s->g.rows = choose_rows(chunk->x - 2 * settings->halo_depth, chunk->y - 2 * settings->halo_depth, s->sm_count);
     const long x = chunk->x, y = chunk->y, n = x * y;
     const long mi = settings->max_iters > 0 ? settings->max_iters : 1;
 
@@ -206,8 +213,8 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     };
     s->table_len = (int)mi;
     // Reduction partials: one slot set per block of the largest reduction launch.
-    const dim3 gi = fused_grid(s->g), gf = full_grid(s->g);
-    const long blocks = std::max<long>((long)gi.x * gi.y, (long)gf.x * gf.y);
+    const dim3 gh = fused_grid(s->g), gi = interior_grid(s->g), gf = full_grid(s->g);
+    const long blocks = std::max<long>({(long)gh.x * gh.y, (long)gi.x * gi.y, (long)gf.x * gf.y});
     s->partial_capacity = blocks * tl::kMaxSums;
 
     auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -372,9 +379,9 @@ void run_field_summary(Chunk* chunk, Settings* settings, double* vol, double* ma
     TlSuite2D* s = ready(chunk);
     if (!s) return;
     TL_LAUNCH(s, "k_field_summary_ordered",
-              tl::k_field_summary_ordered<<<1, 32, 0, s->stream>>>(s->g.x, s->g.y, 1, s->g.hd, 0, chunk->volume,
-                                                                 chunk->density, chunk->energy0, chunk->u,
-                                                                 s->rs.out_dev, s->rs.out_host));
+              tl::launch_field_summary_ordered(s->stream, s->g.x, s->g.y, 1, s->g.hd, 0, chunk->volume,
+                                               chunk->density, chunk->energy0, chunk->u, s->rs.out_dev,
+                                               s->rs.out_host));
     double o[4];
     if (!fetch(s, 4, o)) return;
     *vol += o[0];

@@ -7,6 +7,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 // Buffers that alternate between two slices (fused sweeps read the old values
 // at stencil neighbours while writing the new ones). The Chunk always points
 // at the current slice; the suite keeps the other.
@@ -61,9 +63,12 @@ struct TlSuite2D {
 namespace tl2d {
 
 TlSuite2D* suite_of(Chunk* chunk);
+// Interior sweeps: BX columns x g.rows rows per block. Every interior
+// reduction uses this one partition, so the kernel-interface path and the
+// device-resident driver add the same partial sums in the same order.
 inline dim3 interior_grid(const Geo& g)
 {
-    return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, ROWS));
+    return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, g.rows));
 }
 inline dim3 full_grid(const Geo& g) { return dim3(tl::ceil_div(g.x, 32), tl::ceil_div(g.y, FB / 32)); }
 // Interior grid plus the halo-duty block row of the fused sweeps.
@@ -72,6 +77,20 @@ inline dim3 fused_grid(const Geo& g)
     dim3 d = interior_grid(g);
     d.y += 1;
     return d;
+}
+// Rows per thread of the interior sweeps: the grid is cut into whole waves
+// of resident blocks (sm_count * TL2D_MINB) so no SM idles in a partial last
+// wave; the fewest waves whose strips are at most 64 rows (longer strips:
+// fewer boundary re-reads and reduction partials). At least 2 rows.
+inline int choose_rows(int nx, int ny, int sm_count)
+{
+    const long slots = (long)sm_count * TL2D_MINB;
+    const long bx = tl::ceil_div(nx, BX);
+    for (long waves = 1;; ++waves) {
+        const long strips = std::max(1L, waves * slots / bx);   // strips per column band
+        const int rows = std::max(2, tl::ceil_div(ny, strips));
+        if (rows <= 64) return rows;
+    }
 }
 // Waits for the stream and returns the published sums.
 bool fetch(TlSuite2D* s, int n, double* out);

@@ -150,6 +150,12 @@ void tl3d_profile_reset(Chunk* chunk)
     TlSuite3D* s = suite_of(chunk);
     if (s) s->prof.reset();
 }
+long long tl3d_launch_count(Chunk* chunk)
+{
+    TlSuite3D* s = suite_of(chunk);
+    return s ? s->prof.launches : -1;
+}
+
 int tl3d_profile_read(Chunk* chunk, int index, char* name, int name_len, long long* calls, double* ms)
 {
     TlSuite3D* s = suite_of(chunk);
@@ -355,9 +361,9 @@ void run_field_summary(Chunk* chunk, Settings* settings, double* vol, double* ma
     TlSuite3D* s = ready(chunk);
     if (!s) return;
     TL3_LAUNCH(s, "k_field_summary_ordered",
-               tl::k_field_summary_ordered<<<1, 32, 0, s->stream>>>(s->g.x, s->g.y, s->g.z, s->g.hd, s->g.hd,
-                                                                  chunk->volume, chunk->density, chunk->energy0,
-                                                                  chunk->vec_u, s->rs.out_dev, s->rs.out_host));
+               tl::launch_field_summary_ordered(s->stream, s->g.x, s->g.y, s->g.z, s->g.hd, s->g.hd, chunk->volume,
+                                                chunk->density, chunk->energy0, chunk->vec_u, s->rs.out_dev,
+                                                s->rs.out_host));
     double o[4];
     if (!fetch(s, 4, o)) return;
     *vol += o[0];
