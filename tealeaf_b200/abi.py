@@ -108,6 +108,12 @@ class StepStats(C.Structure):
                 ("exact_error", _d)]
 
 
+class RefineStats(C.Structure):
+    """TlRefineStats of the iterative-refinement timestep."""
+    _fields_ = [("iterations", _i), ("residual_updates", _i), ("converged", _i), ("pad", _i),
+                ("rel_residual", _d), ("device_ms", _d)]
+
+
 # Entry points shared by both suites (name -> extra argtypes after Chunk*, Settings*).
 _COMMON = {
     "run_set_chunk_data": [], "run_kernel_initialise": [],
@@ -185,6 +191,10 @@ def load(dims: int) -> C.CDLL:
         f = getattr(lib, pre + "solve_step")
         f.argtypes = head + [_i, C.POINTER(StepStats)]
         f.restype = None
+    if hasattr(lib, pre + "refine_solve_step"):
+        f = getattr(lib, pre + "refine_solve_step")
+        f.argtypes = head + [_i, _d, _i, C.POINTER(RefineStats)]
+        f.restype = _i
     if hasattr(lib, "diffuse_overload"):
         lib.diffuse_overload.argtypes = head
         lib.diffuse_overload.restype = None

@@ -262,6 +262,7 @@ void run_kernel_finalise(Chunk* chunk, Settings* settings)
     TlSuite2D* s = chunk->ext->suite;
     cudaStreamSynchronize(s->stream);
     cudaFree(s->slab);
+    if (s->mx_slab) cudaFree(s->mx_slab);
     cudaFreeHost(s->h_out);
     if (s->d_states) cudaFree(s->d_states);
     if (s->d_comm) cudaFree(s->d_comm);

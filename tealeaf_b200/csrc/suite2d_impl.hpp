@@ -49,6 +49,10 @@ struct TlSuite2D {
     double* d_cheby_alphas = nullptr;
     double* d_cheby_betas = nullptr;
     int table_len = 0;
+
+    // FP32 buffers of the iterative-refinement form (mixed2d.cu), on first use.
+    void* mx_slab = nullptr;
+    size_t mx_bytes = 0;
 };
 
 // Launch on the suite stream, bracketed by profiler events when enabled.
@@ -82,9 +86,10 @@ inline dim3 fused_grid(const Geo& g)
 // of resident blocks (sm_count * TL2D_MINB) so no SM idles in a partial last
 // wave; the fewest waves whose strips are at most 64 rows (longer strips:
 // fewer boundary re-reads and reduction partials). At least 2 rows.
-inline int choose_rows(int nx, int ny, int sm_count)
+// `min_blocks`: resident blocks per SM of the kernels the grid is for.
+inline int choose_rows(int nx, int ny, int sm_count, int min_blocks = TL2D_MINB)
 {
-    const long slots = (long)sm_count * TL2D_MINB;
+    const long slots = (long)sm_count * min_blocks;
     const long bx = tl::ceil_div(nx, BX);
     for (long waves = 1;; ++waves) {
         const long strips = std::max(1L, waves * slots / bx);   // strips per column band

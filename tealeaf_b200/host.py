@@ -52,6 +52,16 @@ class StepResult:
     est_iterations: int = 0
 
 
+@dataclass
+class RefineResult:
+    iterations: int = 0
+    residual_updates: int = 0
+    converged: bool = False
+    rel_residual: float = 0.0
+    device_ms: float = 0.0
+    summary: List[float] = field(default_factory=list)      # vol, mass, ie, temp
+
+
 class DriverError(RuntimeError):
     pass
 
@@ -486,6 +496,23 @@ class Host:
             res.iterations["PPCG"] = stats.ppcg_iters
         elif s == JACOBI_SOLVER:
             res.iterations = {"Jacobi": stats.jacobi_iters}
+        if summary:
+            res.summary = self.field_summary()
+        return res
+
+    # -- iterative-refinement timestep (tl2d_refine_solve_step) -------------------------
+    def refine_step(self, tt: int, rel_tol: float, precision: int, summary: bool = True) -> RefineResult:
+        """One timestep whose solve stops at ||u0 - A u|| / ||u0|| <= rel_tol (FP64
+        residual); precision 32 = FP32-stored CG with FP64 refinement, 64 = FP64 CG."""
+        if self.dims != 2:
+            raise DriverError("the refinement form is 2D")
+        st = abi.RefineStats()
+        rc = self.lib.tl2d_refine_solve_step(C.byref(self.chunk), C.byref(self.settings), tt, rel_tol,
+                                             precision, C.byref(st))
+        abi.check(self.lib, self.dims)
+        if rc:
+            raise DriverError("tl2d_refine_solve_step returned %d" % rc)
+        res = RefineResult(st.iterations, st.residual_updates, bool(st.converged), st.rel_residual, st.device_ms)
         if summary:
             res.summary = self.field_summary()
         return res

@@ -1,0 +1,77 @@
+"""Iterative-refinement timestep (tl2d_refine_solve_step) on the B200.
+
+Stated accuracy of the form: every timestep stops at a relative FP64
+residual ||u0 - A u||_2 / ||u0||_2 <= 1e-10 (checked on the residual the
+suite recomputes in FP64 after the solve), in both precisions. Against the
+FP64 oracle (the C restatement of the reference solve, run to r.r < 1e-28,
+i.e. far below the 1e-10 residual) the field summary of either form is held
+to: vol and mass exact (they do not depend on the solve), temp within
+TEMP_RTOL relative, step after step (the energy of each step feeds the next).
+"""
+import numpy as np
+import pytest
+
+from tealeaf_b200 import problems
+from tealeaf_b200.config import read_config
+from tealeaf_b200.host import DriverError, Host
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-10
+TEMP_RTOL = 1e-9   # temp vs the oracle's converged solve, after 3 timesteps
+
+
+def _problem(steps=3, eps=1e-15, n=(160, 120)):
+    return problems.seeded(2, n, 11, 16, 0, solver="cg", eps=eps, end_step=steps, name="refine_small")
+
+
+@pytest.fixture(scope="module")
+def oracle_steps(oracle_lib):
+    cfg, states = read_config(_problem(eps=1e-28).tea_in(), 2)
+    return oracle_lib.run(cfg, states)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_refine_reaches_residual_and_matches_oracle(precision, oracle_steps):
+    h = Host(_problem().tea_in(), 2)
+    try:
+        for tt, ref in enumerate(oracle_steps):
+            r = h.refine_step(tt, REL_TOL, precision)
+            assert r.converged, (precision, tt, r)
+            assert 0.0 < r.rel_residual <= REL_TOL
+            assert r.iterations > 0 and r.residual_updates >= 1
+            vol, mass, ie, temp = r.summary
+            assert vol == ref.summary[0] and mass == ref.summary[1]
+            assert ie == pytest.approx(ref.summary[2], rel=1e-14)
+            assert abs(temp / ref.summary[3] - 1.0) < TEMP_RTOL, (precision, tt, temp, ref.summary[3])
+    finally:
+        h.finalise()
+
+
+def test_fp32_and_fp64_forms_agree_and_fp32_updates_residual():
+    a, b = Host(_problem().tea_in(), 2), Host(_problem().tea_in(), 2)
+    try:
+        for tt in range(3):
+            r64 = a.refine_step(tt, REL_TOL, 64)
+            r32 = b.refine_step(tt, REL_TOL, 32)
+            # several FP64 residual replacements over ten decades of reduction
+            assert r32.residual_updates >= 5
+            # the FP32-stored CG needs at most a modest number of extra iterations
+            assert r32.iterations <= 1.5 * r64.iterations + 20, (r32.iterations, r64.iterations)
+            assert abs(r32.summary[3] / r64.summary[3] - 1.0) < TEMP_RTOL
+            ua, ub = a.download("u"), b.download("u")
+            hd = 2
+            ia, ib = ua[hd:-hd, hd:-hd], ub[hd:-hd, hd:-hd]
+            assert np.linalg.norm(ia - ib) / np.linalg.norm(ia) < 1e-8
+    finally:
+        a.finalise()
+        b.finalise()
+
+
+def test_refine_rejects_bad_arguments():
+    h = Host(_problem(steps=1).tea_in(), 2)
+    try:
+        with pytest.raises(Exception):
+            h.refine_step(0, REL_TOL, 16)
+    finally:
+        h.finalise()
