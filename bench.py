@@ -339,6 +339,8 @@ def bench_b200(args, rank, world, local_rank):
                     "the reference drivers (two synchronous reductions per CG iteration)"},
         "clocks": sampler.summary(),
     }
+    if world == 1 and args.refine_size > 0:
+        line["refine"] = bench_refine(args.refine_size, peak)
     if world == 1 and not args.no_cpu_baseline:
         try:
             threads = host_threads()
@@ -350,6 +352,34 @@ def bench_b200(args, rank, world, local_rank):
         except Exception as exc:  # baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     return line
+
+
+def bench_refine(n: int, peak: float) -> dict:
+    """The iterative-refinement form against FP64 on identical inputs: one
+    timestep of the seeded mixed-precision case (16 rectangles, seed 3), each
+    solved to the relative FP64 residual 1e-10 (tl2d_refine_solve_step)."""
+    from tealeaf_b200 import problems
+    from tealeaf_b200.host import Host
+    tol = 1e-10
+    prob = problems.mixed_2d(n, seed=3, steps=1)
+    out = {"workload": "mixed_2d_%d (16 rectangles, seed 3), timestep 1" % n, "rel_tol": tol,
+           "metric": "device time of the timestep to rel_tol (ms)"}
+    temps = {}
+    for prec in (64, 32):
+        h = Host(prob.tea_in(), dims=2)
+        try:
+            r = h.refine_step(0, tol, prec)
+        finally:
+            h.finalise()
+        bpc = 96 if prec == 64 else 48
+        gbs = bpc * n * n * r.iterations / (r.device_ms / 1000.0) / 1e9
+        out["fp%d" % prec] = {"ms": r.device_ms, "iterations": r.iterations,
+                              "residual_updates": r.residual_updates, "rel_residual": r.rel_residual,
+                              "converged": r.converged, "cg_gbs_effective": gbs, "cg_frac_of_peak": gbs / peak}
+        temps[prec] = r.summary[3]
+    out["time_ratio_fp32_over_fp64"] = out["fp32"]["ms"] / out["fp64"]["ms"]
+    out["temp_rel_diff_fp32_vs_fp64"] = temps[32] / temps[64] - 1.0
+    return out
 
 
 def traffic_per_launch(kernel: str, cells: int):
@@ -376,6 +406,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-cap", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--refine-size", type=int, default=8192,
+                    help="mesh of the FP32-refinement vs FP64 comparison (0: skip)")
     ap.add_argument("--driver", default="device", choices=["device", "run"])
     ap.add_argument("--e2e-kernel-interface", type=int, default=1)
     args = ap.parse_args()

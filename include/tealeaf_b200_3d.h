@@ -298,6 +298,41 @@ void tl3d_field_summary_fast(Chunk* chunk, Settings* settings,
 /* One timestep of solve() (3d/diffuse.c:21-81) on the device-resident path. */
 void tl3d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats3* stats);
 
+/* Adjoint of the implicit CG timestep: no counterpart in the reference.
+ * Backward of one timestep u = A(rho)^-1 u0: solves A lam = g_u with the
+ * forward CG sweeps (A is symmetric) to lam-residual <= rel_tol * ||g_u||, then
+ * accumulates into grad (dJ/drho) the face-coefficient term
+ * -sum_f dk_f/drho_c (lam_a - lam_b)(u_a - u_b). g_u, u (this step's forward
+ * solution), lam and grad are device arrays in the chunk layout. The chunk's
+ * p, r and w are overwritten. One chunk, six external faces, CG solver.
+ * Returns 0, or an error code (message from tl3d_get_error). */
+int tl3d_solve_step_backward(Chunk* chunk, Settings* settings, const double* g_u, const double* u,
+        double* lam, double* grad, double rel_tol, int* iterations);
+
+/* Statistics of tl3d_adjoint_gradient. */
+typedef struct TlAdjointStats
+{
+    double J;               /* the functional at the final step */
+    double device_ms;       /* device time of the whole call */
+    int forward_steps;      /* timesteps run forward, recomputation included */
+    int forward_iters;      /* CG iterations of those timesteps */
+    int adjoint_iters;      /* CG iterations of the adjoint solves */
+    int checkpoints;        /* energy checkpoints kept */
+} TlAdjointStats;
+
+/* Gradient of J = sum over the cells whose centre lies in the box
+ * {box[0] <= x <= box[1], box[2] <= y <= box[3], box[4] <= z <= box[5]} of
+ * volume * density * u after `steps` timesteps (the field summary's
+ * temperature restricted to the box), with respect to log(density) of every
+ * interior cell. Runs the timesteps forward from the chunk's current state
+ * (tl3d_solve_step, settings->eps as the forward stop), keeps the energy
+ * every `every` steps, then walks back segment by segment, recomputing each
+ * segment's forward solutions from its checkpoint, with the adjoint solves
+ * stopped at rel_tol. dj_dlogrho: host array of nx*ny*nz values, x fastest.
+ * The chunk ends in its state after the forward steps. */
+int tl3d_adjoint_gradient(Chunk* chunk, Settings* settings, int steps, int every, const double* box,
+        double rel_tol, double* dj_dlogrho, TlAdjointStats* stats);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

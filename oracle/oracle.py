@@ -97,8 +97,8 @@ class OracleLib:
         return getattr(self.lib, name)
 
     # -- whole runs --------------------------------------------------------
-    def run(self, config, states, want_energy: bool = False):
-        """Run initialise + end_step timesteps; config/states from tealeaf_b200.config."""
+    @staticmethod
+    def _settings(config):
         s = OSettings()
         s.dims = config.dims
         s.nx, s.ny = config.grid_x_cells, config.grid_y_cells
@@ -111,10 +111,43 @@ class OracleLib:
         s.coefficient, s.presteps, s.ppcg_inner_steps = config.coefficient, config.presteps, config.ppcg_inner_steps
         s.error_switch, s.check_result = int(config.error_switch), int(config.check_result)
         s.summary_frequency = config.summary_frequency
+        return s
+
+    @staticmethod
+    def _states(states):
         arr = (OState * len(states))()
         for n, st in enumerate(states):
             arr[n] = OState(st.density, st.energy, st.x_min, st.y_min, st.z_min, st.x_max,
                             st.y_max, st.z_max, st.radius, st.geometry)
+        return arr
+
+    # -- the CPU adjoint (3D CG timestep) ----------------------------------
+    def adjoint3d(self, config, states, box, adj_tol: float):
+        """(J, dJ/dlog(density) as an (nz, ny, nx) array) after end_step timesteps."""
+        s, arr = self._settings(config), self._states(states)
+        out = np.zeros((s.nz, s.ny, s.nx))
+        J = C.c_double()
+        b = (C.c_double * 6)(*box)
+        rc = self.lib.oracle_adjoint3d(C.byref(s), arr, len(states), b, C.c_double(adj_tol), C.byref(J), _ptr(out))
+        if rc != 0:
+            raise RuntimeError("oracle adjoint failed with code %d" % rc)
+        return J.value, out
+
+    def objective3d(self, config, states, box, cell: int = -1, log_scale: float = 0.0) -> float:
+        """J with density[cell] (interior index, x fastest) scaled by exp(log_scale)."""
+        s, arr = self._settings(config), self._states(states)
+        J = C.c_double()
+        b = (C.c_double * 6)(*box)
+        rc = self.lib.oracle_objective3d(C.byref(s), arr, len(states), b, C.c_long(cell), C.c_double(log_scale),
+                                         C.byref(J))
+        if rc != 0:
+            raise RuntimeError("oracle objective failed with code %d" % rc)
+        return J.value
+
+    def run(self, config, states, want_energy: bool = False):
+        """Run initialise + end_step timesteps; config/states from tealeaf_b200.config."""
+        s = self._settings(config)
+        arr = self._states(states)
         steps = (OStep * config.end_step)()
         hd = config.halo_depth
         if config.dims == 3:

@@ -880,14 +880,10 @@ static void oc_summary(OChunk* c, double* out)
     else o3_field_summary(c->x, c->y, c->z, c->hd, c->volume, c->density, c->energy0, c->u, out);
 }
 
-/* Runs initialise_application + end_step x solve() (2d/initialise.c:11-31,
- * 2d/diffuse.c:10-80). One chunk, every face external (NO_MPI, 1 rank).
- * steps_out[end_step]; energy_out (nullable) receives the final energy field
- * (x*y[*z] values). Returns 0, or a negative driver failure code. */
-int oracle_run(const OSettings* s, const OState* states, int num_states, OStep* steps_out, double* energy_out)
+/* initialise_application (2d/initialise.c:11-31) for one chunk with every
+ * face external (NO_MPI, 1 rank): allocation, mesh, states, halos, store_energy. */
+static void oc_setup(OChunk* c, const OSettings* s, const OState* states, int num_states, double* dxyz)
 {
-    OChunk cc;
-    OChunk* c = &cc;
     memset(c, 0, sizeof(*c));
     c->dims = s->dims;
     c->hd = s->halo_depth;
@@ -896,11 +892,9 @@ int oracle_run(const OSettings* s, const OState* states, int num_states, OStep* 
     c->z = s->dims == 3 ? s->nz + 2 * c->hd : 1;
     c->n = (long)c->x * c->y * c->z;
     for (int f = 0; f < 6; ++f) c->nb[f] = -1;
-    double* all[13];
-    for (int f = 0; f < 13; ++f) all[f] = zalloc(c->n);
-    c->density = all[0]; c->energy0 = all[1]; c->energy = all[2]; c->u = all[3]; c->u0 = all[4];
-    c->p = all[5]; c->r = all[6]; c->w = all[7]; c->kx = all[8]; c->ky = all[9]; c->kz = all[10];
-    c->sd = all[11]; c->volume = all[12];
+    c->density = zalloc(c->n); c->energy0 = zalloc(c->n); c->energy = zalloc(c->n); c->u = zalloc(c->n);
+    c->u0 = zalloc(c->n); c->p = zalloc(c->n); c->r = zalloc(c->n); c->w = zalloc(c->n); c->kx = zalloc(c->n);
+    c->ky = zalloc(c->n); c->kz = zalloc(c->n); c->sd = zalloc(c->n); c->volume = zalloc(c->n);
     c->xa = zalloc(c->n + c->y * c->z); c->ya = zalloc(c->n + c->x * c->z); c->za = zalloc(c->n + c->x * c->y);
     c->vx = zalloc(c->x + 1); c->vy = zalloc(c->y + 1); c->vz = zalloc(c->z + 1);
     c->cx = zalloc(c->x); c->cy = zalloc(c->y); c->cz = zalloc(c->z);
@@ -910,6 +904,7 @@ int oracle_run(const OSettings* s, const OState* states, int num_states, OStep* 
     double dx = (s->xmax - s->xmin) / (double)s->nx;
     double dy = (s->ymax - s->ymin) / (double)s->ny;
     double dz = s->dims == 3 ? (s->zmax - s->zmin) / (double)s->nz : 1.0;
+    dxyz[0] = dx; dxyz[1] = dy; dxyz[2] = dz;
     if (s->dims == 2) {
         o2_set_chunk_data(c->x, c->y, c->hd, s->xmin, s->ymin, dx, dy, c->vx, c->vy, c->cx, c->cy, c->volume, c->xa, c->ya);
         o2_set_chunk_state(c->x, c->y, c->vx, c->vy, c->cx, c->cy, c->density, c->energy0, c->u, num_states, states);
@@ -923,44 +918,230 @@ int oracle_run(const OSettings* s, const OState* states, int num_states, OStep* 
     c->flags[0] = c->flags[1] = c->flags[2] = true;
     oc_halo(c, 2);
     memcpy(c->energy, c->energy0, sizeof(double) * (size_t)c->n);   /* store_energy */
+}
 
+static void oc_free(OChunk* c)
+{
+    double* f[] = {c->density, c->energy0, c->energy, c->u, c->u0, c->p, c->r, c->w, c->kx, c->ky, c->kz,
+                   c->sd, c->volume, c->xa, c->ya, c->za, c->vx, c->vy, c->vz, c->cx, c->cy, c->cz,
+                   c->cg_alphas, c->cg_betas, c->cheby_alphas, c->cheby_betas};
+    for (size_t k = 0; k < sizeof(f) / sizeof(f[0]); ++k) free(f[k]);
+}
+
+/* One solve() (2d/diffuse.c:22-80): halos, the solver driver,
+ * solve_finished_driver, field summary. */
+static int oc_step(OChunk* c, const OSettings* s, const double* dxyz, OStep* st)
+{
+    memset(st, 0, sizeof(*st));
+    double dt = s->dt_init;
+    double rx = dt / (dxyz[0] * dxyz[0]), ry = dt / (dxyz[1] * dxyz[1]), rz = dt / (dxyz[2] * dxyz[2]);
+    oc_reset_flags(c);
+    c->flags[2] = c->flags[0] = true;
+    oc_halo(c, 2);
+    double error = 1e+10;
+    int rc;
+    switch (s->solver) {
+        case O_JACOBI: rc = oc_jacobi(c, s, rx, ry, rz, &error, st); break;
+        case O_CG: rc = oc_cg(c, s, rx, ry, rz, &error, st); break;
+        case O_CHEBY: rc = oc_cheby(c, s, rx, ry, rz, &error, st); break;
+        case O_PPCG: rc = oc_ppcg(c, s, rx, ry, rz, &error, st); break;
+        default: rc = -3;
+    }
+    if (rc) return rc;
+    st->error = error;
+    /* solve_finished_driver, 2d/drivers/solve_finished_driver.c:7-43 */
+    if (s->check_result) {
+        oc_residual(c);
+        st->exact_error = oc_2norm(c, c->r);
+    }
+    if (c->dims == 2) o2_finalise(c->x, c->y, c->hd, c->energy, c->density, c->u);
+    else o3_finalise(c->x, c->y, c->z, c->hd, c->energy, c->density, c->u);
+    c->flags[2] = true;
+    oc_halo(c, 1);
+    double out[4];
+    oc_summary(c, out);
+    st->vol = out[0]; st->mass = out[1]; st->ie = out[2]; st->temp = out[3];
+    return 0;
+}
+
+/* Runs initialise_application + end_step x solve() (2d/initialise.c:11-31,
+ * 2d/diffuse.c:10-80). One chunk, every face external (NO_MPI, 1 rank).
+ * steps_out[end_step]; energy_out (nullable) receives the final energy field
+ * (x*y[*z] values). Returns 0, or a negative driver failure code. */
+int oracle_run(const OSettings* s, const OState* states, int num_states, OStep* steps_out, double* energy_out)
+{
+    OChunk cc;
+    OChunk* c = &cc;
+    double dxyz[3];
+    oc_setup(c, s, states, num_states, dxyz);
+    int rc = 0;
+    for (int tt = 0; tt < s->end_step && rc == 0; ++tt) rc = oc_step(c, s, dxyz, &steps_out[tt]);
+    if (energy_out) memcpy(energy_out, c->energy, sizeof(double) * (size_t)c->n);
+    oc_free(c);
+    return rc;
+}
+
+/* ======================================================================== */
+/* FP64 CPU adjoint of the 3D CG timestep (the B200 suite's adjoint3d.cu     */
+/* restated serially; the reference has no adjoint). Test infrastructure.    */
+/* ======================================================================== */
+
+/* A lam = rhs from lam = 0 by CG (the operator of o3_cg_calc_w with the
+ * reflective depth-1 halo of p each trip), to r.r <= tol^2 rhs.rhs. */
+static int oa_solve(OChunk* c, const double* rhs, double* lam, double tol, int max_iters)
+{
+    const long n = c->n;
+    const int hd = c->hd;
+    double gg = 0.0;
+    for (int i3 = 0; i3 < c->z; ++i3)
+        for (int j = 0; j < c->y; ++j)
+            for (int k = 0; k < c->x; ++k) {
+                const long i = k + (long)j * c->x + (long)i3 * c->x * c->y;
+                const int in = k >= hd && k < c->x - hd && j >= hd && j < c->y - hd && i3 >= hd && i3 < c->z - hd;
+                const double v = in ? rhs[i] : 0.0;
+                c->r[i] = v;
+                c->p[i] = v;
+                gg += v * v;
+            }
+    memset(lam, 0, sizeof(double) * (size_t)n);
+    if (gg == 0.0) return 0;
+    double rro = gg;
+    int tt;
+    for (tt = 0; tt < max_iters; ++tt) {
+        o3_halo_field(c->x, c->y, c->z, hd, 1, c->nb, c->p);
+        const double pw = o3_cg_calc_w(c->x, c->y, c->z, hd, c->p, c->w, c->kx, c->ky, c->kz);
+        const double alpha = rro / pw;
+        const double rrn = o3_cg_calc_ur(c->x, c->y, c->z, hd, alpha, lam, c->p, c->r, c->w);
+        const double beta = rrn / rro;
+        o3_cg_calc_p(c->x, c->y, c->z, hd, beta, c->p, c->r);
+        rro = rrn;
+        if (rrn < tol * tol * gg) { ++tt; break; }
+    }
+    return tt;
+}
+
+/* grad_c -= dk/drho_c sum_{interior nb} r_axis (lam_c - lam_nb)(u_c - u_nb) */
+static void oa_face_grad(OChunk* c, int coefficient, double rx, double ry, double rz, const double* lam,
+                         const double* u, double* grad)
+{
+    const int x = c->x, y = c->y, z = c->z, hd = c->hd;
+    const long xy = (long)x * y;
+    for (int i3 = hd; i3 < z - hd; ++i3)
+        for (int j = hd; j < y - hd; ++j)
+            for (int k = hd; k < x - hd; ++k) {
+                const long i = k + (long)j * x + (long)i3 * xy;
+                const double rho = c->density[i];
+                const double w = coefficient == O_CONDUCTIVITY ? rho : 1.0 / rho;
+                const double dwdrho = coefficient == O_CONDUCTIVITY ? 1.0 : -w * w;
+                const double dk = -dwdrho / (2.0 * w * w);
+                double sx = 0.0, sy = 0.0, sz = 0.0;
+                if (k > hd) sx += (lam[i] - lam[i - 1]) * (u[i] - u[i - 1]);
+                if (k < x - hd - 1) sx += (lam[i] - lam[i + 1]) * (u[i] - u[i + 1]);
+                if (j > hd) sy += (lam[i] - lam[i - x]) * (u[i] - u[i - x]);
+                if (j < y - hd - 1) sy += (lam[i] - lam[i + x]) * (u[i] - u[i + x]);
+                if (i3 > hd) sz += (lam[i] - lam[i - xy]) * (u[i] - u[i - xy]);
+                if (i3 < z - hd - 1) sz += (lam[i] - lam[i + xy]) * (u[i] - u[i + xy]);
+                grad[i] -= dk * (rx * sx + ry * sy + rz * sz);
+            }
+}
+
+/* J = sum over cells whose centre is in box[6] of volume*density*u after
+ * end_step CG timesteps, and dJ/dlog(density) of every interior cell
+ * (grad_out: nx*ny*nz, x fastest). Every forward solution is kept (small
+ * meshes only). Returns 0 or a negative code. */
+int oracle_adjoint3d(const OSettings* s, const OState* states, int num_states, const double* box, double adj_tol,
+                     double* J_out, double* grad_out)
+{
+    if (s->dims != 3 || s->solver != O_CG) return -10;
+    OChunk cc;
+    OChunk* c = &cc;
+    double dxyz[3];
+    oc_setup(c, s, states, num_states, dxyz);
+    const long n = c->n;
+    const int N = s->end_step, hd = c->hd, x = c->x, y = c->y, z = c->z;
+    const long xy = (long)x * y;
+    double* e0 = zalloc(n);
+    memcpy(e0, c->energy, sizeof(double) * (size_t)n);
+    double* us = zalloc(n * (long)N);
+    int rc = 0;
+    for (int tt = 0; tt < N && rc == 0; ++tt) {
+        OStep st;
+        rc = oc_step(c, s, dxyz, &st);
+        memcpy(us + n * (long)tt, c->u, sizeof(double) * (size_t)n);
+    }
+    double* rhs = zalloc(n);
+    double* grad = zalloc(n);
+    double* lam = zalloc(n);
+    double J = 0.0;
+    const double* uN = us + n * (long)(N - 1);
+    for (int i3 = hd; i3 < z - hd; ++i3)
+        for (int j = hd; j < y - hd; ++j)
+            for (int k = hd; k < x - hd; ++k) {
+                const double cxv = s->xmin + dxyz[0] * (k - hd + 0.5);
+                const double cyv = s->ymin + dxyz[1] * (j - hd + 0.5);
+                const double czv = s->zmin + dxyz[2] * (i3 - hd + 0.5);
+                if (cxv < box[0] || cxv > box[1] || cyv < box[2] || cyv > box[3] || czv < box[4] || czv > box[5])
+                    continue;
+                const long i = k + (long)j * x + (long)i3 * xy;
+                rhs[i] = c->volume[i] * c->density[i];
+                grad[i] = c->volume[i] * uN[i];
+                J += rhs[i] * uN[i];
+            }
+    const double dt = s->dt_init;
+    const double rx = dt / (dxyz[0] * dxyz[0]), ry = dt / (dxyz[1] * dxyz[1]), rz = dt / (dxyz[2] * dxyz[2]);
+    for (int step = N; step >= 1 && rc == 0; --step) {
+        oa_solve(c, rhs, lam, adj_tol, s->max_iters);
+        oa_face_grad(c, s->coefficient, rx, ry, rz, lam, us + n * (long)(step - 1), grad);
+        memcpy(rhs, lam, sizeof(double) * (size_t)n);
+    }
+    const long nx = x - 2 * hd, ny = y - 2 * hd;
+    for (int i3 = hd; i3 < z - hd; ++i3)
+        for (int j = hd; j < y - hd; ++j)
+            for (int k = hd; k < x - hd; ++k) {
+                const long i = k + (long)j * x + (long)i3 * xy;
+                grad_out[(k - hd) + (j - hd) * nx + (i3 - hd) * nx * ny] = c->density[i] * (grad[i] + lam[i] * e0[i]);
+            }
+    *J_out = J;
+    free(e0); free(us); free(rhs); free(grad); free(lam);
+    oc_free(c);
+    return rc;
+}
+
+/* J of oracle_adjoint3d after end_step CG timesteps with density[cell] (an
+ * interior index, x fastest) multiplied by exp(log_scale) before the first
+ * step; for central differences on the CPU. */
+int oracle_objective3d(const OSettings* s, const OState* states, int num_states, const double* box, long cell,
+                       double log_scale, double* J_out)
+{
+    if (s->dims != 3) return -10;
+    OChunk cc;
+    OChunk* c = &cc;
+    double dxyz[3];
+    oc_setup(c, s, states, num_states, dxyz);
+    const int hd = c->hd, x = c->x, y = c->y, z = c->z;
+    const long xy = (long)x * y, nx = x - 2 * hd, ny = y - 2 * hd;
+    if (cell >= 0) {
+        const long k = cell % nx, j = (cell / nx) % ny, i3 = cell / (nx * ny);
+        c->density[(k + hd) + (j + hd) * x + (i3 + hd) * xy] *= exp(log_scale);
+    }
     int rc = 0;
     for (int tt = 0; tt < s->end_step && rc == 0; ++tt) {
-        OStep* st = &steps_out[tt];
-        memset(st, 0, sizeof(*st));
-        double dt = s->dt_init;
-        double rx = dt / (dx * dx), ry = dt / (dy * dy), rz = dt / (dz * dz);
-        oc_reset_flags(c);
-        c->flags[2] = c->flags[0] = true;
-        oc_halo(c, 2);
-        double error = 1e+10;
-        switch (s->solver) {
-            case O_JACOBI: rc = oc_jacobi(c, s, rx, ry, rz, &error, st); break;
-            case O_CG: rc = oc_cg(c, s, rx, ry, rz, &error, st); break;
-            case O_CHEBY: rc = oc_cheby(c, s, rx, ry, rz, &error, st); break;
-            case O_PPCG: rc = oc_ppcg(c, s, rx, ry, rz, &error, st); break;
-            default: rc = -3;
-        }
-        if (rc) break;
-        st->error = error;
-        /* solve_finished_driver, 2d/drivers/solve_finished_driver.c:7-43 */
-        if (s->check_result) {
-            oc_residual(c);
-            st->exact_error = oc_2norm(c, c->r);
-        }
-        if (c->dims == 2) o2_finalise(c->x, c->y, c->hd, c->energy, c->density, c->u);
-        else o3_finalise(c->x, c->y, c->z, c->hd, c->energy, c->density, c->u);
-        c->flags[2] = true;
-        oc_halo(c, 1);
-        double out[4];
-        oc_summary(c, out);
-        st->vol = out[0]; st->mass = out[1]; st->ie = out[2]; st->temp = out[3];
+        OStep st;
+        rc = oc_step(c, s, dxyz, &st);
     }
-    if (energy_out) memcpy(energy_out, c->energy, sizeof(double) * (size_t)c->n);
-
-    for (int f = 0; f < 13; ++f) free(all[f]);
-    free(c->xa); free(c->ya); free(c->za); free(c->vx); free(c->vy); free(c->vz);
-    free(c->cx); free(c->cy); free(c->cz);
-    free(c->cg_alphas); free(c->cg_betas); free(c->cheby_alphas); free(c->cheby_betas);
+    double J = 0.0;
+    for (int i3 = hd; i3 < z - hd; ++i3)
+        for (int j = hd; j < y - hd; ++j)
+            for (int k = hd; k < x - hd; ++k) {
+                const double cxv = s->xmin + dxyz[0] * (k - hd + 0.5);
+                const double cyv = s->ymin + dxyz[1] * (j - hd + 0.5);
+                const double czv = s->zmin + dxyz[2] * (i3 - hd + 0.5);
+                if (cxv < box[0] || cxv > box[1] || cyv < box[2] || cyv > box[3] || czv < box[4] || czv > box[5])
+                    continue;
+                const long i = k + (long)j * x + (long)i3 * xy;
+                J += c->volume[i] * c->density[i] * c->u[i];
+            }
+    *J_out = J;
+    oc_free(c);
     return rc;
 }

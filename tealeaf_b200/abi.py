@@ -114,6 +114,12 @@ class RefineStats(C.Structure):
                 ("rel_residual", _d), ("device_ms", _d)]
 
 
+class AdjointStats(C.Structure):
+    """TlAdjointStats of the 3D adjoint."""
+    _fields_ = [("J", _d), ("device_ms", _d), ("forward_steps", _i), ("forward_iters", _i),
+                ("adjoint_iters", _i), ("checkpoints", _i)]
+
+
 # Entry points shared by both suites (name -> extra argtypes after Chunk*, Settings*).
 _COMMON = {
     "run_set_chunk_data": [], "run_kernel_initialise": [],
@@ -194,6 +200,13 @@ def load(dims: int) -> C.CDLL:
     if hasattr(lib, pre + "refine_solve_step"):
         f = getattr(lib, pre + "refine_solve_step")
         f.argtypes = head + [_i, _d, _i, C.POINTER(RefineStats)]
+        f.restype = _i
+    if hasattr(lib, pre + "adjoint_gradient"):
+        f = getattr(lib, pre + "adjoint_gradient")
+        f.argtypes = head + [_i, _i, C.POINTER(_d), _d, _p, C.POINTER(AdjointStats)]
+        f.restype = _i
+        f = getattr(lib, pre + "solve_step_backward")
+        f.argtypes = head + [_p, _p, _p, _p, _d, C.POINTER(_i)]
         f.restype = _i
     if hasattr(lib, "diffuse_overload"):
         lib.diffuse_overload.argtypes = head

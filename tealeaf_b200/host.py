@@ -517,6 +517,23 @@ class Host:
             res.summary = self.field_summary()
         return res
 
+    # -- 3D adjoint (tl3d_adjoint_gradient) ----------------------------------------
+    def adjoint_gradient(self, steps: int, every: int, box, rel_tol: float):
+        """(J, dJ/dlog(density) as an (nz, ny, nx) array, stats) for J = sum over the
+        box of volume*density*u after `steps` timesteps from the current state."""
+        if self.dims != 3:
+            raise DriverError("the adjoint is 3D")
+        c = self.cfg
+        out = np.zeros((c.grid_z_cells, c.grid_y_cells, c.grid_x_cells))
+        st = abi.AdjointStats()
+        b = (C.c_double * 6)(*box)
+        rc = self.lib.tl3d_adjoint_gradient(C.byref(self.chunk), C.byref(self.settings), steps, every, b, rel_tol,
+                                            out.ctypes.data_as(C.c_void_p), C.byref(st))
+        abi.check(self.lib, self.dims)
+        if rc:
+            raise DriverError("tl3d_adjoint_gradient returned %d" % rc)
+        return st.J, out, st
+
     def run_device(self, steps: Optional[int] = None) -> List[StepResult]:
         n = self.cfg.end_step if steps is None else steps
         return [self.solve_device(tt) for tt in range(n)]
