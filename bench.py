@@ -382,6 +382,85 @@ def bench_refine(n: int, peak: float) -> dict:
     return out
 
 
+def bench_adjoint(args) -> dict:
+    """The 3D adjoint form: dJ/dlog(density) for J = sum over [6,9]^3 of
+    volume*density*u after 20 CG timesteps (checkpoints every 5) on the seeded
+    adjoint case, timed on the device; checked against central differences
+    (h = 1e-6) at `--fd-cells` seeded cells of the same mesh and against the
+    oracle's FP64 CPU adjoint at `--adjoint-cpu-size`^3."""
+    import numpy as np
+
+    from tealeaf_b200 import problems
+    from tealeaf_b200.config import read_config
+    from tealeaf_b200.host import Host
+    n, steps, every, tol, h = args.size, 20, 5, 1e-12, 1e-6
+    box = [6.0, 9.0, 6.0, 9.0, 6.0, 9.0]
+    prob = problems.adjoint_3d(n, seed=4, steps=steps)
+    host = Host(prob.tea_in(), dims=3)
+    hd = host.cfg.halo_depth
+    rho0, e0 = host.download("density"), host.download("energy")
+    J, g, st = host.adjoint_gradient(steps, every, box, tol)
+    line = {"metric": "adjoint_gradient_seconds", "value": st.device_ms / 1000.0, "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic (seeded tea.in generator, "
+            "adjoint_3d seed 4)",
+            "config": {"workload": "adjoint_3d_%d" % n, "cells": n ** 3, "steps": steps, "checkpoint_every": every,
+                       "box": box, "adjoint_rel_tol": tol, "forward_eps": prob.eps},
+            "J": J, "forward_steps": st.forward_steps, "forward_iters": st.forward_iters,
+            "adjoint_iters": st.adjoint_iters, "checkpoints": st.checkpoints,
+            "cg_cells_iterations_per_s": n ** 3 * (st.forward_iters + st.adjoint_iters) / (st.device_ms / 1000.0)}
+    gf = g.ravel()
+
+    def objective(cell, scale):
+        rho = rho0.copy()
+        k, j, i = cell % n, (cell // n) % n, cell // (n * n)
+        rho[i + hd, j + hd, k + hd] *= np.exp(scale)
+        host.upload("density", rho)
+        host.upload("energy", e0)
+        for tt in range(steps):
+            host.solve_device(tt, summary=False)
+        u, v, d = host.download("u"), host.download("volume"), host.download("density")
+        c = host.cfg
+        sl = (slice(hd, hd + n),) * 3
+        xs = c.grid_x_min + c.dx * (np.arange(n) + 0.5)
+        inb = (xs >= box[0]) & (xs <= box[1])
+        m = inb[:, None, None] & inb[None, :, None] & inb[None, None, :]
+        return float(np.sum((v[sl] * d[sl] * u[sl])[m]))
+
+    if args.fd_cells > 0:
+        rng = np.random.default_rng(4)
+        top = np.argsort(-np.abs(gf))[: max(1, gf.size // 100)]
+        cells = list(rng.choice(top, args.fd_cells // 2, replace=False)) + \
+            list(rng.integers(0, gf.size, args.fd_cells - args.fd_cells // 2))
+        noise = 8.0 * np.finfo(float).eps * abs(J) / (2 * h)
+        rows = []
+        for c in cells:
+            fd = (objective(int(c), h) - objective(int(c), -h)) / (2 * h)
+            rows.append((int(c), float(gf[c]), fd, abs(fd - gf[c]) / abs(gf[c]) if gf[c] else float("inf")))
+        strong = [r for r in rows if abs(r[1]) > 1e4 * noise]
+        line["fd_check"] = {"h": h, "cells": len(rows), "noise_floor_abs": noise,
+                            "max_rel_err_strong_cells": max((r[3] for r in strong), default=None),
+                            "strong_cells": len(strong),
+                            "max_abs_err_over_noise": max(abs(r[2] - r[1]) / noise for r in rows),
+                            "per_cell": [{"cell": r[0], "adjoint": r[1], "fd": r[2], "rel": r[3]} for r in rows]}
+    host.finalise()
+    if args.adjoint_cpu_size > 0:
+        m = args.adjoint_cpu_size
+        small = problems.adjoint_3d(m, seed=4, steps=steps)
+        hs = Host(small.tea_in(), dims=3)
+        try:
+            Jg, gg, _ = hs.adjoint_gradient(steps, every, box, tol)
+        finally:
+            hs.finalise()
+        from oracle.oracle import OracleLib  # checker only
+        cfg, states = read_config(small.tea_in(), 3)
+        t0 = time.time()
+        Jc, gc = OracleLib().adjoint3d(cfg, states, box, tol)
+        line["cpu_adjoint_check"] = {"mesh": m, "J_rel_diff": Jg / Jc - 1.0,
+                                     "grad_rel_norm_diff": float(np.linalg.norm(gg - gc) / np.linalg.norm(gc)),
+                                     "cpu_seconds": time.time() - t0}
+    return line
+
+
 def traffic_per_launch(kernel: str, cells: int):
     """DRAM bytes per launch from the committed ncu summary (scaled per cell), if any."""
     p = REPO / "profiles" / "ncu_traffic.json"
@@ -409,13 +488,21 @@ def main():
     ap.add_argument("--refine-size", type=int, default=8192,
                     help="mesh of the FP32-refinement vs FP64 comparison (0: skip)")
     ap.add_argument("--driver", default="device", choices=["device", "run"])
+    ap.add_argument("--workload", default="dropin", choices=["dropin", "adjoint"],
+                    help="dropin: the 2D FP64 drop-in line (default); adjoint: the 3D adjoint form")
+    ap.add_argument("--fd-cells", type=int, default=32)
+    ap.add_argument("--adjoint-cpu-size", type=int, default=64)
     ap.add_argument("--e2e-kernel-interface", type=int, default=1)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.workload == "adjoint":
+        if args.size == 4096:
+            args.size = 256
+        line = bench_adjoint(args) if rank == 0 else None
+    elif args.impl == "reference":
         line = bench_reference(args, rank, world)
     else:
         if world > 1:

@@ -348,6 +348,43 @@ typedef struct TlRefineStats
 int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, double rel_tol,
         int precision, TlRefineStats* stats);
 
+/* Batched timesteps: no counterpart in the reference. A batch holds `count`
+ * initialised chunks of any sizes (each one chunk with four external faces,
+ * with its own settings). tl2d_batch_step runs one solve() of every problem
+ * (halos, cg_init, u0 = u, the solve, finalise, energy halo) with the CG
+ * solve of all problems in one persistent cooperative kernel: FP32 vectors
+ * and coefficients, FP64 arithmetic, dot products and solution, FP64
+ * residual replacement, each problem stopped when its FP64 residual gives
+ * r.r < its settings->eps (the reference's 2D stop test). The whole timestep
+ * is captured once into a CUDA graph and replayed. */
+typedef struct TlBatch TlBatch;
+
+typedef struct TlBatchStats
+{
+    int problems;
+    int converged;          /* problems whose FP64 residual met eps */
+    int max_iterations;     /* CG iterations of the slowest problem */
+    int total_iterations;   /* summed over the problems */
+    int kernel_iterations;  /* iterations the persistent kernel ran */
+    int tile_rows;          /* tile height in use */
+    int grid_blocks;        /* persistent grid in use */
+    int graph;              /* 1 when the step ran as a CUDA graph replay */
+    double device_ms;       /* device time of the whole batched timestep */
+} TlBatchStats;
+
+/* tile_rows, grid_blocks: 0 for the defaults (16; the co-residency limit). */
+TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int tile_rows, int grid_blocks);
+void tl2d_batch_destroy(TlBatch* batch);
+/* Autotuner: times trial_iters iterations of the batch for each tile height
+ * in {2,4,8,16,32,64} and persistent grid of {2,4,6,8} blocks per SM and keeps
+ * the fastest (best_ms: its time). Leaves the energy fields unchanged. */
+int tl2d_batch_tune(TlBatch* batch, int trial_iters, double* best_ms);
+void tl2d_batch_config(TlBatch* batch, int* tile_rows, int* grid_blocks);
+int tl2d_batch_step(TlBatch* batch, TlBatchStats* stats);
+/* Per problem of the last step: CG iterations, FP64 r.r, converged flag
+ * (arrays of count; any may be NULL). */
+int tl2d_batch_results(TlBatch* batch, int* iterations, double* rr, int* converged);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

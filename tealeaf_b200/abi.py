@@ -120,6 +120,13 @@ class AdjointStats(C.Structure):
                 ("adjoint_iters", _i), ("checkpoints", _i)]
 
 
+class BatchStats(C.Structure):
+    """TlBatchStats of the batched timestep."""
+    _fields_ = [("problems", _i), ("converged", _i), ("max_iterations", _i), ("total_iterations", _i),
+                ("kernel_iterations", _i), ("tile_rows", _i), ("grid_blocks", _i), ("graph", _i),
+                ("device_ms", _d)]
+
+
 # Entry points shared by both suites (name -> extra argtypes after Chunk*, Settings*).
 _COMMON = {
     "run_set_chunk_data": [], "run_kernel_initialise": [],
@@ -201,6 +208,19 @@ def load(dims: int) -> C.CDLL:
         f = getattr(lib, pre + "refine_solve_step")
         f.argtypes = head + [_i, _d, _i, C.POINTER(RefineStats)]
         f.restype = _i
+    if hasattr(lib, pre + "batch_create"):
+        lib.tl2d_batch_create.argtypes = [C.POINTER(C.POINTER(chunk_t)), C.POINTER(C.POINTER(settings_t)), _i, _i, _i]
+        lib.tl2d_batch_create.restype = _p
+        lib.tl2d_batch_destroy.argtypes = [_p]
+        lib.tl2d_batch_destroy.restype = None
+        lib.tl2d_batch_tune.argtypes = [_p, _i, C.POINTER(_d)]
+        lib.tl2d_batch_tune.restype = _i
+        lib.tl2d_batch_config.argtypes = [_p, C.POINTER(_i), C.POINTER(_i)]
+        lib.tl2d_batch_config.restype = None
+        lib.tl2d_batch_step.argtypes = [_p, C.POINTER(BatchStats)]
+        lib.tl2d_batch_step.restype = _i
+        lib.tl2d_batch_results.argtypes = [_p, _p, _p, _p]
+        lib.tl2d_batch_results.restype = _i
     if hasattr(lib, pre + "adjoint_gradient"):
         f = getattr(lib, pre + "adjoint_gradient")
         f.argtypes = head + [_i, _i, C.POINTER(_d), _d, _p, C.POINTER(AdjointStats)]

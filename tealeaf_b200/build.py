@@ -33,7 +33,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibilit
 FMAD_SOURCES = set()   # filled as FP32 sources are added
 
 LIBS = {
-    "tealeaf_b200_2d": ["suite2d.cu", "driver2d.cu", "noalloc2d.cu", "mixed2d.cu"],
+    "tealeaf_b200_2d": ["suite2d.cu", "driver2d.cu", "noalloc2d.cu", "mixed2d.cu", "batch2d.cu"],
     "tealeaf_b200_3d": ["suite3d.cu", "driver3d.cu", "adjoint3d.cu"],
 }
 

@@ -1,0 +1,618 @@
+// batch2d.cu -- many independent 2D timesteps in one persistent launch.
+//
+// A batch holds `count` initialised chunks of different sizes (each with its
+// own tea.in settings). One batched timestep runs, for every problem, the
+// reference's solve() (2d/diffuse.c:22-80) with the CG solve replaced by the
+// refinement CG of refine2d.cuh (FP32 vectors and coefficients, FP64
+// arithmetic, dot products and solution, FP64 residual replacement) stopped
+// when the FP64 residual satisfies the problem's own r.r < eps:
+//
+//   per problem: energy/density halos, cg_init, u0 = u, T-layout setup
+//   ONE persistent cooperative kernel: the CG iterations of all problems
+//   per problem: energy = u / density, energy halo
+//
+// captured once into a CUDA graph and replayed for every timestep.
+//
+// The persistent kernel walks a global list of tiles (BX threads x 2 cells x
+// tile_rows rows, every tile of every problem) with a grid-stride loop, phase
+// by phase: w = A p, then u/r update, then (only when some problem asked for
+// one) the FP64 fold and residual. Phases are separated by a grid barrier
+// whose every wait is bounded (a timeout sets an error word and all blocks
+// return). Per-problem dot products are reduced deterministically: each tile
+// writes its block sum, and the block finishing a problem's last tile of the
+// phase sums that problem's tile partials in a fixed order and runs the CG
+// scalar update (alpha, beta, replacement and stop decisions) for it.
+// Problems that have converged drop out of the tile walk.
+//
+// tile_rows (and the persistent grid size) come from the autotuner
+// (tl2d_batch_tune): it times a few iterations of the real batch with each
+// candidate and keeps the fastest.
+#include "refine2d.cuh"
+#include "suite2d_impl.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+using namespace tl2d;
+using namespace tl2d::rf;
+
+namespace {
+
+constexpr int kBatchMinB = 8;                    // resident blocks per SM of the persistent kernel
+constexpr long long kBarrierLimit = 4000000000LL;   // SM clocks a barrier wait may take (~2 s)
+
+enum { BF_KX = 0, BF_KY, BF_P0, BF_P1, BF_W, BF_R, BF_XS, BF_COUNT };
+
+struct BProb {
+    Lay L;
+    int tx, ty;      // tiles per row / column
+    int tile0;       // first global tile of this problem
+    int gx, hd;      // FP64 chunk arrays: row length, halo depth
+    float* f[BF_COUNT];
+    double* u;
+    const double* u0;
+    const double* kx;
+    const double* ky;
+};
+
+struct BCtl {
+    unsigned count;   // grid barrier arrivals
+    unsigned gen;     // grid barrier generation
+    int err;          // a barrier wait timed out
+    int upd_iter;     // last iteration in which some problem asked for a residual replacement
+    int ndone;        // problems finished
+    int iters;        // iterations the kernel ran
+};
+
+__device__ bool grid_barrier(BCtl* c)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &c->gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&c->count, 1u) == gridDim.x - 1) {
+            atomicExch(&c->count, 0u);
+            __threadfence();
+            atomicAdd(&c->gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (*vgen == g) {
+                if (*(volatile int*)&c->err) break;
+                if (clock64() - t0 > kBarrierLimit) {
+                    atomicExch(&c->err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok = *(volatile int*)&c->err == 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Block sum of this thread's values; returns true in every thread of the
+// block that completed problem b's last tile of the phase, with the
+// problem's totals (fixed-order sum of its tile partials) in tot (thread 0).
+template <int N>
+__device__ bool tile_done(double (&v)[N], int t, const BProb& P, unsigned* ticket, double* partials,
+                          double (&tot)[N])
+{
+    __shared__ double smem[N][BX / tl::kWarp];
+    __shared__ bool last;
+    __syncthreads();
+    tl::block_sum<N, BX>(v, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < N; ++r) partials[(long)t * 2 + r] = v[r];
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == (unsigned)(P.tx * P.ty - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double s[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) s[r] = 0.0;
+    const int nt = P.tx * P.ty;
+    for (int k = threadIdx.x; k < nt; k += BX)
+#pragma unroll
+        for (int r = 0; r < N; ++r) s[r] += *(volatile double*)&partials[(long)(P.tile0 + k) * 2 + r];
+    __syncthreads();
+    tl::block_sum<N, BX>(s, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < N; ++r) tot[r] = s[r];
+        *ticket = 0u;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __restrict__ P, int np,
+                                                             const int* __restrict__ tile_prob, int ntiles,
+                                                             MxState* st, unsigned* tickets, double* partials,
+                                                             BCtl* ctl, int max_iters)
+{
+    for (int it = 0; it < max_iters; ++it) {
+        // phase 1: [p = beta p + r], w = A p, p.w
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const int b = tile_prob[t];
+            if (mx_idle(&st[b])) continue;
+            const BProb& Q = P[b];
+            const int lt = t - Q.tile0, tx = lt % Q.tx, ty = lt / Q.tx;
+            float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
+            float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
+            double v[1];
+            if (it == 0)
+                v[0] = rf_w_tile<float, false>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W], Q.f[BF_KX],
+                                               Q.f[BF_KY]);
+            else
+                v[0] = rf_w_tile<float, true>(Q.L, tx, ty, st[b].beta, pin, pout, Q.f[BF_R], Q.f[BF_W],
+                                              Q.f[BF_KX], Q.f[BF_KY]);
+            double tot[1];
+            if (tile_done<1>(v, t, Q, &tickets[b], partials, tot) && threadIdx.x == 0) FinMxW{&st[b]}(tot);
+        }
+        if (!grid_barrier(ctl)) return;
+        // phase 2: xs += alpha p, r -= alpha w, r.r; replacement requests
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const int b = tile_prob[t];
+            if (mx_idle(&st[b])) continue;
+            const BProb& Q = P[b];
+            const int lt = t - Q.tile0, tx = lt % Q.tx, ty = lt / Q.tx;
+            double v[1] = {rf_ur_tile<float>(Q.L, tx, ty, st[b].alpha, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0],
+                                             Q.f[BF_R], Q.f[BF_W])};
+            double tot[1];
+            if (tile_done<1>(v, t, Q, &tickets[b], partials, tot) && threadIdx.x == 0) {
+                FinMxUr{&st[b], nullptr}(tot);
+                if (st[b].upd) atomicExch(&ctl->upd_iter, it);
+            }
+        }
+        if (!grid_barrier(ctl)) return;
+        if (*(volatile int*)&ctl->upd_iter == it) {
+            // phase 3: fold the FP32 correction into the FP64 solution
+            for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+                const int b = tile_prob[t];
+                if (mx_no_update(&st[b])) continue;
+                const BProb& Q = P[b];
+                const int lt = t - Q.tile0;
+                rf_fold_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
+            }
+            if (!grid_barrier(ctl)) return;
+            // phase 4: FP64 residual replaces the FP32 one; stop tests
+            for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+                const int b = tile_prob[t];
+                if (mx_no_update(&st[b])) continue;
+                const BProb& Q = P[b];
+                const int lt = t - Q.tile0;
+                double v[2] = {0.0, 0.0};
+                rf_resid_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, Q.gx, Q.hd, Q.u, Q.u0, Q.kx, Q.ky, Q.f[BF_R], v);
+                double tot[2];
+                if (tile_done<2>(v, t, Q, &tickets[b], partials, tot) && threadIdx.x == 0) {
+                    FinMxRes{&st[b], nullptr}(tot);
+                    if (st[b].done) atomicAdd(&ctl->ndone, 1);
+                }
+            }
+            if (!grid_barrier(ctl)) return;
+        }
+        if (*(volatile int*)&ctl->ndone >= np) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = it + 1;
+            return;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = max_iters;
+}
+
+// Counts problems already converged by the setup (done before any iteration).
+__global__ void k_batch_count_done(const MxState* st, int np, BCtl* ctl)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int n = 0;
+    for (int b = 0; b < np; ++b) n += st[b].done ? 1 : 0;
+    ctl->count = 0;
+    ctl->gen = 0;
+    ctl->err = 0;
+    ctl->upd_iter = -1;
+    ctl->ndone = n;
+    ctl->iters = 0;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ batch --
+
+struct TlBatch {
+    int count = 0;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<Chunk*> chunks;
+    std::vector<Settings*> settings;
+    std::vector<TlSuite2D*> suites;
+    std::vector<Lay> lay;
+    void* slab = nullptr;            // FP32 arrays of every problem
+    size_t slab_bytes = 0;
+    std::vector<size_t> field_off;   // per problem: offset of its first FP32 array
+    std::vector<size_t> field_bytes; // per problem: bytes of one FP32 array
+    BProb* d_prob = nullptr;
+    int* d_tile_prob = nullptr;
+    MxState* d_st = nullptr;
+    unsigned* d_tickets = nullptr;
+    double* d_partials = nullptr;
+    BCtl* d_ctl = nullptr;
+    tl::ReduceSlots rs{};
+    long rs_capacity = 0;
+    DevState* d_scratch_state = nullptr;
+    int max_tiles = 0;               // capacity of the tile tables
+    int ntiles = 0;
+    int tile_rows = 0;
+    int grid_blocks = 0;
+    int max_grid = 0;
+    int max_iters = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graph_ok = false;
+};
+
+namespace {
+
+void batch_free(TlBatch* B)
+{
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    void* ptrs[] = {B->slab, B->d_prob, B->d_tile_prob, B->d_st, B->d_tickets, B->d_partials, B->d_ctl,
+                    B->rs.partials, B->rs.ticket, B->rs.out_dev, B->d_scratch_state};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (B->stream) cudaStreamDestroy(B->stream);
+    delete B;
+}
+
+// Lays out the tiles for tile_rows and uploads the problem and tile tables.
+bool batch_layout(TlBatch* B, int tile_rows)
+{
+    std::vector<BProb> P(B->count);
+    std::vector<int> tp;
+    for (int b = 0; b < B->count; ++b) {
+        Lay L = B->lay[b];
+        L.rows = tile_rows;
+        B->lay[b] = L;
+        const dim3 t = lay_tiles<float>(L);
+        BProb& Q = P[b];
+        Q.L = L;
+        Q.tx = (int)t.x;
+        Q.ty = (int)t.y;
+        Q.tile0 = (int)tp.size();
+        Q.gx = B->suites[b]->g.x;
+        Q.hd = B->suites[b]->g.hd;
+        char* base = (char*)B->slab + B->field_off[b];
+        for (int k = 0; k < BF_COUNT; ++k) Q.f[k] = (float*)(base + B->field_bytes[b] * k);
+        Chunk* c = B->chunks[b];
+        Q.u = c->u;
+        Q.u0 = c->u0;
+        Q.kx = c->kx;
+        Q.ky = c->ky;
+        for (int k = 0; k < Q.tx * Q.ty; ++k) tp.push_back(b);
+    }
+    if ((int)tp.size() > B->max_tiles) {
+        tl::fail(62, "batch: %zu tiles exceed the table capacity %d", tp.size(), B->max_tiles);
+        return false;
+    }
+    B->ntiles = (int)tp.size();
+    B->tile_rows = tile_rows;
+    if (!TL_CUDA(cudaMemcpyAsync(B->d_prob, P.data(), sizeof(BProb) * P.size(), cudaMemcpyHostToDevice, B->stream)))
+        return false;
+    if (!TL_CUDA(cudaMemcpyAsync(B->d_tile_prob, tp.data(), sizeof(int) * tp.size(), cudaMemcpyHostToDevice,
+                                 B->stream)))
+        return false;
+    return TL_CUDA(cudaStreamSynchronize(B->stream));
+}
+
+void launch_halos(TlBatch* B, int b, int depth, std::initializer_list<double*> fields)
+{
+    TlSuite2D* s = B->suites[b];
+    Chunk* c = B->chunks[b];
+    HaloArgs a{};
+    for (double* f : fields) a.f[a.nf++] = f;
+    for (int f = 0; f < 4; ++f) a.ext[f] = c->neighbours[f] == TL_EXTERNAL_FACE;
+    const long per = (long)depth * (2L * (s->g.y - 2 * s->g.hd) + 2L * (s->g.x - 2 * s->g.hd));
+    k_local_halos<<<dim3(tl::ceil_div(per, 256), a.nf), 256, 0, B->stream>>>(s->g, depth, a);
+}
+
+// Everything of one batched timestep, issued on B->stream (capturable).
+// iter_cap limits the iterations of the persistent kernel; finish = run the
+// per-problem finalise (a full timestep) or stop after the solve (tuning).
+void issue_step(TlBatch* B, int iter_cap, bool finish)
+{
+    for (int b = 0; b < B->count; ++b) {
+        TlSuite2D* s = B->suites[b];
+        Chunk* c = B->chunks[b];
+        Settings* st = B->settings[b];
+        const double dt = c->dt_init < st->dt_init ? c->dt_init : st->dt_init;
+        const double rx = dt / (st->dx * st->dx), ry = dt / (st->dy * st->dy);
+        launch_halos(B, b, 2, {c->density, c->energy});
+        k_cg_init<<<full_grid(s->g), FB, 0, B->stream>>>(s->g, st->coefficient, rx, ry, c->density, c->energy, c->u,
+                                                          c->p, nullptr, c->r, c->w, c->kx, c->ky, B->rs,
+                                                          FinCgInit{B->d_scratch_state, nullptr});
+        k_copy_u<<<interior_grid(s->g), BX, 0, B->stream>>>(s->g, c->u0, c->u);
+        char* base = (char*)B->slab + B->field_off[b];
+        float* f[BF_COUNT];
+        for (int k = 0; k < BF_COUNT; ++k) f[k] = (float*)(base + B->field_bytes[b] * k);
+        k_rf_init<float><<<B->sm_count, 256, 0, B->stream>>>(
+            s->g.x, s->g.hd, B->lay[b], c->r, c->u0, c->kx, c->ky, f[BF_KX], f[BF_KY], f[BF_R], f[BF_P0], f[BF_P1],
+            f[BF_W], f[BF_XS], B->rs, FinMxInit{&B->d_st[b], 0.0, st->eps, st->max_iters, nullptr});
+    }
+    k_batch_count_done<<<1, 32, 0, B->stream>>>(B->d_st, B->count, B->d_ctl);
+    void* args[] = {&B->d_prob, &B->count, &B->d_tile_prob, &B->ntiles, &B->d_st, &B->d_tickets, &B->d_partials,
+                    &B->d_ctl, &iter_cap};
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(B->grid_blocks);
+    cfg.blockDim = dim3(BX);
+    cfg.stream = B->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelExC(&cfg, (const void*)k_batch_cg, args);
+    if (!finish) return;
+    for (int b = 0; b < B->count; ++b) {
+        TlSuite2D* s = B->suites[b];
+        Chunk* c = B->chunks[b];
+        k_finalise<<<interior_grid(s->g), BX, 0, B->stream>>>(s->g, c->energy, c->density, c->u);
+        launch_halos(B, b, 1, {c->energy});
+    }
+}
+
+bool check_ctl(TlBatch* B, BCtl* out)
+{
+    BCtl h{};
+    if (!TL_CUDA(cudaMemcpyAsync(&h, B->d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, B->stream))) return false;
+    if (!TL_CUDA(cudaStreamSynchronize(B->stream))) return false;
+    if (h.err) {
+        tl::fail(63, "batch: a grid barrier of the persistent kernel timed out");
+        return false;
+    }
+    if (out) *out = h;
+    return true;
+}
+
+void drop_graph(TlBatch* B)
+{
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    B->exec = nullptr;
+    B->graph = nullptr;
+    B->graph_ok = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int tile_rows, int grid_blocks)
+{
+    if (tl::failed()) return nullptr;
+    if (!chunks || !settings || count < 1) {
+        tl::fail(60, "tl2d_batch_create: need count >= 1 chunks and settings");
+        return nullptr;
+    }
+    TlBatch* B = new TlBatch();
+    B->count = count;
+    TL_CUDA(cudaGetDevice(&B->device));
+    TL_CUDA(cudaDeviceGetAttribute(&B->sm_count, cudaDevAttrMultiProcessorCount, B->device));
+    if (!TL_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking))) {
+        batch_free(B);
+        return nullptr;
+    }
+    long max_full = 1;
+    size_t total = 0;
+    for (int b = 0; b < count; ++b) {
+        TlSuite2D* s = suite_of(chunks[b]);
+        if (!s) {
+            batch_free(B);
+            return nullptr;
+        }
+        const Faces fc = faces_of(chunks[b]);
+        if (settings[b]->num_chunks_per_rank != 1 || !(fc.l && fc.r && fc.b && fc.t) ||
+            (settings[b]->coefficient != TL_CONDUCTIVITY && settings[b]->coefficient != TL_RECIP_CONDUCTIVITY)) {
+            tl::fail(61, "tl2d_batch_create: problem %d needs one chunk, four external faces, a valid coefficient", b);
+            batch_free(B);
+            return nullptr;
+        }
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+        B->chunks.push_back(chunks[b]);
+        B->settings.push_back(settings[b]);
+        B->suites.push_back(s);
+        const int nx = s->g.x - 2 * s->g.hd, ny = s->g.y - 2 * s->g.hd;
+        B->lay.push_back(make_lay<float>(nx, ny, 2));
+        const size_t fbytes = ((size_t)B->lay.back().cells() * sizeof(float) + 255) & ~(size_t)255;
+        B->field_off.push_back(total);
+        B->field_bytes.push_back(fbytes);
+        total += fbytes * BF_COUNT;
+        const dim3 gf = full_grid(s->g);
+        max_full = std::max<long>(max_full, (long)gf.x * gf.y);
+        B->max_iters = std::max(B->max_iters, settings[b]->max_iters);
+    }
+    // tile tables sized for the shortest tiles (2 rows)
+    long tiles = 0;
+    for (int b = 0; b < count; ++b) {
+        const dim3 t = lay_tiles<float>(B->lay[b]);
+        tiles += (long)t.x * t.y;
+    }
+    B->max_tiles = (int)tiles;
+    B->rs_capacity = std::max<long>(max_full, B->sm_count) * tl::kMaxSums;
+    bool ok = TL_CUDA(cudaMalloc(&B->slab, total)) && TL_CUDA(cudaMalloc(&B->d_prob, sizeof(BProb) * count)) &&
+              TL_CUDA(cudaMalloc(&B->d_tile_prob, sizeof(int) * tiles)) &&
+              TL_CUDA(cudaMalloc(&B->d_st, sizeof(MxState) * count)) &&
+              TL_CUDA(cudaMalloc(&B->d_tickets, sizeof(unsigned) * count)) &&
+              TL_CUDA(cudaMalloc(&B->d_partials, sizeof(double) * 2 * tiles)) &&
+              TL_CUDA(cudaMalloc(&B->d_ctl, sizeof(BCtl))) &&
+              TL_CUDA(cudaMalloc(&B->rs.partials, sizeof(double) * B->rs_capacity)) &&
+              TL_CUDA(cudaMalloc(&B->rs.ticket, 256)) && TL_CUDA(cudaMalloc(&B->rs.out_dev, 256)) &&
+              TL_CUDA(cudaMalloc(&B->d_scratch_state, sizeof(DevState)));
+    if (!ok) {
+        batch_free(B);
+        return nullptr;
+    }
+    B->slab_bytes = total;
+    B->rs.out_host = nullptr;
+    TL_CUDA(cudaMemsetAsync(B->rs.ticket, 0, 256, B->stream));
+    TL_CUDA(cudaMemsetAsync(B->d_tickets, 0, sizeof(unsigned) * count, B->stream));
+    TL_CUDA(cudaMemsetAsync(B->d_ctl, 0, sizeof(BCtl), B->stream));
+    int per_sm = 0;
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, BX, 0));
+    B->max_grid = std::max(1, per_sm) * B->sm_count;
+    B->grid_blocks = grid_blocks > 0 ? std::min(grid_blocks, B->max_grid) : B->max_grid;
+    if (!batch_layout(B, tile_rows > 0 ? tile_rows : 16)) {
+        batch_free(B);
+        return nullptr;
+    }
+    return B;
+}
+
+void tl2d_batch_destroy(TlBatch* B)
+{
+    if (!B) return;
+    cudaStreamSynchronize(B->stream);
+    batch_free(B);
+}
+
+// Autotuner: times `trial_iters` iterations of the batch's own CG (setup
+// included, energy untouched) for each tile height in {2, 4, 8, 16, 32, 64}
+// and each persistent grid of {2, 4, 6, 8} blocks per SM (within the
+// co-residency limit), and keeps the fastest. Returns 0 or an error code;
+// the choice is readable with tl2d_batch_config.
+int tl2d_batch_tune(TlBatch* B, int trial_iters, double* best_ms)
+{
+    if (tl::failed()) return tl::error_state().code;
+    if (!B || trial_iters < 1) {
+        tl::fail(64, "tl2d_batch_tune: batch and trial_iters >= 1 are required");
+        return 64;
+    }
+    drop_graph(B);
+    const int rows_c[] = {2, 4, 8, 16, 32, 64};
+    const int per_sm_c[] = {2, 4, 6, 8};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int best_rows = B->tile_rows, best_grid = B->grid_blocks;
+    for (int rows : rows_c) {
+        if (!batch_layout(B, rows)) break;
+        for (int k : per_sm_c) {
+            const int grid = std::min(B->max_grid, k * B->sm_count);
+            B->grid_blocks = grid;
+            for (int rep = 0; rep < 2; ++rep) {   // first run warms up
+                cudaEventRecord(e0, B->stream);
+                issue_step(B, trial_iters, false);
+                cudaEventRecord(e1, B->stream);
+                if (!check_ctl(B, nullptr)) break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                best_rows = rows;
+                best_grid = grid;
+            }
+            if (grid == B->max_grid) break;
+        }
+        if (tl::failed()) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (tl::failed()) return tl::error_state().code;
+    B->grid_blocks = best_grid;
+    batch_layout(B, best_rows);
+    if (best_ms) *best_ms = best;
+    return tl::failed() ? tl::error_state().code : 0;
+}
+
+void tl2d_batch_config(TlBatch* B, int* tile_rows, int* grid_blocks)
+{
+    if (!B) return;
+    if (tile_rows) *tile_rows = B->tile_rows;
+    if (grid_blocks) *grid_blocks = B->grid_blocks;
+}
+
+// One timestep of every problem of the batch (a CUDA graph replay after the
+// first call). Per-problem outcomes through tl2d_batch_results.
+int tl2d_batch_step(TlBatch* B, TlBatchStats* stats)
+{
+    if (tl::failed()) return tl::error_state().code;
+    if (!B) {
+        tl::fail(64, "tl2d_batch_step: null batch");
+        return 64;
+    }
+    TlBatchStats local{};
+    TlBatchStats* out = stats ? stats : &local;
+    *out = TlBatchStats{};
+    for (TlSuite2D* s : B->suites) TL_CUDA(cudaStreamSynchronize(s->stream));
+    if (!B->exec && !B->graph_ok) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            issue_step(B, B->max_iters, true);
+            e = cudaStreamEndCapture(B->stream, &g);
+        }
+        if (e == cudaSuccess && g) e = cudaGraphInstantiate(&B->exec, g, 0);
+        if (e == cudaSuccess) {
+            B->graph = g;
+            B->graph_ok = true;
+        } else {
+            cudaGetLastError();   // capture unsupported here: the same launches run directly
+            if (g) cudaGraphDestroy(g);
+            B->exec = nullptr;
+        }
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, B->stream);
+    if (B->exec) TL_CUDA(cudaGraphLaunch(B->exec, B->stream));
+    else issue_step(B, B->max_iters, true);
+    cudaEventRecord(e1, B->stream);
+    TL_CUDA(cudaGetLastError());
+    BCtl ctl{};
+    const bool ok = check_ctl(B, &ctl);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!ok) return tl::error_state().code;
+    std::vector<MxState> st(B->count);
+    TL_CUDA(cudaMemcpy(st.data(), B->d_st, sizeof(MxState) * B->count, cudaMemcpyDeviceToHost));
+    out->problems = B->count;
+    for (const MxState& m : st) {
+        out->converged += m.reason == 1 ? 1 : 0;
+        out->max_iterations = std::max(out->max_iterations, m.trip);
+        out->total_iterations += m.trip;
+    }
+    out->kernel_iterations = ctl.iters;
+    out->tile_rows = B->tile_rows;
+    out->grid_blocks = B->grid_blocks;
+    out->graph = B->exec ? 1 : 0;
+    out->device_ms = ms;
+    return tl::failed() ? tl::error_state().code : 0;
+}
+
+// Per-problem CG iterations and final FP64 residual r.r of the last step.
+int tl2d_batch_results(TlBatch* B, int* iterations, double* rr, int* converged)
+{
+    if (!B) return 64;
+    std::vector<MxState> st(B->count);
+    if (!TL_CUDA(cudaMemcpy(st.data(), B->d_st, sizeof(MxState) * B->count, cudaMemcpyDeviceToHost)))
+        return tl::error_state().code;
+    for (int b = 0; b < B->count; ++b) {
+        if (iterations) iterations[b] = st[b].trip;
+        if (rr) rr[b] = st[b].rtrue;
+        if (converged) converged[b] = st[b].reason == 1 ? 1 : 0;
+    }
+    return 0;
+}
+
+}  // extern "C"

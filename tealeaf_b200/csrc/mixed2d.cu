@@ -3,31 +3,10 @@
 // tl2d_refine_solve_step solves one timestep's system A u = u0 (the operator
 // of 2d/c_kernels/omp3/cg.c:9-85 with the reflective boundary) to a stated
 // relative residual ||u0 - A u||_2 / ||u0||_2 <= rel_tol, with one algorithm
-// in two storage precisions on identical inputs:
-//
-//  * CG whose vectors (p, r, w, the solution correction xs) and operator
-//    coefficients (kx, ky) are stored in T (float or double). Every kernel
-//    computes in FP64 registers and every dot product (p.w, r.r) is
-//    accumulated in FP64, so w is the FP64 image of the stored p and only the
-//    stores round.
-//  * The solution is accumulated in FP64 (the chunk's u): when r.r of the
-//    stored residual has dropped by kUpdateDelta^2 since the last replacement
-//    (or looks converged), xs is folded into u, the residual u0 - A u is
-//    recomputed in FP64 with the FP64 coefficients and replaces the stored
-//    one, and the search direction is kept (reliable updates / residual
-//    replacement: Sleijpen & van der Vorst 1996; van der Vorst & Ye 2000).
-//    Convergence is only ever declared on that FP64 residual.
-//
-// With T = float one iteration moves 48 B per cell instead of 96.
-//
-// Layout of the T arrays: interior cells only, row pitch xp (>= nx + 2 cells
-// per thread, a multiple of 64), one zero row above and below, so element
-// (k, j) of the interior is at (j + 1) * xp + k. The face coefficient
-// arrays hold kx of the face left of cell k and ky of the face below cell j,
-// with the boundary faces set to zero: with the depth-1 reflective halo the
-// boundary terms of the 5-point operator cancel (neighbour = centre), so the
-// operator is the same in exact arithmetic and the sweeps need no boundary
-// branches. Each thread owns 8 bytes of a row (2 floats or 1 double).
+// (refine2d.cuh: CG on T-stored vectors and coefficients, FP64 arithmetic
+// and dot products, FP64 solution with reliable FP64 residual replacement) in
+// two storage precisions on identical inputs: T = float (48 B per cell per
+// iteration) and T = double (96 B).
 //
 // Around the solve the timestep is the reference's: energy/density halos,
 // cg_init, u0 = u (cg_driver.c:30-62), and energy = u / density afterwards
@@ -35,379 +14,58 @@
 // last block of each reduction computes alpha, beta and the update/stop
 // decisions; the FP64 fold and residual kernels are launched every trip and
 // return at once unless an update was requested.
+#include "refine2d.cuh"
 #include "suite2d_impl.hpp"
 
 #include <cmath>
 
 using namespace tl2d;
+using namespace tl2d::rf;
 
 namespace {
 
 constexpr int kBatch = 16;
-constexpr double kUpdateDelta = 0.1;   // replace the residual when ||r|| fell by this factor
 
-struct MxState {
-    double rr;       // r.r of the stored residual (FP64 sum)
-    double pw, alpha, beta;
-    double bb;       // u0.u0
-    double tol2bb;   // rel_tol^2 * bb
-    double rref;     // r.r right after the last replacement
-    double rtrue;    // FP64 r.r of the last FP64 residual
-    double rsloppy;  // r.r of the stored residual when the last update was requested
-    int trip, done, upd, updates, reason, max_iters;
-};
-
-__device__ __forceinline__ int vol_read(const int* p) { return *(volatile const int*)p; }
-__device__ __forceinline__ bool mx_idle(const MxState* st) { return vol_read(&st->done) != 0; }
-__device__ __forceinline__ bool mx_no_update(const MxState* st)
-{
-    return vol_read(&st->done) != 0 || vol_read(&st->upd) == 0;
-}
-__device__ __forceinline__ void mirror(const MxState* st, int* hm)
-{
-    if (hm) {
-        hm[0] = st->done;
-        hm[1] = st->trip;
-        hm[2] = st->reason;
-    }
-}
-
-struct FinMxInit {   // t: rT.rT, u0.u0, r.r (FP64 residual of cg_init)
-    MxState* st;
-    double tol2;
-    int max_iters;
-    int* hm;
-    __device__ void operator()(const double* t) const
-    {
-        st->rr = t[0];
-        st->rref = t[0];
-        st->bb = t[1];
-        st->tol2bb = tol2 * t[1];
-        st->rtrue = t[2];
-        st->rsloppy = t[0];
-        st->pw = st->alpha = st->beta = 0.0;
-        st->trip = 0;
-        st->upd = 0;
-        st->updates = 0;
-        st->max_iters = max_iters;
-        st->done = 0;
-        st->reason = 0;
-        if (t[2] <= st->tol2bb) {
-            st->done = 1;
-            st->reason = 1;
-        } else if (max_iters <= 0) {
-            st->done = 1;
-            st->reason = 3;
-        }
-        mirror(st, hm);
-    }
-};
-
-struct FinMxW {   // alpha = rr / pw
-    MxState* st;
-    __device__ void operator()(const double* t) const
-    {
-        st->pw = t[0];
-        st->alpha = st->rr / t[0];
-    }
-};
-
-struct FinMxUr {   // beta = rrn / rr, or request an FP64 residual replacement
-    MxState* st;
-    int* hm;
-    __device__ void operator()(const double* t) const
-    {
-        const double rrn = t[0];
-        st->trip += 1;
-        const bool upd = rrn < kUpdateDelta * kUpdateDelta * st->rref || rrn <= st->tol2bb ||
-                         st->trip >= st->max_iters || !(rrn == rrn);
-        if (upd) {
-            st->upd = 1;
-            st->rsloppy = rrn;
-        } else {
-            st->beta = rrn / st->rr;
-            st->rr = rrn;
-        }
-        mirror(st, hm);
-    }
-};
-
-struct FinMxRes {   // t: r.r (FP64 residual), rT.rT
-    MxState* st;
-    int* hm;
-    __device__ void operator()(const double* t) const
-    {
-        st->rtrue = t[0];
-        st->updates += 1;
-        st->upd = 0;
-        if (t[0] <= st->tol2bb) {
-            st->done = 1;
-            st->reason = 1;
-        } else if (st->trip >= st->max_iters || !(t[0] == t[0])) {
-            st->done = 1;
-            st->reason = 3;
-        } else {
-            st->beta = t[1] / st->rr;
-            st->rr = t[1];
-            st->rref = t[1];
-        }
-        mirror(st, hm);
-    }
-};
-
-// ----------------------------------------------------------- T layout ----
-
-// Cells per thread (8 bytes of a row) and resident blocks per SM of the
-// sweeps (FP64 arithmetic on N cells needs 48 / 40 registers a thread).
-template <typename T> struct Pack;
-template <> struct Pack<float> {
-    static constexpr int N = 2;
-    static constexpr int MINB = 10;
-    using V = float2;
-};
-template <> struct Pack<double> {
-    static constexpr int N = 1;
-    static constexpr int MINB = 12;
-    using V = double;
-};
-
-template <typename T>
-union Cells {
-    typename Pack<T>::V v;
-    T e[Pack<T>::N];
-};
-
-template <typename T>
-__device__ __forceinline__ Cells<T> ld(const T* p)
-{
-    Cells<T> c;
-    c.v = *reinterpret_cast<const typename Pack<T>::V*>(p);
-    return c;
-}
-template <typename T>
-__device__ __forceinline__ void st8(T* p, const Cells<T>& c)
-{
-    *reinterpret_cast<typename Pack<T>::V*>(p) = c.v;
-}
-
-struct Lay {
-    int nx, ny, xp, rows;
-    __host__ __device__ long cells() const { return (long)(ny + 2) * xp; }
-};
-
-// Interior column range and rows of this thread.
-template <int N>
-struct Span {
-    int c0, cc, j0, j1, lane;
-    bool any;   // at least one of the N cells is interior
-    __device__ Span(const Lay& L)
-    {
-        c0 = (blockIdx.x * BX + threadIdx.x) * N;
-        cc = min(c0, L.xp - N);   // clamped: lanes past the row load valid padding cells
-        j0 = blockIdx.y * L.rows;
-        j1 = min(j0 + L.rows, L.ny);
-        lane = threadIdx.x & 31;
-        any = c0 < L.nx;
-    }
-};
-
-template <typename T>
-dim3 lay_grid(const Lay& L)
-{
-    constexpr int N = Pack<T>::N;
-    return dim3(tl::ceil_div(tl::ceil_div(L.nx, N), BX), tl::ceil_div(L.ny, L.rows));
-}
-
-// Fills the T arrays from the FP64 state after cg_init, padding included:
-// kxT/kyT (interior faces; boundary faces and padding 0), rT = p0 = r,
-// p1 = w = xs = 0. Sums rT.rT, u0.u0 and r.r over the interior.
-template <typename T, typename Finish>
-__global__ void __launch_bounds__(256) k_rf_init(Geo g, Lay L, const double* __restrict__ r,
-                                                 const double* __restrict__ u0, const double* __restrict__ kx,
-                                                 const double* __restrict__ ky, T* __restrict__ kxT,
-                                                 T* __restrict__ kyT, T* __restrict__ rT, T* __restrict__ p0,
-                                                 T* __restrict__ p1, T* __restrict__ w, T* __restrict__ xs,
-                                                 ReduceSlots rs, Finish fin)
-{
-    double acc[3] = {0.0, 0.0, 0.0};
-    const long n = L.cells();
-    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
-        const int k = (int)(e % L.xp);
-        const int j = (int)(e / L.xp) - 1;
-        const bool in = k < L.nx && j >= 0 && j < L.ny;
-        const long i = in ? (long)(g.hd + k) + (long)(g.hd + j) * g.x : 0;
-        T kxv = 0, kyv = 0, rv = 0;
-        if (in) {
-            if (k >= 1) kxv = (T)kx[i];
-            if (j >= 1) kyv = (T)ky[i];
-            const double r64 = r[i];
-            rv = (T)r64;
-            acc[0] += (double)rv * (double)rv;
-            acc[1] += u0[i] * u0[i];
-            acc[2] += r64 * r64;
-        }
-        kxT[e] = kxv;
-        kyT[e] = kyv;
-        rT[e] = rv;
-        p0[e] = rv;
-        p1[e] = 0;
-        w[e] = 0;
-        xs[e] = 0;
-    }
-    tl::grid_sum<3, 256>(acc, rs, blockIdx.x, gridDim.x, fin);
-}
-
-// CG sweep 1 on the T layout, FP64 arithmetic: [p = beta p + r] (rounded to
-// T as stored), w = A p, sum(w p) over the stored values.
 template <typename T, bool FUSE_P>
 __global__ void __launch_bounds__(BX, Pack<T>::MINB) k_rf_w(Lay L, const MxState* __restrict__ st,
-                                                        const T* __restrict__ p_in, T* __restrict__ p_out,
-                                                        const T* __restrict__ r, T* __restrict__ w,
-                                                        const T* __restrict__ kx, const T* __restrict__ ky,
-                                                        ReduceSlots rs, FinMxW fin)
+                                                            const T* __restrict__ p_in, T* __restrict__ p_out,
+                                                            const T* __restrict__ r, T* __restrict__ w,
+                                                            const T* __restrict__ kx, const T* __restrict__ ky,
+                                                            ReduceSlots rs, FinMxW fin)
 {
-    constexpr int N = Pack<T>::N;
     if (mx_idle(st)) return;
-    double acc[1] = {0.0};
-    const Span<N> s(L);
     const double bt = FUSE_P ? st->beta : 0.0;
-    auto cur = [&](long idx) -> Cells<T> {
-        Cells<T> c = ld(p_in + idx);
-        if (FUSE_P) {
-            const Cells<T> q = ld(r + idx);
-#pragma unroll
-            for (int m = 0; m < N; ++m) c.e[m] = (T)(bt * (double)c.e[m] + (double)q.e[m]);
-        }
-        return c;
-    };
-    auto cur1 = [&](long idx) -> T {
-        return FUSE_P ? (T)(bt * (double)p_in[idx] + (double)r[idx]) : p_in[idx];
-    };
-    const long xp = L.xp;
-    long i = (long)(s.j0 + 1) * xp + s.cc;
-    Cells<T> pc = cur(i), pd = cur(i - xp), kyc = ld(ky + i);
-TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
-    for (int j = s.j0; j < s.j1; ++j, i += xp) {
-        const Cells<T> pu = cur(i + xp), kyu = ld(ky + i + xp), kxc = ld(kx + i);
-        T pl = __shfl_up_sync(kFull, pc.e[N - 1], 1);
-        T pr = __shfl_down_sync(kFull, pc.e[0], 1);
-        T kxr = __shfl_down_sync(kFull, kxc.e[0], 1);
-        if (s.lane == 0) pl = cur1(i - 1);
-        if (s.lane == 31) {
-            pr = cur1(i + N);
-            kxr = kx[i + N];
-        }
-        Cells<T> wv;
-#pragma unroll
-        for (int m = 0; m < N; ++m) {
-            const double c = (double)pc.e[m];
-            const double l = m == 0 ? (double)pl : (double)pc.e[m - 1];
-            const double rr = m == N - 1 ? (double)pr : (double)pc.e[m + 1];
-            const double kr = m == N - 1 ? (double)kxr : (double)kxc.e[m + 1];
-            wv.e[m] = (T)smvp((double)kxc.e[m], kr, (double)kyc.e[m], (double)kyu.e[m], c, l, rr, (double)pd.e[m],
-                              (double)pu.e[m]);
-        }
-        if (s.any) {
-            st8(w + i, wv);
-            if (FUSE_P) st8(p_out + i, pc);
-#pragma unroll
-            for (int m = 0; m < N; ++m)
-                if (s.c0 + m < L.nx) acc[0] += (double)wv.e[m] * (double)pc.e[m];
-        }
-        pd = pc;
-        pc = pu;
-        kyc = kyu;
-    }
+    double acc[1] = {rf_w_tile<T, FUSE_P>(L, blockIdx.x, blockIdx.y, bt, p_in, p_out, r, w, kx, ky)};
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
-// CG sweep 2 on the T layout: xs += alpha p ; r -= alpha w ; sum(r r).
 template <typename T>
 __global__ void __launch_bounds__(BX, Pack<T>::MINB) k_rf_ur(Lay L, const MxState* __restrict__ st, T* __restrict__ xs,
-                                                         const T* __restrict__ p, T* __restrict__ r,
-                                                         const T* __restrict__ w, ReduceSlots rs, FinMxUr fin)
+                                                             const T* __restrict__ p, T* __restrict__ r,
+                                                             const T* __restrict__ w, ReduceSlots rs, FinMxUr fin)
 {
-    constexpr int N = Pack<T>::N;
     if (mx_idle(st)) return;
-    const Span<N> s(L);
-    double acc[1] = {0.0};
-    if (s.any) {
-        const double a = st->alpha;
-        long i = (long)(s.j0 + 1) * L.xp + s.c0;
-TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
-        for (int j = s.j0; j < s.j1; ++j, i += L.xp) {
-            Cells<T> xv = ld(xs + i), rv = ld(r + i);
-            const Cells<T> pv = ld(p + i), wv = ld(w + i);
-#pragma unroll
-            for (int m = 0; m < N; ++m) {
-                xv.e[m] = (T)((double)xv.e[m] + a * (double)pv.e[m]);
-                rv.e[m] = (T)((double)rv.e[m] - a * (double)wv.e[m]);
-                if (s.c0 + m < L.nx) acc[0] += (double)rv.e[m] * (double)rv.e[m];
-            }
-            st8(xs + i, xv);
-            st8(r + i, rv);
-        }
-    }
+    double acc[1] = {rf_ur_tile<T>(L, blockIdx.x, blockIdx.y, st->alpha, xs, p, r, w)};
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
-// Reliable update, part 1 (only when requested): u += xs (FP64), xs = 0.
 template <typename T>
-__global__ void __launch_bounds__(BX) k_rf_fold(Geo g, Lay L, const MxState* __restrict__ st, double* __restrict__ u,
-                                                T* __restrict__ xs)
+__global__ void __launch_bounds__(BX) k_rf_fold(Lay L, const MxState* __restrict__ st, int gx, int hd,
+                                                double* __restrict__ u, T* __restrict__ xs)
 {
     if (mx_no_update(st)) return;
-    Strip s(g);
-    if (!s.active) return;
-    const int k = s.k - g.hd;
-    long i = s.k + (long)s.j0 * g.x;
-    for (int j = s.j0; j < s.j1; ++j, i += g.x) {
-        const long e = (long)(j - g.hd + 1) * L.xp + k;
-        u[i] += (double)xs[e];
-        xs[e] = 0;
-    }
+    rf_fold_tile<T>(L, blockIdx.x, blockIdx.y, gx, hd, u, xs);
 }
 
-// Reliable update, part 2: r = u0 - A u in FP64 with the FP64 coefficients
-// and the reflective boundary; rT = r; sums r.r and rT.rT.
 template <typename T>
-__global__ void __launch_bounds__(BX) k_rf_resid(Geo g, Lay L, const MxState* __restrict__ st,
+__global__ void __launch_bounds__(BX) k_rf_resid(Lay L, const MxState* __restrict__ st, int gx, int hd,
                                                  const double* __restrict__ u, const double* __restrict__ u0,
                                                  const double* __restrict__ kx, const double* __restrict__ ky,
                                                  T* __restrict__ rT, ReduceSlots rs, FinMxRes fin)
 {
     if (mx_no_update(st)) return;
     double acc[2] = {0.0, 0.0};
-    const StripC s(g);
-    const int x = g.x;
-    const int jt = g.y - g.hd - 1;
-    long i = s.kk + (long)s.j0 * x;
-    double uc = u[i];
-    double ud = (s.j0 == g.hd) ? uc : u[i - x];
-    double kyc = ky[i];
-    for (int j = s.j0; j < s.j1; ++j, i += x) {
-        const double uu = (j == jt) ? uc : u[i + x];
-        const double kyu = ky[i + x];
-        const double kxc = kx[i];
-        double ul = __shfl_up_sync(kFull, uc, 1);
-        double ur = __shfl_down_sync(kFull, uc, 1);
-        double kxr = __shfl_down_sync(kFull, kxc, 1);
-        if (s.at_l) ul = uc;
-        else if (s.lane == 0) ul = u[i - 1];
-        if (s.at_r) ur = uc;
-        else if (s.lane == 31) ur = u[i + 1];
-        if (s.at_r || s.lane == 31) kxr = kx[i + 1];
-        const double rv = u0[i] - smvp(kxc, kxr, kyc, kyu, uc, ul, ur, ud, uu);
-        const T rt = (T)rv;
-        if (s.active) {
-            rT[(long)(j - g.hd + 1) * L.xp + (s.k - g.hd)] = rt;
-            acc[0] += rv * rv;
-            acc[1] += (double)rt * (double)rt;
-        }
-        ud = uc;
-        uc = uu;
-        kyc = kyu;
-    }
+    rf_resid_tile<T>(L, blockIdx.x, blockIdx.y, gx, hd, u, u0, kx, ky, rT, acc);
     tl::grid_sum<2, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
@@ -428,12 +86,9 @@ RfBuffers<T> rf_buffers(TlSuite2D* s)
     constexpr int N = Pack<T>::N;
     RfBuffers<T> b{};
     const int nx = s->g.x - 2 * s->g.hd, ny = s->g.y - 2 * s->g.hd;
-    b.L.nx = nx;
-    b.L.ny = ny;
-    b.L.xp = ((nx + 2 * N + 63) / 64) * 64;
-    b.L.rows = choose_rows(tl::ceil_div(nx, N), ny, s->sm_count, Pack<T>::MINB);
+    b.L = make_lay<T>(nx, ny, choose_rows(tl::ceil_div(nx, N), ny, s->sm_count, Pack<T>::MINB));
     {
-        const dim3 t = lay_grid<T>(b.L);   // the reduction partials must fit
+        const dim3 t = lay_tiles<T>(b.L);   // the reduction partials must fit
         if ((long)t.x * t.y * tl::kMaxSums > s->partial_capacity) b.L.rows = s->g.rows;
     }
     const size_t field = ((size_t)b.L.cells() * sizeof(T) + 255) & ~(size_t)255;
@@ -499,12 +154,12 @@ int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int
     if (!b.st) return 0;
     const char* const* nm = Names<T>::n;
     const Lay L = b.L;
-    const dim3 gl = lay_grid<T>(L), gi = interior_grid(s->g);
+    const dim3 gl = lay_tiles<T>(L);
     s->h_mirror[0] = 0;
     TL_LAUNCH(s, nm[0], (k_rf_init<T><<<s->sm_count * 4, 256, 0, s->stream>>>(
-                            s->g, L, chunk->r, chunk->u0, chunk->kx, chunk->ky, b.f[RF_KX], b.f[RF_KY], b.f[RF_R],
+                            s->g.x, s->g.hd, L, chunk->r, chunk->u0, chunk->kx, chunk->ky, b.f[RF_KX], b.f[RF_KY], b.f[RF_R],
                             b.f[RF_P0], b.f[RF_P1], b.f[RF_W], b.f[RF_XS], s->rs,
-                            FinMxInit{b.st, rel_tol * rel_tol, max_iters, s->d_mirror})));
+                            FinMxInit{b.st, rel_tol * rel_tol, 0.0, max_iters, s->d_mirror})));
     T* pb[2] = {b.f[RF_P0], b.f[RF_P1]};
     int cur = 0;
     batched(s, max_iters, [&](int t) {
@@ -520,10 +175,11 @@ int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int
         }
         TL_LAUNCH(s, nm[2], (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(L, b.st, b.f[RF_XS], pb[cur], b.f[RF_R],
                                                                    b.f[RF_W], s->rs, FinMxUr{b.st, s->d_mirror})));
-        TL_LAUNCH(s, nm[3], (k_rf_fold<T><<<gi, BX, 0, s->stream>>>(s->g, L, b.st, chunk->u, b.f[RF_XS])));
-        TL_LAUNCH(s, nm[4], (k_rf_resid<T><<<gi, BX, 0, s->stream>>>(s->g, L, b.st, chunk->u, chunk->u0, chunk->kx,
-                                                                      chunk->ky, b.f[RF_R], s->rs,
-                                                                      FinMxRes{b.st, s->d_mirror})));
+        TL_LAUNCH(s, nm[3], (k_rf_fold<T><<<gl, BX, 0, s->stream>>>(L, b.st, s->g.x, s->g.hd, chunk->u,
+                                                                     b.f[RF_XS])));
+        TL_LAUNCH(s, nm[4], (k_rf_resid<T><<<gl, BX, 0, s->stream>>>(L, b.st, s->g.x, s->g.hd, chunk->u,
+                                                                      chunk->u0, chunk->kx, chunk->ky, b.f[RF_R],
+                                                                      s->rs, FinMxRes{b.st, s->d_mirror})));
     });
     MxState st{};
     TL_CUDA(cudaMemcpy(&st, b.st, sizeof(MxState), cudaMemcpyDeviceToHost));

@@ -1,0 +1,403 @@
+// refine2d.cuh -- CG with FP64 refinement on the padded "T layout" (2D):
+// the solver state, the finishers and the tile sweeps shared by the
+// iterative-refinement timestep (mixed2d.cu) and the batched solver
+// (batch2d.cu).
+//
+// CG whose vectors (p, r, w, the solution correction xs) and operator
+// coefficients (kx, ky) are stored in T (float or double). Every sweep
+// computes in FP64 registers and every dot product (p.w, r.r) is accumulated
+// in FP64, so w is the FP64 image of the stored p and only the stores round.
+// The solution is accumulated in FP64 (the chunk's u): when r.r of the stored
+// residual has dropped by kUpdateDelta^2 since the last replacement (or looks
+// converged), xs is folded into u, the residual u0 - A u is recomputed in
+// FP64 with the FP64 coefficients and replaces the stored one, and the search
+// direction is kept (reliable updates / residual replacement: Sleijpen & van
+// der Vorst 1996; van der Vorst & Ye 2000). Convergence is only ever declared
+// on that FP64 residual. With T = float one iteration moves 48 B per cell.
+//
+// T layout: interior cells only, row pitch xp (>= nx + 2 cells per thread, a
+// multiple of 64), one zero row above and below, so element (k, j) of the
+// interior is at (j + 1) * xp + k. The face coefficient arrays hold kx of the
+// face left of cell k and ky of the face below cell j, with the boundary faces
+// set to zero: with the depth-1 reflective halo the boundary terms of the
+// 5-point operator cancel (neighbour = centre), so the operator is the same
+// in exact arithmetic and the sweeps need no boundary branches. The padding
+// stays zero through the iteration (zero coefficients, zero start). A tile is
+// BX threads x N cells (8 bytes of a row per thread) x L.rows rows.
+#pragma once
+
+#include "kernels2d.cuh"
+
+namespace tl2d {
+namespace rf {
+
+constexpr double kUpdateDelta = 0.1;   // replace the residual when ||r|| fell by this factor
+
+struct MxState {
+    double rr;       // r.r of the stored residual (FP64 sum)
+    double pw, alpha, beta;
+    double bb;       // u0.u0
+    double tol2bb;   // stop when the FP64 r.r <= tol2bb
+    double rref;     // r.r right after the last replacement
+    double rtrue;    // FP64 r.r of the last FP64 residual
+    double rsloppy;  // r.r of the stored residual when the last update was requested
+    int trip, done, upd, updates, reason, max_iters;
+};
+
+__device__ __forceinline__ int vol_read(const int* p) { return *(volatile const int*)p; }
+__device__ __forceinline__ bool mx_idle(const MxState* st) { return vol_read(&st->done) != 0; }
+__device__ __forceinline__ bool mx_no_update(const MxState* st)
+{
+    return vol_read(&st->done) != 0 || vol_read(&st->upd) == 0;
+}
+__device__ __forceinline__ void mirror(const MxState* st, int* hm)
+{
+    if (hm) {
+        hm[0] = st->done;
+        hm[1] = st->trip;
+        hm[2] = st->reason;
+    }
+}
+
+// t: rT.rT, u0.u0, r.r (FP64 residual of cg_init). Stop test: FP64 r.r <=
+// tol2 * u0.u0 (relative), or <= abs_eps when abs_eps > 0 (the reference's
+// r.r < eps of 2d/diffuse.c, on the FP64 residual).
+struct FinMxInit {
+    MxState* st;
+    double tol2;
+    double abs_eps;
+    int max_iters;
+    int* hm;
+    __device__ void operator()(const double* t) const
+    {
+        st->rr = t[0];
+        st->rref = t[0];
+        st->bb = t[1];
+        st->tol2bb = abs_eps > 0.0 ? abs_eps : tol2 * t[1];
+        st->rtrue = t[2];
+        st->rsloppy = t[0];
+        st->pw = st->alpha = st->beta = 0.0;
+        st->trip = 0;
+        st->upd = 0;
+        st->updates = 0;
+        st->max_iters = max_iters;
+        st->done = 0;
+        st->reason = 0;
+        if (t[2] <= st->tol2bb) {
+            st->done = 1;
+            st->reason = 1;
+        } else if (max_iters <= 0) {
+            st->done = 1;
+            st->reason = 3;
+        }
+        mirror(st, hm);
+    }
+};
+
+struct FinMxW {   // alpha = rr / pw
+    MxState* st;
+    __device__ void operator()(const double* t) const
+    {
+        st->pw = t[0];
+        st->alpha = st->rr / t[0];
+    }
+};
+
+struct FinMxUr {   // beta = rrn / rr, or request an FP64 residual replacement
+    MxState* st;
+    int* hm;
+    __device__ void operator()(const double* t) const
+    {
+        const double rrn = t[0];
+        st->trip += 1;
+        const bool upd = rrn < kUpdateDelta * kUpdateDelta * st->rref || rrn <= st->tol2bb ||
+                         st->trip >= st->max_iters || !(rrn == rrn);
+        if (upd) {
+            st->upd = 1;
+            st->rsloppy = rrn;
+        } else {
+            st->beta = rrn / st->rr;
+            st->rr = rrn;
+        }
+        mirror(st, hm);
+    }
+};
+
+struct FinMxRes {   // t: r.r (FP64 residual), rT.rT
+    MxState* st;
+    int* hm;
+    __device__ void operator()(const double* t) const
+    {
+        st->rtrue = t[0];
+        st->updates += 1;
+        st->upd = 0;
+        if (t[0] <= st->tol2bb) {
+            st->done = 1;
+            st->reason = 1;
+        } else if (st->trip >= st->max_iters || !(t[0] == t[0])) {
+            st->done = 1;
+            st->reason = 3;
+        } else {
+            st->beta = t[1] / st->rr;
+            st->rr = t[1];
+            st->rref = t[1];
+        }
+        mirror(st, hm);
+    }
+};
+
+// ----------------------------------------------------------- T layout ----
+
+// Cells per thread (8 bytes of a row) and resident blocks per SM of the
+// sweeps (FP64 arithmetic on N cells needs 48 / 40 registers a thread).
+template <typename T> struct Pack;
+template <> struct Pack<float> {
+    static constexpr int N = 2;
+    static constexpr int MINB = 10;
+    using V = float2;
+};
+template <> struct Pack<double> {
+    static constexpr int N = 1;
+    static constexpr int MINB = 12;
+    using V = double;
+};
+
+template <typename T>
+union Cells {
+    typename Pack<T>::V v;
+    T e[Pack<T>::N];
+};
+
+template <typename T>
+__device__ __forceinline__ Cells<T> ld(const T* p)
+{
+    Cells<T> c;
+    c.v = *reinterpret_cast<const typename Pack<T>::V*>(p);
+    return c;
+}
+template <typename T>
+__device__ __forceinline__ void st8(T* p, const Cells<T>& c)
+{
+    *reinterpret_cast<typename Pack<T>::V*>(p) = c.v;
+}
+
+struct Lay {
+    int nx, ny, xp, rows;
+    __host__ __device__ long cells() const { return (long)(ny + 2) * xp; }
+};
+
+template <typename T>
+inline Lay make_lay(int nx, int ny, int rows)
+{
+    constexpr int N = Pack<T>::N;
+    Lay L;
+    L.nx = nx;
+    L.ny = ny;
+    L.xp = ((nx + 2 * N + 63) / 64) * 64;
+    L.rows = rows;
+    return L;
+}
+
+template <typename T>
+inline dim3 lay_tiles(const Lay& L)
+{
+    constexpr int N = Pack<T>::N;
+    return dim3(tl::ceil_div(tl::ceil_div(L.nx, N), BX), tl::ceil_div(L.ny, L.rows));
+}
+
+// Columns and rows of this thread in tile (tx, ty).
+template <int N>
+struct Span {
+    int c0, cc, j0, j1, lane;
+    bool any;   // at least one of the N cells is interior
+    __device__ Span(const Lay& L, int tx, int ty)
+    {
+        c0 = (tx * BX + threadIdx.x) * N;
+        cc = min(c0, L.xp - N);   // clamped: lanes past the row load valid padding cells
+        j0 = ty * L.rows;
+        j1 = min(j0 + L.rows, L.ny);
+        lane = threadIdx.x & 31;
+        any = c0 < L.nx;
+    }
+};
+
+// Fills the T arrays from the FP64 state after cg_init, padding included:
+// kxT/kyT (interior faces; boundary faces and padding 0), rT = p0 = r,
+// p1 = w = xs = 0. Sums rT.rT, u0.u0 and r.r over the interior. gx: row
+// length of the FP64 chunk arrays, hd: their halo depth.
+template <typename T, typename Finish>
+__global__ void __launch_bounds__(256) k_rf_init(int gx, int hd, Lay L, const double* __restrict__ r,
+                                                 const double* __restrict__ u0, const double* __restrict__ kx,
+                                                 const double* __restrict__ ky, T* __restrict__ kxT,
+                                                 T* __restrict__ kyT, T* __restrict__ rT, T* __restrict__ p0,
+                                                 T* __restrict__ p1, T* __restrict__ w, T* __restrict__ xs,
+                                                 ReduceSlots rs, Finish fin)
+{
+    double acc[3] = {0.0, 0.0, 0.0};
+    const long n = L.cells();
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+        const int k = (int)(e % L.xp);
+        const int j = (int)(e / L.xp) - 1;
+        const bool in = k < L.nx && j >= 0 && j < L.ny;
+        const long i = in ? (long)(hd + k) + (long)(hd + j) * gx : 0;
+        T kxv = 0, kyv = 0, rv = 0;
+        if (in) {
+            if (k >= 1) kxv = (T)kx[i];
+            if (j >= 1) kyv = (T)ky[i];
+            const double r64 = r[i];
+            rv = (T)r64;
+            acc[0] += (double)rv * (double)rv;
+            acc[1] += u0[i] * u0[i];
+            acc[2] += r64 * r64;
+        }
+        kxT[e] = kxv;
+        kyT[e] = kyv;
+        rT[e] = rv;
+        p0[e] = rv;
+        p1[e] = 0;
+        w[e] = 0;
+        xs[e] = 0;
+    }
+    tl::grid_sum<3, 256>(acc, rs, blockIdx.x, gridDim.x, fin);
+}
+
+// CG sweep 1 over tile (tx, ty), FP64 arithmetic: [p = beta p + r] (rounded
+// to T as stored), w = A p; returns this thread's share of sum(w p) over the
+// stored values. All threads of the block take part (warp shuffles).
+template <typename T, bool FUSE_P>
+__device__ __forceinline__ double rf_w_tile(const Lay& L, int tx, int ty, double bt, const T* __restrict__ p_in,
+                                            T* __restrict__ p_out, const T* __restrict__ r, T* __restrict__ w,
+                                            const T* __restrict__ kx, const T* __restrict__ ky)
+{
+    constexpr int N = Pack<T>::N;
+    double acc = 0.0;
+    const Span<N> s(L, tx, ty);
+    auto cur = [&](long idx) -> Cells<T> {
+        Cells<T> c = ld(p_in + idx);
+        if (FUSE_P) {
+            const Cells<T> q = ld(r + idx);
+#pragma unroll
+            for (int m = 0; m < N; ++m) c.e[m] = (T)(bt * (double)c.e[m] + (double)q.e[m]);
+        }
+        return c;
+    };
+    auto cur1 = [&](long idx) -> T {
+        return FUSE_P ? (T)(bt * (double)p_in[idx] + (double)r[idx]) : p_in[idx];
+    };
+    const long xp = L.xp;
+    long i = (long)(s.j0 + 1) * xp + s.cc;
+    Cells<T> pc = cur(i), pd = cur(i - xp), kyc = ld(ky + i);
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
+    for (int j = s.j0; j < s.j1; ++j, i += xp) {
+        const Cells<T> pu = cur(i + xp), kyu = ld(ky + i + xp), kxc = ld(kx + i);
+        T pl = __shfl_up_sync(kFull, pc.e[N - 1], 1);
+        T pr = __shfl_down_sync(kFull, pc.e[0], 1);
+        T kxr = __shfl_down_sync(kFull, kxc.e[0], 1);
+        if (s.lane == 0) pl = cur1(i - 1);
+        if (s.lane == 31) {
+            pr = cur1(i + N);
+            kxr = kx[i + N];
+        }
+        Cells<T> wv;
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const double c = (double)pc.e[m];
+            const double l = m == 0 ? (double)pl : (double)pc.e[m - 1];
+            const double rr = m == N - 1 ? (double)pr : (double)pc.e[m + 1];
+            const double kr = m == N - 1 ? (double)kxr : (double)kxc.e[m + 1];
+            wv.e[m] = (T)smvp((double)kxc.e[m], kr, (double)kyc.e[m], (double)kyu.e[m], c, l, rr, (double)pd.e[m],
+                              (double)pu.e[m]);
+        }
+        if (s.any) {
+            st8(w + i, wv);
+            if (FUSE_P) st8(p_out + i, pc);
+#pragma unroll
+            for (int m = 0; m < N; ++m)
+                if (s.c0 + m < L.nx) acc += (double)wv.e[m] * (double)pc.e[m];
+        }
+        pd = pc;
+        pc = pu;
+        kyc = kyu;
+    }
+    return acc;
+}
+
+// CG sweep 2 over tile (tx, ty): xs += alpha p ; r -= alpha w ; returns this
+// thread's share of sum(r r).
+template <typename T>
+__device__ __forceinline__ double rf_ur_tile(const Lay& L, int tx, int ty, double a, T* __restrict__ xs,
+                                             const T* __restrict__ p, T* __restrict__ r, const T* __restrict__ w)
+{
+    constexpr int N = Pack<T>::N;
+    const Span<N> s(L, tx, ty);
+    double acc = 0.0;
+    if (s.any) {
+        long i = (long)(s.j0 + 1) * L.xp + s.c0;
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
+        for (int j = s.j0; j < s.j1; ++j, i += L.xp) {
+            Cells<T> xv = ld(xs + i), rv = ld(r + i);
+            const Cells<T> pv = ld(p + i), wv = ld(w + i);
+#pragma unroll
+            for (int m = 0; m < N; ++m) {
+                xv.e[m] = (T)((double)xv.e[m] + a * (double)pv.e[m]);
+                rv.e[m] = (T)((double)rv.e[m] - a * (double)wv.e[m]);
+                if (s.c0 + m < L.nx) acc += (double)rv.e[m] * (double)rv.e[m];
+            }
+            st8(xs + i, xv);
+            st8(r + i, rv);
+        }
+    }
+    return acc;
+}
+
+// Reliable update, part 1, tile (tx, ty): u += xs in FP64 (u in the chunk
+// layout: row length gx, halo depth hd), xs = 0.
+template <typename T>
+__device__ __forceinline__ void rf_fold_tile(const Lay& L, int tx, int ty, int gx, int hd, double* __restrict__ u,
+                                             T* __restrict__ xs)
+{
+    constexpr int N = Pack<T>::N;
+    const Span<N> s(L, tx, ty);
+    for (int j = s.j0; j < s.j1; ++j)
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const int k = s.c0 + m;
+            if (k >= L.nx) break;
+            const long e = (long)(j + 1) * L.xp + k;
+            u[(long)(hd + k) + (long)(hd + j) * gx] += (double)xs[e];
+            xs[e] = 0;
+        }
+}
+
+// Reliable update, part 2, tile (tx, ty): r = u0 - A u in FP64 with the FP64
+// coefficients and the reflective boundary (a neighbour outside the interior
+// is the centre value); rT = r; adds r.r and rT.rT to acc.
+template <typename T>
+__device__ __forceinline__ void rf_resid_tile(const Lay& L, int tx, int ty, int gx, int hd,
+                                              const double* __restrict__ u, const double* __restrict__ u0,
+                                              const double* __restrict__ kx, const double* __restrict__ ky,
+                                              T* __restrict__ rT, double (&acc)[2])
+{
+    constexpr int N = Pack<T>::N;
+    const Span<N> s(L, tx, ty);
+    for (int j = s.j0; j < s.j1; ++j)
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const int k = s.c0 + m;
+            if (k >= L.nx) break;
+            const long i = (long)(hd + k) + (long)(hd + j) * gx;
+            const double c = u[i];
+            const double l = k > 0 ? u[i - 1] : c;
+            const double rr = k < L.nx - 1 ? u[i + 1] : c;
+            const double d = j > 0 ? u[i - gx] : c;
+            const double up = j < L.ny - 1 ? u[i + gx] : c;
+            const double rv = u0[i] - smvp(kx[i], kx[i + 1], ky[i], ky[i + gx], c, l, rr, d, up);
+            const T rt = (T)rv;
+            rT[(long)(j + 1) * L.xp + k] = rt;
+            acc[0] += rv * rv;
+            acc[1] += (double)rt * (double)rt;
+        }
+}
+
+}  // namespace rf
+}  // namespace tl2d

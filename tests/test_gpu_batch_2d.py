@@ -1,0 +1,71 @@
+"""Batched timesteps (tl2d_batch_*) on the B200.
+
+Every problem of a batch of uneven sizes is stopped by its FP64 residual,
+r.r < eps (1e-12, the reference's 2D stop test); its field summary agrees
+with the same timestep solved alone by the FP64 device driver (whose stop
+test is the recursive residual) within TEMP_RTOL: both residuals are below
+sqrt(eps) = 1e-6 in norm, so the solutions differ by at most that much per
+unit of A's smallest eigenvalue (>= 1), which bounds temp to ~1e-6 relative.
+vol, mass and ie do not depend on the solve and match exactly.
+"""
+import numpy as np
+import pytest
+
+from tealeaf_b200 import problems
+from tealeaf_b200.batch import Batch
+from tealeaf_b200.host import Host
+
+pytestmark = pytest.mark.gpu
+
+TEMP_RTOL = 1e-6
+
+
+def _probs(count=6):
+    return problems.batched_2d(count, seed=9, lo=40, hi=300, steps=2)
+
+
+def _sequential(prob, steps):
+    h = Host(prob.tea_in(), 2)
+    try:
+        out = []
+        for tt in range(steps):
+            r = h.solve_device(tt)
+            out.append((r.iterations["CG"], r.summary))
+        return out
+    finally:
+        h.finalise()
+
+
+def test_batch_matches_sequential_fp64_solves():
+    probs = _probs()
+    b = Batch([p.tea_in() for p in probs])
+    try:
+        for tt in range(2):
+            st = b.step()
+            assert st.problems == len(probs) and st.converged == len(probs)
+            assert st.graph == 1
+            it, rr, conv = b.results()
+            assert conv.all() and (rr < 1e-12).all()
+            for k, (p, s) in enumerate(zip(probs, b.summaries())):
+                ref_it, ref = _sequential(p, tt + 1)[tt]
+                assert s[0] == ref[0] and s[1] == ref[1] and s[2] == ref[2]
+                assert abs(s[3] / ref[3] - 1.0) < TEMP_RTOL, (k, tt, s[3], ref[3])
+                # FP32 storage costs at most a few extra iterations here
+                assert it[k] <= 1.25 * ref_it + 10, (k, it[k], ref_it)
+    finally:
+        b.close()
+
+
+def test_autotuner_picks_a_candidate_and_step_still_converges():
+    probs = _probs(4)
+    b = Batch([p.tea_in() for p in probs])
+    try:
+        before = [h.download("energy") for h in b.hosts]
+        cfg = b.tune(trial_iters=5)
+        assert cfg["tile_rows"] in (2, 4, 8, 16, 32, 64) and cfg["grid_blocks"] > 0
+        for h, e in zip(b.hosts, before):   # tuning leaves the energy untouched
+            assert np.array_equal(h.download("energy"), e)
+        st = b.step()
+        assert st.converged == len(probs) and st.tile_rows == cfg["tile_rows"]
+    finally:
+        b.close()
