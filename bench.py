@@ -461,6 +461,59 @@ def bench_adjoint(args) -> dict:
     return line
 
 
+def bench_batch(args) -> dict:
+    """The batched form: one timestep of 64 seeded 2D problems (sides
+    log-uniform in [128, 2048], 3 rectangles each, CG to eps 1e-12) as one
+    graph-captured persistent launch with the autotuned tile shape, against
+    the same 64 timesteps solved one after another by the FP64 device driver."""
+    import ctypes as C
+
+    import torch
+
+    from tealeaf_b200 import problems
+    from tealeaf_b200.batch import Batch
+    from tealeaf_b200.host import Host
+    probs = problems.batched_2d(args.batch_count, seed=5)
+    cells = sum(p.cells[0] * p.cells[1] for p in probs)
+    b = Batch([p.tea_in() for p in probs])
+    try:
+        tuned = b.tune(trial_iters=args.tune_iters)
+        st = b.step()
+        it, rr, conv = b.results()
+        sums = b.summaries()
+    finally:
+        b.close()
+    seq_ms, seq_iters, worst = 0.0, 0, 0.0
+    for p, s in zip(probs, sums):
+        h = Host(p.tea_in(), dims=2)
+        try:
+            stream = torch.cuda.ExternalStream(h.lib.tl2d_stream(C.byref(h.chunk)))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r = h.solve_device(0, summary=False)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            seq_ms += e0.elapsed_time(e1)
+            seq_iters += r.iterations["CG"]
+            ref = h.field_summary()
+            worst = max(worst, abs(s[3] / ref[3] - 1.0))
+        finally:
+            h.finalise()
+    return {"metric": "batched_timestep_ms", "value": st.device_ms, "unit": "ms", "higher_is_better": False,
+            "n_gpus": 1, "dtype": "f32 vectors, f64 reductions/solution", "data": "synthetic (seeded tea.in "
+            "generator, batched_2d seed 5)",
+            "config": {"workload": "batched_2d_%d" % len(probs), "problems": len(probs), "cells": cells,
+                       "eps": 1e-12, "graph": bool(st.graph)},
+            "autotuner": tuned, "converged": st.converged, "max_iterations": st.max_iterations,
+            "total_iterations": st.total_iterations, "kernel_iterations": st.kernel_iterations,
+            "max_fp64_rr": float(rr.max()),
+            "sequential_fp64": {"ms": seq_ms, "total_iterations": seq_iters,
+                                "path": "tl2d_solve_step per problem, one after another"},
+            "speedup_vs_sequential": seq_ms / st.device_ms,
+            "temp_max_rel_diff_vs_sequential": worst}
+
+
 def traffic_per_launch(kernel: str, cells: int):
     """DRAM bytes per launch from the committed ncu summary (scaled per cell), if any."""
     p = REPO / "profiles" / "ncu_traffic.json"
@@ -488,8 +541,11 @@ def main():
     ap.add_argument("--refine-size", type=int, default=8192,
                     help="mesh of the FP32-refinement vs FP64 comparison (0: skip)")
     ap.add_argument("--driver", default="device", choices=["device", "run"])
-    ap.add_argument("--workload", default="dropin", choices=["dropin", "adjoint"],
-                    help="dropin: the 2D FP64 drop-in line (default); adjoint: the 3D adjoint form")
+    ap.add_argument("--workload", default="dropin", choices=["dropin", "adjoint", "batch"],
+                    help="dropin: the 2D FP64 drop-in line (default); adjoint: the 3D adjoint form; "
+                         "batch: the batched form")
+    ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--tune-iters", type=int, default=30)
     ap.add_argument("--fd-cells", type=int, default=32)
     ap.add_argument("--adjoint-cpu-size", type=int, default=64)
     ap.add_argument("--e2e-kernel-interface", type=int, default=1)
@@ -498,7 +554,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == "adjoint":
+    if args.workload == "batch":
+        line = bench_batch(args) if rank == 0 else None
+    elif args.workload == "adjoint":
         if args.size == 4096:
             args.size = 256
         line = bench_adjoint(args) if rank == 0 else None
