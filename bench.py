@@ -42,6 +42,8 @@ KERNEL_BYTES_PER_CELL = {
     "k_cg_ur_fused": 48,     # reads u, p, r, w; writes u, r
     "k_cheby_trip": 56,      # reads u, p, u0, kx, ky; writes u, p (w, r only on norm trips)
     "k_ppcg_step": 64,       # reads sd, r, kx, ky, u; writes sd, r, u
+    "k_blocked<cheby>": 56,  # per launch of L Chebyshev trips: reads u, p, u0, kx, ky; writes u, p
+    "k_blocked<ppcg>": 64,   # per launch of L PPCG inner steps: reads sd, r, u, kx, ky; writes sd, r, u
     "k_cg_calc_w": 32, "k_cg_calc_ur": 48, "k_cg_calc_p": 24,
     "k_cheby_sweep": 64, "k_add_p": 24, "k_ppcg_inner_a": 56, "k_ppcg_inner_b": 24,
     "k_norm2": 8, "k_residual": 40,
@@ -180,6 +182,8 @@ def bench_b200(args, rank, world, local_rank):
     lib.tl2d_set_device(local_rank)
     prob = problems.dropin_2d(args.size, seed=2, steps=args.warmup + 2 * args.steps + 8, solver=args.solver)
     h = Host(prob.tea_in(), dims=2)
+    if args.no_temporal_blocking:
+        h.lib.tl2d_set_temporal_blocking(C.byref(h.chunk), 0)
     stream = torch.cuda.ExternalStream(h.lib.tl2d_stream(C.byref(h.chunk)))
     cells = args.size * args.size
     interior_launch_cells = cells
@@ -298,7 +302,7 @@ def bench_b200(args, rank, world, local_rank):
     if dom:
         kname, (kcalls, kms_tot) = dom
         base = kname.split("<")[0]
-        bpc = KERNEL_BYTES_PER_CELL.get(base)
+        bpc = KERNEL_BYTES_PER_CELL.get(kname, KERNEL_BYTES_PER_CELL.get(base))
         if bpc:
             avg_s = kms_tot / kcalls / 1000.0
             achieved = bpc * interior_launch_cells / avg_s / 1e9
@@ -549,6 +553,8 @@ def main():
     ap.add_argument("--fd-cells", type=int, default=32)
     ap.add_argument("--adjoint-cpu-size", type=int, default=64)
     ap.add_argument("--e2e-kernel-interface", type=int, default=1)
+    ap.add_argument("--no-temporal-blocking", action="store_true",
+                    help="Chebyshev/PPCG: one launch per trip instead of shared-memory blocks")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

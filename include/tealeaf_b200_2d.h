@@ -247,6 +247,11 @@ void tl2d_set_device(int device);
 /* The cudaStream_t every kernel of this chunk is issued on (as void*). */
 void* tl2d_stream(Chunk* chunk);
 
+/* Device-resident driver (tl2d_solve_step): run Chebyshev trips and PPCG
+ * inner steps temporally blocked in shared memory (1, the default; results
+ * are bit-identical) or one launch per step (0). */
+void tl2d_set_temporal_blocking(Chunk* chunk, int on);
+
 /* Per-kernel device-time profile (CUDA events around every launch on the
  * chunk's stream, resolved at the next synchronisation): enable/disable,
  * reset, and read entry `index` (returns 0 past the last entry). */

@@ -63,7 +63,8 @@ def _run(cmd):
 
 
 def _deps():
-    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
+    return (list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.h"))
+            + list(INCLUDE.glob("*.h")))
 
 
 def build(verbose: bool = False, force: bool = False):

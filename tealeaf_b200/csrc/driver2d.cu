@@ -17,6 +17,7 @@
 // reference's halo flags (e.g. the halo of u is not refreshed during PPCG).
 //
 // diffuse_overload (2d/application.h:9-11) runs every timestep this way.
+#include "blocked2d.cuh"
 #include "host_maths.hpp"
 #include "suite2d_impl.hpp"
 
@@ -92,6 +93,42 @@ struct Run {
         cudaEventDestroy(ev[0]);
         cudaEventDestroy(ev[1]);
         return read_state();
+    }
+
+    // Launches blocks of trips: block(t) launches the block starting at trip t
+    // and returns its length; batches of about kBatch trips, the done word of
+    // the previous batch looked at while the current one runs. Returns the
+    // state read back and, in `starts`, the first trip of every block launched.
+    template <typename F>
+    DevState loop_blocks(int first_trip, F&& block, std::vector<int>& starts)
+    {
+        cudaEvent_t ev[2];
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+        int t = first_trip, batch = 0;
+        bool pending_prev = false;
+        while (t < prm.max_iters && !tl::failed()) {
+            const int end = std::min(prm.max_iters, t + kBatch);
+            while (t < end) {
+                starts.push_back(t);
+                t += block(t);
+            }
+            cudaEventRecord(ev[batch & 1], s->stream);
+            if (pending_prev) {
+                cudaEventSynchronize(ev[(batch + 1) & 1]);
+                if (*(volatile int*)&s->h_mirror[0]) break;
+            }
+            pending_prev = true;
+            ++batch;
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        return read_state();
+    }
+
+    bool blocking() const
+    {
+        return s->temporal_blocking && fc.l && fc.r && fc.b && fc.t;
     }
 
     // ------------------------------------------------------------- CG phase
@@ -197,14 +234,47 @@ struct Run {
         const double error = s->h_out[0];
         const int est = cheby_est(chunk, error, bb);
         if (stats) stats->est_iters = est;
+        int flips = 1;   // buffer flips of the launches that ran
         if (!st.done) {
             st.est = est;
             write_state(st);
-            st = loop(tt + 1, [&](int t) { trip(t, 0); });
+            if (blocking()) {
+                // trip t takes the norm when nch >= est and (t + 1) % 10 == 0
+                // (FinChebyTrip); a block ends at such a trip, at max_iters or
+                // after kTB trips
+                auto is_norm = [&](int t) { return t - tt + 1 >= est && ((t + 1) % 10) == 0; };
+                const size_t smem = blocked_smem<0>();
+                cudaFuncSetAttribute(k_blocked<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                std::vector<int> starts;
+                st = loop_blocks(tt + 1, [&](int t) {
+                    int L = 1;
+                    while (!(is_norm(t + L - 1) || L == kTB || t + L >= prm.max_iters)) ++L;
+                    const int last = t + L - 1;
+                    const int norm = is_norm(last) ? 1 : 0;
+                    BlockedArgs a{L, t - tt + 1, (norm || last + 1 >= prm.max_iters) ? 1 : 0, 0.0, s->d_cheby_alphas,
+                                  s->d_cheby_betas};
+                    TL_LAUNCH(s, "k_blocked<cheby>", (k_blocked<0><<<blocked_grid(s->g), kTBThreads, smem,
+                                                                      s->stream>>>(
+                                  s->g, a, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->u0, nullptr, chunk->w,
+                                  chunk->r, chunk->kx, chunk->ky, done())));
+                    const FinChebyBlock fin{s->d_state, pc, s->d_mirror, L, norm};
+                    if (norm)
+                        TL_LAUNCH(s, "k_norm2_fin", (k_norm2_fin<<<gi, BX, 0, s->stream>>>(s->g, chunk->r, s->rs,
+                                                                                            done(), fin)));
+                    else
+                        TL_LAUNCH(s, "k_finish_only", (k_finish_only<<<1, 32, 0, s->stream>>>(done(), fin)));
+                    cur ^= 1;
+                    return L;
+                }, starts);
+                for (int t0 : starts) flips += t0 < st.trip ? 1 : 0;
+            } else {
+                st = loop(tt + 1, [&](int t) { trip(t, 0); });
+                flips = st.nch - 1;
+            }
         }
         const int trips = st.nch - 1;           // Chebyshev trips run
-        if (ub[trips & 1] != chunk->u) swap_alt(s, chunk, ALT_U);
-        if (pb[trips & 1] != chunk->p) swap_alt(s, chunk, ALT_P);
+        if (ub[flips & 1] != chunk->u) swap_alt(s, chunk, ALT_U);
+        if (pb[flips & 1] != chunk->p) swap_alt(s, chunk, ALT_P);
         TL_LAUNCH(s, "k_add_p_close", k_add_p_close<<<gi, BX, 0, s->stream>>>(s->g, fc, chunk->u, chunk->p));
         TL_CUDA(cudaStreamSynchronize(s->stream));
         if (stats) stats->cheby_iters = trips;
@@ -242,6 +312,10 @@ struct Run {
         pp_prm.switch_enabled = 0;   // already switched
         FinPpcgW fin_w{s->d_state};
         FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
+        const bool blocked = blocking();
+        const size_t smem = blocked_smem<1>();
+        if (blocked) cudaFuncSetAttribute(k_blocked<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const int inner_flips = blocked ? (ni + kTB - 1) / kTB : ni;   // r/sd buffer flips per outer trip
         auto trip = [&](int t) {
             if (t == tt) {
                 TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gh, BX, 0, s->stream>>>(
@@ -255,6 +329,23 @@ struct Run {
             }
             TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
                           s->g, alpha, chunk->u, pb[pc], rb[rc], chunk->w, s->rs, done(), tl::NoFinish())));
+            if (blocked) {
+                for (int pp0 = 0; pp0 < ni; pp0 += kTB) {
+                    const int L = std::min(kTB, ni - pp0);
+                    const bool last = pp0 + L == ni;
+                    BlockedArgs a{L, pp0, 0, chunk->theta, s->d_cheby_alphas, s->d_cheby_betas};
+                    TL_LAUNCH(s, "k_blocked<ppcg>", (k_blocked<1><<<blocked_grid(s->g), kTBThreads, smem,
+                                                                     s->stream>>>(
+                                  s->g, a, sb[sc], rb[rc], sb[sc ^ 1], rb[rc ^ 1], nullptr, chunk->u, nullptr,
+                                  nullptr, chunk->kx, chunk->ky, done())));
+                    sc ^= 1;
+                    rc ^= 1;
+                    if (last)
+                        TL_LAUNCH(s, "k_norm2_fin", (k_norm2_fin<<<gi, BX, 0, s->stream>>>(s->g, rb[rc], s->rs,
+                                                                                            done(), fin_n)));
+                }
+                return;
+            }
             for (int pp = 0; pp < ni; ++pp) {
                 const bool last = pp == ni - 1;
                 if (pp == 0 && last)
@@ -280,7 +371,7 @@ struct Run {
         st = loop(tt, trip);
         const int outer = st.nch;               // PPCG trips run
         const int pflips = std::max(0, outer - 1);
-        const int rflips = outer * ni;
+        const int rflips = outer * inner_flips;
         if (pb[pflips & 1] != chunk->p) swap_alt(s, chunk, ALT_P);
         if (rb[rflips & 1] != chunk->r) swap_alt(s, chunk, ALT_R);
         if (sb[rflips & 1] != chunk->sd) swap_alt(s, chunk, ALT_SD);

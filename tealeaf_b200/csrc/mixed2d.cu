@@ -156,7 +156,9 @@ int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int
     const Lay L = b.L;
     const dim3 gl = lay_tiles<T>(L);
     s->h_mirror[0] = 0;
-    TL_LAUNCH(s, nm[0], (k_rf_init<T><<<s->sm_count * 4, 256, 0, s->stream>>>(
+    // grid-stride init: as many blocks as the reduction partials hold (3 sums each)
+    const int init_blocks = (int)std::max<long>(1, std::min<long>(s->sm_count * 4L, s->partial_capacity / 3));
+    TL_LAUNCH(s, nm[0], (k_rf_init<T><<<init_blocks, 256, 0, s->stream>>>(
                             s->g.x, s->g.hd, L, chunk->r, chunk->u0, chunk->kx, chunk->ky, b.f[RF_KX], b.f[RF_KY], b.f[RF_R],
                             b.f[RF_P0], b.f[RF_P1], b.f[RF_W], b.f[RF_XS], s->rs,
                             FinMxInit{b.st, rel_tol * rel_tol, 0.0, max_iters, s->d_mirror})));

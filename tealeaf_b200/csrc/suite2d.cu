@@ -148,6 +148,12 @@ void* tl2d_stream(Chunk* chunk)
     return s ? (void*)s->stream : nullptr;
 }
 
+void tl2d_set_temporal_blocking(Chunk* chunk, int on)
+{
+    TlSuite2D* s = suite_of(chunk);
+    if (s) s->temporal_blocking = on != 0;
+}
+
 void tl2d_profile_enable(Chunk* chunk, int on)
 {
     TlSuite2D* s = suite_of(chunk);

@@ -50,6 +50,10 @@ struct TlSuite2D {
     double* d_cheby_betas = nullptr;
     int table_len = 0;
 
+    // Device-resident driver: Chebyshev trips / PPCG inner steps temporally
+    // blocked in shared memory (blocked2d.cuh); off = one launch per step.
+    bool temporal_blocking = true;
+
     // FP32 buffers of the iterative-refinement form (mixed2d.cu), on first use.
     void* mx_slab = nullptr;
     size_t mx_bytes = 0;

@@ -60,3 +60,25 @@ def test_device_driver_memory_state_equals_run_path(solver):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("solver", ["cheby", "ppcg"])
+def test_temporal_blocking_is_bit_identical(solver):
+    """Chebyshev trips / PPCG inner steps run temporally blocked in shared
+    memory give the same memory state, bit for bit, as one launch per step,
+    on a mesh of many tiles with ragged edges."""
+    prob = problems.seeded(2, (203, 141), 17, 5, 2, solver=solver, end_step=2, name="blocked")
+    text = prob.tea_in()
+    a, b = Host(text, 2), Host(text, 2)
+    try:
+        b.lib.tl2d_set_temporal_blocking(b.chunk, 0)
+        for tt in range(2):
+            ra = a.solve_device(tt)
+            rb = b.solve_device(tt)
+            assert ra.iterations == rb.iterations
+            assert ra.summary == rb.summary
+            for f in FIELDS:
+                assert np.array_equal(a.download(f), b.download(f)), (solver, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()
