@@ -27,12 +27,13 @@
 
 namespace tl2d {
 
-constexpr int kTX = 64;                 // tile columns
-constexpr int kTY = 32;                 // tile rows
 constexpr int kTB = 5;                  // most steps per launch
+constexpr int kTW = 64;                 // shared row pitch: one column per thread of a row group
+constexpr int kTH = 48;                 // shared rows
+constexpr int kTX = kTW - 2 * kTB;      // tile columns (54)
+constexpr int kTY = kTH - 2 * kTB;      // tile rows (38)
 constexpr int kTBThreads = 256;
-constexpr int kTW = kTX + 2 * kTB;      // shared row pitch
-constexpr int kTH = kTY + 2 * kTB;      // shared rows
+constexpr int kTRows = kTBThreads / kTW;   // row groups (4): thread = (column, row group)
 
 struct BlockedArgs {
     int steps;          // L <= kTB
@@ -64,23 +65,32 @@ static __global__ void __launch_bounds__(kTBThreads) k_blocked(Geo g, BlockedArg
     const int H = a.steps;
     const int ox = X0 - kTB, oy = Y0 - kTB;   // shared origin
     const int tid = threadIdx.x;
-    auto sidx = [&](int xx, int yy) { return (yy - oy) * kTW + (xx - ox); };
+
+    // Thread (cx, cy): shared column cx of every kTRows-th row from cy; the
+    // region of margin m of this tile is [xl, xh) x [yl, yh).
+    const int cx = tid % kTW, cy = tid / kTW;
+    const int gxc = ox + cx;   // this thread's grid column
+    auto bounds = [&](int m, int& xl, int& xh, int& yl, int& yh) {
+        xl = max(ilo, X0 - m);
+        xh = min(ihi, X1 + m);
+        yl = max(jlo, Y0 - m);
+        yh = min(jhi, Y1 + m);
+    };
+    // first row >= yl of this thread's row group
+    auto first_row = [&](int yl) { return yl + ((cy - (yl - oy)) % kTRows + kTRows) % kTRows; };
 
     // load the region of margin H (interior cells only)
     {
-        const int xl = max(ilo, X0 - H), xh = min(ihi, X1 + H), yl = max(jlo, Y0 - H), yh = min(jhi, Y1 + H);
-        const int wdt = xh - xl, n = wdt * (yh - yl);
-        for (int c = tid; c < n; c += kTBThreads) {
-            const int xx = xl + c % wdt, yy = yl + c / wdt;
-            const long gi = xx + (long)yy * x;
-            As[sidx(xx, yy)] = A_in[gi];
-            Bs[sidx(xx, yy)] = B_in[gi];
-        }
-        if (MODE == 1) {
-            const int tw = X1 - X0, tn = tw * (Y1 - Y0);
-            for (int c = tid; c < tn; c += kTBThreads) {
-                const int xx = X0 + c % tw, yy = Y0 + c / tw;
-                Us[(yy - Y0) * kTX + (xx - X0)] = u[xx + (long)yy * x];
+        int xl, xh, yl, yh;
+        bounds(H, xl, xh, yl, yh);
+        if (gxc >= xl && gxc < xh) {
+            for (int yy = first_row(yl); yy < yh; yy += kTRows) {
+                const long gi = gxc + (long)yy * x;
+                const int s = (yy - oy) * kTW + cx;
+                As[s] = A_in[gi];
+                Bs[s] = B_in[gi];
+                if (MODE == 1 && gxc >= X0 && gxc < X1 && yy >= Y0 && yy < Y1)
+                    Us[(yy - Y0) * kTX + (gxc - X0)] = u[gi];
             }
         }
     }
@@ -88,72 +98,73 @@ static __global__ void __launch_bounds__(kTBThreads) k_blocked(Geo g, BlockedArg
     for (int i = 0; i < H; ++i) {
         // pass A: pointwise over margin H - i
         {
-            const int m = H - i;
-            const int xl = max(ilo, X0 - m), xh = min(ihi, X1 + m), yl = max(jlo, Y0 - m), yh = min(jhi, Y1 + m);
-            const int wdt = xh - xl, n = wdt * (yh - yl);
+            int xl, xh, yl, yh;
+            bounds(H - i, xl, xh, yl, yh);
             double fa = 0.0, fb = 0.0;
             const int pp = a.first + i;
             if (MODE == 1 && pp > 0) {
                 fa = a.alphas[pp - 1];
                 fb = a.betas[pp - 1];
             }
-            for (int c = tid; c < n; c += kTBThreads) {
-                const int s = sidx(xl + c % wdt, yl + c / wdt);
-                if (MODE == 0) As[s] = As[s] + Bs[s];
-                else As[s] = pp == 0 ? Bs[s] / a.theta : fa * As[s] + fb * Bs[s];
+            if (gxc >= xl && gxc < xh) {
+                for (int yy = first_row(yl); yy < yh; yy += kTRows) {
+                    const int s = (yy - oy) * kTW + cx;
+                    if (MODE == 0) As[s] = As[s] + Bs[s];
+                    else As[s] = pp == 0 ? Bs[s] / a.theta : fa * As[s] + fb * Bs[s];
+                }
             }
         }
         __syncthreads();
         // pass B: stencil over margin H - i - 1
         {
-            const int m = H - i - 1;
-            const int xl = max(ilo, X0 - m), xh = min(ihi, X1 + m), yl = max(jlo, Y0 - m), yh = min(jhi, Y1 + m);
-            const int wdt = xh - xl, n = wdt * (yh - yl);
+            int xl, xh, yl, yh;
+            bounds(H - i - 1, xl, xh, yl, yh);
             const bool last = i == H - 1;
             double ca = 0.0, cb = 0.0;
             if (MODE == 0) {
                 ca = a.alphas[a.first + i];
                 cb = a.betas[a.first + i];
             }
-            for (int c = tid; c < n; c += kTBThreads) {
-                const int xx = xl + c % wdt, yy = yl + c / wdt;
-                const int s = sidx(xx, yy);
-                const long gi = xx + (long)yy * x;
-                const double cc = As[s];
-                const double l = xx == ilo ? cc : As[s - 1];
-                const double rr = xx == ihi - 1 ? cc : As[s + 1];
-                const double d = yy == jlo ? cc : As[s - kTW];
-                const double up = yy == jhi - 1 ? cc : As[s + kTW];
-                const double v = smvp(kx[gi], kx[gi + 1], ky[gi], ky[gi + x], cc, l, rr, d, up);
-                const bool in_tile = xx >= X0 && xx < X1 && yy >= Y0 && yy < Y1;
-                if (MODE == 0) {
-                    const double res = u0[gi] - v;
-                    Bs[s] = ca * Bs[s] + cb * res;
-                    if (last && in_tile && a.wr_last) {
-                        w[gi] = v;
-                        r[gi] = res;
+            if (gxc >= xl && gxc < xh) {
+                const bool in_tx = gxc >= X0 && gxc < X1;
+                for (int yy = first_row(yl); yy < yh; yy += kTRows) {
+                    const int s = (yy - oy) * kTW + cx;
+                    const long gi = gxc + (long)yy * x;
+                    const double cc = As[s];
+                    const double l = gxc == ilo ? cc : As[s - 1];
+                    const double rr = gxc == ihi - 1 ? cc : As[s + 1];
+                    const double d = yy == jlo ? cc : As[s - kTW];
+                    const double up = yy == jhi - 1 ? cc : As[s + kTW];
+                    const double v = smvp(__ldg(kx + gi), __ldg(kx + gi + 1), __ldg(ky + gi), __ldg(ky + gi + x), cc,
+                                          l, rr, d, up);
+                    const bool in_tile = in_tx && yy >= Y0 && yy < Y1;
+                    if (MODE == 0) {
+                        const double res = __ldg(u0 + gi) - v;
+                        Bs[s] = ca * Bs[s] + cb * res;
+                        if (last && in_tile && a.wr_last) {
+                            w[gi] = v;
+                            r[gi] = res;
+                        }
+                    } else {
+                        Bs[s] = Bs[s] - v;
+                        if (in_tile) Us[(yy - Y0) * kTX + (gxc - X0)] += cc;
                     }
-                } else {
-                    Bs[s] = Bs[s] - v;
-                    if (in_tile) Us[(yy - Y0) * kTX + (xx - X0)] += cc;
                 }
             }
         }
         __syncthreads();
     }
     // write the tile: A (u, resp. sd) with its reflective depth-1 halo, B (p, resp. r)
-    {
-        const int tw = X1 - X0, tn = tw * (Y1 - Y0);
-        for (int c = tid; c < tn; c += kTBThreads) {
-            const int xx = X0 + c % tw, yy = Y0 + c / tw;
-            const int s = sidx(xx, yy);
-            const long gi = xx + (long)yy * x;
+    if (gxc >= X0 && gxc < X1) {
+        for (int yy = first_row(Y0); yy < Y1; yy += kTRows) {
+            const int s = (yy - oy) * kTW + cx;
+            const long gi = gxc + (long)yy * x;
             const double av = As[s];
             A_out[gi] = av;
             B_out[gi] = Bs[s];
-            if (MODE == 1) u[gi] = Us[(yy - Y0) * kTX + (xx - X0)];
-            if (xx == ilo) A_out[gi - 1] = av;
-            if (xx == ihi - 1) A_out[gi + 1] = av;
+            if (MODE == 1) u[gi] = Us[(yy - Y0) * kTX + (gxc - X0)];
+            if (gxc == ilo) A_out[gi - 1] = av;
+            if (gxc == ihi - 1) A_out[gi + 1] = av;
             if (yy == jlo) A_out[gi - x] = av;
             if (yy == jhi - 1) A_out[gi + x] = av;
         }
