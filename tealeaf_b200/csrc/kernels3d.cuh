@@ -34,20 +34,24 @@ using tl::Scalar;
 #define TL3D_UNROLL 4
 #endif
 #ifndef TL3D_MINB
-#define TL3D_MINB 16
+#define TL3D_MINB 4
 #endif
 #define TL3D_STR(x) #x
 #define TL3D_PRAGMA_UNROLL(n) _Pragma(TL3D_STR(unroll n))
 constexpr unsigned kFull3 = 0xffffffffu;
 
-constexpr int BX = 32;   // x threads per block of an interior sweep (one warp per y row)
-constexpr int BY = 4;    // y threads per block
-constexpr int ZR = 8;    // z cells per thread
+constexpr int BX = 32;   // x threads per block of an interior sweep
+constexpr int BY = 8;    // y threads per block
+#ifndef TL3D_ZR
+#define TL3D_ZR 16
+#endif
+constexpr int ZR = TL3D_ZR;   // default z cells per thread (Geo::zr)
 constexpr int NT = BX * BY;
 constexpr int FBX = 32, FBY = 8;   // full-array kernels
 
 struct Geo {
     int x, y, z, hd;
+    int zr = ZR;   // z cells per thread of the interior sweeps (chosen per chunk)
     __host__ __device__ long xy() const { return (long)x * y; }
 };
 
@@ -81,8 +85,8 @@ struct Pencil {
     {
         k = g.hd + blockIdx.x * BX + threadIdx.x;
         j = g.hd + blockIdx.y * BY + threadIdx.y;
-        i0 = g.hd + blockIdx.z * ZR;
-        i1 = min(i0 + ZR, g.z - g.hd);
+        i0 = g.hd + blockIdx.z * g.zr;
+        i1 = min(i0 + g.zr, g.z - g.hd);
         active = k < g.x - g.hd && j < g.y - g.hd;
     }
 };
@@ -100,8 +104,8 @@ struct PencilC {
         active = rowok && k0 < g.x - g.hd;
         k = min(k0, g.x - g.hd - 1);
         j = min(j0, g.y - g.hd - 1);
-        i0 = g.hd + blockIdx.z * ZR;
-        i1 = min(i0 + ZR, g.z - g.hd);
+        i0 = g.hd + blockIdx.z * g.zr;
+        i1 = min(i0 + g.zr, g.z - g.hd);
         lane = threadIdx.x;
         at_l = k == g.hd;
         at_r = k == g.x - g.hd - 1;
@@ -150,41 +154,109 @@ __device__ __forceinline__ void halo_duty3(const Geo& g, const Faces& fc, int de
     }
 }
 
-// Fused stencil walker: like walk() but with x-neighbours from warp shuffles,
-// clamped lanes, and no halo stores. body(i, centre, smvp, active).
-template <bool REFLECT, typename Cur, typename Body>
-__device__ __forceinline__ void walkc(const Geo& g, const Faces& fc, const PencilC& s,
-                                      const double* __restrict__ raw, const double* __restrict__ kx,
-                                      const double* __restrict__ ky, const double* __restrict__ kz, Cur cur, Body body)
+// Operand planes of the fused sweeps, staged in shared memory: the block's
+// BX x BY cells of the two operand arrays A, B with a one-cell ring (x and y
+// neighbours), and the face coefficients kx (one extra column), ky (one extra
+// row) and kz of one z-plane.
+struct Plane3 {
+    double A[BY + 2][BX + 2];
+    double B[BY + 2][BX + 2];
+    double kx[BY][BX + 1];
+    double ky[BY + 1][BX];
+    double kz[BY][BX];
+};
+constexpr int kStages3 = 4;   // ring of planes: plane ii is computed while ii+1 .. ii+3 are in flight
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
 {
-    const int x = g.x;
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Fused stencil walker. The operand of a cell is comb(A, B) in the interior
+// and A (as stored) in the halo; the depth-1 reflective halo of an external
+// face is applied on the fly with REFLECT. Each thread copies its cell (and,
+// at the block edges, the ring cells, the extra kx column and ky row) of
+// planes i0 .. i1 into a ring of kStages3 shared planes with asynchronous
+// copies (cp.async; the waits are the hardware's wait_group), so three planes
+// are in flight while one is computed from shared memory. Addresses are
+// clamped into the array, so edge blocks load valid memory for cells they do
+// not use. All threads of the block must call it (uniform pencil length).
+// body(ii, i, centre, smvp).
+template <bool REFLECT, typename Comb, typename Body>
+__device__ __forceinline__ void walkc(const Geo& g, const Faces& fc, const PencilC& s, const double* __restrict__ A,
+                                      const double* __restrict__ B, const double* __restrict__ kx,
+                                      const double* __restrict__ ky, const double* __restrict__ kz, Comb comb,
+                                      Body body)
+{
+    __shared__ Plane3 ring[kStages3];
+    const int x = g.x, y = g.y;
     const long xy = g.xy();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int zlast = g.z - g.hd - 1;
+    const int kb = g.hd + blockIdx.x * BX, jb = g.hd + blockIdx.y * BY;   // block origin
+    auto gi = [&](int k, int j, int iz) {
+        k = min(max(k, 0), x - 1);
+        j = min(max(j, 0), y - 1);
+        return (long)k + (long)j * x + (long)iz * xy;
+    };
+    // asynchronous copies of plane iz into ring slot st (coefficients only for computed planes)
+    auto issue = [&](int iz, int st, bool coef) {
+        Plane3& P = ring[st];
+        const int k = kb + tx, j = jb + ty;
+        auto ab = [&](int yy, int xx, long idx) {
+            cp_async8(&P.A[yy][xx], A + idx);
+            if (B) cp_async8(&P.B[yy][xx], B + idx);
+        };
+        ab(ty + 1, tx + 1, gi(k, j, iz));
+        if (tx == 0) ab(ty + 1, 0, gi(k - 1, j, iz));
+        if (tx == BX - 1) ab(ty + 1, BX + 1, gi(k + 1, j, iz));
+        if (ty == 0) ab(0, tx + 1, gi(k, j - 1, iz));
+        if (ty == BY - 1) ab(BY + 1, tx + 1, gi(k, j + 1, iz));
+        cp_async8(&P.kz[ty][tx], kz + gi(k, j, iz));
+        if (coef) {
+            cp_async8(&P.kx[ty][tx], kx + gi(k, j, iz));
+            if (tx == BX - 1) cp_async8(&P.kx[ty][BX], kx + gi(k + 1, j, iz));
+            cp_async8(&P.ky[ty][tx], ky + gi(k, j, iz));
+            if (ty == BY - 1) cp_async8(&P.ky[BY][tx], ky + gi(k, j + 1, iz));
+        }
+    };
+    const int np = s.i1 - s.i0 + 1;   // planes i0 .. i1 (i1: the last plane's front neighbour)
+    for (int q = 0; q < kStages3 - 1; ++q) {
+        if (q < np) issue(s.i0 + q, q, s.i0 + q < s.i1);
+        cp_async_commit();
+    }
     long i = s.k + (long)s.j * x + (long)s.i0 * xy;
-    double c = cur(i);
-    double bk = (s.i0 == g.hd) ? ((REFLECT && fc.k) ? c : raw[i - xy]) : cur(i - xy);
-    double kzc = kz[i];
-    TL3D_PRAGMA_UNROLL(TL3D_UNROLL)
+    double bk = (s.i0 == g.hd) ? 0.0 : comb(A[i - xy], B ? B[i - xy] : 0.0);
+    const bool bk_reflect = s.i0 == g.hd;
+#pragma unroll 1
     for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
-        const bool at_f = ii == g.z - g.hd - 1;
-        const double fr = at_f ? ((REFLECT && fc.f) ? c : raw[i + xy]) : cur(i + xy);
-        const double kxc = kx[i];
-        double l = __shfl_up_sync(kFull3, c, 1);
-        double r = __shfl_down_sync(kFull3, c, 1);
-        double kxr = __shfl_down_sync(kFull3, kxc, 1);
-        if (s.at_l) l = (REFLECT && fc.l) ? c : raw[i - 1];
-        else if (s.lane == 0) l = cur(i - 1);
-        if (s.at_r) r = (REFLECT && fc.r) ? c : raw[i + 1];
-        else if (s.lane == 31) r = cur(i + 1);
-        if (s.at_r || s.lane == 31) kxr = kx[i + 1];
-        const double d = s.at_b ? ((REFLECT && fc.b) ? c : raw[i - x]) : cur(i - x);
-        const double u = s.at_t ? ((REFLECT && fc.t) ? c : raw[i + x]) : cur(i + x);
-        const double kzf = kz[i + xy];
-        const double v = smvp(kxc, kxr, ky[i], ky[i + x], kzc, kzf, c, l, r, d, u, bk, fr);
+        const int q = ii - s.i0;
+        cp_async_wait<kStages3 - 3>();   // planes ii and ii+1 have landed (this thread's copies)
+        __syncthreads();                 // ... everyone's; slot of plane ii-1 is free
+        if (q + kStages3 - 1 < np) issue(ii + kStages3 - 1, (q + kStages3 - 1) % kStages3, ii + kStages3 - 1 < s.i1);
+        cp_async_commit();
+        const Plane3& P = ring[q % kStages3];
+        const Plane3& F = ring[(q + 1) % kStages3];
+        const int cx = tx + 1, cy = ty + 1;
+        auto cell = [&](const Plane3& S, int yy, int xx) { return comb(S.A[yy][xx], B ? S.B[yy][xx] : 0.0); };
+        const double c = cell(P, cy, cx);
+        if (ii == s.i0 && bk_reflect) bk = (REFLECT && fc.k) ? c : A[i - xy];
+        const double l = s.at_l ? ((REFLECT && fc.l) ? c : P.A[cy][cx - 1]) : cell(P, cy, cx - 1);
+        const double r = s.at_r ? ((REFLECT && fc.r) ? c : P.A[cy][cx + 1]) : cell(P, cy, cx + 1);
+        const double d = s.at_b ? ((REFLECT && fc.b) ? c : P.A[cy - 1][cx]) : cell(P, cy - 1, cx);
+        const double u = s.at_t ? ((REFLECT && fc.t) ? c : P.A[cy + 1][cx]) : cell(P, cy + 1, cx);
+        const double fr = ii == zlast ? ((REFLECT && fc.f) ? c : F.A[cy][cx]) : cell(F, cy, cx);
+        const double v = smvp(P.kx[ty][tx], P.kx[ty][tx + 1], P.ky[ty][tx], P.ky[ty + 1][tx], P.kz[ty][tx],
+                              F.kz[ty][tx], c, l, r, d, u, bk, fr);
         body(ii, i, c, v);
         bk = c;
-        c = fr;
-        kzc = kzf;
     }
+    cp_async_wait<0>();
+    __syncthreads();
 }
 
 __device__ __forceinline__ void reflect_store(double* f, const Geo& g, const Faces& fc, int depth, int k, int j,
@@ -253,7 +325,9 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_w(Geo g, Faces fc,
     auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
     if (blockIdx.z + 1 < gridDim.z) {
         const PencilC s(g);
-        walkc<REFLECT>(g, fc, s, p_in, kx, ky, kz, cur, [&](int, long i, double c, double v) {
+        walkc<REFLECT>(g, fc, s, p_in, FUSE_P ? r : nullptr, kx, ky, kz,
+                       [&](double pa, double rb) { return FUSE_P ? bt * pa + rb : pa; },
+                       [&](int, long i, double c, double v) {
             if (s.active) {
                 w[i] = v;
                 acc[0] += v * c;
@@ -269,7 +343,7 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_w(Geo g, Faces fc,
 
 // u += alpha p ; r -= alpha w ; rrn = sum(r r)  (cg_solver.c:134-160)
 template <typename Finish>
-static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_ur(Geo g, Scalar alpha, double* __restrict__ u,
+static __global__ void __launch_bounds__(NT, 8) k3_cg_ur(Geo g, Scalar alpha, double* __restrict__ u,
                                                                 const double* __restrict__ p, double* __restrict__ r,
                                                                 const double* __restrict__ w, ReduceSlots rs,
                                                                 const int* __restrict__ done, Finish fin)
@@ -336,7 +410,9 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cheby_trip(Geo g, Fac
     auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
     if (blockIdx.z + 1 < gridDim.z) {
         const PencilC s(g);
-        walkc<REFLECT>(g, fc, s, u_in, kx, ky, kz, cur, [&](int, long i, double c, double v) {
+        walkc<REFLECT>(g, fc, s, u_in, ADD ? p_in : nullptr, kx, ky, kz,
+                       [&](double ua, double pb) { return ADD ? ua + pb : ua; },
+                       [&](int, long i, double c, double v) {
             if (s.active) {
                 const double rr = u0[i] - v;
                 const double pn = INIT ? rr / theta : a * p_in[i] + b * rr;
@@ -398,7 +474,13 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_ppcg_step(Geo g, Face
     };
     if (blockIdx.z + 1 < gridDim.z) {
         const PencilC s(g);
-        walkc<true>(g, fc, s, sd_in, kx, ky, kz, cur, [&](int, long i, double c, double v) {
+        walkc<true>(g, fc, s, sd_in, FOLD == 0 ? nullptr : r_in, kx, ky, kz,
+                    [&](double sa, double rb) {
+                        if (FOLD == 0) return sa;
+                        if (FOLD == 1) return rb / theta;
+                        return a * sa + b * rb;
+                    },
+                    [&](int, long i, double c, double v) {
             if (s.active) {
                 const double rn = r_in[i] - v;
                 r_out[i] = rn;

@@ -186,6 +186,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     TL_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     if (!TL_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) return;
     s->g = Geo{chunk->x, chunk->y, chunk->z, hd};
+    s->g.zr = choose_zr(chunk->x - 2 * hd, chunk->y - 2 * hd, chunk->z - 2 * hd, s->sm_count);
     const long x = chunk->x, y = chunk->y, z = chunk->z, n = x * y * z;
     const long mi = settings->max_iters > 0 ? settings->max_iters : 1;
     struct Req { double** dst; long count; };

@@ -53,7 +53,30 @@ namespace tl3d {
 TlSuite3D* suite_of(Chunk* chunk);
 inline dim3 interior_grid(const Geo& g)
 {
-    return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, BY), tl::ceil_div(g.z - 2 * g.hd, ZR));
+    return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, BY), tl::ceil_div(g.z - 2 * g.hd, g.zr));
+}
+// z cells per thread of the interior sweeps: the grid should be whole waves
+// both for the staged stencil sweeps (TL3D_MINB blocks per SM) and for the
+// pointwise ones (8 per SM); longer pencils carry less prologue (one extra
+// staged plane per pencil).
+inline int choose_zr(int nx, int ny, int nz, int sm_count)
+{
+    const long bxy = (long)tl::ceil_div(nx, BX) * tl::ceil_div(ny, BY);
+    int best = ZR;
+    double best_score = -1.0;
+    for (int zr = 4; zr <= 32; ++zr) {
+        const long blocks = bxy * tl::ceil_div(nz, zr);
+        auto eff = [&](long slots) {
+            const long waves = (blocks + slots - 1) / slots;
+            return (double)blocks / (double)(waves * slots);
+        };
+        const double score = eff((long)sm_count * TL3D_MINB) * eff((long)sm_count * 8) * zr / (zr + 1.0);
+        if (score > best_score + 1e-12) {
+            best_score = score;
+            best = zr;
+        }
+    }
+    return best;
 }
 inline dim3 full_grid(const Geo& g) { return dim3(tl::ceil_div(g.x, FBX), tl::ceil_div(g.y, FBY), g.z); }
 // Interior grid plus the halo-duty z-plane of the fused sweeps.
