@@ -44,6 +44,10 @@ KERNEL_BYTES_PER_CELL = {
     "k_ppcg_step": 64,       # reads sd, r, kx, ky, u; writes sd, r, u
     "k_blocked<cheby>": 56,  # per launch of L Chebyshev trips: reads u, p, u0, kx, ky; writes u, p
     "k_blocked<ppcg>": 64,   # per launch of L PPCG inner steps: reads sd, r, u, kx, ky; writes sd, r, u
+    "k3_cg_w": 56,           # 3D: reads p_old, r, kx, ky, kz; writes p, w
+    "k3_cg_ur": 48,          # 3D: reads u, p, r, w; writes u, r
+    "k3_cheby_trip": 64,     # 3D: reads u, p, u0, kx, ky, kz; writes u, p
+    "k3_ppcg_step": 72,      # 3D: reads sd, r, u, kx, ky, kz; writes sd, r, u
     "k_cg_calc_w": 32, "k_cg_calc_ur": 48, "k_cg_calc_p": 24,
     "k_cheby_sweep": 64, "k_add_p": 24, "k_ppcg_inner_a": 56, "k_ppcg_inner_b": 24,
     "k_norm2": 8, "k_residual": 40,
@@ -118,10 +122,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_sample(tea_in: str, steps: int, cap: int, threads: int):
+def cpu_reference_sample(tea_in: str, steps: int, cap: int, threads: int, dims: int = 2):
     """Reference omp3 program (stock flags) on this host: per-step (iterations, seconds)."""
     from oracle.oracle import run_reference  # checker/baseline only
-    res = run_reference(tea_in, dims=2, suite="omp3", threads=threads, fast=True, max_iters=cap)
+    res = run_reference(tea_in, dims=dims, suite="omp3", threads=threads, fast=True, max_iters=cap)
     out = []
     for s in res[:steps]:
         it = sum(s.iterations.values())
@@ -358,6 +362,125 @@ def bench_b200(args, rank, world, local_rank):
     return line
 
 
+def bench_dropin3d(args) -> dict:
+    """The 3D FP64 drop-in: device-resident timesteps (tl3d_solve_step) of the
+    seeded 3D case (6 boxes on [0,10]^3, recip-conductivity, eps 1e-15 on
+    sqrt(r.r) as the reference 3D driver tests it), iterations/s; per-kernel
+    breakdown from a second profiled pass; e2e through the C ABI with the
+    step's density/energy uploaded from pinned host memory and the energy read
+    back; the reference omp3 3D program as CPU baseline."""
+    import ctypes as C
+
+    import torch
+
+    from tealeaf_b200 import problems
+    from tealeaf_b200.host import Host
+    n = args.size
+    cells = n ** 3
+    prob = problems.adjoint_3d(n, seed=4, steps=args.warmup + 2 * args.steps + 4).with_(solver=args.solver)
+    h = Host(prob.tea_in(), dims=3)
+    lib = h.lib
+    stream = torch.cuda.ExternalStream(lib.tl3d_stream(C.byref(h.chunk)))
+    tt = 0
+    for _ in range(args.warmup):
+        h.solve_device(tt, summary=False)
+        tt += 1
+    torch.cuda.synchronize()
+
+    def timed(profile):
+        nonlocal tt
+        lib.tl3d_profile_reset(C.byref(h.chunk))
+        lib.tl3d_profile_enable(C.byref(h.chunk), 1 if profile else 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its = 0
+        n0 = lib.tl3d_launch_count(C.byref(h.chunk))
+        e0.record(stream)
+        for _ in range(args.steps):
+            r = h.solve_device(tt, summary=(tt % h.cfg.summary_frequency == 0))
+            its += sum(r.iterations.values())
+            tt += 1
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = lib.tl3d_launch_count(C.byref(h.chunk)) - n0
+        prof, idx = {}, 0
+        name = C.create_string_buffer(128)
+        calls, kms = C.c_longlong(), C.c_double()
+        while profile and lib.tl3d_profile_read(C.byref(h.chunk), idx, name, 128, C.byref(calls), C.byref(kms)):
+            if calls.value:
+                prof[name.value.decode()] = (calls.value, kms.value)
+            idx += 1
+        lib.tl3d_profile_enable(C.byref(h.chunk), 0)
+        return e0.elapsed_time(e1), its, launches, prof
+
+    sampler = ClockSampler(0)
+    with sampler:
+        ms, iters, launches, _ = timed(False)
+    ms_p, iters_p, _, prof = timed(True)
+    value = iters / (ms / 1000.0)
+    peak, peak_kind = measured_peaks()
+    kname, (kc, kms_tot) = max(prof.items(), key=lambda kv: kv[1][1])
+    bpc = KERNEL_BYTES_PER_CELL.get(kname, KERNEL_BYTES_PER_CELL.get(kname.split("<")[0]))
+    roofline = None
+    if bpc:
+        achieved = bpc * cells / (kms_tot / kc / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic_per_launch(kname, cells),
+                    "bytes_per_launch": bpc * cells, "avg_launch_ms": kms_tot / kc,
+                    "timing": "CUDA events around every launch on the suite stream, second timed pass of "
+                              "%d steps (%.1f iter/s with the events in place)" % (args.steps, iters_p / (ms_p / 1e3)),
+                    "peak_source": peak_kind}
+    # e2e: host buffers in, energy out, every step
+    init = Host(prob.tea_in(), dims=3)
+    dens_h = torch.from_numpy(init.download("density")).pin_memory()
+    en_h = torch.from_numpy(init.download("energy")).pin_memory()
+    init.finalise()
+    out_h = torch.empty_like(en_h).pin_memory()
+    nel = dens_h.numel()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    its_e = 0
+    for _ in range(max(1, min(args.steps, args.e2e_steps))):
+        lib.tl3d_upload_field(C.byref(h.chunk), C.byref(h.settings), 1, C.c_void_p(dens_h.data_ptr()), nel)
+        lib.tl3d_upload_field(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(en_h.data_ptr()), nel)
+        r = h.solve_device(0, summary=False)
+        lib.tl3d_download_field(C.byref(h.chunk), C.byref(h.settings), 3, C.c_void_p(out_h.data_ptr()), nel)
+        its_e += sum(r.iterations.values())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e = its_e / (e0.elapsed_time(e1) / 1000.0)
+    h.finalise()
+    tot = sum(v[1] for v in prof.values())
+    line = {
+        "metric": "solver_iterations_per_s", "value": value, "unit": "iter/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tea.in generator, adjoint_3d seed 4)",
+        "config": {"workload": "dropin_3d_%d_%s" % (n, args.solver), "cells": cells, "solver": args.solver,
+                   "eps": prob.eps, "dt": 0.004, "parallelism": "replicas",
+                   "l2": "no flush: working set %.2f GB > 126 MB L2" % (8 * (n + 4) ** 3 * 8 / 1e9),
+                   "driver": "device-resident solver loop (tl3d_solve_step)"},
+        "cells_iterations_per_s": value * cells,
+        "roofline": roofline,
+        "kernels": {k: {"calls": c, "ms": round(m, 3), "share": round(m / tot, 4)}
+                    for k, (c, m) in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e, "unit": "iter/s", "h2d_bytes_per_step": 2 * nel * 8, "d2h_bytes_per_step": nel * 8,
+                "path": "C ABI: tl3d_upload_field -> tl3d_solve_step -> tl3d_download_field"},
+        "clocks": sampler.summary(),
+    }
+    if not args.no_cpu_baseline:
+        try:
+            threads = host_threads()
+            samples = cpu_reference_sample(prob.tea_in(), 2, args.cpu_cap, threads, dims=3)
+            it_s = sum(i for i, _ in samples) / sum(t for _, t in samples)
+            line["cpu_baseline"] = {"value": it_s, "unit": "iter/s", "cores": threads, "kind": "reference",
+                                    "sample": "reference omp3 3D (stock flags), 2 timesteps of the same workload "
+                                              "capped at %d iterations each" % args.cpu_cap}
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    return line
+
+
 def bench_refine(n: int, peak: float) -> dict:
     """The iterative-refinement form against FP64 on identical inputs: one
     timestep of the seeded mixed-precision case (16 rectangles, seed 3), each
@@ -525,7 +648,7 @@ def traffic_per_launch(kernel: str, cells: int):
         return None
     try:
         d = json.loads(p.read_text())
-        per_cell = d["bytes_per_cell"].get(kernel.split("<")[0])
+        per_cell = d["bytes_per_cell"].get(kernel, d["bytes_per_cell"].get(kernel.split("<")[0]))
         return None if per_cell is None else per_cell * cells
     except Exception:
         return None
@@ -545,7 +668,7 @@ def main():
     ap.add_argument("--refine-size", type=int, default=8192,
                     help="mesh of the FP32-refinement vs FP64 comparison (0: skip)")
     ap.add_argument("--driver", default="device", choices=["device", "run"])
-    ap.add_argument("--workload", default="dropin", choices=["dropin", "adjoint", "batch"],
+    ap.add_argument("--workload", default="dropin", choices=["dropin", "dropin3d", "adjoint", "batch"],
                     help="dropin: the 2D FP64 drop-in line (default); adjoint: the 3D adjoint form; "
                          "batch: the batched form")
     ap.add_argument("--batch-count", type=int, default=64)
@@ -562,6 +685,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batch":
         line = bench_batch(args) if rank == 0 else None
+    elif args.workload == "dropin3d":
+        if args.size == 4096:
+            args.size = 256
+        line = bench_dropin3d(args) if rank == 0 else None
     elif args.workload == "adjoint":
         if args.size == 4096:
             args.size = 256
