@@ -178,7 +178,7 @@ def bench_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from tealeaf_b200 import abi, problems
+    from tealeaf_b200 import abi, problems, replicas
     from tealeaf_b200.host import Host
 
     torch.cuda.set_device(local_rank)
@@ -247,15 +247,7 @@ def bench_b200(args, rank, world, local_rank):
     ms_prof, iters_prof, _, prof = timed_pass(True)
 
     # whole-job aggregate: max device time over ranks, iterations summed
-    t = torch.tensor([ms, float(iters)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, iters_all = mx[0].item(), sm[1].item()
-    else:
-        ms_max, iters_all = ms, float(iters)
+    ms_max, iters_all = replicas.aggregate(ms, iters, world)
     value = iters_all / (ms_max / 1000.0)
 
     # e2e through the C ABI with host buffers: every step uploads the step's
@@ -285,13 +277,7 @@ def bench_b200(args, rank, world, local_rank):
             its += sum(r.iterations.values())
         ev[1].record(stream)
         torch.cuda.synchronize()
-        t2 = torch.tensor([ev[0].elapsed_time(ev[1]), float(its)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            mx, sm = t2.clone(), t2.clone()
-            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-            dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-            return sm[1].item() / (mx[0].item() / 1000.0)
-        return t2[1].item() / (t2[0].item() / 1000.0)
+        return replicas.throughput(ev[0].elapsed_time(ev[1]), its, world)
 
     e2e_device = e2e(lambda t: h.solve_device(t, summary=False))
     e2e_kernel_interface = e2e(h.solve) if args.e2e_kernel_interface else None
