@@ -377,11 +377,14 @@ typedef struct TlBatchStats
     double device_ms;       /* device time of the whole batched timestep */
 } TlBatchStats;
 
-/* tile_rows, grid_blocks: 0 for the defaults (16; the co-residency limit). */
+/* tile_rows, grid_blocks: 0 for the defaults (16; the co-residency limit);
+ * tile_rows -1: per-problem heights (see tl2d_batch_tune). */
 TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int tile_rows, int grid_blocks);
 void tl2d_batch_destroy(TlBatch* batch);
-/* Autotuner: times trial_iters iterations of the batch for each tile height
- * in {2,4,8,16,32,64} and persistent grid of {2,4,6,8} blocks per SM and keeps
+/* Autotuner: times trial_iters iterations of the batch (0: the whole solve)
+ * for each tile height in {-1 = per problem, about one tile per block of the
+ * grid, 8..64 rows; 4, 8, 16, 32, 64} and persistent grid of {2,4,6,8} blocks
+ * per SM and keeps
  * the fastest (best_ms: its time). Leaves the energy fields unchanged. */
 int tl2d_batch_tune(TlBatch* batch, int trial_iters, double* best_ms);
 void tl2d_batch_config(TlBatch* batch, int* tile_rows, int* grid_blocks);

@@ -272,13 +272,25 @@ void batch_free(TlBatch* B)
 }
 
 // Lays out the tiles for tile_rows and uploads the problem and tile tables.
+// tile_rows > 0: that height for every problem; tile_rows == kAdaptiveRows:
+// per problem the height that gives it about one tile per block of the
+// persistent grid (between 8 and 64 rows), so a large problem still fills
+// the grid once the small ones have converged.
+constexpr int kAdaptiveRows = -1;
+
 bool batch_layout(TlBatch* B, int tile_rows)
 {
     std::vector<BProb> P(B->count);
     std::vector<int> tp;
     for (int b = 0; b < B->count; ++b) {
         Lay L = B->lay[b];
-        L.rows = tile_rows;
+        if (tile_rows == kAdaptiveRows) {
+            L.rows = 64;
+            const long tx = lay_tiles<float>(L).x;
+            L.rows = (int)std::min<long>(64, std::max<long>(8, (L.ny * tx + B->grid_blocks - 1) / B->grid_blocks));
+        } else {
+            L.rows = tile_rows;
+        }
         B->lay[b] = L;
         const dim3 t = lay_tiles<float>(L);
         BProb& Q = P[b];
@@ -467,7 +479,7 @@ TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int t
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, BX, 0));
     B->max_grid = std::max(1, per_sm) * B->sm_count;
     B->grid_blocks = grid_blocks > 0 ? std::min(grid_blocks, B->max_grid) : B->max_grid;
-    if (!batch_layout(B, tile_rows > 0 ? tile_rows : 16)) {
+    if (!batch_layout(B, tile_rows != 0 ? tile_rows : 16)) {
         batch_free(B);
         return nullptr;
     }
@@ -482,33 +494,35 @@ void tl2d_batch_destroy(TlBatch* B)
 }
 
 // Autotuner: times `trial_iters` iterations of the batch's own CG (setup
-// included, energy untouched) for each tile height in {2, 4, 8, 16, 32, 64}
+// included, energy untouched; 0: the whole solve) for each tile height in
+// {adaptive (-1), 4, 8, 16, 32, 64}
 // and each persistent grid of {2, 4, 6, 8} blocks per SM (within the
 // co-residency limit), and keeps the fastest. Returns 0 or an error code;
 // the choice is readable with tl2d_batch_config.
 int tl2d_batch_tune(TlBatch* B, int trial_iters, double* best_ms)
 {
     if (tl::failed()) return tl::error_state().code;
-    if (!B || trial_iters < 1) {
-        tl::fail(64, "tl2d_batch_tune: batch and trial_iters >= 1 are required");
+    if (!B || trial_iters < 0) {
+        tl::fail(64, "tl2d_batch_tune: batch and trial_iters >= 0 are required");
         return 64;
     }
+    const int iters = trial_iters > 0 ? trial_iters : B->max_iters;   // 0: the whole solve
     drop_graph(B);
-    const int rows_c[] = {2, 4, 8, 16, 32, 64};
+    const int rows_c[] = {kAdaptiveRows, 4, 8, 16, 32, 64};
     const int per_sm_c[] = {2, 4, 6, 8};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double best = 1e300;
     int best_rows = B->tile_rows, best_grid = B->grid_blocks;
-    for (int rows : rows_c) {
-        if (!batch_layout(B, rows)) break;
-        for (int k : per_sm_c) {
-            const int grid = std::min(B->max_grid, k * B->sm_count);
-            B->grid_blocks = grid;
+    for (int k : per_sm_c) {
+        const int grid = std::min(B->max_grid, k * B->sm_count);
+        B->grid_blocks = grid;
+        for (int rows : rows_c) {
+            if (!batch_layout(B, rows)) break;   // the adaptive heights depend on the grid
             for (int rep = 0; rep < 2; ++rep) {   // first run warms up
                 cudaEventRecord(e0, B->stream);
-                issue_step(B, trial_iters, false);
+                issue_step(B, iters, false);
                 cudaEventRecord(e1, B->stream);
                 if (!check_ctl(B, nullptr)) break;
             }
@@ -519,9 +533,8 @@ int tl2d_batch_tune(TlBatch* B, int trial_iters, double* best_ms)
                 best_rows = rows;
                 best_grid = grid;
             }
-            if (grid == B->max_grid) break;
         }
-        if (tl::failed()) break;
+        if (tl::failed() || grid == B->max_grid) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
