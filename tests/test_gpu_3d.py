@@ -226,3 +226,42 @@ def test_3d_reference_host_binary_dropin(name, golden_dir):
         pytest.skip("oracle/_ref/harness3d_b200 not built")
     g = golden(golden_dir)[name]
     compare(run_reference(g["tea_in"], dims=3, suite="b200"), g)
+
+
+FIELDS3 = ("u", "u0", "p", "r", "w", "kx", "ky", "kz", "sd", "energy", "density")
+
+
+@pytest.mark.parametrize("solver", ["cg", "cheby", "ppcg"])
+def test_3d_device_driver_memory_state_equals_run_path(solver):
+    """The device-resident 3D timestep and the run_* path driven like the
+    reference drivers leave every field bit-identical (same sweeps, launch
+    shapes and reduction trees), on a mesh with ragged tiles in x, y and z."""
+    prob = problems.seeded(3, (37, 19, 23), 29, 3, 1, solver=solver, end_step=2, name="state3")
+    text = prob.tea_in()
+    a, b = Host(text, 3), Host(text, 3)
+    try:
+        for tt in range(2):
+            ra = a.solve(tt)
+            rb = b.solve_device(tt)
+            assert ra.iterations == rb.iterations
+            assert ra.summary == rb.summary
+            for f in FIELDS3:
+                assert np.array_equal(a.download(f), b.download(f)), (solver, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()
+
+
+def test_3d_adjoint_rejects_bad_arguments():
+    h = Host(problems.seeded(3, (12, 10, 8), 3, 2, 0, solver="cheby", end_step=1, name="adjbad").tea_in(), 3)
+    try:
+        with pytest.raises(Exception):          # the adjoint differentiates the CG timestep only
+            h.adjoint_gradient(1, 1, [0, 10, 0, 10, 0, 10], 1e-10)
+    finally:
+        h.finalise()
+    h = Host(problems.seeded(3, (12, 10, 8), 3, 2, 0, solver="cg", end_step=1, name="adjbad2").tea_in(), 3)
+    try:
+        with pytest.raises(Exception):          # at least one step
+            h.adjoint_gradient(0, 1, [0, 10, 0, 10, 0, 10], 1e-10)
+    finally:
+        h.finalise()

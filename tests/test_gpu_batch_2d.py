@@ -69,3 +69,12 @@ def test_autotuner_picks_a_candidate_and_step_still_converges():
         assert st.converged == len(probs) and st.tile_rows == cfg["tile_rows"]
     finally:
         b.close()
+
+
+def test_batch_rejects_an_empty_batch():
+    from tealeaf_b200 import abi
+    lib = abi.load(2)
+    handle = lib.tl2d_batch_create(None, None, 0, 0, 0)
+    with pytest.raises(Exception):
+        abi.check(lib, 2)
+    assert not handle
