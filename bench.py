@@ -470,20 +470,25 @@ def bench_dropin3d(args) -> dict:
 def bench_refine(n: int, peak: float) -> dict:
     """The iterative-refinement form against FP64 on identical inputs: one
     timestep of the seeded mixed-precision case (16 rectangles, seed 3), each
-    solved to the relative FP64 residual 1e-10 (tl2d_refine_solve_step)."""
+    solved to the relative FP64 residual 1e-10 (tl2d_refine_solve_step), with
+    CG and with PPCG (presteps 30, 10 inner steps)."""
     from tealeaf_b200 import problems
     from tealeaf_b200.host import Host
     tol = 1e-10
     prob = problems.mixed_2d(n, seed=3, steps=1)
     out = {"workload": "mixed_2d_%d (16 rectangles, seed 3), timestep 1" % n, "rel_tol": tol,
            "metric": "device time of the timestep to rel_tol (ms)"}
-    temps = {}
-    for prec in (64, 32):
-        h = Host(prob.tea_in(), dims=2)
+
+    def run(p, prec):
+        h = Host(p.tea_in(), dims=2)
         try:
-            r = h.refine_step(0, tol, prec)
+            return h.refine_step(0, tol, prec)
         finally:
             h.finalise()
+
+    temps = {}
+    for prec in (64, 32):
+        r = run(prob, prec)
         bpc = 96 if prec == 64 else 48
         gbs = bpc * n * n * r.iterations / (r.device_ms / 1000.0) / 1e9
         out["fp%d" % prec] = {"ms": r.device_ms, "iterations": r.iterations,
@@ -492,6 +497,16 @@ def bench_refine(n: int, peak: float) -> dict:
         temps[prec] = r.summary[3]
     out["time_ratio_fp32_over_fp64"] = out["fp32"]["ms"] / out["fp64"]["ms"]
     out["temp_rel_diff_fp32_vs_fp64"] = temps[32] / temps[64] - 1.0
+    pp = {}
+    for prec in (64, 32):
+        r = run(prob.with_(solver="ppcg"), prec)
+        pp["fp%d" % prec] = {"ms": r.device_ms, "iterations": r.iterations,
+                             "residual_updates": r.residual_updates, "rel_residual": r.rel_residual,
+                             "converged": r.converged}
+        temps["ppcg%d" % prec] = r.summary[3]
+    pp["time_ratio_fp32_over_fp64"] = pp["fp32"]["ms"] / pp["fp64"]["ms"]
+    pp["temp_rel_diff_fp32_vs_fp64_cg"] = temps["ppcg32"] / temps[64] - 1.0
+    out["ppcg"] = pp
     return out
 
 

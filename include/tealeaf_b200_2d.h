@@ -332,24 +332,27 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
 /* Statistics of one iterative-refinement timestep. */
 typedef struct TlRefineStats
 {
-    int iterations;        /* CG iterations */
+    int iterations;        /* CG iterations; for PPCG the CG trips plus the outer PPCG steps */
     int residual_updates;  /* FP64 residual recomputations */
     int converged;         /* 1 when rel_residual <= rel_tol */
-    int pad;
+    int cg_trips;          /* PPCG: CG trips before the switch (CG: equal to iterations) */
     double rel_residual;   /* ||u0 - A u||_2 / ||u0||_2 in FP64 at exit */
     double device_ms;      /* device time of the whole timestep on the chunk stream */
 } TlRefineStats;
 
 /* Iterative-refinement timestep: no counterpart in the reference. Runs the
  * timestep of solve() (2d/diffuse.c:22-80: halos, cg_init, u0 = u, solve,
- * finalise) with the solve replaced by CG to the relative FP64 residual
+ * finalise) with the solve run to the relative FP64 residual
  * ||u0 - A u||_2 / ||u0||_2 <= rel_tol. precision 32: vectors and operator
  * coefficients stored in FP32, FP64 arithmetic and FP64 dot products, the
  * solution accumulated in FP64 with the residual recomputed in FP64 (reliable
- * updates); precision 64: the FP64 sweeps of the drop-in path with the same
- * stop test. Needs one chunk with four external faces; at most
- * settings->max_iters iterations. Returns 0, or an error code with the message
- * available from tl2d_get_error. */
+ * updates); precision 64: the same iteration with FP64 storage. The solve is
+ * CG, or PPCG when settings->solver is TL_PPCG_SOLVER (2d/drivers/ppcg_driver.c:
+ * CG trips to the reference's switch test, Lanczos eigenvalue bounds and
+ * Chebyshev coefficients in FP64 from the FP64 CG scalars, outer steps with
+ * settings->ppcg_inner_steps inner steps). Needs one chunk with four external
+ * faces; at most settings->max_iters iterations. Returns 0, or an error code
+ * with the message available from tl2d_get_error. */
 int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, double rel_tol,
         int precision, TlRefineStats* stats);
 

@@ -110,7 +110,7 @@ class StepStats(C.Structure):
 
 class RefineStats(C.Structure):
     """TlRefineStats of the iterative-refinement timestep."""
-    _fields_ = [("iterations", _i), ("residual_updates", _i), ("converged", _i), ("pad", _i),
+    _fields_ = [("iterations", _i), ("residual_updates", _i), ("converged", _i), ("cg_trips", _i),
                 ("rel_residual", _d), ("device_ms", _d)]
 
 

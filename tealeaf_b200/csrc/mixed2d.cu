@@ -14,6 +14,7 @@
 // last block of each reduction computes alpha, beta and the update/stop
 // decisions; the FP64 fold and residual kernels are launched every trip and
 // return at once unless an update was requested.
+#include "host_maths.hpp"
 #include "refine2d.cuh"
 #include "suite2d_impl.hpp"
 
@@ -49,6 +50,48 @@ __global__ void __launch_bounds__(BX, Pack<T>::MINB) k_rf_ur(Lay L, const MxStat
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
+// Inner step pp < ni - 1 of the PPCG preconditioner z = q(A) r (FOLD 1 for
+// pp == 0: sd = r / theta, z = sd; else FOLD 2 with the coefficients of
+// pp - 1).
+template <typename T, int FOLD>
+__global__ void __launch_bounds__(BX, Pack<T>::MINB - 2) k_rf_pc(Lay L, const MxState* __restrict__ st, double theta,
+                                                               const double* __restrict__ alphas,
+                                                               const double* __restrict__ betas, int pp,
+                                                               const T* __restrict__ sd_in, T* __restrict__ sd_out,
+                                                               const T* __restrict__ s_in, T* __restrict__ s_out,
+                                                               T* __restrict__ z, const T* __restrict__ kx,
+                                                               const T* __restrict__ ky)
+{
+    if (mx_idle(st)) return;
+    const double fa = FOLD == 2 ? alphas[pp - 1] : 0.0, fb = FOLD == 2 ? betas[pp - 1] : 0.0;
+    rf_pc_tile<T, FOLD, FOLD == 2>(L, blockIdx.x, blockIdx.y, theta, fa, fb, sd_in, sd_out, s_in, s_out, z, kx, ky);
+}
+
+// Last inner step (pp = ni - 1) of the preconditioner and r.z -> beta.
+template <typename T, int FOLD>
+__global__ void __launch_bounds__(BX, Pack<T>::MINB - 2) k_rf_pc_last(Lay L, const MxState* __restrict__ st,
+                                                                  double theta, const double* __restrict__ alphas,
+                                                                  const double* __restrict__ betas, int pp,
+                                                                  const T* __restrict__ sd,
+                                                                  const T* __restrict__ s_in, T* __restrict__ z,
+                                                                  const T* __restrict__ r, ReduceSlots rs,
+                                                                  FinPcgZ fin)
+{
+    if (mx_idle(st)) return;
+    const double fa = FOLD == 2 ? alphas[pp - 1] : 0.0, fb = FOLD == 2 ? betas[pp - 1] : 0.0;
+    double acc[1] = {rf_pc_last_tile<T, FOLD>(L, blockIdx.x, blockIdx.y, theta, fa, fb, sd, s_in, z, r)};
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
+// Resumes the iteration after the CG phase stopped for the switch (reason 2).
+__global__ void k_rf_resume(MxState* st)
+{
+    if (threadIdx.x == 0 && st->reason == 2) {
+        st->done = 0;
+        st->reason = 0;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(BX) k_rf_fold(Lay L, const MxState* __restrict__ st, int gx, int hd,
                                                 double* __restrict__ u, T* __restrict__ xs)
@@ -71,7 +114,7 @@ __global__ void __launch_bounds__(BX) k_rf_resid(Lay L, const MxState* __restric
 
 // ------------------------------------------------------------ host side --
 
-enum RfField { RF_KX = 0, RF_KY, RF_P0, RF_P1, RF_W, RF_R, RF_XS, RF_COUNT };
+enum RfField { RF_KX = 0, RF_KY, RF_P0, RF_P1, RF_W, RF_R, RF_XS, RF_SD0, RF_SD1, RF_S0, RF_S1, RF_Z, RF_COUNT };
 
 template <typename T>
 struct RfBuffers {
@@ -80,8 +123,9 @@ struct RfBuffers {
     Lay L;
 };
 
+// The state word and `fields` T arrays in the suite's slab (grown on demand).
 template <typename T>
-RfBuffers<T> rf_buffers(TlSuite2D* s)
+RfBuffers<T> rf_buffers(TlSuite2D* s, int fields)
 {
     constexpr int N = Pack<T>::N;
     RfBuffers<T> b{};
@@ -92,7 +136,7 @@ RfBuffers<T> rf_buffers(TlSuite2D* s)
         if ((long)t.x * t.y * tl::kMaxSums > s->partial_capacity) b.L.rows = s->g.rows;
     }
     const size_t field = ((size_t)b.L.cells() * sizeof(T) + 255) & ~(size_t)255;
-    const size_t need = field * RF_COUNT + 256;
+    const size_t need = 256 + field * fields;
     if (!s->mx_slab || s->mx_bytes < need) {
         if (s->mx_slab) cudaFree(s->mx_slab);
         s->mx_slab = nullptr;
@@ -101,8 +145,9 @@ RfBuffers<T> rf_buffers(TlSuite2D* s)
         s->mx_bytes = need;
     }
     char* base = (char*)s->mx_slab;
-    for (int k = 0; k < RF_COUNT; ++k) b.f[k] = (T*)(base + field * k);
-    b.st = (MxState*)(base + field * RF_COUNT);
+    static_assert(sizeof(MxState) <= 256, "the state word sits in the slab's first 256 bytes");
+    b.st = (MxState*)base;
+    for (int k = 0; k < fields; ++k) b.f[k] = (T*)(base + 256 + field * k);
     return b;
 }
 
@@ -136,13 +181,13 @@ template <typename T>
 struct Names;
 template <>
 struct Names<float> {
-    static constexpr const char* n[5] = {"k_rf_init<f32>", "k_rf_w<f32>", "k_rf_ur<f32>", "k_rf_fold<f32>",
-                                         "k_rf_resid<f32>"};
+    static constexpr const char* n[6] = {"k_rf_init<f32>", "k_rf_w<f32>", "k_rf_ur<f32>", "k_rf_fold<f32>",
+                                         "k_rf_resid<f32>", "k_rf_pc<f32>"};
 };
 template <>
 struct Names<double> {
-    static constexpr const char* n[5] = {"k_rf_init<f64>", "k_rf_w<f64>", "k_rf_ur<f64>", "k_rf_fold<f64>",
-                                         "k_rf_resid<f64>"};
+    static constexpr const char* n[6] = {"k_rf_init<f64>", "k_rf_w<f64>", "k_rf_ur<f64>", "k_rf_fold<f64>",
+                                         "k_rf_resid<f64>", "k_rf_pc<f64>"};
 };
 
 // CG in T storage with FP64 refinement; returns the trips run.
@@ -150,7 +195,7 @@ template <typename T>
 int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int* updates, double* rtrue,
                   double* bb)
 {
-    RfBuffers<T> b = rf_buffers<T>(s);
+    RfBuffers<T> b = rf_buffers<T>(s, RF_SD0);
     if (!b.st) return 0;
     const char* const* nm = Names<T>::n;
     const Lay L = b.L;
@@ -191,6 +236,127 @@ int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int
     return st.trip;
 }
 
+// PPCG in T storage with FP64 refinement. As 2d/drivers/ppcg_driver.c: CG
+// trips recording the FP64 alphas and betas until the reference's switch test
+// holds (more than presteps trips and error < 1, or with error_switch more
+// than 20 trips and error < eps_lim), an FP64 residual replacement on the
+// switch trip (the reference recomputes r = u0 - A u there too), the Lanczos
+// eigenvalue bounds and Chebyshev coefficients of the inner steps on the host
+// in FP64 (eigenvalue_driver.c, cheby_driver.c:163-183). The outer steps then
+// use the inner Chebyshev recurrence (ppcg.c:9-61) as a polynomial
+// preconditioner in standard PCG: z = q(A) r from ppcg_inner_steps steps on
+// A z = r from z = 0, beta = r.z / r.z_old, p = z + beta p, w = A p, alpha =
+// r.z / p.w, u += alpha p, r -= alpha w, with r.r driving the stop test and
+// the residual replacements. (The reference applies the polynomial to u and r
+// themselves and takes beta from r.r; that recurrence drifts from the true
+// residual on ill-conditioned meshes and cannot be refined to a fixed
+// residual.) Returns the trips run (CG + PPCG outer).
+template <typename T>
+int solve_refined_ppcg(TlSuite2D* s, Chunk* chunk, Settings* settings, double rel_tol, int* updates, double* rtrue,
+                       double* bb, int* cg_trips)
+{
+    RfBuffers<T> b = rf_buffers<T>(s, RF_COUNT);
+    if (!b.st) return 0;
+    const char* const* nm = Names<T>::n;
+    const Lay L = b.L;
+    const dim3 gl = lay_tiles<T>(L);
+    const int max_iters = settings->max_iters, ni = settings->ppcg_inner_steps;   // checked by the caller
+    s->h_mirror[0] = 0;
+    const size_t fb = (size_t)L.cells() * sizeof(T);
+    for (int f : {RF_SD0, RF_SD1, RF_S0, RF_S1, RF_Z}) TL_CUDA(cudaMemsetAsync(b.f[f], 0, fb, s->stream));
+    const int init_blocks = (int)std::max<long>(1, std::min<long>(s->sm_count * 4L, s->partial_capacity / 3));
+    TL_LAUNCH(s, nm[0], (k_rf_init<T><<<init_blocks, 256, 0, s->stream>>>(
+                            s->g.x, s->g.hd, L, chunk->r, chunk->u0, chunk->kx, chunk->ky, b.f[RF_KX], b.f[RF_KY],
+                            b.f[RF_R], b.f[RF_P0], b.f[RF_P1], b.f[RF_W], b.f[RF_XS], s->rs,
+                            FinMxInit{b.st, rel_tol * rel_tol, 0.0, max_iters, s->d_mirror})));
+    T* pb[2] = {b.f[RF_P0], b.f[RF_P1]};
+    T* sb[2] = {b.f[RF_SD0], b.f[RF_SD1]};
+    T* qb[2] = {b.f[RF_S0], b.f[RF_S1]};
+    T* const r = b.f[RF_R];
+    T* const z = b.f[RF_Z];
+    int cur = 0;
+    auto fold_resid = [&](double* betas) {
+        TL_LAUNCH(s, nm[3], (k_rf_fold<T><<<gl, BX, 0, s->stream>>>(L, b.st, s->g.x, s->g.hd, chunk->u,
+                                                                     b.f[RF_XS])));
+        TL_LAUNCH(s, nm[4], (k_rf_resid<T><<<gl, BX, 0, s->stream>>>(L, b.st, s->g.x, s->g.hd, chunk->u,
+                                                                      chunk->u0, chunk->kx, chunk->ky, r, s->rs,
+                                                                      FinMxRes{b.st, s->d_mirror, betas})));
+    };
+    auto w_sweep = [&](int t, double* alphas) {
+        if (t == 0) {
+            TL_LAUNCH(s, nm[1], (k_rf_w<T, false><<<gl, BX, 0, s->stream>>>(
+                                    L, b.st, pb[cur], pb[cur], r, b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
+                                    FinMxW{b.st, alphas})));
+        } else {
+            TL_LAUNCH(s, nm[1], (k_rf_w<T, true><<<gl, BX, 0, s->stream>>>(
+                                    L, b.st, pb[cur], pb[cur ^ 1], r, b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
+                                    FinMxW{b.st, alphas})));
+            cur ^= 1;
+        }
+    };
+    // CG trips up to the switch (2d/shared.h:41-42 for the constants)
+    const FinMxUr cg_fin = settings->error_switch
+                               ? FinMxUr{b.st, s->d_mirror, s->d_cg_betas, 20, settings->eps_lim}
+                               : FinMxUr{b.st, s->d_mirror, s->d_cg_betas, settings->presteps, 1.0};
+    batched(s, max_iters, [&](int t) {
+        w_sweep(t, s->d_cg_alphas);
+        TL_LAUNCH(s, nm[2], (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(L, b.st, b.f[RF_XS], pb[cur], r, b.f[RF_W],
+                                                                   s->rs, cg_fin)));
+        fold_resid(s->d_cg_betas);
+    });
+    MxState st{};
+    TL_CUDA(cudaMemcpy(&st, b.st, sizeof(MxState), cudaMemcpyDeviceToHost));
+    *cg_trips = st.trip;
+    if (st.done && st.reason == 2) {
+        // the inner steps' polynomial from the presteps' FP64 Lanczos matrix
+        const int ncg = st.trip;
+        TL_CUDA(cudaMemcpy(chunk->cg_alphas, s->d_cg_alphas, sizeof(double) * ncg, cudaMemcpyDeviceToHost));
+        TL_CUDA(cudaMemcpy(chunk->cg_betas, s->d_cg_betas, sizeof(double) * ncg, cudaMemcpyDeviceToHost));
+        if (!tl::eigen_bounds(chunk, ncg)) return st.trip;
+        tl::cheby_coefs(chunk, ni);
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, chunk->cheby_alphas, sizeof(double) * ni, cudaMemcpyHostToDevice,
+                                s->stream));
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, chunk->cheby_betas, sizeof(double) * ni, cudaMemcpyHostToDevice,
+                                s->stream));
+        const double theta = chunk->theta;
+        TL_LAUNCH(s, "k_rf_resume", (k_rf_resume<<<1, 32, 0, s->stream>>>(b.st)));
+        TL_CUDA(cudaStreamSynchronize(s->stream));
+        s->h_mirror[0] = 0;
+        const double* ca = s->d_cheby_alphas;
+        const double* cb = s->d_cheby_betas;
+        batched(s, max_iters - ncg, [&](int) {
+            // z = q(A) r and beta
+            if (ni == 1) {
+                TL_LAUNCH(s, nm[5], (k_rf_pc_last<T, 1><<<gl, BX, 0, s->stream>>>(
+                                        L, b.st, theta, ca, cb, 0, sb[0], r, z, r, s->rs, FinPcgZ{b.st})));
+            } else {
+                TL_LAUNCH(s, nm[5], (k_rf_pc<T, 1><<<gl, BX, 0, s->stream>>>(L, b.st, theta, ca, cb, 0, sb[1], sb[0],
+                                                                             r, qb[0], z, b.f[RF_KX], b.f[RF_KY])));
+                int c = 0;
+                for (int pp = 1; pp < ni - 1; ++pp, c ^= 1)
+                    TL_LAUNCH(s, nm[5], (k_rf_pc<T, 2><<<gl, BX, 0, s->stream>>>(
+                                            L, b.st, theta, ca, cb, pp, sb[c], sb[c ^ 1], qb[c], qb[c ^ 1], z,
+                                            b.f[RF_KX], b.f[RF_KY])));
+                TL_LAUNCH(s, nm[5], (k_rf_pc_last<T, 2><<<gl, BX, 0, s->stream>>>(
+                                        L, b.st, theta, ca, cb, ni - 1, sb[c], qb[c], z, r, s->rs, FinPcgZ{b.st})));
+            }
+            // p = z + beta p, w = A p, alpha = r.z / p.w
+            TL_LAUNCH(s, nm[1], (k_rf_w<T, true><<<gl, BX, 0, s->stream>>>(
+                                    L, b.st, pb[cur], pb[cur ^ 1], z, b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
+                                    FinMxW{b.st, nullptr, true})));
+            cur ^= 1;
+            TL_LAUNCH(s, nm[2], (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(L, b.st, b.f[RF_XS], pb[cur], r, b.f[RF_W],
+                                                                       s->rs, FinMxUr{b.st, s->d_mirror})));
+            fold_resid(nullptr);
+        });
+        TL_CUDA(cudaMemcpy(&st, b.st, sizeof(MxState), cudaMemcpyDeviceToHost));
+    }
+    *updates = st.updates;
+    *rtrue = st.rtrue;
+    *bb = st.bb;
+    return st.trip;
+}
+
 }  // namespace
 
 extern "C" int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, double rel_tol, int precision,
@@ -216,6 +382,18 @@ extern "C" int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, 
     if (settings->coefficient != TL_CONDUCTIVITY && settings->coefficient != TL_RECIP_CONDUCTIVITY) {
         tl::fail(7, "Coefficient %d is not valid.", settings->coefficient);
         return 7;
+    }
+    if (settings->solver == TL_PPCG_SOLVER) {
+        if (settings->max_iters > s->table_len) {
+            tl::fail(32, "max_iters %d exceeds the %d the chunk was initialised with", settings->max_iters,
+                     s->table_len);
+            return 32;
+        }
+        if (settings->ppcg_inner_steps < 1 || settings->ppcg_inner_steps > s->table_len) {
+            tl::fail(43, "tl2d_refine_solve_step: ppcg_inner_steps %d outside 1..%d", settings->ppcg_inner_steps,
+                     s->table_len);
+            return 43;
+        }
     }
     TlRefineStats local{};
     TlRefineStats* out = stats ? stats : &local;
@@ -243,9 +421,18 @@ extern "C" int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, 
 
     double rtrue = 0.0, bb = 0.0;
     const int max_iters = settings->max_iters;
-    out->iterations = precision == 32
-                          ? solve_refined<float>(s, chunk, max_iters, rel_tol, &out->residual_updates, &rtrue, &bb)
-                          : solve_refined<double>(s, chunk, max_iters, rel_tol, &out->residual_updates, &rtrue, &bb);
+    if (settings->solver == TL_PPCG_SOLVER)
+        out->iterations =
+            precision == 32
+                ? solve_refined_ppcg<float>(s, chunk, settings, rel_tol, &out->residual_updates, &rtrue, &bb,
+                                            &out->cg_trips)
+                : solve_refined_ppcg<double>(s, chunk, settings, rel_tol, &out->residual_updates, &rtrue, &bb,
+                                             &out->cg_trips);
+    else
+        out->iterations = precision == 32
+                              ? solve_refined<float>(s, chunk, max_iters, rel_tol, &out->residual_updates, &rtrue, &bb)
+                              : solve_refined<double>(s, chunk, max_iters, rel_tol, &out->residual_updates, &rtrue, &bb);
+    if (settings->solver != TL_PPCG_SOLVER) out->cg_trips = out->iterations;
     // finalise (solver_methods.c), energy halo as solve_finished_driver
     TL_LAUNCH(s, "k_finalise", k_finalise<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->energy,
                                                                                      chunk->density, chunk->u));

@@ -41,7 +41,9 @@ struct MxState {
     double rref;     // r.r right after the last replacement
     double rtrue;    // FP64 r.r of the last FP64 residual
     double rsloppy;  // r.r of the stored residual when the last update was requested
+    double rz;       // PPCG: r.z of the last preconditioned residual (0 before the first)
     int trip, done, upd, updates, reason, max_iters;
+    int sw;          // the switch to PPCG is due after the pending replacement
 };
 
 __device__ __forceinline__ int vol_read(const int* p) { return *(volatile const int*)p; }
@@ -76,9 +78,10 @@ struct FinMxInit {
         st->tol2bb = abs_eps > 0.0 ? abs_eps : tol2 * t[1];
         st->rtrue = t[2];
         st->rsloppy = t[0];
-        st->pw = st->alpha = st->beta = 0.0;
+        st->pw = st->alpha = st->beta = st->rz = 0.0;
         st->trip = 0;
         st->upd = 0;
+        st->sw = 0;
         st->updates = 0;
         st->max_iters = max_iters;
         st->done = 0;
@@ -94,38 +97,65 @@ struct FinMxInit {
     }
 };
 
-struct FinMxW {   // alpha = rr / pw
+struct FinMxW {   // alpha = rr / pw (PCG: rz / pw) [recorded in alphas[trip]]
     MxState* st;
+    double* alphas = nullptr;
+    bool pcg = false;
     __device__ void operator()(const double* t) const
     {
         st->pw = t[0];
-        st->alpha = st->rr / t[0];
+        st->alpha = (pcg ? st->rz : st->rr) / t[0];
+        if (alphas) alphas[st->trip] = st->alpha;
     }
 };
 
-struct FinMxUr {   // beta = rrn / rr, or request an FP64 residual replacement
+// With sw_after >= 0 the CG-to-PPCG switch test of 2d/drivers/ppcg_driver.c:
+// 27-29 runs on the trips completed and error = rrn (switch once more than
+// sw_after trips ran and rrn < sw_below); a due switch requests a residual
+// replacement, after which FinMxRes stops the CG phase with reason 2.
+struct FinMxUr {   // beta = rrn / rr [recorded in betas[trip]], or request an FP64 residual replacement
     MxState* st;
     int* hm;
+    double* betas = nullptr;
+    int sw_after = -1;
+    double sw_below = 0.0;
     __device__ void operator()(const double* t) const
     {
         const double rrn = t[0];
-        st->trip += 1;
-        const bool upd = rrn < kUpdateDelta * kUpdateDelta * st->rref || rrn <= st->tol2bb ||
+        const int tt = st->trip;
+        st->trip = tt + 1;
+        const bool sw = sw_after >= 0 && st->trip > sw_after && rrn < sw_below;
+        if (sw) st->sw = 1;
+        const bool upd = sw || rrn < kUpdateDelta * kUpdateDelta * st->rref || rrn <= st->tol2bb ||
                          st->trip >= st->max_iters || !(rrn == rrn);
         if (upd) {
             st->upd = 1;
             st->rsloppy = rrn;
+            if (betas) betas[tt] = rrn / st->rr;   // the recurrence's beta for the Lanczos matrix
         } else {
             st->beta = rrn / st->rr;
             st->rr = rrn;
+            if (betas) betas[tt] = st->beta;
         }
         mirror(st, hm);
     }
 };
 
-struct FinMxRes {   // t: r.r (FP64 residual), rT.rT
+// PCG: t = r.z of the new preconditioned residual; beta = rz / rz_old (0 on
+// the first step after the switch, which restarts the directions at p = z).
+struct FinPcgZ {
+    MxState* st;
+    __device__ void operator()(const double* t) const
+    {
+        st->beta = st->rz > 0.0 ? t[0] / st->rz : 0.0;
+        st->rz = t[0];
+    }
+};
+
+struct FinMxRes {   // t: r.r (FP64 residual), rT.rT [beta recorded in betas[trip - 1]]
     MxState* st;
     int* hm;
+    double* betas = nullptr;
     __device__ void operator()(const double* t) const
     {
         st->rtrue = t[0];
@@ -141,6 +171,12 @@ struct FinMxRes {   // t: r.r (FP64 residual), rT.rT
             st->beta = t[1] / st->rr;
             st->rr = t[1];
             st->rref = t[1];
+            if (betas && st->trip > 0) betas[st->trip - 1] = st->beta;
+            if (st->sw) {
+                st->sw = 0;
+                st->done = 1;
+                st->reason = 2;
+            }
         }
         mirror(st, hm);
     }
@@ -345,6 +381,110 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
             }
             st8(xs + i, xv);
             st8(r + i, rv);
+        }
+    }
+    return acc;
+}
+
+// Chebyshev inner step of the PPCG preconditioner over tile (tx, ty): the
+// recurrence of ppcg.c:29-61 applied to A z = r from z = 0 (s: its residual),
+// on the T layout with FP64 arithmetic. sd = fold(sd_in, s_in) (FOLD 1: s /
+// theta; FOLD 2: fa sd + fb s), rounded to T as stored and read at the
+// stencil points; s_out = s_in - A sd; z = sd (ACC false) or z += sd;
+// sd_out = sd.
+template <typename T, int FOLD, bool ACC>
+__device__ __forceinline__ void rf_pc_tile(const Lay& L, int tx, int ty, double theta, double fa, double fb,
+                                           const T* __restrict__ sd_in, T* __restrict__ sd_out,
+                                           const T* __restrict__ s_in, T* __restrict__ s_out, T* __restrict__ z,
+                                           const T* __restrict__ kx, const T* __restrict__ ky)
+{
+    constexpr int N = Pack<T>::N;
+    const Span<N> s(L, tx, ty);
+    auto fold1 = [&](T sdv, T sv) -> T {
+        return FOLD == 1 ? (T)((double)sv / theta) : (T)(fa * (double)sdv + fb * (double)sv);
+    };
+    auto cur = [&](long idx) -> Cells<T> {
+        Cells<T> a = ld(s_in + idx);
+        if (FOLD == 1) {
+#pragma unroll
+            for (int m = 0; m < N; ++m) a.e[m] = fold1(a.e[m], a.e[m]);
+        } else {
+            const Cells<T> d = ld(sd_in + idx);
+#pragma unroll
+            for (int m = 0; m < N; ++m) a.e[m] = fold1(d.e[m], a.e[m]);
+        }
+        return a;
+    };
+    auto cur1 = [&](long idx) -> T { return fold1(FOLD == 1 ? T(0) : sd_in[idx], s_in[idx]); };
+    const long xp = L.xp;
+    long i = (long)(s.j0 + 1) * xp + s.cc;
+    Cells<T> sc = cur(i), sdn = cur(i - xp), kyc = ld(ky + i);
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
+    for (int j = s.j0; j < s.j1; ++j, i += xp) {
+        const Cells<T> su = cur(i + xp), kyu = ld(ky + i + xp), kxc = ld(kx + i);
+        T sl = __shfl_up_sync(kFull, sc.e[N - 1], 1);
+        T sr = __shfl_down_sync(kFull, sc.e[0], 1);
+        T kxr = __shfl_down_sync(kFull, kxc.e[0], 1);
+        if (s.lane == 0) sl = cur1(i - 1);
+        if (s.lane == 31) {
+            sr = cur1(i + N);
+            kxr = kx[i + N];
+        }
+        if (s.any) {
+            const Cells<T> rc = ld(s_in + i);
+            Cells<T> rn, zv;
+            if (ACC) zv = ld(z + i);
+#pragma unroll
+            for (int m = 0; m < N; ++m) {
+                const double c = (double)sc.e[m];
+                const double l = m == 0 ? (double)sl : (double)sc.e[m - 1];
+                const double rr = m == N - 1 ? (double)sr : (double)sc.e[m + 1];
+                const double kr = m == N - 1 ? (double)kxr : (double)kxc.e[m + 1];
+                const double v = smvp((double)kxc.e[m], kr, (double)kyc.e[m], (double)kyu.e[m], c, l, rr,
+                                      (double)sdn.e[m], (double)su.e[m]);
+                rn.e[m] = (T)((double)rc.e[m] - v);
+                zv.e[m] = ACC ? (T)((double)zv.e[m] + c) : sc.e[m];
+            }
+            st8(s_out + i, rn);
+            st8(sd_out + i, sc);
+            st8(z + i, zv);
+        }
+        sdn = sc;
+        sc = su;
+        kyc = kyu;
+    }
+}
+
+// Last inner step of the PPCG preconditioner over tile (tx, ty), cell-local:
+// sd = fold(sd, s) as rf_pc_tile; z = sd (FOLD 1) or z += sd (FOLD 2). Returns
+// this thread's share of sum(r z) over the stored values.
+template <typename T, int FOLD>
+__device__ __forceinline__ double rf_pc_last_tile(const Lay& L, int tx, int ty, double theta, double fa, double fb,
+                                                  const T* __restrict__ sd, const T* __restrict__ s_in,
+                                                  T* __restrict__ z, const T* __restrict__ r)
+{
+    constexpr int N = Pack<T>::N;
+    const Span<N> s(L, tx, ty);
+    double acc = 0.0;
+    if (s.any) {
+        long i = (long)(s.j0 + 1) * L.xp + s.c0;
+TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
+        for (int j = s.j0; j < s.j1; ++j, i += L.xp) {
+            const Cells<T> sv = ld(s_in + i), rv = ld(r + i);
+            Cells<T> zv;
+            Cells<T> dv;
+            if (FOLD == 2) {
+                zv = ld(z + i);
+                dv = ld(sd + i);
+            }
+#pragma unroll
+            for (int m = 0; m < N; ++m) {
+                const T d = FOLD == 1 ? (T)((double)sv.e[m] / theta)
+                                      : (T)(fa * (double)dv.e[m] + fb * (double)sv.e[m]);
+                zv.e[m] = FOLD == 1 ? d : (T)((double)zv.e[m] + (double)d);
+                if (s.c0 + m < L.nx) acc += (double)rv.e[m] * (double)zv.e[m];
+            }
+            st8(z + i, zv);
         }
     }
     return acc;

@@ -60,6 +60,7 @@ class RefineResult:
     rel_residual: float = 0.0
     device_ms: float = 0.0
     summary: List[float] = field(default_factory=list)      # vol, mass, ie, temp
+    cg_trips: int = 0      # PPCG: CG trips before the switch (CG: all of them)
 
 
 class DriverError(RuntimeError):
@@ -503,7 +504,8 @@ class Host:
     # -- iterative-refinement timestep (tl2d_refine_solve_step) -------------------------
     def refine_step(self, tt: int, rel_tol: float, precision: int, summary: bool = True) -> RefineResult:
         """One timestep whose solve stops at ||u0 - A u|| / ||u0|| <= rel_tol (FP64
-        residual); precision 32 = FP32-stored CG with FP64 refinement, 64 = FP64 CG."""
+        residual); precision 32 = FP32-stored CG (or PPCG when the deck selects it) with FP64
+        refinement, 64 = the same iteration with FP64 storage."""
         if self.dims != 2:
             raise DriverError("the refinement form is 2D")
         st = abi.RefineStats()
@@ -512,7 +514,8 @@ class Host:
         abi.check(self.lib, self.dims)
         if rc:
             raise DriverError("tl2d_refine_solve_step returned %d" % rc)
-        res = RefineResult(st.iterations, st.residual_updates, bool(st.converged), st.rel_residual, st.device_ms)
+        res = RefineResult(st.iterations, st.residual_updates, bool(st.converged), st.rel_residual, st.device_ms,
+                           cg_trips=st.cg_trips)
         if summary:
             res.summary = self.field_summary()
         return res

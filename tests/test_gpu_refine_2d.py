@@ -75,3 +75,47 @@ def test_refine_rejects_bad_arguments():
             h.refine_step(0, REL_TOL, 16)
     finally:
         h.finalise()
+
+
+# Forward-error bound of a solve stopped at relative residual REL_TOL:
+# |du|/|u| <= cond(A) * REL_TOL. The oracle's PPCG run of this deck estimates
+# eigmax / eigmin = 672 / 1.18 (Lanczos, with the 5% margins), so cond < 600.
+TEMP_RTOL_BOUND = 600 * REL_TOL
+
+
+def _ppcg_problem(steps=3, **kw):
+    return _problem(steps=steps).with_(solver="ppcg", name="refine_ppcg_small", **kw)
+
+
+@pytest.mark.parametrize("precision,inner,error_switch", [(64, 10, False), (32, 10, False), (32, 1, False),
+                                                          (64, 10, True)])
+def test_refined_ppcg_reaches_residual_and_matches_oracle(precision, inner, error_switch, oracle_steps):
+    """PPCG with FP64 refinement converges to the same solution as the oracle's
+    tight CG (same operator), in fewer outer steps than CG takes trips."""
+    p = _ppcg_problem(ppcg_inner_steps=inner, presteps=10, error_switch=error_switch)
+    h, c = Host(p.tea_in(), 2), Host(_problem().tea_in(), 2)
+    try:
+        for tt, ref in enumerate(oracle_steps):
+            r = h.refine_step(tt, REL_TOL, precision)
+            rc = c.refine_step(tt, REL_TOL, precision, summary=False)
+            assert r.converged, (precision, inner, tt, r)
+            assert 0.0 < r.rel_residual <= REL_TOL
+            assert r.residual_updates >= 1
+            vol, mass, ie, temp = r.summary
+            assert vol == ref.summary[0] and mass == ref.summary[1]
+            assert abs(temp / ref.summary[3] - 1.0) < TEMP_RTOL_BOUND, (precision, inner, tt, temp, ref.summary[3])
+            if inner == 10:
+                # ten inner steps per outer step: far fewer outer steps than CG trips
+                assert r.iterations < 0.6 * rc.iterations, (r.iterations, rc.iterations)
+    finally:
+        h.finalise()
+        c.finalise()
+
+
+def test_refined_ppcg_rejects_bad_inner_steps():
+    h = Host(_ppcg_problem(steps=1, ppcg_inner_steps=0).tea_in(), 2)
+    try:
+        with pytest.raises(Exception):
+            h.refine_step(0, REL_TOL, 32)
+    finally:
+        h.finalise()
