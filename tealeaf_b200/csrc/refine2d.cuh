@@ -386,12 +386,20 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
     return acc;
 }
 
+// The operator in T arithmetic (the order of smvp).
+template <typename T>
+__device__ __forceinline__ T smvp_t(T kxc, T kxr, T kyc, T kyu, T c, T l, T r, T d, T u)
+{
+    return (T(1) + (kxr + kxc) + (kyu + kyc)) * c - (kxr * r + kxc * l) - (kyu * u + kyc * d);
+}
+
 // Chebyshev inner step of the PPCG preconditioner over tile (tx, ty): the
 // recurrence of ppcg.c:29-61 applied to A z = r from z = 0 (s: its residual),
-// on the T layout with FP64 arithmetic. sd = fold(sd_in, s_in) (FOLD 1: s /
-// theta; FOLD 2: fa sd + fb s), rounded to T as stored and read at the
-// stencil points; s_out = s_in - A sd; z = sd (ACC false) or z += sd;
-// sd_out = sd.
+// on the T layout in T arithmetic (the preconditioner only steers the
+// iteration; the dot products, the solution and the residual replacements
+// stay FP64). sd = fold(sd_in, s_in) (FOLD 1: s / theta; FOLD 2: fa sd +
+// fb s), read at the stencil points; s_out = s_in - A sd; z = sd (ACC false)
+// or z += sd; sd_out = sd.
 template <typename T, int FOLD, bool ACC>
 __device__ __forceinline__ void rf_pc_tile(const Lay& L, int tx, int ty, double theta, double fa, double fb,
                                            const T* __restrict__ sd_in, T* __restrict__ sd_out,
@@ -400,9 +408,8 @@ __device__ __forceinline__ void rf_pc_tile(const Lay& L, int tx, int ty, double 
 {
     constexpr int N = Pack<T>::N;
     const Span<N> s(L, tx, ty);
-    auto fold1 = [&](T sdv, T sv) -> T {
-        return FOLD == 1 ? (T)((double)sv / theta) : (T)(fa * (double)sdv + fb * (double)sv);
-    };
+    const T th = (T)theta, ta = (T)fa, tb = (T)fb;
+    auto fold1 = [&](T sdv, T sv) -> T { return FOLD == 1 ? sv / th : ta * sdv + tb * sv; };
     auto cur = [&](long idx) -> Cells<T> {
         Cells<T> a = ld(s_in + idx);
         if (FOLD == 1) {
@@ -436,14 +443,13 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
             if (ACC) zv = ld(z + i);
 #pragma unroll
             for (int m = 0; m < N; ++m) {
-                const double c = (double)sc.e[m];
-                const double l = m == 0 ? (double)sl : (double)sc.e[m - 1];
-                const double rr = m == N - 1 ? (double)sr : (double)sc.e[m + 1];
-                const double kr = m == N - 1 ? (double)kxr : (double)kxc.e[m + 1];
-                const double v = smvp((double)kxc.e[m], kr, (double)kyc.e[m], (double)kyu.e[m], c, l, rr,
-                                      (double)sdn.e[m], (double)su.e[m]);
-                rn.e[m] = (T)((double)rc.e[m] - v);
-                zv.e[m] = ACC ? (T)((double)zv.e[m] + c) : sc.e[m];
+                const T c = sc.e[m];
+                const T l = m == 0 ? sl : sc.e[m - 1];
+                const T rr = m == N - 1 ? sr : sc.e[m + 1];
+                const T kr = m == N - 1 ? kxr : kxc.e[m + 1];
+                const T v = smvp_t<T>(kxc.e[m], kr, kyc.e[m], kyu.e[m], c, l, rr, sdn.e[m], su.e[m]);
+                rn.e[m] = rc.e[m] - v;
+                zv.e[m] = ACC ? zv.e[m] + c : c;
             }
             st8(s_out + i, rn);
             st8(sd_out + i, sc);
@@ -456,8 +462,9 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
 }
 
 // Last inner step of the PPCG preconditioner over tile (tx, ty), cell-local:
-// sd = fold(sd, s) as rf_pc_tile; z = sd (FOLD 1) or z += sd (FOLD 2). Returns
-// this thread's share of sum(r z) over the stored values.
+// sd = fold(sd, s) as rf_pc_tile; z = sd (FOLD 1) or z += sd (FOLD 2), in T
+// arithmetic. Returns this thread's share of sum(r z) over the stored values,
+// accumulated in FP64.
 template <typename T, int FOLD>
 __device__ __forceinline__ double rf_pc_last_tile(const Lay& L, int tx, int ty, double theta, double fa, double fb,
                                                   const T* __restrict__ sd, const T* __restrict__ s_in,
@@ -465,6 +472,7 @@ __device__ __forceinline__ double rf_pc_last_tile(const Lay& L, int tx, int ty, 
 {
     constexpr int N = Pack<T>::N;
     const Span<N> s(L, tx, ty);
+    const T th = (T)theta, ta = (T)fa, tb = (T)fb;
     double acc = 0.0;
     if (s.any) {
         long i = (long)(s.j0 + 1) * L.xp + s.c0;
@@ -479,9 +487,8 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
             }
 #pragma unroll
             for (int m = 0; m < N; ++m) {
-                const T d = FOLD == 1 ? (T)((double)sv.e[m] / theta)
-                                      : (T)(fa * (double)dv.e[m] + fb * (double)sv.e[m]);
-                zv.e[m] = FOLD == 1 ? d : (T)((double)zv.e[m] + (double)d);
+                const T d = FOLD == 1 ? sv.e[m] / th : ta * dv.e[m] + tb * sv.e[m];
+                zv.e[m] = FOLD == 1 ? d : zv.e[m] + d;
                 if (s.c0 + m < L.nx) acc += (double)rv.e[m] * (double)zv.e[m];
             }
             st8(z + i, zv);
