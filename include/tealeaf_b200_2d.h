@@ -249,7 +249,9 @@ void* tl2d_stream(Chunk* chunk);
 
 /* Device-resident driver (tl2d_solve_step): run Chebyshev trips and PPCG
  * inner steps temporally blocked in shared memory (1, the default; results
- * are bit-identical) or one launch per step (0). */
+ * are bit-identical) or one launch per step (0). The same switch selects the
+ * blocked preconditioner of the refinement form's PPCG (tl2d_refine_solve_step;
+ * its fields are bit-identical, its r.z is summed over another partition). */
 void tl2d_set_temporal_blocking(Chunk* chunk, int on);
 
 /* Per-kernel device-time profile (CUDA events around every launch on the

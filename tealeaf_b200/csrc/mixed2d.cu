@@ -15,6 +15,7 @@
 // decisions; the FP64 fold and residual kernels are launched every trip and
 // return at once unless an update was requested.
 #include "host_maths.hpp"
+#include "pcblock2d.cuh"
 #include "refine2d.cuh"
 #include "suite2d_impl.hpp"
 
@@ -236,6 +237,20 @@ int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int
     return st.trip;
 }
 
+// One launch of the blocked preconditioner (pcblock2d.cuh).
+template <typename T, bool FIRST, bool LAST>
+void pc_launch(TlSuite2D* s, dim3 grid, const PcArgs& a, const RfBuffers<T>& b, const T* sd_in, const T* s_in,
+               T* sd_out, T* s_out, T* z, const T* r)
+{
+    static const char* const name = sizeof(T) == 4 ? "k_rf_pc_blocked<f32>" : "k_rf_pc_blocked<f64>";
+    constexpr size_t smem = pc_smem<T>();
+    TL_CUDA(cudaFuncSetAttribute(k_rf_pc_blocked<T, FIRST, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    TL_LAUNCH(s, name, (k_rf_pc_blocked<T, FIRST, LAST><<<grid, kPcThreads, smem, s->stream>>>(
+                           b.L, b.st, a, sd_in, s_in, sd_out, s_out, z, b.f[RF_KX], b.f[RF_KY], r, s->rs,
+                           FinPcgZ{b.st})));
+}
+
 // PPCG in T storage with FP64 refinement. As 2d/drivers/ppcg_driver.c: CG
 // trips recording the FP64 alphas and betas until the reference's switch test
 // holds (more than presteps trips and error < 1, or with error_switch more
@@ -324,11 +339,33 @@ int solve_refined_ppcg(TlSuite2D* s, Chunk* chunk, Settings* settings, double re
         s->h_mirror[0] = 0;
         const double* ca = s->d_cheby_alphas;
         const double* cb = s->d_cheby_betas;
+        // the blocked preconditioner reduces r.z with one partial per tile
+        const dim3 pg = pc_grid(L);
+        const bool blocked = s->temporal_blocking && (long)pg.x * pg.y <= s->partial_capacity;
         batched(s, max_iters - ncg, [&](int) {
             // z = q(A) r and beta
             if (ni == 1) {
                 TL_LAUNCH(s, nm[5], (k_rf_pc_last<T, 1><<<gl, BX, 0, s->stream>>>(
                                         L, b.st, theta, ca, cb, 0, sb[0], r, z, r, s->rs, FinPcgZ{b.st})));
+            } else if (blocked) {
+                // ni - 1 stencil steps in launches of up to kPcMax, the last one with the final fold and r.z
+                int c = 0;
+                for (int pp = 0; pp < ni - 1;) {
+                    const int h = std::min(kPcMax, ni - 1 - pp);
+                    const PcArgs pa{h, pp, theta, ca, cb};
+                    const bool first = pp == 0, last = pp + h == ni - 1;
+                    const T* s_in = first ? r : qb[c];
+                    if (first && last)
+                        pc_launch<T, true, true>(s, pg, pa, b, sb[c], s_in, sb[c ^ 1], qb[c ^ 1], z, r);
+                    else if (first)
+                        pc_launch<T, true, false>(s, pg, pa, b, sb[c], s_in, sb[c ^ 1], qb[c ^ 1], z, r);
+                    else if (last)
+                        pc_launch<T, false, true>(s, pg, pa, b, sb[c], s_in, sb[c ^ 1], qb[c ^ 1], z, r);
+                    else
+                        pc_launch<T, false, false>(s, pg, pa, b, sb[c], s_in, sb[c ^ 1], qb[c ^ 1], z, r);
+                    c ^= 1;
+                    pp += h;
+                }
             } else {
                 TL_LAUNCH(s, nm[5], (k_rf_pc<T, 1><<<gl, BX, 0, s->stream>>>(L, b.st, theta, ca, cb, 0, sb[1], sb[0],
                                                                              r, qb[0], z, b.f[RF_KX], b.f[RF_KY])));

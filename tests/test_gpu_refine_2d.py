@@ -119,3 +119,26 @@ def test_refined_ppcg_rejects_bad_inner_steps():
             h.refine_step(0, REL_TOL, 32)
     finally:
         h.finalise()
+
+
+@pytest.mark.parametrize("precision,inner", [(32, 2), (32, 6), (32, 7), (32, 12), (64, 10)])
+def test_blocked_preconditioner_matches_one_step_chain(precision, inner):
+    """The temporally blocked preconditioner (up to 5 inner steps per launch)
+    against one launch per inner step. The fields are the same operations in
+    the same order; only r.z is summed over another partition, so the runs
+    may part in the last bits of beta: same CG phase, outer steps within 2,
+    both at the residual bound, temp within TEMP_RTOL of each other."""
+    p = _ppcg_problem(ppcg_inner_steps=inner, presteps=10)
+    a, b = Host(p.tea_in(), 2), Host(p.tea_in(), 2)
+    try:
+        b.lib.tl2d_set_temporal_blocking(b.chunk, 0)
+        for tt in range(3):
+            ra = a.refine_step(tt, REL_TOL, precision)
+            rb = b.refine_step(tt, REL_TOL, precision)
+            assert ra.converged and rb.converged
+            assert ra.cg_trips == rb.cg_trips
+            assert abs(ra.iterations - rb.iterations) <= 2, (ra.iterations, rb.iterations)
+            assert abs(ra.summary[3] / rb.summary[3] - 1.0) < TEMP_RTOL
+    finally:
+        a.finalise()
+        b.finalise()
