@@ -4,18 +4,19 @@
 // z = q(A) r takes ppcg_inner_steps Chebyshev steps on A z = r from z = 0
 // (ppcg.c:29-61): ni - 1 stencil steps and a final cell-local fold. Between
 // the dot products of the outer PCG step nothing global happens, so up to
-// kPcMax stencil steps run in one launch: a block loads a 64 x 64 region (its
-// 54 x 54 tile plus a halo of `steps` cells) and keeps it on chip, each
-// thread holding a column segment of 16 rows in registers (sd, s, z) with
-// the face coefficients and the folded sd of the current step in shared
-// memory; the valid region shrinks by one cell per side and step, and the
-// tile is written back once. Cells outside the interior hold 0 and stay 0
-// (their face coefficients are 0, as in the T layout). Every tile cell goes
-// through the operations of k_rf_pc / k_rf_pc_last in the same order and
-// precision, so the fields are bit-identical to the one-step chain; with
-// `last` the launch also applies the final fold and sums r.z over its tile
-// (a different partition from k_rf_pc_last: the sum may differ in the last
-// bits).
+// kPcMax stencil steps run in one launch: a block takes a 64 x 64 region (its
+// 54 x 54 tile plus a halo of `steps` cells) on chip, each thread holding a
+// column segment of 16 rows in registers (sd, s, z and the face
+// coefficients); only the folded sd of the current step goes through shared
+// memory (two buffers, alternating by step, one barrier per step), for the
+// neighbours in other warps and segments. The valid region shrinks by one
+// cell per side and step, and the tile is written back once. Cells outside
+// the interior hold 0 and stay 0 (their face coefficients are 0, as in the T
+// layout). Every tile cell goes through the operations of k_rf_pc /
+// k_rf_pc_last (pc_fold, pc_op) in the same order and precision, so the
+// fields are bit-identical to the one-step chain; with `last` the launch also
+// applies the final fold and sums r.z over its tile (a different partition
+// from k_rf_pc_last: the sum may differ in the last bits).
 #pragma once
 
 #include "refine2d.cuh"
@@ -40,11 +41,11 @@ struct PcArgs {
     const double* betas;
 };
 
-// A0, A1 (the folded sd, alternating by step), KX, KY: kPcH x kPcW each.
+// A0, A1: the folded sd, alternating by step, kPcH x kPcW each.
 template <typename T>
 constexpr size_t pc_smem()
 {
-    return sizeof(T) * 4 * kPcH * kPcW;
+    return sizeof(T) * 2 * kPcH * kPcW;
 }
 
 inline dim3 pc_grid(const Lay& L) { return dim3(tl::ceil_div(L.nx, kPcX), tl::ceil_div(L.ny, kPcY)); }
@@ -56,18 +57,15 @@ inline dim3 pc_grid(const Lay& L) { return dim3(tl::ceil_div(L.nx, kPcX), tl::ce
 // and z. sd_out / s_out must not alias sd_in / s_in (neighbouring tiles read
 // the halo of the inputs); z is read and written at tile cells only.
 template <typename T, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(kPcThreads) k_rf_pc_blocked(Lay L, const MxState* __restrict__ st, PcArgs a,
-                                                              const T* __restrict__ sd_in,
-                                                              const T* __restrict__ s_in, T* __restrict__ sd_out,
-                                                              T* __restrict__ s_out, T* __restrict__ z,
-                                                              const T* __restrict__ kx, const T* __restrict__ ky,
-                                                              const T* __restrict__ r, ReduceSlots rs, FinPcgZ fin)
+__global__ void __launch_bounds__(kPcThreads, sizeof(T) == 4 ? 2 : 1)
+    k_rf_pc_blocked(Lay L, const MxState* __restrict__ st, PcArgs a, const T* __restrict__ sd_in,
+                    const T* __restrict__ s_in, T* __restrict__ sd_out, T* __restrict__ s_out, T* __restrict__ z,
+                    const T* __restrict__ kx, const T* __restrict__ ky, const T* __restrict__ r, ReduceSlots rs,
+                    FinPcgZ fin)
 {
     extern __shared__ __align__(16) unsigned char pc_raw[];
     T* const A0 = reinterpret_cast<T*>(pc_raw);
     T* const A1 = A0 + kPcH * kPcW;
-    T* const Ks = A1 + kPcH * kPcW;
-    T* const Ys = Ks + kPcH * kPcW;
     if (mx_idle(st)) return;
     const int tid = threadIdx.x, cx = tid % kPcW, cy = tid / kPcW, lane = tid & 31;
     const int X0 = blockIdx.x * kPcX, Y0 = blockIdx.y * kPcY;
@@ -77,35 +75,29 @@ __global__ void __launch_bounds__(kPcThreads) k_rf_pc_blocked(Lay L, const MxSta
     const int H = a.steps;
     const bool colin = gx >= 0 && gx < L.nx;
     const int mxc = max(max(kPcMax - cx, cx - (kPcMax + kPcX - 1)), 0);   // column distance outside the tile
+    // the one neighbour column of this warp held by another warp (none at the region's edges)
+    const bool hi_half = cx >= 32;
+    const int edge_lane = hi_half ? 0 : 31, edge_dx = hi_half ? -1 : 1;
 
-    T av[kPcSeg], bv[kPcSeg], zv[kPcSeg];
+    T av[kPcSeg], bv[kPcSeg], zv[kPcSeg], kxc[kPcSeg], kxr[kPcSeg], kyc[kPcSeg + 1];
 #pragma unroll
-    for (int k = 0; k < kPcSeg; ++k) {
+    for (int k = 0; k <= kPcSeg; ++k) {
         const int ry = r0 + k, gy = oy + ry;
         const int my = max(max(kPcMax - ry, ry - (kPcMax + kPcY - 1)), 0);
         const bool in = colin && gy >= 0 && gy < L.ny && max(mxc, my) <= H;
-        const bool tile = in && mxc == 0 && my == 0;
         const long gi = (long)(gy + 1) * L.xp + gx;
+        kyc[k] = in ? ky[gi] : T(0);   // k == kPcSeg: ky_u of the segment's top row
+        if (k == kPcSeg) break;
+        const bool tile = in && mxc == 0 && my == 0;
         av[k] = (!FIRST && in) ? sd_in[gi] : T(0);
         bv[k] = in ? s_in[gi] : T(0);
         zv[k] = (!FIRST && tile) ? z[gi] : T(0);
-        Ks[ry * kPcW + cx] = in ? kx[gi] : T(0);
-        Ys[ry * kPcW + cx] = in ? ky[gi] : T(0);
+        kxc[k] = in ? kx[gi] : T(0);
+        kxr[k] = in ? kx[gi + 1] : T(0);
     }
     const T th = (T)a.theta;
-    for (int i = 0; i < H; ++i) {
-        const int pp = a.first + i;
-        T* const As = (i & 1) ? A1 : A0;
-        const bool init = FIRST && i == 0;
-        const T fa = pp > 0 ? (T)a.alphas[pp - 1] : T(0), fb = pp > 0 ? (T)a.betas[pp - 1] : T(0);
-        // fold, pointwise
-#pragma unroll
-        for (int k = 0; k < kPcSeg; ++k) {
-            av[k] = init ? bv[k] / th : fa * av[k] + fb * bv[k];
-            As[(r0 + k) * kPcW + cx] = av[k];
-        }
-        __syncthreads();
-        // s -= A sd ; z += sd (z = sd on pp == 0)
+    // one stencil step on the folded av[] (in As): s -= A sd ; z += sd (z = sd when INIT)
+    auto stencil = [&](const T* As, bool init) {
 #pragma unroll
         for (int k = 0; k < kPcSeg; ++k) {
             const int ry = r0 + k, o = ry * kPcW + cx;
@@ -114,18 +106,35 @@ __global__ void __launch_bounds__(kPcThreads) k_rf_pc_blocked(Lay L, const MxSta
             const T u = k < kPcSeg - 1 ? av[k + 1] : (ry < kPcH - 1 ? As[o + kPcW] : T(0));
             T l = __shfl_up_sync(kFull, c, 1);
             T rr = __shfl_down_sync(kFull, c, 1);
-            const T kxc = Ks[o];
-            T kxr = __shfl_down_sync(kFull, kxc, 1);
-            if (lane == 0) l = cx > 0 ? As[o - 1] : T(0);
-            if (lane == 31) {
-                rr = cx < kPcW - 1 ? As[o + 1] : T(0);
-                kxr = cx < kPcW - 1 ? Ks[o + 1] : T(0);
-            }
-            const T kyc = Ys[o];
-            const T kyu = ry < kPcH - 1 ? Ys[o + kPcW] : T(0);
-            const T v = smvp_t<T>(kxc, kxr, kyc, kyu, c, l, rr, d, u);
+            const bool edge = lane == edge_lane;
+            const T nb = edge ? As[o + edge_dx] : T(0);
+            if (lane == 0) l = hi_half ? nb : T(0);
+            if (lane == 31) rr = hi_half ? T(0) : nb;
+            const T v = pc_op<T>(kxc[k], kxr[k], kyc[k], kyc[k + 1], c, l, rr, d, u);
             bv[k] = bv[k] - v;
             zv[k] = init ? c : zv[k] + c;
+        }
+    };
+    for (int i = 0; i < H; ++i) {
+        const int pp = a.first + i;
+        T* const As = (i & 1) ? A1 : A0;
+        if (FIRST && i == 0) {
+#pragma unroll
+            for (int k = 0; k < kPcSeg; ++k) {
+                av[k] = bv[k] / th;
+                As[(r0 + k) * kPcW + cx] = av[k];
+            }
+            __syncthreads();
+            stencil(As, true);
+        } else {
+            const T fa = (T)a.alphas[pp - 1], fb = (T)a.betas[pp - 1];
+#pragma unroll
+            for (int k = 0; k < kPcSeg; ++k) {
+                av[k] = pc_fold(fa, fb, av[k], bv[k]);
+                As[(r0 + k) * kPcW + cx] = av[k];
+            }
+            __syncthreads();
+            stencil(As, false);
         }
     }
     double acc[1] = {0.0};
@@ -137,8 +146,7 @@ __global__ void __launch_bounds__(kPcThreads) k_rf_pc_blocked(Lay L, const MxSta
             if (ry < kPcMax || ry >= kPcMax + kPcY || gy >= L.ny) continue;
             const long gi = (long)(gy + 1) * L.xp + gx;
             if (LAST) {
-                const T dv = fa * av[k] + fb * bv[k];
-                const T zn = zv[k] + dv;
+                const T zn = zv[k] + pc_fold(fa, fb, av[k], bv[k]);
                 z[gi] = zn;
                 acc[0] += (double)r[gi] * (double)zn;
             } else {

@@ -386,11 +386,25 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
     return acc;
 }
 
-// The operator in T arithmetic (the order of smvp).
+// Preconditioner arithmetic in T with explicit fused multiply-adds (the
+// file is compiled without contraction; the one-step and the blocked kernels
+// share these, so their results are bit-identical).
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// A sd at a cell: (1 + kx_c + kx_r + ky_c + ky_u) c - kx_c l - kx_r r - ky_c d - ky_u u.
 template <typename T>
-__device__ __forceinline__ T smvp_t(T kxc, T kxr, T kyc, T kyu, T c, T l, T r, T d, T u)
+__device__ __forceinline__ T pc_op(T kxc, T kxr, T kyc, T kyu, T c, T l, T r, T d, T u)
 {
-    return (T(1) + (kxr + kxc) + (kyu + kyc)) * c - (kxr * r + kxc * l) - (kyu * u + kyc * d);
+    const T dg = T(1) + (kxr + kxc) + (kyu + kyc);
+    return fma_t(dg, c, -fma_t(kxc, l, kxr * r)) - fma_t(kyc, d, kyu * u);
+}
+
+// The Chebyshev fold sd = a sd + b s (pp > 0).
+template <typename T>
+__device__ __forceinline__ T pc_fold(T a, T b, T sd, T s)
+{
+    return fma_t(a, sd, b * s);
 }
 
 // Chebyshev inner step of the PPCG preconditioner over tile (tx, ty): the
@@ -409,7 +423,7 @@ __device__ __forceinline__ void rf_pc_tile(const Lay& L, int tx, int ty, double 
     constexpr int N = Pack<T>::N;
     const Span<N> s(L, tx, ty);
     const T th = (T)theta, ta = (T)fa, tb = (T)fb;
-    auto fold1 = [&](T sdv, T sv) -> T { return FOLD == 1 ? sv / th : ta * sdv + tb * sv; };
+    auto fold1 = [&](T sdv, T sv) -> T { return FOLD == 1 ? sv / th : pc_fold(ta, tb, sdv, sv); };
     auto cur = [&](long idx) -> Cells<T> {
         Cells<T> a = ld(s_in + idx);
         if (FOLD == 1) {
@@ -447,7 +461,7 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
                 const T l = m == 0 ? sl : sc.e[m - 1];
                 const T rr = m == N - 1 ? sr : sc.e[m + 1];
                 const T kr = m == N - 1 ? kxr : kxc.e[m + 1];
-                const T v = smvp_t<T>(kxc.e[m], kr, kyc.e[m], kyu.e[m], c, l, rr, sdn.e[m], su.e[m]);
+                const T v = pc_op<T>(kxc.e[m], kr, kyc.e[m], kyu.e[m], c, l, rr, sdn.e[m], su.e[m]);
                 rn.e[m] = rc.e[m] - v;
                 zv.e[m] = ACC ? zv.e[m] + c : c;
             }
@@ -487,7 +501,7 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
             }
 #pragma unroll
             for (int m = 0; m < N; ++m) {
-                const T d = FOLD == 1 ? sv.e[m] / th : ta * dv.e[m] + tb * sv.e[m];
+                const T d = FOLD == 1 ? sv.e[m] / th : pc_fold(ta, tb, dv.e[m], sv.e[m]);
                 zv.e[m] = FOLD == 1 ? d : zv.e[m] + d;
                 if (s.c0 + m < L.nx) acc += (double)rv.e[m] * (double)zv.e[m];
             }
