@@ -471,7 +471,8 @@ def bench_refine(n: int, peak: float) -> dict:
     """The iterative-refinement form against FP64 on identical inputs: one
     timestep of the seeded mixed-precision case (16 rectangles, seed 3), each
     solved to the relative FP64 residual 1e-10 (tl2d_refine_solve_step), with
-    CG and with PPCG (presteps 30, 10 inner steps)."""
+    CG and with PPCG (presteps 30, 10 inner steps; the deck's switch test and
+    an early switch)."""
     from tealeaf_b200 import problems
     from tealeaf_b200.host import Host
     tol = 1e-10
@@ -497,16 +498,20 @@ def bench_refine(n: int, peak: float) -> dict:
         temps[prec] = r.summary[3]
     out["time_ratio_fp32_over_fp64"] = out["fp32"]["ms"] / out["fp64"]["ms"]
     out["temp_rel_diff_fp32_vs_fp64"] = temps[32] / temps[64] - 1.0
-    pp = {}
-    for prec in (64, 32):
-        r = run(prob.with_(solver="ppcg"), prec)
-        pp["fp%d" % prec] = {"ms": r.device_ms, "iterations": r.iterations,
-                             "residual_updates": r.residual_updates, "rel_residual": r.rel_residual,
-                             "converged": r.converged}
-        temps["ppcg%d" % prec] = r.summary[3]
-    pp["time_ratio_fp32_over_fp64"] = pp["fp32"]["ms"] / pp["fp64"]["ms"]
-    pp["temp_rel_diff_fp32_vs_fp64_cg"] = temps["ppcg32"] / temps[64] - 1.0
-    out["ppcg"] = pp
+    # PPCG with the deck's switch test (presteps 30, r.r < 1), and with
+    # errswitch and epslim 1e30 (the switch after 21 CG trips)
+    for key, p in (("ppcg", prob.with_(solver="ppcg")),
+                   ("ppcg_errswitch", prob.with_(solver="ppcg", error_switch=True, eps_lim=1e30))):
+        pp = {}
+        for prec in (64, 32):
+            r = run(p, prec)
+            pp["fp%d" % prec] = {"ms": r.device_ms, "iterations": r.iterations, "cg_trips": r.cg_trips,
+                                 "residual_updates": r.residual_updates, "rel_residual": r.rel_residual,
+                                 "converged": r.converged}
+            temps[key + str(prec)] = r.summary[3]
+        pp["time_ratio_fp32_over_fp64"] = pp["fp32"]["ms"] / pp["fp64"]["ms"]
+        pp["temp_rel_diff_fp32_vs_fp64_cg"] = temps[key + "32"] / temps[64] - 1.0
+        out[key] = pp
     return out
 
 
