@@ -3,19 +3,20 @@
 //
 // Between two norm evaluations a Chebyshev trip (cheby.c:57-85) and a PPCG
 // inner step (ppcg.c:29-61) are local stencil updates with no global
-// reduction, so L of them (L <= kTB) run in one launch: a block loads its
-// tile of kTX x kTY cells plus an L-cell halo of the two carried fields into
-// shared memory, advances them L times on chip (each step's valid region
+// reduction, so L of them (L <= kTB) run in one launch: a block takes its
+// tile of kTX x kTY cells plus an L-cell halo on chip, each thread holding a
+// 16-row column segment of the carried fields, u0 (resp. u) and the face
+// coefficients in registers, advances them L times (each step's valid region
 // shrinks by one cell per side; the domain boundary is the depth-1 reflective
-// halo applied on the fly, so boundary tiles need no halo data), and writes
-// the tile back once. Every cell goes through exactly the operations of the
-// one-step kernels (k_cheby_trip, k_ppcg_step) in the same order, so the
-// results are bit-identical; global traffic per step drops from 56 B (64 B)
-// per cell to about 13 B (15 B) at L = 5. The reflective depth-1 halo of the
-// written stencil field (u, resp. sd) is stored by the boundary tiles. A norm
-// the last step needs is not reduced here: k_norm2_fin sums the stored
-// residual over the interior strip partition, the partition and order of the
-// one-step kernels, so the norms (and the PPCG beta) are bit-identical too.
+// halo applied on the fly, in regions that reach it), and writes the tile
+// back once. Every cell goes through exactly the operations of the one-step
+// kernels (k_cheby_trip, k_ppcg_step) in the same order, so the results are
+// bit-identical; global traffic per step drops from 56 B (64 B) per cell to
+// about 13 B (15 B) at L = 5. The reflective depth-1 halo of the written
+// stencil field (u, resp. sd) is stored by the boundary tiles. A norm the
+// last step needs is not reduced here: k_norm2_fin sums the stored residual
+// over the interior strip partition, the partition and order of the one-step
+// kernels, so the norms (and the PPCG beta) are bit-identical too.
 //
 // Chebyshev (MODE 0), carried fields A = u, B = p, state (u_{n-1}, p_{n-1})
 // with the add pending:   A += B ;  B = a_n B + b_n (u0 - A A)
@@ -25,15 +26,18 @@
 
 #include "kernels2d.cuh"
 
+#include <type_traits>
+
 namespace tl2d {
 
 constexpr int kTB = 5;                  // most steps per launch
-constexpr int kTW = 64;                 // shared row pitch: one column per thread of a row group
-constexpr int kTH = 48;                 // shared rows
+constexpr int kTW = 64;                 // region columns: one per thread of a row group
+constexpr int kTSeg = 16;               // region rows per thread (a column segment in registers)
+constexpr int kTRows = 4;               // row groups
+constexpr int kTBThreads = kTW * kTRows;   // 256
+constexpr int kTH = kTSeg * kTRows;     // region rows (64)
 constexpr int kTX = kTW - 2 * kTB;      // tile columns (54)
-constexpr int kTY = kTH - 2 * kTB;      // tile rows (38)
-constexpr int kTBThreads = 256;
-constexpr int kTRows = kTBThreads / kTW;   // row groups (4): thread = (column, row group)
+constexpr int kTY = kTH - 2 * kTB;      // tile rows (54)
 
 struct BlockedArgs {
     int steps;          // L <= kTB
@@ -44,129 +48,144 @@ struct BlockedArgs {
     const double* betas;
 };
 
+// Thread (cx, cy) holds column cx of the region, rows cy * kTSeg .. + kTSeg,
+// in registers: the two carried fields, u0 (Chebyshev) or u (PPCG, tile cells)
+// and the face coefficients. Each step's stencil field A goes through shared
+// memory (two buffers, alternating by step) for the neighbours held by other
+// warps (one column per warp) and other segments (one row each side);
+// neighbours within a warp come by shuffle, within the segment from
+// registers. A neighbour outside the interior is the cell itself (the
+// reflective depth-1 halo); cells outside the interior or beyond the loaded
+// margin compute values nothing valid reads.
 template <int MODE>
-static __global__ void __launch_bounds__(kTBThreads) k_blocked(Geo g, BlockedArgs a, const double* __restrict__ A_in,
-                                                               const double* __restrict__ B_in, double* A_out,
-                                                               double* __restrict__ B_out, const double* __restrict__ u0,
-                                                               double* __restrict__ u, double* __restrict__ w,
-                                                               double* __restrict__ r, const double* __restrict__ kx,
-                                                               const double* __restrict__ ky,
-                                                               const int* __restrict__ done)
+static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, BlockedArgs a, const double* __restrict__ A_in,
+                                                                  const double* __restrict__ B_in, double* A_out,
+                                                                  double* __restrict__ B_out,
+                                                                  const double* __restrict__ u0,
+                                                                  double* __restrict__ u, double* __restrict__ w,
+                                                                  double* __restrict__ r,
+                                                                  const double* __restrict__ kx,
+                                                                  const double* __restrict__ ky,
+                                                                  const int* __restrict__ done)
 {
     extern __shared__ double tb_smem[];
-    double* As = tb_smem;             // [kTH * kTW]
-    double* Bs = As + kTH * kTW;      // [kTH * kTW]
-    double* Us = Bs + kTH * kTW;      // [kTX * kTY], PPCG only
+    double* const S0 = tb_smem;           // [kTH * kTW]
+    double* const S1 = S0 + kTH * kTW;    // [kTH * kTW]
     if (gate_closed(done)) return;
     const int x = g.x, hd = g.hd;
     const int ilo = hd, ihi = g.x - hd, jlo = hd, jhi = g.y - hd;   // interior [lo, hi)
     const int X0 = hd + blockIdx.x * kTX, Y0 = hd + blockIdx.y * kTY;
-    const int X1 = min(X0 + kTX, ihi), Y1 = min(Y0 + kTY, jhi);
     const int H = a.steps;
-    const int ox = X0 - kTB, oy = Y0 - kTB;   // shared origin
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, cx = tid % kTW, cy = tid / kTW, lane = tid & 31;
+    const int gx = X0 - kTB + cx;    // grid column of this thread
+    const int oy = Y0 - kTB;         // grid row of region row 0
+    const int r0 = cy * kTSeg;       // first region row of this thread
+    const bool colin = gx >= ilo && gx < ihi;
+    const int mxc = max(max(kTB - cx, cx - (kTB + kTX - 1)), 0);   // column distance outside the tile
+    const bool at_l = gx == ilo, at_r = gx == ihi - 1;
+    const bool hi_half = cx >= 32;
+    const int edge_lane = hi_half ? 0 : 31, edge_dx = hi_half ? -1 : 1;
+    // does the region reach the domain boundary (then neighbours are reflected)?
+    const bool touches = X0 - kTB <= ilo || X0 - kTB + kTW > ihi - 1 || oy <= jlo || oy + kTH > jhi - 1;
 
-    // Thread (cx, cy): shared column cx of every kTRows-th row from cy; the
-    // region of margin m of this tile is [xl, xh) x [yl, yh).
-    const int cx = tid % kTW, cy = tid / kTW;
-    const int gxc = ox + cx;   // this thread's grid column
-    auto bounds = [&](int m, int& xl, int& xh, int& yl, int& yh) {
-        xl = max(ilo, X0 - m);
-        xh = min(ihi, X1 + m);
-        yl = max(jlo, Y0 - m);
-        yh = min(jhi, Y1 + m);
-    };
-    // first row >= yl of this thread's row group
-    auto first_row = [&](int yl) { return yl + ((cy - (yl - oy)) % kTRows + kTRows) % kTRows; };
-
-    // load the region of margin H (interior cells only)
-    {
-        int xl, xh, yl, yh;
-        bounds(H, xl, xh, yl, yh);
-        if (gxc >= xl && gxc < xh) {
-            for (int yy = first_row(yl); yy < yh; yy += kTRows) {
-                const long gi = gxc + (long)yy * x;
-                const int s = (yy - oy) * kTW + cx;
-                As[s] = A_in[gi];
-                Bs[s] = B_in[gi];
-                if (MODE == 1 && gxc >= X0 && gxc < X1 && yy >= Y0 && yy < Y1)
-                    Us[(yy - Y0) * kTX + (gxc - X0)] = u[gi];
-            }
-        }
+    double av[kTSeg], bv[kTSeg], cv[kTSeg], kxc[kTSeg], kxr[kTSeg], kyc[kTSeg + 1];
+#pragma unroll
+    for (int k = 0; k <= kTSeg; ++k) {
+        const int ry = r0 + k, gy = oy + ry;
+        const int my = max(max(kTB - ry, ry - (kTB + kTY - 1)), 0);
+        const bool in = colin && gy >= jlo && gy < jhi && max(mxc, my) <= H;
+        const long gi = gx + (long)gy * x;
+        // ky of rows jlo..jhi: the face above the top interior row is read as the one-step kernels do
+        const bool in_ky = colin && gy >= jlo && gy <= jhi && max(mxc, my) <= H + 1;
+        kyc[k] = in_ky ? ky[gi] : 0.0;   // k == kTSeg: ky_u of the segment's top row
+        if (k == kTSeg) break;
+        av[k] = in ? A_in[gi] : 0.0;
+        bv[k] = in ? B_in[gi] : 0.0;
+        if (MODE == 0) cv[k] = in ? u0[gi] : 0.0;
+        else cv[k] = (in && mxc == 0 && my == 0) ? u[gi] : 0.0;
+        kxc[k] = in ? kx[gi] : 0.0;
+        kxr[k] = in ? kx[gi + 1] : 0.0;
     }
-    __syncthreads();
     for (int i = 0; i < H; ++i) {
-        // pass A: pointwise over margin H - i
+        double* const As = (i & 1) ? S1 : S0;
+        // pass A, pointwise
         {
-            int xl, xh, yl, yh;
-            bounds(H - i, xl, xh, yl, yh);
-            double fa = 0.0, fb = 0.0;
             const int pp = a.first + i;
-            if (MODE == 1 && pp > 0) {
-                fa = a.alphas[pp - 1];
-                fb = a.betas[pp - 1];
-            }
-            if (gxc >= xl && gxc < xh) {
-                for (int yy = first_row(yl); yy < yh; yy += kTRows) {
-                    const int s = (yy - oy) * kTW + cx;
-                    if (MODE == 0) As[s] = As[s] + Bs[s];
-                    else As[s] = pp == 0 ? Bs[s] / a.theta : fa * As[s] + fb * Bs[s];
+            const double fa = (MODE == 1 && pp > 0) ? a.alphas[pp - 1] : 0.0;
+            const double fb = (MODE == 1 && pp > 0) ? a.betas[pp - 1] : 0.0;
+            if (MODE == 1 && pp == 0) {
+#pragma unroll
+                for (int k = 0; k < kTSeg; ++k) {
+                    av[k] = bv[k] / a.theta;
+                    As[(r0 + k) * kTW + cx] = av[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kTSeg; ++k) {
+                    av[k] = MODE == 0 ? av[k] + bv[k] : fa * av[k] + fb * bv[k];
+                    As[(r0 + k) * kTW + cx] = av[k];
                 }
             }
         }
         __syncthreads();
-        // pass B: stencil over margin H - i - 1
-        {
-            int xl, xh, yl, yh;
-            bounds(H - i - 1, xl, xh, yl, yh);
+        // pass B, the stencil on A (reflection only in regions at the boundary)
+        auto pass_b = [&](auto reflect) {
+            constexpr bool REFLECT = decltype(reflect)::value;
             const bool last = i == H - 1;
-            double ca = 0.0, cb = 0.0;
-            if (MODE == 0) {
-                ca = a.alphas[a.first + i];
-                cb = a.betas[a.first + i];
-            }
-            if (gxc >= xl && gxc < xh) {
-                const bool in_tx = gxc >= X0 && gxc < X1;
-                for (int yy = first_row(yl); yy < yh; yy += kTRows) {
-                    const int s = (yy - oy) * kTW + cx;
-                    const long gi = gxc + (long)yy * x;
-                    const double cc = As[s];
-                    const double l = gxc == ilo ? cc : As[s - 1];
-                    const double rr = gxc == ihi - 1 ? cc : As[s + 1];
-                    const double d = yy == jlo ? cc : As[s - kTW];
-                    const double up = yy == jhi - 1 ? cc : As[s + kTW];
-                    const double v = smvp(__ldg(kx + gi), __ldg(kx + gi + 1), __ldg(ky + gi), __ldg(ky + gi + x), cc,
-                                          l, rr, d, up);
-                    const bool in_tile = in_tx && yy >= Y0 && yy < Y1;
-                    if (MODE == 0) {
-                        const double res = __ldg(u0 + gi) - v;
-                        Bs[s] = ca * Bs[s] + cb * res;
-                        if (last && in_tile && a.wr_last) {
-                            w[gi] = v;
-                            r[gi] = res;
-                        }
-                    } else {
-                        Bs[s] = Bs[s] - v;
-                        if (in_tile) Us[(yy - Y0) * kTX + (gxc - X0)] += cc;
+            const double ca = MODE == 0 ? a.alphas[a.first + i] : 0.0;
+            const double cb = MODE == 0 ? a.betas[a.first + i] : 0.0;
+#pragma unroll
+            for (int k = 0; k < kTSeg; ++k) {
+                const int ry = r0 + k, gy = oy + ry, o = ry * kTW + cx;
+                const double c = av[k];
+                double dn = k > 0 ? av[k - 1] : (ry > 0 ? As[o - kTW] : 0.0);
+                double up = k < kTSeg - 1 ? av[k + 1] : (ry < kTH - 1 ? As[o + kTW] : 0.0);
+                double l = __shfl_up_sync(kFull, c, 1);
+                double rr = __shfl_down_sync(kFull, c, 1);
+                // lane 0 / 31 at the region's edges keep 0 (nb is 0 off the edge lane)
+                const double nb = lane == edge_lane ? As[o + edge_dx] : 0.0;
+                if (lane == 0) l = nb;
+                if (lane == 31) rr = nb;
+                if (REFLECT) {
+                    if (at_l) l = c;
+                    if (at_r) rr = c;
+                    if (gy == jlo) dn = c;
+                    if (gy == jhi - 1) up = c;
+                }
+                const double v = smvp(kxc[k], kxr[k], kyc[k], kyc[k + 1], c, l, rr, dn, up);
+                if (MODE == 0) {
+                    const double res = cv[k] - v;
+                    bv[k] = ca * bv[k] + cb * res;
+                    const bool in_tile = colin && mxc == 0 && ry >= kTB && ry < kTB + kTY && gy < jhi;
+                    if (last && in_tile && a.wr_last) {
+                        const long gi = gx + (long)gy * x;
+                        w[gi] = v;
+                        r[gi] = res;
                     }
+                } else {
+                    bv[k] = bv[k] - v;
+                    cv[k] += c;   // u; only tile cells (loaded, written back) matter
                 }
             }
-        }
-        __syncthreads();
+        };
+        if (touches) pass_b(std::true_type());
+        else pass_b(std::false_type());
     }
     // write the tile: A (u, resp. sd) with its reflective depth-1 halo, B (p, resp. r)
-    if (gxc >= X0 && gxc < X1) {
-        for (int yy = first_row(Y0); yy < Y1; yy += kTRows) {
-            const int s = (yy - oy) * kTW + cx;
-            const long gi = gxc + (long)yy * x;
-            const double av = As[s];
-            A_out[gi] = av;
-            B_out[gi] = Bs[s];
-            if (MODE == 1) u[gi] = Us[(yy - Y0) * kTX + (gxc - X0)];
-            if (gxc == ilo) A_out[gi - 1] = av;
-            if (gxc == ihi - 1) A_out[gi + 1] = av;
-            if (yy == jlo) A_out[gi - x] = av;
-            if (yy == jhi - 1) A_out[gi + x] = av;
+    if (colin && mxc == 0) {
+#pragma unroll
+        for (int k = 0; k < kTSeg; ++k) {
+            const int ry = r0 + k, gy = oy + ry;
+            if (ry < kTB || ry >= kTB + kTY || gy >= jhi) continue;
+            const long gi = gx + (long)gy * x;
+            const double av_ = av[k];
+            A_out[gi] = av_;
+            B_out[gi] = bv[k];
+            if (MODE == 1) u[gi] = cv[k];
+            if (at_l) A_out[gi - 1] = av_;
+            if (at_r) A_out[gi + 1] = av_;
+            if (gy == jlo) A_out[gi - x] = av_;
+            if (gy == jhi - 1) A_out[gi + x] = av_;
         }
     }
 }
@@ -199,7 +218,7 @@ static __global__ void k_finish_only(const int* __restrict__ done, Finish fin)
 template <int MODE>
 constexpr size_t blocked_smem()
 {
-    return sizeof(double) * (2 * kTH * kTW + (MODE == 1 ? kTX * kTY : 0));
+    return sizeof(double) * 2 * kTH * kTW;
 }
 
 inline dim3 blocked_grid(const Geo& g)
