@@ -252,6 +252,10 @@ int tl3d_profile_read(Chunk* chunk, int index, char* name, int name_len,
 /* Kernel launches issued for this chunk since initialisation (counted
  * whether or not the profile is enabled); -1 for an unknown chunk. */
 long long tl3d_launch_count(Chunk* chunk);
+/* No counterpart in the reference. Feed the CG w sweep's operand planes by
+ * TMA tile loads (1, the default, where the halo depth and row length are
+ * even; results are bit-identical) or by per-thread asynchronous copies (0). */
+void tl3d_set_tma(Chunk* chunk, int on);
 
 /* Field ids for the host-buffer staging calls (x*y*z values each). */
 #define TL3D_DENSITY0 0

@@ -194,14 +194,11 @@ int adjoint_solve(TlSuite3D* s, Chunk* chunk, const double* rhs, double* lam, do
     int cur = 0;
     batched(s, max_iters, [&](int t) {
         if (t == 0) {
-            TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gh, bl, 0, s->stream>>>(
-                                         s->g, fc, beta, buf[cur], buf[cur], chunk->vec_r, chunk->vec_w, chunk->vec_kx,
-                                         chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done, fin_w)));
+            launch_cg_w3<false, false>(s, chunk, gh, fc, beta, buf[cur], buf[cur], chunk->vec_r, chunk->vec_w,
+                                       nullptr, 0, done, fin_w);
         } else {
-            TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gh, bl, 0, s->stream>>>(
-                                         s->g, fc, beta, buf[cur], buf[cur ^ 1], chunk->vec_r, chunk->vec_w,
-                                         chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done,
-                                         fin_w)));
+            launch_cg_w3<true, true>(s, chunk, gh, fc, beta, buf[cur], buf[cur ^ 1], chunk->vec_r, chunk->vec_w,
+                                     nullptr, 0, done, fin_w);
             cur ^= 1;
         }
         TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(s->g, alpha, lam, buf[cur], chunk->vec_r,
@@ -376,5 +373,6 @@ extern "C" int tl3d_adjoint_gradient(Chunk* chunk, Settings* settings, int steps
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(slab);
+    if (tma_failed(s)) tl::fail(35, "a TMA plane load of the w sweep did not complete (bounded barrier wait gave up)");
     return tl::failed() ? tl::error_state().code : 0;
 }

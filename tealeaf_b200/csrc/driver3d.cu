@@ -101,13 +101,11 @@ struct Run3 {
         int cur = 0;
         auto trip = [&](int t) {
             if (fresh && t == from) {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gh, bl, 0, s->stream>>>(
-                               s->g, fc, beta, buf[cur], buf[cur], chunk->vec_r, chunk->vec_w, chunk->vec_kx,
-                               chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
+                launch_cg_w3<false, false>(s, chunk, gh, fc, beta, buf[cur], buf[cur], chunk->vec_r, chunk->vec_w,
+                                           nullptr, 0, done(), fin_w);
             } else {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gh, bl, 0, s->stream>>>(
-                               s->g, fc, beta, buf[cur], buf[cur ^ 1], chunk->vec_r, chunk->vec_w, chunk->vec_kx,
-                               chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
+                launch_cg_w3<true, true>(s, chunk, gh, fc, beta, buf[cur], buf[cur ^ 1], chunk->vec_r, chunk->vec_w,
+                                         nullptr, 0, done(), fin_w);
                 cur ^= 1;
             }
             TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(
@@ -219,13 +217,11 @@ struct Run3 {
         tl::FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
         auto trip = [&](int t) {
             if (t == tt) {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<false, false><<<gh, bl, 0, s->stream>>>(
-                               s->g, fc, beta, pb[pc], pb[pc], rb[rc], chunk->vec_w, chunk->vec_kx, chunk->vec_ky,
-                               chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
+                launch_cg_w3<false, false>(s, chunk, gh, fc, beta, pb[pc], pb[pc], rb[rc], chunk->vec_w, nullptr, 0,
+                                           done(), fin_w);
             } else {
-                TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<true, true><<<gh, bl, 0, s->stream>>>(
-                               s->g, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->vec_w, chunk->vec_kx,
-                               chunk->vec_ky, chunk->vec_kz, nullptr, 0, s->rs, done(), fin_w)));
+                launch_cg_w3<true, true>(s, chunk, gh, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->vec_w, nullptr,
+                                         0, done(), fin_w);
                 pc ^= 1;
             }
             TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(
@@ -398,6 +394,10 @@ void tl3d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats3* sta
         flags[TL3_FIELD_U] = flags[TL3_FIELD_P] = true;
     }
     if (tl::failed()) return;
+    if (tma_failed(s)) {
+        tl::fail(35, "a TMA plane load of the w sweep did not complete (bounded barrier wait gave up)");
+        return;
+    }
     const int tt_exit = st.reason == 1 ? st.trip - 1 : st.trip;
     st_out->total_iters = tt_exit;
     if (settings->solver == TL3_CHEBY_SOLVER) st_out->cg_iters = tt_exit - st_out->cheby_iters + 1;

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 #include "solver_common.cuh"
 #include "tealeaf_b200_3d.h"
 
@@ -259,6 +260,97 @@ __device__ __forceinline__ void walkc(const Geo& g, const Faces& fc, const Penci
     __syncthreads();
 }
 
+// The operand planes of walkc fed by TMA (tma.cuh), each array one box of a
+// tensor map at a 128-byte aligned offset: A and B with columns kb-2 ..
+// kb+33 (the box must start on a 16-byte boundary; kb = hd + 32 bx is even
+// for an even halo depth) and rows jb-1 .. jb+8, kx with one extra column, ky
+// with one extra row, kz.
+struct PlaneT {
+    alignas(128) double A[BY + 2][BX + 4];
+    alignas(128) double B[BY + 2][BX + 4];
+    alignas(128) double kx[BY][BX + 2];
+    alignas(128) double ky[BY + 1][BX];
+    alignas(128) double kz[BY][BX];
+};
+
+// Tensor maps of one fused sweep: the operand arrays (box (BX+4) x (BY+2) x 1)
+// and the face coefficients (boxes (BX+2) x BY, BX x (BY+1), BX x BY).
+struct Tma3Maps {
+    CUtensorMap a, b, kx, ky, kz;
+};
+
+constexpr size_t kTmaRingBytes = kStages3 * sizeof(PlaneT) + kStages3 * 8 + 128;   // + barriers + alignment
+
+// walkc with the planes brought in by TMA: one thread issues the plane's
+// boxes on the slot's shared-memory barrier; every thread waits (bounded) for
+// planes ii and ii+1, then computes exactly as walkc. All threads of the
+// block must call it.
+template <bool REFLECT, typename Comb, typename Body>
+__device__ __forceinline__ void walkt(const Geo& g, const Faces& fc, const PencilC& s, const Tma3Maps& m,
+                                      bool has_b, const double* __restrict__ A, const double* __restrict__ B,
+                                      unsigned char* raw, int* err, Comb comb, Body body)
+{
+    unsigned char* base = raw + ((128 - (tl::smem_addr(raw) & 127)) & 127);
+    PlaneT* ring = reinterpret_cast<PlaneT*>(base);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStages3 * sizeof(PlaneT));
+    const int x = g.x;
+    const long xy = g.xy();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = tx == 0 && ty == 0;
+    const int zlast = g.z - g.hd - 1;
+    const int kb = g.hd + blockIdx.x * BX, jb = g.hd + blockIdx.y * BY;   // block origin
+    constexpr unsigned kAB = sizeof(double) * (BY + 2) * (BX + 4);
+    constexpr unsigned kKZ = sizeof(double) * BY * BX;
+    constexpr unsigned kKXY = sizeof(double) * (BY * (BX + 2) + (BY + 1) * BX);
+    auto issue = [&](int iz, int st, bool coef) {
+        PlaneT& P = ring[st];
+        tl::mbar_expect_tx(&bars[st], kAB * (has_b ? 2u : 1u) + kKZ + (coef ? kKXY : 0u));
+        tl::tma_load_3d(&P.A[0][0], &m.a, kb - 2, jb - 1, iz, &bars[st]);
+        if (has_b) tl::tma_load_3d(&P.B[0][0], &m.b, kb - 2, jb - 1, iz, &bars[st]);
+        tl::tma_load_3d(&P.kz[0][0], &m.kz, kb, jb, iz, &bars[st]);
+        if (coef) {
+            tl::tma_load_3d(&P.kx[0][0], &m.kx, kb, jb, iz, &bars[st]);
+            tl::tma_load_3d(&P.ky[0][0], &m.ky, kb, jb, iz, &bars[st]);
+        }
+    };
+    const int np = s.i1 - s.i0 + 1;   // planes i0 .. i1 (i1: the last plane's front neighbour)
+    if (leader) {
+        for (int q = 0; q < kStages3; ++q) tl::mbar_init(&bars[q], 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (leader)
+        for (int q = 0; q < kStages3 - 1 && q < np; ++q) issue(s.i0 + q, q, s.i0 + q < s.i1);
+    long i = s.k + (long)s.j * x + (long)s.i0 * xy;
+    double bk = (s.i0 == g.hd) ? 0.0 : comb(A[i - xy], B ? B[i - xy] : 0.0);
+    const bool bk_reflect = s.i0 == g.hd;
+#pragma unroll 1
+    for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+        const int q = ii - s.i0;
+        tl::mbar_wait(&bars[q % kStages3], (unsigned)(q / kStages3) & 1u, err);
+        tl::mbar_wait(&bars[(q + 1) % kStages3], (unsigned)((q + 1) / kStages3) & 1u, err);
+        __syncthreads();   // every thread is past plane ii-1: its slot is free
+        if (leader && q + kStages3 - 1 < np)
+            issue(ii + kStages3 - 1, (q + kStages3 - 1) % kStages3, ii + kStages3 - 1 < s.i1);
+        const PlaneT& P = ring[q % kStages3];
+        const PlaneT& F = ring[(q + 1) % kStages3];
+        const int cx = tx + 2, cy = ty + 1;
+        auto cell = [&](const PlaneT& S, int yy, int xx) { return comb(S.A[yy][xx], has_b ? S.B[yy][xx] : 0.0); };
+        const double c = cell(P, cy, cx);
+        if (ii == s.i0 && bk_reflect) bk = (REFLECT && fc.k) ? c : A[i - xy];
+        const double l = s.at_l ? ((REFLECT && fc.l) ? c : P.A[cy][cx - 1]) : cell(P, cy, cx - 1);
+        const double r = s.at_r ? ((REFLECT && fc.r) ? c : P.A[cy][cx + 1]) : cell(P, cy, cx + 1);
+        const double d = s.at_b ? ((REFLECT && fc.b) ? c : P.A[cy - 1][cx]) : cell(P, cy - 1, cx);
+        const double u = s.at_t ? ((REFLECT && fc.t) ? c : P.A[cy + 1][cx]) : cell(P, cy + 1, cx);
+        const double fr = ii == zlast ? ((REFLECT && fc.f) ? c : F.A[cy][cx]) : cell(F, cy, cx);
+        const double v = smvp(P.kx[ty][tx], P.kx[ty][tx + 1], P.ky[ty][tx], P.ky[ty + 1][tx], P.kz[ty][tx],
+                              F.kz[ty][tx], c, l, r, d, u, bk, fr);
+        body(ii, i, c, v);
+        bk = c;
+    }
+    __syncthreads();   // every issued plane has been waited for: no copy is in flight
+}
+
 __device__ __forceinline__ void reflect_store(double* f, const Geo& g, const Faces& fc, int depth, int k, int j,
                                              int i, double v)
 {
@@ -326,6 +418,40 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_w(Geo g, Faces fc,
     if (blockIdx.z + 1 < gridDim.z) {
         const PencilC s(g);
         walkc<REFLECT>(g, fc, s, p_in, FUSE_P ? r : nullptr, kx, ky, kz,
+                       [&](double pa, double rb) { return FUSE_P ? bt * pa + rb : pa; },
+                       [&](int, long i, double c, double v) {
+            if (s.active) {
+                w[i] = v;
+                acc[0] += v * c;
+                if (FUSE_P) p_out[i] = c;
+            }
+        });
+    } else {
+        if (REFLECT) halo_duty3(g, fc, 1, p_out, cur);
+        if (u_halo) halo_duty3(g, fc, uhd, u_halo, [&](long idx) { return u_halo[idx]; });
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+}
+
+// k3_cg_w with the operand planes brought in by TMA (walkt); the same
+// arithmetic, so the same results. `err`: the bounded barrier waits' flag.
+template <bool FUSE_P, bool REFLECT, typename Finish>
+static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cg_w_tma(Geo g, Faces fc, Scalar beta,
+                                                                   const __grid_constant__ Tma3Maps maps,
+                                                                   const double* __restrict__ p_in, double* p_out,
+                                                                   const double* __restrict__ r,
+                                                                   double* __restrict__ w, double* u_halo, int uhd,
+                                                                   ReduceSlots rs, const int* __restrict__ done,
+                                                                   Finish fin, int* err)
+{
+    extern __shared__ __align__(128) unsigned char t3_raw[];
+    if (gate_closed(done)) return;
+    double acc[1] = {0.0};
+    const double bt = FUSE_P ? beta.get() : 0.0;
+    auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
+    if (blockIdx.z + 1 < gridDim.z) {
+        const PencilC s(g);
+        walkt<REFLECT>(g, fc, s, maps, FUSE_P, p_in, FUSE_P ? r : nullptr, t3_raw, err,
                        [&](double pa, double rb) { return FUSE_P ? bt * pa + rb : pa; },
                        [&](int, long i, double c, double v) {
             if (s.active) {

@@ -12,6 +12,7 @@
 #include "suite3d_impl.hpp"
 
 #include <algorithm>
+#include <cstring>
 
 using namespace tl3d;
 using tl::ReduceSlots;
@@ -150,6 +151,11 @@ void tl3d_profile_reset(Chunk* chunk)
     TlSuite3D* s = suite_of(chunk);
     if (s) s->prof.reset();
 }
+void tl3d_set_tma(Chunk* chunk, int on)
+{
+    TlSuite3D* s = suite_of(chunk);
+    if (s) s->tma = on != 0;
+}
 long long tl3d_launch_count(Chunk* chunk)
 {
     TlSuite3D* s = suite_of(chunk);
@@ -232,6 +238,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     if (!TL_CUDA(cudaHostGetDevicePointer((void**)&dev_view, s->h_out, 0))) return;
     s->rs.out_host = dev_view;
     s->h_mirror = (int*)(s->h_out + tl::kMaxSums);
+    memset(s->h_mirror, 0, 64);
     s->d_mirror = (int*)(dev_view + tl::kMaxSums);
     chunk->cg_alphas = (double*)calloc((size_t)mi, sizeof(double));
     chunk->cg_betas = (double*)calloc((size_t)mi, sizeof(double));
@@ -426,10 +433,8 @@ void run_cg_solver_calc_w(Chunk* chunk, Settings* settings, double* pw)
     const dim3 gr = fused_grid(s->g), bl = interior_block();
     double* p_out = fuse ? s->alt[ALT3_P] : chunk->vec_p;
 #define W3(F, R)                                                                                                   \
-    TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<F, R><<<gr, bl, 0, s->stream>>>(s->g, fc, beta, chunk->vec_p, p_out,         \
-                                                                      chunk->vec_r, chunk->vec_w, chunk->vec_kx,   \
-                                                                      chunk->vec_ky, chunk->vec_kz, u_halo, ud,    \
-                                                                      s->rs, nullptr, tl::NoFinish())))
+    launch_cg_w3<F, R>(s, chunk, gr, fc, beta, chunk->vec_p, p_out, chunk->vec_r, chunk->vec_w, u_halo, ud, nullptr, \
+                       tl::NoFinish())
     if (fuse && refl) W3(true, true);
     else if (fuse) W3(true, false);
     else if (refl) W3(false, true);
@@ -601,6 +606,10 @@ void run_solver_finalise(Chunk* chunk, Settings* settings)
     (void)settings;
     TlSuite3D* s = ready(chunk);
     if (!s) return;
+    if (tma_failed(s)) {
+        tl::fail(35, "a TMA plane load of the w sweep did not complete (bounded barrier wait gave up)");
+        return;
+    }
     TL3_LAUNCH(s, "k3_finalise", k3_finalise<<<interior_grid(s->g), interior_block(), 0, s->stream>>>(
                                      s->g, chunk->energy, chunk->density, chunk->vec_u));
 }

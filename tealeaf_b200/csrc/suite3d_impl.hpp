@@ -38,7 +38,19 @@ struct TlSuite3D {
     double* d_cheby_alphas = nullptr;
     double* d_cheby_betas = nullptr;
     int table_len = 0;
+    bool tma = true;   // feed the CG w sweep by TMA where the layout allows (tl3d_set_tma)
+    struct TmaEntry {
+        const double* ptr;
+        int kind;
+        CUtensorMap map;
+    };
+    TmaEntry tma_cache[12];
+    int tma_n = 0;
 };
+
+// Index of the int, in the mapped mirror words, that the bounded TMA barrier
+// waits set when one gives up.
+constexpr int kTmaErrWord = 15;
 
 #define TL3_LAUNCH(s, name, ...)               \
     do {                                       \
@@ -51,6 +63,7 @@ struct TlSuite3D {
 namespace tl3d {
 
 TlSuite3D* suite_of(Chunk* chunk);
+
 inline dim3 interior_grid(const Geo& g)
 {
     return dim3(tl::ceil_div(g.x - 2 * g.hd, BX), tl::ceil_div(g.y - 2 * g.hd, BY), tl::ceil_div(g.z - 2 * g.hd, g.zr));
@@ -94,4 +107,57 @@ Faces faces_of(const Chunk* chunk);
 double** field_slot(Chunk* chunk, AltField3 f);
 void swap_alt(TlSuite3D* s, Chunk* chunk, AltField3 f);
 
+
+// Tensor map of a chunk array for walkt: kind 0 operand (box (BX+4) x (BY+2)),
+// 1 kx (BX+2) x BY, 2 ky BX x (BY+1), 3 kz BX x BY; encoded once per array.
+inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
+{
+    for (int i = 0; i < s->tma_n; ++i)
+        if (s->tma_cache[i].ptr == ptr && s->tma_cache[i].kind == kind) return &s->tma_cache[i].map;
+    if (s->tma_n == (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]))) return nullptr;
+    static const unsigned box[4][2] = {{BX + 4, BY + 2}, {BX + 2, BY}, {BX, BY + 1}, {BX, BY}};
+    TlSuite3D::TmaEntry& e = s->tma_cache[s->tma_n];
+    if (!tl::tma_encode_3d(&e.map, ptr, s->g.x, s->g.y, s->g.z, box[kind][0], box[kind][1], 1)) return nullptr;
+    e.ptr = ptr;
+    e.kind = kind;
+    ++s->tma_n;
+    return &e.map;
+}
+
+// The TMA boxes start at x = hd - 2 + 32 bx: an even halo depth and an even
+// row length keep every start and stride on a 16-byte boundary.
+inline bool tma_usable(const TlSuite3D* s) { return s->tma && s->g.hd % 2 == 0 && s->g.x % 2 == 0; }
+
+inline bool tma_failed(const TlSuite3D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord] != 0; }
+
+// The fused CG w sweep (k3_cg_w semantics), by TMA where possible.
+template <bool F, bool R, typename Finish>
+void launch_cg_w3(TlSuite3D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
+                  double* p_out, const double* r, double* w, double* u_halo, int uhd, const int* done, Finish fin)
+{
+    const dim3 bl = interior_block();
+    if (tma_usable(s)) {
+        const CUtensorMap* a = tma_map(s, p_in, 0);
+        const CUtensorMap* b = F ? tma_map(s, r, 0) : a;
+        const CUtensorMap* kx = tma_map(s, chunk->vec_kx, 1);
+        const CUtensorMap* ky = tma_map(s, chunk->vec_ky, 2);
+        const CUtensorMap* kz = tma_map(s, chunk->vec_kz, 3);
+        if (a && b && kx && ky && kz) {
+            const Tma3Maps m{*a, *b, *kx, *ky, *kz};
+            static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k3_cg_w_tma<F, R, Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kTmaRingBytes));
+                attr_set |= 1u << (s->device & 31);
+            }
+            TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w_tma<F, R><<<grid, bl, kTmaRingBytes, s->stream>>>(
+                                         s->g, fc, beta, m, p_in, p_out, r, w, u_halo, uhd, s->rs, done, fin,
+                                         s->d_mirror + kTmaErrWord)));
+            return;
+        }
+    }
+    TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<F, R><<<grid, bl, 0, s->stream>>>(s->g, fc, beta, p_in, p_out, r, w,
+                                                                      chunk->vec_kx, chunk->vec_ky, chunk->vec_kz,
+                                                                      u_halo, uhd, s->rs, done, fin)));
+}
 }  // namespace tl3d
