@@ -254,6 +254,11 @@ void* tl2d_stream(Chunk* chunk);
  * its fields are bit-identical, its r.z is summed over another partition). */
 void tl2d_set_temporal_blocking(Chunk* chunk, int on);
 
+/* No counterpart in the reference. Feed the CG w sweep's operand rows by TMA
+ * tile loads (1, the default, where the halo depth and row length are even;
+ * results are bit-identical) or by per-thread loads (0). */
+void tl2d_set_tma(Chunk* chunk, int on);
+
 /* Per-kernel device-time profile (CUDA events around every launch on the
  * chunk's stream, resolved at the next synchronisation): enable/disable,
  * reset, and read entry `index` (returns 0 past the last entry). */

@@ -208,7 +208,7 @@ def load(dims: int) -> C.CDLL:
         f = getattr(lib, pre + "refine_solve_step")
         f.argtypes = head + [_i, _d, _i, C.POINTER(RefineStats)]
         f.restype = _i
-    if hasattr(lib, pre + "set_tma"):
+    if hasattr(lib, pre + "set_tma"):  # 2D and 3D
         f = getattr(lib, pre + "set_tma")
         f.argtypes = [C.POINTER(chunk_t), _i]
         f.restype = None

@@ -145,13 +145,11 @@ struct Run {
         int cur = 0;
         auto trip = [&](int t) {
             if (fresh && t == from) {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gh, BX, 0, s->stream>>>(
-                              s->g, fc, beta, buf[cur], buf[cur], chunk->r, chunk->w, chunk->kx, chunk->ky,
-                              nullptr, 0, s->rs, done(), fin_w)));
+                launch_cg_w2<false, false>(s, chunk, gh, fc, beta, buf[cur], buf[cur], chunk->r, chunk->w, nullptr,
+                                           0, done(), fin_w);
             } else {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gh, BX, 0, s->stream>>>(
-                              s->g, fc, beta, buf[cur], buf[cur ^ 1], chunk->r, chunk->w, chunk->kx,
-                              chunk->ky, nullptr, 0, s->rs, done(), fin_w)));
+                launch_cg_w2<true, true>(s, chunk, gh, fc, beta, buf[cur], buf[cur ^ 1], chunk->r, chunk->w,
+                                         nullptr, 0, done(), fin_w);
                 cur ^= 1;
             }
             TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
@@ -318,13 +316,11 @@ struct Run {
         const int inner_flips = blocked ? (ni + kTB - 1) / kTB : ni;   // r/sd buffer flips per outer trip
         auto trip = [&](int t) {
             if (t == tt) {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<false, false><<<gh, BX, 0, s->stream>>>(
-                              s->g, fc, beta, pb[pc], pb[pc], rb[rc], chunk->w, chunk->kx, chunk->ky, nullptr, 0,
-                              s->rs, done(), fin_w)));
+                launch_cg_w2<false, false>(s, chunk, gh, fc, beta, pb[pc], pb[pc], rb[rc], chunk->w, nullptr, 0,
+                                           done(), fin_w);
             } else {
-                TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<true, true><<<gh, BX, 0, s->stream>>>(
-                              s->g, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->w, chunk->kx, chunk->ky, nullptr,
-                              0, s->rs, done(), fin_w)));
+                launch_cg_w2<true, true>(s, chunk, gh, fc, beta, pb[pc], pb[pc ^ 1], rb[rc], chunk->w, nullptr, 0,
+                                         done(), fin_w);
                 pc ^= 1;
             }
             TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
@@ -529,6 +525,10 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
         flags[TL_FIELD_U] = flags[TL_FIELD_P] = true;
     }
     if (tl::failed()) return;
+    if (tma_failed(s)) {
+        tl::fail(35, "a TMA row load of the w sweep did not complete (bounded barrier wait gave up)");
+        return;
+    }
     // the reference's printed iteration count is the loop index at exit
     const int tt_exit = st.reason == 1 ? st.trip - 1 : st.trip;
     st_out->total_iters = tt_exit;

@@ -28,6 +28,7 @@
 
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cstring>
 
 using namespace tl2d;
 using tl::ReduceSlots;
@@ -153,6 +154,11 @@ void tl2d_set_temporal_blocking(Chunk* chunk, int on)
     TlSuite2D* s = suite_of(chunk);
     if (s) s->temporal_blocking = on != 0;
 }
+void tl2d_set_tma(Chunk* chunk, int on)
+{
+    TlSuite2D* s = suite_of(chunk);
+    if (s) s->tma = on != 0;
+}
 
 void tl2d_profile_enable(Chunk* chunk, int on)
 {
@@ -248,6 +254,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     if (!TL_CUDA(cudaHostGetDevicePointer((void**)&dev_view, s->h_out, 0))) return;
     s->rs.out_host = dev_view;
     s->h_mirror = (int*)(s->h_out + tl::kMaxSums);
+    memset(s->h_mirror, 0, 64);
     s->d_mirror = (int*)(dev_view + tl::kMaxSums);
 
     chunk->cg_alphas = (double*)calloc((size_t)mi, sizeof(double));
@@ -453,10 +460,8 @@ void run_cg_calc_w(Chunk* chunk, Settings* settings, double* pw)
     const dim3 gr = fused_grid(s->g);
     double* p_out = fuse ? s->alt[ALT_P] : chunk->p;
 #define W2(F, R)                                                                                                    \
-    TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<F, R><<<gr, BX, 0, s->stream>>>(s->g, fc, beta, chunk->p, p_out,    \
-                                                                               chunk->r, chunk->w, chunk->kx,      \
-                                                                               chunk->ky, u_halo, ud, s->rs,       \
-                                                                               nullptr, tl::NoFinish())))
+    launch_cg_w2<F, R>(s, chunk, gr, fc, beta, chunk->p, p_out, chunk->r, chunk->w, u_halo, ud, nullptr,            \
+                       tl::NoFinish())
     if (fuse && refl) W2(true, true);
     else if (fuse) W2(true, false);
     else if (refl) W2(false, true);
@@ -620,6 +625,10 @@ void run_finalise(Chunk* chunk, Settings* settings)
     (void)settings;
     TlSuite2D* s = ready(chunk);
     if (!s) return;
+    if (tma_failed(s)) {
+        tl::fail(35, "a TMA row load of the w sweep did not complete (bounded barrier wait gave up)");
+        return;
+    }
     TL_LAUNCH(s, "k_finalise",
               k_finalise<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->energy, chunk->density, chunk->u));
 }

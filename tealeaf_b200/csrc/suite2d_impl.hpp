@@ -57,7 +57,22 @@ struct TlSuite2D {
     // FP32 buffers of the iterative-refinement form (mixed2d.cu), on first use.
     void* mx_slab = nullptr;
     size_t mx_bytes = 0;
+
+    // CG w sweep fed by TMA where the layout allows (tl2d_set_tma); tensor
+    // maps encoded once per array.
+    bool tma = true;
+    struct TmaEntry {
+        const double* ptr;
+        int kind;
+        CUtensorMap map;
+    };
+    TmaEntry tma_cache[8];
+    int tma_n = 0;
 };
+
+// Index of the int, in the mapped mirror words, that the bounded TMA barrier
+// waits set when one gives up.
+constexpr int kTmaErrWord2 = 15;
 
 // Launch on the suite stream, bracketed by profiler events when enabled.
 #define TL_LAUNCH(s, name, ...)                \
@@ -111,4 +126,55 @@ Faces faces_of(const Chunk* chunk);
 FieldBufferType* field_slot(Chunk* chunk, AltField f);
 void swap_alt(TlSuite2D* s, Chunk* chunk, AltField f);
 
+
+// Tensor map of a chunk array for k_cg_w_fused_tma: kind 0 operand rows (box
+// (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT).
+inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
+{
+    for (int i = 0; i < s->tma_n; ++i)
+        if (s->tma_cache[i].ptr == ptr && s->tma_cache[i].kind == kind) return &s->tma_cache[i].map;
+    if (s->tma_n == (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]))) return nullptr;
+    static const unsigned box[3] = {BX + 4, BX + 2, BX};
+    TlSuite2D::TmaEntry& e = s->tma_cache[s->tma_n];
+    if (!tl::tma_encode_3d(&e.map, ptr, s->g.x, s->g.y, 1, box[kind], kRowsT, 1)) return nullptr;
+    e.ptr = ptr;
+    e.kind = kind;
+    ++s->tma_n;
+    return &e.map;
+}
+
+// The boxes start at x = hd - 2 + 128 bx: an even halo depth and an even row
+// length keep every start and stride on a 16-byte boundary.
+inline bool tma_usable(const TlSuite2D* s) { return s->tma && s->g.hd % 2 == 0 && s->g.x % 2 == 0; }
+
+inline bool tma_failed(const TlSuite2D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord2] != 0; }
+
+// The fused CG w sweep (k_cg_w_fused semantics), by TMA where possible.
+template <bool F, bool R, typename Finish>
+void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
+                  double* p_out, const double* r, double* w, double* u_halo, int uhd, const int* done, Finish fin)
+{
+    if (tma_usable(s)) {
+        const CUtensorMap* a = tma_map(s, p_in, 0);
+        const CUtensorMap* b = F ? tma_map(s, r, 0) : a;
+        const CUtensorMap* kx = tma_map(s, chunk->kx, 1);
+        const CUtensorMap* ky = tma_map(s, chunk->ky, 2);
+        if (a && b && kx && ky) {
+            const Tma2Maps m{*a, *b, *kx, *ky};
+            static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k_cg_w_fused_tma<F, R, Finish>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaRowsBytes));
+                attr_set |= 1u << (s->device & 31);
+            }
+            TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused_tma<F, R><<<grid, BX, kTmaRowsBytes, s->stream>>>(
+                                             s->g, fc, beta, m, p_in, p_out, r, w, u_halo, uhd, s->rs, done, fin,
+                                             s->d_mirror + kTmaErrWord2)));
+            return;
+        }
+    }
+    TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<F, R><<<grid, BX, 0, s->stream>>>(
+                                     s->g, fc, beta, p_in, p_out, r, w, chunk->kx, chunk->ky, u_halo, uhd, s->rs,
+                                     done, fin)));
+}
 }  // namespace tl2d
