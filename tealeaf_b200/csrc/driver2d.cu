@@ -152,8 +152,7 @@ struct Run {
                                          nullptr, 0, done(), fin_w);
                 cur ^= 1;
             }
-            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
-                          s->g, alpha, chunk->u, buf[cur], chunk->r, chunk->w, s->rs, done(), fin_ur)));
+            launch_cg_ur2(s, gi, alpha, chunk->u, buf[cur], chunk->r, chunk->w, done(), fin_ur);
         };
         DevState st = loop(from, trip);
         // Trips from..st.trip-1 ran; the fused ones flipped the current buffer.
@@ -323,8 +322,7 @@ struct Run {
                                          done(), fin_w);
                 pc ^= 1;
             }
-            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<gi, BX, 0, s->stream>>>(
-                          s->g, alpha, chunk->u, pb[pc], rb[rc], chunk->w, s->rs, done(), tl::NoFinish())));
+            launch_cg_ur2(s, gi, alpha, chunk->u, pb[pc], rb[rc], chunk->w, done(), tl::NoFinish());
             if (blocked) {
                 for (int pp0 = 0; pp0 < ni; pp0 += kTB) {
                     const int L = std::min(kTB, ni - pp0);

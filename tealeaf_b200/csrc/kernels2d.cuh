@@ -843,6 +843,80 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
+// k_cg_ur_fused with its operands brought in by TMA: stages of kRowsU rows
+// of the block's strip of u, p, r, w (128-column boxes starting at the strip's
+// first column, even for an even halo depth). Same strips, rows in the same
+// order per thread, same arithmetic: the same results, partial sums included.
+constexpr int kRowsU = 4;
+constexpr int kStagesU = 3;
+struct RowsU {
+    alignas(128) double U[kRowsU][BX];
+    alignas(128) double P[kRowsU][BX];
+    alignas(128) double R[kRowsU][BX];
+    alignas(128) double W[kRowsU][BX];
+};
+struct TmaUrMaps {
+    CUtensorMap u, p, r, w;
+};
+constexpr size_t kTmaUrBytes = kStagesU * sizeof(RowsU) + kStagesU * 8 + 128;
+
+template <typename Finish>
+static __global__ void __launch_bounds__(BX, 4) k_cg_ur_fused_tma(Geo g, Scalar alpha,
+                                                               const __grid_constant__ TmaUrMaps maps,
+                                                               double* __restrict__ u, double* __restrict__ r,
+                                                               ReduceSlots rs, const int* __restrict__ done,
+                                                               Finish fin, int* err)
+{
+    extern __shared__ __align__(128) unsigned char tu_raw[];
+    if (gate_closed(done)) return;
+    unsigned char* base = tu_raw + ((128 - (tl::smem_addr(tu_raw) & 127)) & 127);
+    RowsU* ring = reinterpret_cast<RowsU*>(base);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesU * sizeof(RowsU));
+    Strip s(g);
+    double acc[1] = {0.0};
+    const int tx = threadIdx.x;
+    const int k0 = g.hd + blockIdx.x * BX;
+    const int np = (s.j1 - s.j0 + kRowsU - 1) / kRowsU;
+    auto issue = [&](int b) {
+        RowsU& S = ring[b % kStagesU];
+        unsigned long long* bar = &bars[b % kStagesU];
+        const int y0 = s.j0 + b * kRowsU;
+        tl::mbar_expect_tx(bar, 4u * sizeof(double) * kRowsU * BX);
+        tl::tma_load_3d(&S.U[0][0], &maps.u, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.P[0][0], &maps.p, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.R[0][0], &maps.r, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.W[0][0], &maps.w, k0, y0, 0, bar);
+    };
+    if (tx == 0) {
+        for (int q = 0; q < kStagesU; ++q) tl::mbar_init(&bars[q], 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (tx == 0)
+        for (int b = 0; b < kStagesU - 1 && b < np; ++b) issue(b);
+    const double a = alpha.get();
+    long i = s.k + (long)s.j0 * g.x;
+    for (int b = 0; b < np; ++b) {
+        tl::mbar_wait(&bars[b % kStagesU], (unsigned)(b / kStagesU) & 1u, err);
+        __syncthreads();   // every thread is past stage b-1: its slot is free
+        if (tx == 0 && b + kStagesU - 1 < np) issue(b + kStagesU - 1);
+        const RowsU& S = ring[b % kStagesU];
+#pragma unroll
+        for (int t = 0; t < kRowsU; ++t) {
+            const int j = s.j0 + b * kRowsU + t;
+            if (j >= s.j1) break;
+            if (s.active) {
+                u[i] = S.U[t][tx] + a * S.P[t][tx];
+                const double rn = S.R[t][tx] - a * S.W[t][tx];
+                r[i] = rn;
+                acc[0] += rn * rn;
+            }
+            i += g.x;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
 // p = beta p + r in place, with the depth-1 halo of p (and of u unless u is
 // null) written from the final values (the end of a device-resident CG phase: the last trip's
 // calc_p and halo update, cg_driver.c:116-123 + halo_update_driver).

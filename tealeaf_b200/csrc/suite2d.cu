@@ -484,9 +484,8 @@ void run_cg_calc_ur(Chunk* chunk, Settings* settings, double alpha, double* rrn)
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
     if (s->pend.calc_p || s->pend.halo[TL_FIELD_U]) flush(s, chunk);
-    TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<interior_grid(s->g), BX, 0, s->stream>>>(
-                                      s->g, Scalar{alpha, nullptr}, chunk->u, chunk->p, chunk->r, chunk->w, s->rs,
-                                      nullptr, tl::NoFinish())));
+    launch_cg_ur2(s, interior_grid(s->g), Scalar{alpha, nullptr}, chunk->u, chunk->p, chunk->r, chunk->w, nullptr,
+                  tl::NoFinish());
     double o;
     if (fetch(s, 1, &o)) *rrn += o;
 }

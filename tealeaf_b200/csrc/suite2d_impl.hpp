@@ -66,7 +66,7 @@ struct TlSuite2D {
         int kind;
         CUtensorMap map;
     };
-    TmaEntry tma_cache[8];
+    TmaEntry tma_cache[16];
     int tma_n = 0;
 };
 
@@ -128,15 +128,16 @@ void swap_alt(TlSuite2D* s, Chunk* chunk, AltField f);
 
 
 // Tensor map of a chunk array for k_cg_w_fused_tma: kind 0 operand rows (box
-// (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT).
+// (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT); for
+// k_cg_ur_fused_tma: kind 3 (BX x kRowsU).
 inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
 {
     for (int i = 0; i < s->tma_n; ++i)
         if (s->tma_cache[i].ptr == ptr && s->tma_cache[i].kind == kind) return &s->tma_cache[i].map;
     if (s->tma_n == (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]))) return nullptr;
-    static const unsigned box[3] = {BX + 4, BX + 2, BX};
+    static const unsigned box[4] = {BX + 4, BX + 2, BX, BX};
     TlSuite2D::TmaEntry& e = s->tma_cache[s->tma_n];
-    if (!tl::tma_encode_3d(&e.map, ptr, s->g.x, s->g.y, 1, box[kind], kRowsT, 1)) return nullptr;
+    if (!tl::tma_encode_3d(&e.map, ptr, s->g.x, s->g.y, 1, box[kind], kind == 3 ? kRowsU : kRowsT, 1)) return nullptr;
     e.ptr = ptr;
     e.kind = kind;
     ++s->tma_n;
@@ -150,8 +151,11 @@ inline bool tma_usable(const TlSuite2D* s) { return s->tma && s->g.hd % 2 == 0 &
 inline bool tma_failed(const TlSuite2D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord2] != 0; }
 
 // The fused CG w sweep (k_cg_w_fused semantics), by TMA where possible.
+// Internal linkage, like the kernels it launches: each translation unit has
+// its own kernel copies, so each keeps its own record of the raised
+// shared-memory limit.
 template <bool F, bool R, typename Finish>
-void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
+static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
                   double* p_out, const double* r, double* w, double* u_halo, int uhd, const int* done, Finish fin)
 {
     if (tma_usable(s)) {
@@ -176,5 +180,33 @@ void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar
     TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused<F, R><<<grid, BX, 0, s->stream>>>(
                                      s->g, fc, beta, p_in, p_out, r, w, chunk->kx, chunk->ky, u_halo, uhd, s->rs,
                                      done, fin)));
+}
+
+// The fused CG u/r update (k_cg_ur_fused semantics), by TMA where possible
+// (internal linkage as launch_cg_w2).
+template <typename Finish>
+static void launch_cg_ur2(TlSuite2D* s, dim3 grid, Scalar alpha, double* u, const double* p, double* r, const double* w,
+                   const int* done, Finish fin)
+{
+    if (tma_usable(s)) {
+        const CUtensorMap* mu = tma_map(s, u, 3);
+        const CUtensorMap* mp = tma_map(s, p, 3);
+        const CUtensorMap* mr = tma_map(s, r, 3);
+        const CUtensorMap* mw = tma_map(s, w, 3);
+        if (mu && mp && mr && mw) {
+            const TmaUrMaps m{*mu, *mp, *mr, *mw};
+            static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k_cg_ur_fused_tma<Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kTmaUrBytes));
+                attr_set |= 1u << (s->device & 31);
+            }
+            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused_tma<<<grid, BX, kTmaUrBytes, s->stream>>>(
+                                              s->g, alpha, m, u, r, s->rs, done, fin, s->d_mirror + kTmaErrWord2)));
+            return;
+        }
+    }
+    TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<grid, BX, 0, s->stream>>>(s->g, alpha, u, p, r, w, s->rs, done,
+                                                                            fin)));
 }
 }  // namespace tl2d

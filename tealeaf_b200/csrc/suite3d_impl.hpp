@@ -131,8 +131,11 @@ inline bool tma_usable(const TlSuite3D* s) { return s->tma && s->g.hd % 2 == 0 &
 inline bool tma_failed(const TlSuite3D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord] != 0; }
 
 // The fused CG w sweep (k3_cg_w semantics), by TMA where possible.
+// Internal linkage, like the kernels it launches: each translation unit has
+// its own kernel copies, so each keeps its own record of the raised
+// shared-memory limit.
 template <bool F, bool R, typename Finish>
-void launch_cg_w3(TlSuite3D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
+static void launch_cg_w3(TlSuite3D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
                   double* p_out, const double* r, double* w, double* u_halo, int uhd, const int* done, Finish fin)
 {
     const dim3 bl = interior_block();
