@@ -201,8 +201,7 @@ int adjoint_solve(TlSuite3D* s, Chunk* chunk, const double* rhs, double* lam, do
                                      nullptr, 0, done, fin_w);
             cur ^= 1;
         }
-        TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(s->g, alpha, lam, buf[cur], chunk->vec_r,
-                                                                       chunk->vec_w, s->rs, done, fin_ur)));
+        launch_cg_ur3(s, gi, alpha, lam, buf[cur], chunk->vec_r, chunk->vec_w, done, fin_ur);
     });
     DevState st{};
     TL_CUDA(cudaMemcpy(&st, s->d_state, sizeof(DevState), cudaMemcpyDeviceToHost));

@@ -108,8 +108,7 @@ struct Run3 {
                                          nullptr, 0, done(), fin_w);
                 cur ^= 1;
             }
-            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(
-                           s->g, alpha, chunk->vec_u, buf[cur], chunk->vec_r, chunk->vec_w, s->rs, done(), fin_ur)));
+            launch_cg_ur3(s, gi, alpha, chunk->vec_u, buf[cur], chunk->vec_r, chunk->vec_w, done(), fin_ur);
         };
         DevState st = loop(from, trip);
         const int ran = st.trip - from;
@@ -224,8 +223,7 @@ struct Run3 {
                                          0, done(), fin_w);
                 pc ^= 1;
             }
-            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<gi, bl, 0, s->stream>>>(
-                           s->g, alpha, chunk->vec_u, pb[pc], rb[rc], chunk->vec_w, s->rs, done(), tl::NoFinish())));
+            launch_cg_ur3(s, gi, alpha, chunk->vec_u, pb[pc], rb[rc], chunk->vec_w, done(), tl::NoFinish());
             for (int pp = 0; pp < ni; ++pp) {
                 const bool last = pp == ni - 1;
 #define STEP3(FOLD, NORM, FIN)                                                                                    \

@@ -492,6 +492,80 @@ static __global__ void __launch_bounds__(NT, 8) k3_cg_ur(Geo g, Scalar alpha, do
     tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
 }
 
+// k3_cg_ur with its operands brought in by TMA: stages of kPlanesU z-planes of
+// the block's 32 x 8 columns of u, p, r, w. Same pencils, planes in the same
+// order per thread, same arithmetic: the same results, partial sums included.
+constexpr int kPlanesU = 2;
+constexpr int kStagesU3 = 3;
+struct PlanesU {
+    alignas(128) double U[kPlanesU][BY][BX];
+    alignas(128) double P[kPlanesU][BY][BX];
+    alignas(128) double R[kPlanesU][BY][BX];
+    alignas(128) double W[kPlanesU][BY][BX];
+};
+struct Tma3UrMaps {
+    CUtensorMap u, p, r, w;
+};
+constexpr size_t kTmaUr3Bytes = kStagesU3 * sizeof(PlanesU) + kStagesU3 * 8 + 128;
+
+template <typename Finish>
+static __global__ void __launch_bounds__(NT, 4) k3_cg_ur_tma(Geo g, Scalar alpha,
+                                                          const __grid_constant__ Tma3UrMaps maps,
+                                                          double* __restrict__ u, double* __restrict__ r,
+                                                          ReduceSlots rs, const int* __restrict__ done, Finish fin,
+                                                          int* err)
+{
+    extern __shared__ __align__(128) unsigned char u3_raw[];
+    if (gate_closed(done)) return;
+    unsigned char* base = u3_raw + ((128 - (tl::smem_addr(u3_raw) & 127)) & 127);
+    PlanesU* ring = reinterpret_cast<PlanesU*>(base);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesU3 * sizeof(PlanesU));
+    Pencil s(g);
+    double acc[1] = {0.0};
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = tx == 0 && ty == 0;
+    const int kb = g.hd + blockIdx.x * BX, jb = g.hd + blockIdx.y * BY;
+    const int np = (s.i1 - s.i0 + kPlanesU - 1) / kPlanesU;
+    auto issue = [&](int b) {
+        PlanesU& S = ring[b % kStagesU3];
+        unsigned long long* bar = &bars[b % kStagesU3];
+        const int z0 = s.i0 + b * kPlanesU;
+        tl::mbar_expect_tx(bar, 4u * sizeof(double) * kPlanesU * BY * BX);
+        tl::tma_load_3d(&S.U[0][0][0], &maps.u, kb, jb, z0, bar);
+        tl::tma_load_3d(&S.P[0][0][0], &maps.p, kb, jb, z0, bar);
+        tl::tma_load_3d(&S.R[0][0][0], &maps.r, kb, jb, z0, bar);
+        tl::tma_load_3d(&S.W[0][0][0], &maps.w, kb, jb, z0, bar);
+    };
+    if (leader) {
+        for (int q = 0; q < kStagesU3; ++q) tl::mbar_init(&bars[q], 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (leader)
+        for (int b = 0; b < kStagesU3 - 1 && b < np; ++b) issue(b);
+    const double a = alpha.get();
+    const long xy = g.xy();
+    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+    for (int b = 0; b < np; ++b) {
+        tl::mbar_wait(&bars[b % kStagesU3], (unsigned)(b / kStagesU3) & 1u, err);
+        __syncthreads();   // every thread is past stage b-1: its slot is free
+        if (leader && b + kStagesU3 - 1 < np) issue(b + kStagesU3 - 1);
+        const PlanesU& S = ring[b % kStagesU3];
+#pragma unroll
+        for (int t = 0; t < kPlanesU; ++t) {
+            if (s.i0 + b * kPlanesU + t >= s.i1) break;
+            if (s.active) {
+                u[i] = S.U[t][ty][tx] + a * S.P[t][ty][tx];
+                const double rn = S.R[t][ty][tx] - a * S.W[t][ty][tx];
+                r[i] = rn;
+                acc[0] += rn * rn;
+            }
+            i += xy;
+        }
+    }
+    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+}
+
 // p = beta p + r (APPLY_P) and the depth-1 halos of p and (unless null) u.
 static __global__ void __launch_bounds__(NT) k3_cg_close(Geo g, Faces fc, Scalar beta, int apply_p,
                                                         double* __restrict__ p, const double* __restrict__ r,

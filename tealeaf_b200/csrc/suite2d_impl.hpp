@@ -68,6 +68,7 @@ struct TlSuite2D {
     };
     TmaEntry tma_cache[16];
     int tma_n = 0;
+    int tma_next = 0;
 };
 
 // Index of the int, in the mapped mirror words, that the bounded TMA barrier
@@ -134,13 +135,17 @@ inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
 {
     for (int i = 0; i < s->tma_n; ++i)
         if (s->tma_cache[i].ptr == ptr && s->tma_cache[i].kind == kind) return &s->tma_cache[i].map;
-    if (s->tma_n == (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]))) return nullptr;
+    // a full cache recycles its entries in turn (arrays of released buffers)
+    const int cap = (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]));
+    const int slot = s->tma_n < cap ? s->tma_n : (s->tma_next++ % cap);
     static const unsigned box[4] = {BX + 4, BX + 2, BX, BX};
-    TlSuite2D::TmaEntry& e = s->tma_cache[s->tma_n];
-    if (!tl::tma_encode_3d(&e.map, ptr, s->g.x, s->g.y, 1, box[kind], kind == 3 ? kRowsU : kRowsT, 1)) return nullptr;
+    CUtensorMap m;
+    if (!tl::tma_encode_3d(&m, ptr, s->g.x, s->g.y, 1, box[kind], kind == 3 ? kRowsU : kRowsT, 1)) return nullptr;
+    TlSuite2D::TmaEntry& e = s->tma_cache[slot];
+    e.map = m;
     e.ptr = ptr;
     e.kind = kind;
-    ++s->tma_n;
+    if (s->tma_n < cap) ++s->tma_n;
     return &e.map;
 }
 

@@ -457,9 +457,8 @@ void run_cg_solver_calc_ur(Chunk* chunk, Settings* settings, double alpha, doubl
     TlSuite3D* s = suite_of(chunk);
     if (!s) return;
     if (s->pend.calc_p || s->pend.halo[TL3_FIELD_U]) flush(s, chunk);
-    TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<interior_grid(s->g), interior_block(), 0, s->stream>>>(
-                                  s->g, Scalar{alpha, nullptr}, chunk->vec_u, chunk->vec_p, chunk->vec_r,
-                                  chunk->vec_w, s->rs, nullptr, tl::NoFinish())));
+    launch_cg_ur3(s, interior_grid(s->g), Scalar{alpha, nullptr}, chunk->vec_u, chunk->vec_p, chunk->vec_r,
+                  chunk->vec_w, nullptr, tl::NoFinish());
     double o;
     if (fetch(s, 1, &o)) *rrn += o;
 }

@@ -44,8 +44,9 @@ struct TlSuite3D {
         int kind;
         CUtensorMap map;
     };
-    TmaEntry tma_cache[12];
+    TmaEntry tma_cache[24];
     int tma_n = 0;
+    int tma_next = 0;
 };
 
 // Index of the int, in the mapped mirror words, that the bounded TMA barrier
@@ -109,18 +110,25 @@ void swap_alt(TlSuite3D* s, Chunk* chunk, AltField3 f);
 
 
 // Tensor map of a chunk array for walkt: kind 0 operand (box (BX+4) x (BY+2)),
-// 1 kx (BX+2) x BY, 2 ky BX x (BY+1), 3 kz BX x BY; encoded once per array.
+// 1 kx (BX+2) x BY, 2 ky BX x (BY+1), 3 kz BX x BY; for k3_cg_ur_tma kind 4
+// BX x BY x kPlanesU; encoded once per array.
 inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
 {
     for (int i = 0; i < s->tma_n; ++i)
         if (s->tma_cache[i].ptr == ptr && s->tma_cache[i].kind == kind) return &s->tma_cache[i].map;
-    if (s->tma_n == (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]))) return nullptr;
-    static const unsigned box[4][2] = {{BX + 4, BY + 2}, {BX + 2, BY}, {BX, BY + 1}, {BX, BY}};
-    TlSuite3D::TmaEntry& e = s->tma_cache[s->tma_n];
-    if (!tl::tma_encode_3d(&e.map, ptr, s->g.x, s->g.y, s->g.z, box[kind][0], box[kind][1], 1)) return nullptr;
+    // a full cache recycles its entries in turn (arrays of released buffers)
+    const int cap = (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]));
+    const int slot = s->tma_n < cap ? s->tma_n : (s->tma_next++ % cap);
+    static const unsigned box[5][3] = {{BX + 4, BY + 2, 1}, {BX + 2, BY, 1}, {BX, BY + 1, 1}, {BX, BY, 1},
+                                       {BX, BY, kPlanesU}};
+    CUtensorMap m;
+    if (!tl::tma_encode_3d(&m, ptr, s->g.x, s->g.y, s->g.z, box[kind][0], box[kind][1], box[kind][2]))
+        return nullptr;
+    TlSuite3D::TmaEntry& e = s->tma_cache[slot];
+    e.map = m;
     e.ptr = ptr;
     e.kind = kind;
-    ++s->tma_n;
+    if (s->tma_n < cap) ++s->tma_n;
     return &e.map;
 }
 
@@ -162,5 +170,33 @@ static void launch_cg_w3(TlSuite3D* s, Chunk* chunk, dim3 grid, const Faces& fc,
     TL3_LAUNCH(s, "k3_cg_w", (k3_cg_w<F, R><<<grid, bl, 0, s->stream>>>(s->g, fc, beta, p_in, p_out, r, w,
                                                                       chunk->vec_kx, chunk->vec_ky, chunk->vec_kz,
                                                                       u_halo, uhd, s->rs, done, fin)));
+}
+
+// The fused CG u/r update (k3_cg_ur semantics), by TMA where possible
+// (internal linkage as launch_cg_w3).
+template <typename Finish>
+static void launch_cg_ur3(TlSuite3D* s, dim3 grid, Scalar alpha, double* u, const double* p, double* r,
+                          const double* w, const int* done, Finish fin)
+{
+    const dim3 bl = interior_block();
+    if (tma_usable(s)) {
+        const CUtensorMap* mu = tma_map(s, u, 4);
+        const CUtensorMap* mp = tma_map(s, p, 4);
+        const CUtensorMap* mr = tma_map(s, r, 4);
+        const CUtensorMap* mw = tma_map(s, w, 4);
+        if (mu && mp && mr && mw) {
+            const Tma3UrMaps m{*mu, *mp, *mr, *mw};
+            static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k3_cg_ur_tma<Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kTmaUr3Bytes));
+                attr_set |= 1u << (s->device & 31);
+            }
+            TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur_tma<<<grid, bl, kTmaUr3Bytes, s->stream>>>(
+                                          s->g, alpha, m, u, r, s->rs, done, fin, s->d_mirror + kTmaErrWord)));
+            return;
+        }
+    }
+    TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<grid, bl, 0, s->stream>>>(s->g, alpha, u, p, r, w, s->rs, done, fin)));
 }
 }  // namespace tl3d
