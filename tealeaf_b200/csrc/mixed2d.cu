@@ -17,6 +17,7 @@
 #include "host_maths.hpp"
 #include "pcblock2d.cuh"
 #include "refine2d.cuh"
+#include "rftma2d.cuh"
 #include "suite2d_impl.hpp"
 
 #include <cmath>
@@ -152,6 +153,73 @@ RfBuffers<T> rf_buffers(TlSuite2D* s, int fields)
     return b;
 }
 
+// Tensor map of a refinement array (T layout: xp x (ny + 2)): tile rows
+// (RfRowsW<T>::W x kRfRows) or the 16-byte ring boxes.
+template <typename T>
+const CUtensorMap* rf_map(TlSuite2D* s, const Lay& L, const T* ptr, bool ring)
+{
+    const int kind = 16 + (sizeof(T) == 4 ? 0 : 8) + (ring ? 1 : 0);
+    return tma_lookup(s, ptr, kind, [&](CUtensorMap* m) {
+        return tl::tma_encode_3d(m, ptr, L.xp, L.ny + 2, 1, ring ? RfRowsW<T>::H : RfRowsW<T>::W, kRfRows, 1,
+                                 (int)sizeof(T));
+    });
+}
+
+// The refinement w sweep (k_rf_w semantics), by TMA where the maps encode.
+// Internal linkage with the kernels, as the drop-in helpers.
+template <typename T, bool FUSE_P>
+void rf_w(TlSuite2D* s, const RfBuffers<T>& b, dim3 gl, const char* name, const T* p_in, T* p_out, const T* r,
+          FinMxW fin)
+{
+    if (s->tma) {
+        const CUtensorMap *mp = rf_map(s, b.L, p_in, false), *mph = rf_map(s, b.L, p_in, true);
+        const CUtensorMap *mr = rf_map(s, b.L, r, false), *mrh = rf_map(s, b.L, r, true);
+        const CUtensorMap *mkx = rf_map<T>(s, b.L, b.f[RF_KX], false), *mkxh = rf_map<T>(s, b.L, b.f[RF_KX], true);
+        const CUtensorMap* mky = rf_map<T>(s, b.L, b.f[RF_KY], false);
+        if (mp && mph && mr && mrh && mkx && mkxh && mky) {
+            const RfWMaps m{*mp, *mr, *mkx, *mky, *mph, *mrh, *mkxh};
+            constexpr size_t smem = rf_w_tma_bytes<T>();
+            static unsigned attr_set = 0;
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k_rf_w_tma<T, FUSE_P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+                attr_set |= 1u << (s->device & 31);
+            }
+            TL_LAUNCH(s, name, (k_rf_w_tma<T, FUSE_P><<<gl, BX, smem, s->stream>>>(
+                                   b.L, b.st, m, p_out, b.f[RF_W], s->rs, fin, s->d_mirror + kTmaErrWord2)));
+            return;
+        }
+    }
+    TL_LAUNCH(s, name, (k_rf_w<T, FUSE_P><<<gl, BX, 0, s->stream>>>(b.L, b.st, p_in, p_out, r, b.f[RF_W],
+                                                                     b.f[RF_KX], b.f[RF_KY], s->rs, fin)));
+}
+
+// The refinement u/r update (k_rf_ur semantics), by TMA where the maps encode.
+template <typename T>
+void rf_ur(TlSuite2D* s, const RfBuffers<T>& b, dim3 gl, const char* name, const T* p, T* r, FinMxUr fin)
+{
+    if (s->tma) {
+        const CUtensorMap* mx = rf_map<T>(s, b.L, b.f[RF_XS], false);
+        const CUtensorMap* mp = rf_map(s, b.L, p, false);
+        const CUtensorMap* mr = rf_map<T>(s, b.L, r, false);
+        const CUtensorMap* mw = rf_map<T>(s, b.L, b.f[RF_W], false);
+        if (mx && mp && mr && mw) {
+            const RfUMaps m{*mx, *mp, *mr, *mw};
+            constexpr size_t smem = rf_u_tma_bytes<T>();
+            static unsigned attr_set = 0;
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k_rf_ur_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+                attr_set |= 1u << (s->device & 31);
+            }
+            TL_LAUNCH(s, name, (k_rf_ur_tma<T><<<gl, BX, smem, s->stream>>>(b.L, b.st, m, b.f[RF_XS], r, s->rs, fin,
+                                                                           s->d_mirror + kTmaErrWord2)));
+            return;
+        }
+    }
+    TL_LAUNCH(s, name, (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(b.L, b.st, b.f[RF_XS], p, r, b.f[RF_W], s->rs, fin)));
+}
+
 // Launches trips t = 0.. in batches of kBatch, looking at the mapped done word
 // of the previous batch while the current one runs (as driver2d.cu).
 template <typename F>
@@ -212,17 +280,12 @@ int solve_refined(TlSuite2D* s, Chunk* chunk, int max_iters, double rel_tol, int
     int cur = 0;
     batched(s, max_iters, [&](int t) {
         if (t == 0) {
-            TL_LAUNCH(s, nm[1], (k_rf_w<T, false><<<gl, BX, 0, s->stream>>>(
-                                    L, b.st, pb[cur], pb[cur], b.f[RF_R], b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
-                                    FinMxW{b.st})));
+            rf_w<T, false>(s, b, gl, nm[1], pb[cur], pb[cur], b.f[RF_R], FinMxW{b.st});
         } else {
-            TL_LAUNCH(s, nm[1], (k_rf_w<T, true><<<gl, BX, 0, s->stream>>>(
-                                    L, b.st, pb[cur], pb[cur ^ 1], b.f[RF_R], b.f[RF_W], b.f[RF_KX], b.f[RF_KY],
-                                    s->rs, FinMxW{b.st})));
+            rf_w<T, true>(s, b, gl, nm[1], pb[cur], pb[cur ^ 1], b.f[RF_R], FinMxW{b.st});
             cur ^= 1;
         }
-        TL_LAUNCH(s, nm[2], (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(L, b.st, b.f[RF_XS], pb[cur], b.f[RF_R],
-                                                                   b.f[RF_W], s->rs, FinMxUr{b.st, s->d_mirror})));
+        rf_ur<T>(s, b, gl, nm[2], pb[cur], b.f[RF_R], FinMxUr{b.st, s->d_mirror});
         TL_LAUNCH(s, nm[3], (k_rf_fold<T><<<gl, BX, 0, s->stream>>>(L, b.st, s->g.x, s->g.hd, chunk->u,
                                                                      b.f[RF_XS])));
         TL_LAUNCH(s, nm[4], (k_rf_resid<T><<<gl, BX, 0, s->stream>>>(L, b.st, s->g.x, s->g.hd, chunk->u,
@@ -299,13 +362,9 @@ int solve_refined_ppcg(TlSuite2D* s, Chunk* chunk, Settings* settings, double re
     };
     auto w_sweep = [&](int t, double* alphas) {
         if (t == 0) {
-            TL_LAUNCH(s, nm[1], (k_rf_w<T, false><<<gl, BX, 0, s->stream>>>(
-                                    L, b.st, pb[cur], pb[cur], r, b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
-                                    FinMxW{b.st, alphas})));
+            rf_w<T, false>(s, b, gl, nm[1], pb[cur], pb[cur], r, FinMxW{b.st, alphas});
         } else {
-            TL_LAUNCH(s, nm[1], (k_rf_w<T, true><<<gl, BX, 0, s->stream>>>(
-                                    L, b.st, pb[cur], pb[cur ^ 1], r, b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
-                                    FinMxW{b.st, alphas})));
+            rf_w<T, true>(s, b, gl, nm[1], pb[cur], pb[cur ^ 1], r, FinMxW{b.st, alphas});
             cur ^= 1;
         }
     };
@@ -315,8 +374,7 @@ int solve_refined_ppcg(TlSuite2D* s, Chunk* chunk, Settings* settings, double re
                                : FinMxUr{b.st, s->d_mirror, s->d_cg_betas, settings->presteps, 1.0};
     batched(s, max_iters, [&](int t) {
         w_sweep(t, s->d_cg_alphas);
-        TL_LAUNCH(s, nm[2], (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(L, b.st, b.f[RF_XS], pb[cur], r, b.f[RF_W],
-                                                                   s->rs, cg_fin)));
+        rf_ur<T>(s, b, gl, nm[2], pb[cur], r, cg_fin);
         fold_resid(s->d_cg_betas);
     });
     MxState st{};
@@ -378,12 +436,9 @@ int solve_refined_ppcg(TlSuite2D* s, Chunk* chunk, Settings* settings, double re
                                         L, b.st, theta, ca, cb, ni - 1, sb[c], qb[c], z, r, s->rs, FinPcgZ{b.st})));
             }
             // p = z + beta p, w = A p, alpha = r.z / p.w
-            TL_LAUNCH(s, nm[1], (k_rf_w<T, true><<<gl, BX, 0, s->stream>>>(
-                                    L, b.st, pb[cur], pb[cur ^ 1], z, b.f[RF_W], b.f[RF_KX], b.f[RF_KY], s->rs,
-                                    FinMxW{b.st, nullptr, true})));
+            rf_w<T, true>(s, b, gl, nm[1], pb[cur], pb[cur ^ 1], z, FinMxW{b.st, nullptr, true});
             cur ^= 1;
-            TL_LAUNCH(s, nm[2], (k_rf_ur<T><<<gl, BX, 0, s->stream>>>(L, b.st, b.f[RF_XS], pb[cur], r, b.f[RF_W],
-                                                                       s->rs, FinMxUr{b.st, s->d_mirror})));
+            rf_ur<T>(s, b, gl, nm[2], pb[cur], r, FinMxUr{b.st, s->d_mirror});
             fold_resid(nullptr);
         });
         TL_CUDA(cudaMemcpy(&st, b.st, sizeof(MxState), cudaMemcpyDeviceToHost));

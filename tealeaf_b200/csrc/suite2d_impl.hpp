@@ -62,11 +62,11 @@ struct TlSuite2D {
     // maps encoded once per array.
     bool tma = true;
     struct TmaEntry {
-        const double* ptr;
+        const void* ptr;
         int kind;
         CUtensorMap map;
     };
-    TmaEntry tma_cache[16];
+    TmaEntry tma_cache[48];
     int tma_n = 0;
     int tma_next = 0;
 };
@@ -128,25 +128,34 @@ FieldBufferType* field_slot(Chunk* chunk, AltField f);
 void swap_alt(TlSuite2D* s, Chunk* chunk, AltField f);
 
 
-// Tensor map of a chunk array for k_cg_w_fused_tma: kind 0 operand rows (box
-// (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT); for
-// k_cg_ur_fused_tma: kind 3 (BX x kRowsU).
-inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
+// A cached tensor map: (ptr, kind) -> map, encoded by `encode` on a miss; a
+// full cache recycles its entries in turn (arrays of released buffers).
+template <typename Encode>
+inline const CUtensorMap* tma_lookup(TlSuite2D* s, const void* ptr, int kind, Encode encode)
 {
     for (int i = 0; i < s->tma_n; ++i)
         if (s->tma_cache[i].ptr == ptr && s->tma_cache[i].kind == kind) return &s->tma_cache[i].map;
-    // a full cache recycles its entries in turn (arrays of released buffers)
     const int cap = (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]));
     const int slot = s->tma_n < cap ? s->tma_n : (s->tma_next++ % cap);
-    static const unsigned box[4] = {BX + 4, BX + 2, BX, BX};
     CUtensorMap m;
-    if (!tl::tma_encode_3d(&m, ptr, s->g.x, s->g.y, 1, box[kind], kind == 3 ? kRowsU : kRowsT, 1)) return nullptr;
+    if (!encode(&m)) return nullptr;
     TlSuite2D::TmaEntry& e = s->tma_cache[slot];
     e.map = m;
     e.ptr = ptr;
     e.kind = kind;
     if (s->tma_n < cap) ++s->tma_n;
     return &e.map;
+}
+
+// Tensor map of a chunk array for k_cg_w_fused_tma: kind 0 operand rows (box
+// (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT); for
+// k_cg_ur_fused_tma: kind 3 (BX x kRowsU).
+inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
+{
+    static const unsigned box[4] = {BX + 4, BX + 2, BX, BX};
+    return tma_lookup(s, ptr, kind, [&](CUtensorMap* m) {
+        return tl::tma_encode_3d(m, ptr, s->g.x, s->g.y, 1, box[kind], kind == 3 ? kRowsU : kRowsT, 1);
+    });
 }
 
 // The boxes start at x = hd - 2 + 128 bx: an even halo depth and an even row

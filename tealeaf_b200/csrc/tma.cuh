@@ -76,11 +76,12 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// Host: a 3D map of doubles over an (nx, ny, nz) array (x fastest) with the
-// given box, out-of-range cells read as zero; false when the driver entry
-// point is missing or the encoding is refused (alignment, sizes).
-inline bool tma_encode_3d(CUtensorMap* map, const double* base, long nx, long ny, long nz, unsigned bx,
-                          unsigned by, unsigned bz)
+// Host: a 3D map of doubles (esize 8) or floats (esize 4) over an
+// (nx, ny, nz) array (x fastest) with the given box, out-of-range cells read
+// as zero; false when the driver entry point is missing or the encoding is
+// refused (alignment, sizes).
+inline bool tma_encode_3d(CUtensorMap* map, const void* base, long nx, long ny, long nz, unsigned bx, unsigned by,
+                          unsigned bz, int esize = 8)
 {
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -98,12 +99,13 @@ inline bool tma_encode_3d(CUtensorMap* map, const double* base, long nx, long ny
             cudaGetLastError();
     }
     if (!encode) return false;
-    if ((reinterpret_cast<unsigned long long>(base) & 15u) != 0 || ((nx * 8) & 15) != 0) return false;
+    if ((reinterpret_cast<unsigned long long>(base) & 15u) != 0 || ((nx * esize) & 15) != 0) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-    const cuuint64_t strides[2] = {(cuuint64_t)(nx * 8), (cuuint64_t)(nx * ny * 8)};
+    const cuuint64_t strides[2] = {(cuuint64_t)(nx * esize), (cuuint64_t)(nx * ny * esize)};
     const cuuint32_t box[3] = {bx, by, bz};
     const cuuint32_t es[3] = {1, 1, 1};
-    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, es,
+    const CUtensorMapDataType dt = esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    return encode(map, dt, 3, const_cast<void*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }

@@ -142,3 +142,27 @@ def test_blocked_preconditioner_matches_one_step_chain(precision, inner):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("precision,solver", [(32, "cg"), (64, "cg"), (32, "ppcg"), (64, "ppcg")])
+def test_tma_sweeps_match_direct_loads(precision, solver):
+    """The refinement sweeps fed by TMA row loads and the ones reading their
+    operands directly give the same solve bit for bit (same tiles, rows and
+    reduction partials), on a mesh of ragged tiles (600 = 2 x 256 + 88 FP32
+    columns, 4 x 128 + 88 FP64) over three timesteps."""
+    p = problems.seeded(2, (600, 157), 19, 8, 2, solver=solver, eps=1e-15, end_step=3, name="rftma")
+    if solver == "ppcg":
+        p = p.with_(presteps=10)
+    a, b = Host(p.tea_in(), 2), Host(p.tea_in(), 2)
+    try:
+        b.lib.tl2d_set_tma(b.chunk, 0)
+        for tt in range(3):
+            ra = a.refine_step(tt, REL_TOL, precision)
+            rb = b.refine_step(tt, REL_TOL, precision)
+            assert (ra.iterations, ra.cg_trips, ra.residual_updates) == (rb.iterations, rb.cg_trips,
+                                                                       rb.residual_updates)
+            assert ra.rel_residual == rb.rel_residual
+            assert ra.summary == rb.summary
+    finally:
+        a.finalise()
+        b.finalise()
