@@ -188,6 +188,8 @@ def bench_b200(args, rank, world, local_rank):
     h = Host(prob.tea_in(), dims=2)
     if args.no_temporal_blocking:
         h.lib.tl2d_set_temporal_blocking(C.byref(h.chunk), 0)
+    if args.no_tma:
+        h.lib.tl2d_set_tma(C.byref(h.chunk), 0)
     stream = torch.cuda.ExternalStream(h.lib.tl2d_stream(C.byref(h.chunk)))
     cells = args.size * args.size
     interior_launch_cells = cells
@@ -366,6 +368,8 @@ def bench_dropin3d(args) -> dict:
     prob = problems.adjoint_3d(n, seed=4, steps=args.warmup + 2 * args.steps + 4).with_(solver=args.solver)
     h = Host(prob.tea_in(), dims=3)
     lib = h.lib
+    if args.no_tma:
+        lib.tl3d_set_tma(C.byref(h.chunk), 0)
     stream = torch.cuda.ExternalStream(lib.tl3d_stream(C.byref(h.chunk)))
     tt = 0
     for _ in range(args.warmup):
@@ -684,6 +688,8 @@ def main():
     ap.add_argument("--e2e-kernel-interface", type=int, default=1)
     ap.add_argument("--no-temporal-blocking", action="store_true",
                     help="Chebyshev/PPCG: one launch per trip instead of shared-memory blocks")
+    ap.add_argument("--no-tma", action="store_true",
+                    help="stencil sweeps read their operands with per-thread loads instead of TMA tile loads")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

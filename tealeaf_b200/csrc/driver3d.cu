@@ -144,7 +144,8 @@ struct Run3 {
                    (k3_cheby_trip<false, false, true><<<gh, bl, 0, s->stream>>>(
                        s->g, none, tl::ChebyCoef{0.0, 0.0, nullptr, nullptr, nullptr}, chunk->theta, 1, chunk->vec_u,
                        chunk->vec_p, chunk->vec_u, chunk->vec_p, chunk->vec_u0, chunk->vec_w, chunk->vec_r,
-                       chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr, tl::NoFinish(), pc)));
+                       chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr, tl::NoFinish(), pc, Tma3Maps{},
+                       nullptr)));
         copy(s->alt[ALT3_U], chunk->vec_u);
         copy(s->alt[ALT3_P], chunk->vec_p);
         DevState st = host_state;
@@ -159,10 +160,22 @@ struct Run3 {
         int cur = 0;
         auto trip = [&](int, int force) {
             tl::FinChebyTrip fin{s->d_state, pc, s->d_mirror, force};
-            TL3_LAUNCH(s, "k3_cheby_trip", (k3_cheby_trip<true, true, false><<<gh, bl, 0, s->stream>>>(
-                           s->g, fc, coef, 0.0, force, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->vec_u0,
-                           chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(),
-                           fin, pc)));
+            Tma3Maps m{};
+            if (sweep_maps(s, chunk, ub[cur], pb[cur], &m)) {
+                static unsigned set = 0;
+                raise_ring_smem(s, k3_cheby_trip<true, true, false, tl::FinChebyTrip, true>, set);
+                TL3_LAUNCH(s, "k3_cheby_trip",
+                           (k3_cheby_trip<true, true, false, tl::FinChebyTrip, true><<<gh, bl, kTmaRingBytes,
+                                                                                       s->stream>>>(
+                               s->g, fc, coef, 0.0, force, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->vec_u0,
+                               chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(),
+                               fin, pc, m, s->d_mirror + kTmaErrWord)));
+            } else {
+                TL3_LAUNCH(s, "k3_cheby_trip", (k3_cheby_trip<true, true, false><<<gh, bl, 0, s->stream>>>(
+                               s->g, fc, coef, 0.0, force, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->vec_u0,
+                               chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(),
+                               fin, pc, Tma3Maps{}, nullptr)));
+            }
             cur ^= 1;
         };
         trip(tt, 1);
@@ -227,10 +240,23 @@ struct Run3 {
             for (int pp = 0; pp < ni; ++pp) {
                 const bool last = pp == ni - 1;
 #define STEP3(FOLD, NORM, FIN)                                                                                    \
-    TL3_LAUNCH(s, "k3_ppcg_step", (k3_ppcg_step<FOLD, NORM><<<gh, bl, 0, s->stream>>>(                            \
-                                      s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1], \
-                                      chunk->vec_u, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(),    \
-                                      FIN)))
+    do {                                                                                                          \
+        Tma3Maps m{};                                                                                             \
+        if (sweep_maps(s, chunk, sb[sc], rb[rc], &m)) {                                                           \
+            static unsigned set = 0;                                                                              \
+            raise_ring_smem(s, k3_ppcg_step<FOLD, NORM, decltype(FIN), true>, set);                               \
+            TL3_LAUNCH(s, "k3_ppcg_step",                                                                         \
+                       (k3_ppcg_step<FOLD, NORM, decltype(FIN), true><<<gh, bl, kTmaRingBytes, s->stream>>>(       \
+                           s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc], rb[rc ^ 1],         \
+                           chunk->vec_u, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, done(), FIN, m,     \
+                           s->d_mirror + kTmaErrWord)));                                                          \
+        } else {                                                                                                  \
+            TL3_LAUNCH(s, "k3_ppcg_step", (k3_ppcg_step<FOLD, NORM><<<gh, bl, 0, s->stream>>>(                    \
+                                              s->g, fc, chunk->theta, coef, pp - 1, sb[sc], sb[sc ^ 1], rb[rc],  \
+                                              rb[rc ^ 1], chunk->vec_u, chunk->vec_kx, chunk->vec_ky,           \
+                                              chunk->vec_kz, s->rs, done(), FIN, Tma3Maps{}, nullptr)));          \
+        }                                                                                                         \
+    } while (0)
                 if (pp == 0 && last) STEP3(1, true, fin_n);
                 else if (pp == 0) STEP3(1, false, tl::NoFinish());
                 else if (last) STEP3(2, true, fin_n);

@@ -587,7 +587,9 @@ static __global__ void __launch_bounds__(NT) k3_cg_close(Geo g, Faces fc, Scalar
 // Chebyshev trip (3d/c_kernels/omp3/cheby_solver.c:62-99) with the previous
 // trip's u += p folded in (ADD), or the init sweep (INIT: p = r / theta).
 // With REFLECT the halo-duty z-plane writes the reflected halo of u_n.
-template <bool ADD, bool REFLECT, bool INIT, typename Finish>
+// TMA: operand planes by walkt (maps of u_in, p_in, kx, ky, kz; err: the
+// bounded waits' flag), else by walkc; the same results either way.
+template <bool ADD, bool REFLECT, bool INIT, typename Finish, bool TMA = false>
 static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cheby_trip(Geo g, Faces fc, ChebyCoef coef, double theta,
                                                                      int write_wr_always,
                                                                      const double* __restrict__ u_in,
@@ -598,8 +600,11 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cheby_trip(Geo g, Fac
                                                                      const double* __restrict__ ky,
                                                                      const double* __restrict__ kz, ReduceSlots rs,
                                                                      const int* __restrict__ done, Finish fin,
-                                                                     DevParams prm)
+                                                                     DevParams prm,
+                                                                     const __grid_constant__ Tma3Maps maps,
+                                                                     int* err)
 {
+    extern __shared__ __align__(128) unsigned char ct_raw[];
     if (gate_closed(done)) return;
     double acc[1] = {0.0};
     double a = 0.0, b = 0.0;
@@ -610,9 +615,8 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cheby_trip(Geo g, Fac
     auto cur = [&](long idx) { return ADD ? u_in[idx] + p_in[idx] : u_in[idx]; };
     if (blockIdx.z + 1 < gridDim.z) {
         const PencilC s(g);
-        walkc<REFLECT>(g, fc, s, u_in, ADD ? p_in : nullptr, kx, ky, kz,
-                       [&](double ua, double pb) { return ADD ? ua + pb : ua; },
-                       [&](int, long i, double c, double v) {
+        auto comb = [&](double ua, double pb) { return ADD ? ua + pb : ua; };
+        auto body = [&](int, long i, double c, double v) {
             if (s.active) {
                 const double rr = u0[i] - v;
                 const double pn = INIT ? rr / theta : a * p_in[i] + b * rr;
@@ -624,7 +628,9 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_cheby_trip(Geo g, Fac
                 p_out[i] = pn;
                 if (ADD) u_out[i] = c;
             }
-        });
+        };
+        if constexpr (TMA) walkt<REFLECT>(g, fc, s, maps, ADD, u_in, ADD ? p_in : nullptr, ct_raw, err, comb, body);
+        else walkc<REFLECT>(g, fc, s, u_in, ADD ? p_in : nullptr, kx, ky, kz, comb, body);
     } else if (REFLECT) {
         halo_duty3(g, fc, 1, ADD ? u_out : const_cast<double*>(u_in), cur);
     }
@@ -651,7 +657,8 @@ static __global__ void __launch_bounds__(NT) k3_add_p(Geo g, Faces fc, double* _
 // PPCG inner step (3d/c_kernels/omp3/ppcg_solver.c:29-73) with the previous
 // step's sd update folded in (FOLD 1: sd = r/theta; FOLD 2: a sd + b r); the
 // halo-duty z-plane writes the reflected halo of sd_out.
-template <int FOLD, bool NORM, typename Finish>
+// TMA as in k3_cheby_trip (maps of sd_in, r_in, kx, ky, kz).
+template <int FOLD, bool NORM, typename Finish, bool TMA = false>
 static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_ppcg_step(Geo g, Faces fc, double theta, PpcgCoef coef,
                                                                     int pp_prev, const double* __restrict__ sd_in,
                                                                     double* __restrict__ sd_out,
@@ -661,8 +668,10 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_ppcg_step(Geo g, Face
                                                                     const double* __restrict__ kx,
                                                                     const double* __restrict__ ky,
                                                                     const double* __restrict__ kz, ReduceSlots rs,
-                                                                    const int* __restrict__ done, Finish fin)
+                                                                    const int* __restrict__ done, Finish fin,
+                                                                    const __grid_constant__ Tma3Maps maps, int* err)
 {
+    extern __shared__ __align__(128) unsigned char ps_raw[];
     if (gate_closed(done)) return;
     double acc[1] = {0.0};
     double a = 0.0, b = 0.0;
@@ -674,13 +683,12 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_ppcg_step(Geo g, Face
     };
     if (blockIdx.z + 1 < gridDim.z) {
         const PencilC s(g);
-        walkc<true>(g, fc, s, sd_in, FOLD == 0 ? nullptr : r_in, kx, ky, kz,
-                    [&](double sa, double rb) {
-                        if (FOLD == 0) return sa;
-                        if (FOLD == 1) return rb / theta;
-                        return a * sa + b * rb;
-                    },
-                    [&](int, long i, double c, double v) {
+        auto comb = [&](double sa, double rb) {
+            if (FOLD == 0) return sa;
+            if (FOLD == 1) return rb / theta;
+            return a * sa + b * rb;
+        };
+        auto body = [&](int, long i, double c, double v) {
             if (s.active) {
                 const double rn = r_in[i] - v;
                 r_out[i] = rn;
@@ -688,7 +696,10 @@ static __global__ void __launch_bounds__(NT, TL3D_MINB) k3_ppcg_step(Geo g, Face
                 sd_out[i] = c;
                 if (NORM) acc[0] += rn * rn;
             }
-        });
+        };
+        if constexpr (TMA)
+            walkt<true>(g, fc, s, maps, FOLD != 0, sd_in, FOLD == 0 ? nullptr : r_in, ps_raw, err, comb, body);
+        else walkc<true>(g, fc, s, sd_in, FOLD == 0 ? nullptr : r_in, kx, ky, kz, comb, body);
     } else {
         halo_duty3(g, fc, 1, sd_out, cur);
     }

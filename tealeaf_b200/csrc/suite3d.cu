@@ -489,7 +489,7 @@ void run_cheby_solver_init(Chunk* chunk, Settings* settings)
                (k3_cheby_trip<false, false, true><<<gf, bl, 0, s->stream>>>(
                    s->g, none, coef, chunk->theta, 1, chunk->vec_u, chunk->vec_p, chunk->vec_u, chunk->vec_p,
                    chunk->vec_u0, chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs,
-                   nullptr, tl::NoFinish(), prm)));
+                   nullptr, tl::NoFinish(), prm, Tma3Maps{}, nullptr)));
     TL3_LAUNCH(s, "k3_add_p", k3_add_p<false><<<gr, bl, 0, s->stream>>>(s->g, none, chunk->vec_u, chunk->vec_p));
 }
 
@@ -507,7 +507,7 @@ void run_cheby_solver_iterate(Chunk* chunk, Settings* settings, double alpha, do
                (k3_cheby_trip<false, false, false><<<gf, bl, 0, s->stream>>>(
                    s->g, none, coef, 0.0, 1, chunk->vec_u, chunk->vec_p, chunk->vec_u, chunk->vec_p, chunk->vec_u0,
                    chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr,
-                   tl::NoFinish(), prm)));
+                   tl::NoFinish(), prm, Tma3Maps{}, nullptr)));
     TL3_LAUNCH(s, "k3_add_p", k3_add_p<false><<<gr, bl, 0, s->stream>>>(s->g, none, chunk->vec_u, chunk->vec_p));
 }
 

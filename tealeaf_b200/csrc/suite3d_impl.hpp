@@ -199,4 +199,29 @@ static void launch_cg_ur3(TlSuite3D* s, dim3 grid, Scalar alpha, double* u, cons
     }
     TL3_LAUNCH(s, "k3_cg_ur", (k3_cg_ur<<<grid, bl, 0, s->stream>>>(s->g, alpha, u, p, r, w, s->rs, done, fin)));
 }
+
+// Tensor maps of a stencil sweep over operands a (and b) with the chunk's
+// coefficients; false when the layout or an encoding rules TMA out.
+static bool sweep_maps(TlSuite3D* s, Chunk* chunk, const double* a, const double* b, Tma3Maps* m)
+{
+    if (!tma_usable(s)) return false;
+    const CUtensorMap* ma = tma_map(s, a, 0);
+    const CUtensorMap* mb = b ? tma_map(s, b, 0) : ma;
+    const CUtensorMap* kx = tma_map(s, chunk->vec_kx, 1);
+    const CUtensorMap* ky = tma_map(s, chunk->vec_ky, 2);
+    const CUtensorMap* kz = tma_map(s, chunk->vec_kz, 3);
+    if (!(ma && mb && kx && ky && kz)) return false;
+    *m = Tma3Maps{*ma, *mb, *kx, *ky, *kz};
+    return true;
+}
+
+// Raises a TMA-fed kernel's dynamic shared-memory limit once per device
+// (`set`: the caller's record of devices done).
+template <typename Kernel>
+static void raise_ring_smem(TlSuite3D* s, Kernel kernel, unsigned& set)
+{
+    if (set & (1u << (s->device & 31))) return;
+    TL_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaRingBytes));
+    set |= 1u << (s->device & 31);
+}
 }  // namespace tl3d

@@ -267,13 +267,13 @@ def test_3d_adjoint_rejects_bad_arguments():
         h.finalise()
 
 
-@pytest.mark.parametrize("path", ["device", "run"])
-def test_3d_tma_sweep_matches_async_copies(path):
-    """The CG w sweep fed by TMA tile loads (even row length: 38 + 4) and the
-    one fed by per-thread asynchronous copies give bit-identical fields and
-    iteration counts, through the device driver and through run_*, on a mesh
-    with ragged tiles in x (32 + 6), y and z."""
-    prob = problems.seeded(3, (38, 19, 23), 29, 3, 1, solver="cg", end_step=2, name="tma3")
+@pytest.mark.parametrize("solver,path", [("cg", "device"), ("cg", "run"), ("cheby", "device"), ("ppcg", "device")])
+def test_3d_tma_sweep_matches_async_copies(solver, path):
+    """The stencil sweeps fed by TMA tile loads (even row length: 38 + 4) and
+    the ones fed by per-thread asynchronous copies give bit-identical fields
+    and iteration counts, through the device driver (CG, Chebyshev, PPCG)
+    and through run_*, on a mesh with ragged tiles in x (32 + 6), y and z."""
+    prob = problems.seeded(3, (38, 19, 23), 29, 3, 1, solver=solver, end_step=2, name="tma3")
     text = prob.tea_in()
     a, b = Host(text, 3), Host(text, 3)
     try:
