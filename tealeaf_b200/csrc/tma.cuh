@@ -1,6 +1,6 @@
 // tma.cuh -- tensor-memory-accelerator (TMA) tile loads into shared memory,
 // completed on shared-memory barriers, and the host-side tensor-map
-// encoding (sm_100a; loads only, no cluster multicast).
+// encoding (sm_100a; loads only, each CTA fetching its own tiles).
 //
 // Rules the callers keep: the global base is 16-byte aligned, every stride
 // is a multiple of 16 bytes, the box's innermost extent in bytes is a
