@@ -540,5 +540,6 @@ extern "C" int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, 
     out->device_ms = ms;
     out->rel_residual = bb > 0.0 ? std::sqrt(rtrue / bb) : 0.0;
     out->converged = out->rel_residual <= rel_tol ? 1 : 0;
+    if (tma_failed(s)) tl::fail(35, "a TMA row load of the refinement sweeps did not complete (bounded barrier wait gave up)");
     return tl::failed() ? tl::error_state().code : 0;
 }
