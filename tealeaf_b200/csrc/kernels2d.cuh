@@ -696,8 +696,14 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
 // of p and r with a two-column ring on each side (columns k0-2 .. k0+129: the
 // box starts on a 16-byte boundary for an even halo depth), kx with one
 // extra column, ky; each array at a 128-byte aligned offset.
-constexpr int kRowsT = 4;
-constexpr int kStagesT = 3;   // rows of stages b and b+1 are read while b+2 is in flight
+#ifndef TL2D_TMA_ROWS
+#define TL2D_TMA_ROWS 4
+#endif
+#ifndef TL2D_TMA_STAGES
+#define TL2D_TMA_STAGES 3
+#endif
+constexpr int kRowsT = TL2D_TMA_ROWS;
+constexpr int kStagesT = TL2D_TMA_STAGES;   // rows of stages b and b+1 are read while the rest are in flight
 struct RowsT {
     alignas(128) double P[kRowsT][BX + 4];
     alignas(128) double R[kRowsT][BX + 4];

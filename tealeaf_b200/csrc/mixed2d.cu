@@ -132,7 +132,9 @@ RfBuffers<T> rf_buffers(TlSuite2D* s, int fields)
     constexpr int N = Pack<T>::N;
     RfBuffers<T> b{};
     const int nx = s->g.x - 2 * s->g.hd, ny = s->g.y - 2 * s->g.hd;
-    b.L = make_lay<T>(nx, ny, choose_rows(tl::ceil_div(nx, N), ny, s->sm_count, Pack<T>::MINB));
+    // tile rows for whole waves of the TMA sweeps (the default path; the
+    // per-thread-load sweeps keep the same tiles so both give the same sums)
+    b.L = make_lay<T>(nx, ny, choose_rows(tl::ceil_div(nx, N), ny, s->sm_count, kRfTmaBlocks));
     {
         const dim3 t = lay_tiles<T>(b.L);   // the reduction partials must fit
         if ((long)t.x * t.y * tl::kMaxSums > s->partial_capacity) b.L.rows = s->g.rows;

@@ -22,6 +22,7 @@ namespace rf {
 
 constexpr int kRfRows = 4;
 constexpr int kRfStages = 3;
+constexpr int kRfTmaBlocks = 4;   // resident blocks per SM of the TMA sweeps (about 50 KB of shared memory each)
 
 template <typename T>
 struct RfRowsW {
