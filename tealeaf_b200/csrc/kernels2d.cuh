@@ -704,6 +704,12 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
 #endif
 constexpr int kRowsT = TL2D_TMA_ROWS;
 constexpr int kStagesT = TL2D_TMA_STAGES;   // rows of stages b and b+1 are read while the rest are in flight
+// TMA alignment: strip starts hd + BX bx and the boxes' widths keep every x
+// start and every box row a multiple of 16 bytes for an even halo depth.
+static_assert((BX * sizeof(double)) % 16 == 0 && ((BX + 4) * sizeof(double)) % 16 == 0 &&
+                  ((BX + 2) * sizeof(double)) % 16 == 0,
+              "TMA boxes of the 2D sweeps must be multiples of 16 bytes wide");
+static_assert(kStagesT >= 3, "row block b reads stages b and b+1 while a later one is in flight");
 struct RowsT {
     alignas(128) double P[kRowsT][BX + 4];
     alignas(128) double R[kRowsT][BX + 4];

@@ -280,6 +280,11 @@ struct Tma3Maps {
 };
 
 constexpr size_t kTmaRingBytes = kStages3 * sizeof(PlaneT) + kStages3 * 8 + 128;   // + barriers + alignment
+// TMA alignment: boxes start at x = hd - 2 + BX bx (operands) or hd + BX bx
+// (coefficients), so BX must keep them even and every box row 16-byte wide.
+static_assert(BX % 2 == 0 && ((BX + 4) * sizeof(double)) % 16 == 0 && ((BX + 2) * sizeof(double)) % 16 == 0 &&
+                  (BX * sizeof(double)) % 16 == 0,
+              "TMA boxes of the 3D sweeps must start and extend on 16-byte boundaries");
 
 // walkc with the planes brought in by TMA: one thread issues the plane's
 // boxes on the slot's shared-memory barrier; every thread waits (bounded) for

@@ -28,6 +28,8 @@ template <typename T>
 struct RfRowsW {
     static constexpr int W = BX * Pack<T>::N;     // tile row: 1024 bytes
     static constexpr int H = 16 / (int)sizeof(T);   // ring box: 16 bytes
+    static_assert(W * sizeof(T) == 1024 && H * sizeof(T) == 16,
+                  "TMA boxes of the refinement sweeps: 1024-byte tile rows (the widest box) and 16-byte rings");
     alignas(128) T P[kRfRows][W];
     alignas(128) T R[kRfRows][W];
     alignas(128) T KX[kRfRows][W];
