@@ -24,6 +24,7 @@
 // one IEEE operation in the reference's expression order; element-wise
 // results equal the reference's strict-IEEE build bit for bit, and dot
 // products differ only by summation order.
+#include "blocked2d.cuh"
 #include "suite2d_impl.hpp"
 
 #include <cuda_runtime.h>
@@ -97,8 +98,53 @@ static void launch_halos(TlSuite2D* s, Chunk* chunk, int depth, const int* which
     TL_LAUNCH(s, "k_local_halos", k_local_halos<<<dim3(tl::ceil_div(per, 256), a.nf), 256, 0, s->stream>>>(s->g, depth, a));
 }
 
+// Runs the deferred PPCG inner steps (ppcg.c:9-61 as the reference drivers
+// call them: sd = r / theta, then per step a depth-1 halo of sd and
+// r -= A sd, u += sd, sd = a sd + b r): temporally blocked launches of up to
+// kTB steps (the fold of each step at its start, sd reflected on the fly)
+// and the last step's sd update, with the same results as one launch per
+// call. With no step queued only sd = r / theta runs.
+static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
+{
+    s->pq.active = false;
+    const int n = (int)s->pq.a.size();
+    if (n == 0) {
+        TL_LAUNCH(s, "k_ppcg_init",
+                  k_ppcg_init<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->theta, chunk->r, chunk->sd));
+        return;
+    }
+    TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, s->pq.a.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                            s->stream));
+    TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, s->pq.b.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                            s->stream));
+    const size_t smem = blocked_smem<1>();
+    TL_CUDA(cudaFuncSetAttribute(k_blocked<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // An even number of launches leaves r and sd in the buffers the chunk
+    // pointed at: the host reads those pointers before its calls (e.g. the r
+    // it passes to run_calculate_2norm), so a flush must not move them. An
+    // odd count gets a closing zero-step launch, which copies the interior of
+    // both and writes the depth-1 halo of sd (r's halo is left as the
+    // one-step path leaves it: untouched).
+    const int launches = (n + kTB - 1) / kTB;
+    for (int q = 0; q < launches + (launches & 1); ++q) {
+        const int pp0 = q * kTB;
+        const BlockedArgs a{std::max(0, std::min(kTB, n - pp0)), std::min(pp0, n), 0, chunk->theta,
+                            s->d_cheby_alphas, s->d_cheby_betas};
+        TL_LAUNCH(s, "k_blocked<ppcg>", (k_blocked<1><<<blocked_grid(s->g), kTBThreads, smem, s->stream>>>(
+                                            s->g, a, chunk->sd, chunk->r, s->alt[ALT_SD], s->alt[ALT_R], nullptr,
+                                            chunk->u, nullptr, nullptr, chunk->kx, chunk->ky, nullptr)));
+        swap_alt(s, chunk, ALT_SD);
+        swap_alt(s, chunk, ALT_R);
+    }
+    TL_LAUNCH(s, "k_ppcg_inner_b", k_ppcg_inner_b<<<interior_grid(s->g), BX, 0, s->stream>>>(
+                                       s->g, s->pq.a[n - 1], s->pq.b[n - 1], chunk->sd, chunk->r));
+    s->pq.a.clear();
+    s->pq.b.clear();
+}
+
 void flush(TlSuite2D* s, Chunk* chunk)
 {
+    if (s->pq.active) run_ppcg_queue(s, chunk);
     if (s->pend.calc_p) {
         TL_LAUNCH(s, "k_cg_calc_p",
                   k_cg_calc_p<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, s->pend.beta, chunk->p, chunk->r));
@@ -450,6 +496,7 @@ void run_cg_calc_w(Chunk* chunk, Settings* settings, double* pw)
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
+    if (s->pq.active) run_ppcg_queue(s, chunk);   // deferred PPCG steps precede everything recorded after them
     if (s->pend.halo[TL_FIELD_P] > 1) flush(s, chunk);
     const bool fuse = s->pend.calc_p;
     const bool refl = s->pend.halo[TL_FIELD_P] == 1;
@@ -483,6 +530,7 @@ void run_cg_calc_ur(Chunk* chunk, Settings* settings, double alpha, double* rrn)
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
+    if (s->pq.active) run_ppcg_queue(s, chunk);
     if (s->pend.calc_p || s->pend.halo[TL_FIELD_U]) flush(s, chunk);
     launch_cg_ur2(s, interior_grid(s->g), Scalar{alpha, nullptr}, chunk->u, chunk->p, chunk->r, chunk->w, nullptr,
                   tl::NoFinish());
@@ -498,6 +546,7 @@ void run_cg_calc_p(Chunk* chunk, Settings* settings, double beta)
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
+    if (s->pq.active) run_ppcg_queue(s, chunk);
     if (s->pend.calc_p || s->pend.halo[TL_FIELD_P]) flush(s, chunk);
     s->pend.calc_p = true;
     s->pend.beta = beta;
@@ -569,6 +618,13 @@ void run_ppcg_init(Chunk* chunk, Settings* settings)
     (void)settings;
     TlSuite2D* s = ready(chunk);
     if (!s) return;
+    const Faces fc = faces_of(chunk);
+    if (s->temporal_blocking && fc.l && fc.r && fc.b && fc.t) {
+        s->pq.active = true;   // sd = r / theta runs with the first queued step
+        s->pq.a.clear();
+        s->pq.b.clear();
+        return;
+    }
     TL_LAUNCH(s, "k_ppcg_init",
               k_ppcg_init<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->theta, chunk->r, chunk->sd));
 }
@@ -577,7 +633,22 @@ void run_ppcg_init(Chunk* chunk, Settings* settings)
 void run_ppcg_inner_iteration(Chunk* chunk, Settings* settings, double alpha, double beta)
 {
     (void)settings;
-    TlSuite2D* s = ready(chunk);
+    if (tl::failed()) return;
+    TlSuite2D* s = suite_of(chunk);
+    if (!s) return;
+    // queued only in the reference drivers' pattern: a depth-1 halo update of
+    // sd (and nothing else) requested right before the step
+    if (s->pq.active && !s->pend.calc_p && s->pend.halo[TL_FIELD_SD] == 1 && (long)s->pq.a.size() < s->table_len) {
+        bool other = false;
+        for (int f = 0; f < TL_NUM_FIELDS; ++f) other |= f != TL_FIELD_SD && s->pend.halo[f] != 0;
+        if (!other) {
+            s->pend.halo[TL_FIELD_SD] = 0;   // the blocked steps reflect sd on the fly and write its halo
+            s->pq.a.push_back(alpha);
+            s->pq.b.push_back(beta);
+            return;
+        }
+    }
+    s = ready(chunk);   // runs the queue, if any, and the pending operations
     if (!s) return;
     TL_LAUNCH(s, "k_ppcg_inner_a",
               k_ppcg_inner_a<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->u, chunk->r, chunk->kx,

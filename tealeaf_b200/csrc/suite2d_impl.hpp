@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 // Buffers that alternate between two slices (fused sweeps read the old values
 // at stencil neighbours while writing the new ones). The Chunk always points
@@ -53,6 +54,15 @@ struct TlSuite2D {
     // Device-resident driver: Chebyshev trips / PPCG inner steps temporally
     // blocked in shared memory (blocked2d.cuh); off = one launch per step.
     bool temporal_blocking = true;
+
+    // Kernel-interface PPCG inner steps deferred for the blocked kernel:
+    // run_ppcg_init opens the queue, run_ppcg_inner_iteration appends its
+    // coefficients (absorbing the depth-1 halo update of sd before it), and
+    // the next other entry point runs them (flush).
+    struct {
+        bool active = false;
+        std::vector<double> a, b;
+    } pq;
 
     // FP32 buffers of the iterative-refinement form (mixed2d.cu), on first use.
     void* mx_slab = nullptr;

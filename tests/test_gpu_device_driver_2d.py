@@ -105,3 +105,28 @@ def test_tma_w_sweep_is_bit_identical(solver, path):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("inner", [10, 7, 1])
+def test_run_path_ppcg_queue_is_bit_identical(inner):
+    """Through run_* (the reference drivers' call sequence), the PPCG inner
+    steps deferred and run temporally blocked give the same memory state, bit
+    for bit, as one launch per call (temporal blocking off), for inner-step
+    counts that fill, split and underfill the 5-step blocks."""
+    prob = problems.seeded(2, (203, 141), 17, 5, 2, solver="ppcg", end_step=2, name="pq").with_(
+        ppcg_inner_steps=inner)
+    text = prob.tea_in()
+    a, b = Host(text, 2), Host(text, 2)
+    try:
+        b.lib.tl2d_set_temporal_blocking(b.chunk, 0)
+        for tt in range(2):
+            ra = a.solve(tt)
+            rb = b.solve(tt)
+            assert ra.iterations == rb.iterations
+            assert ra.summary == rb.summary
+            assert ra.exact_error == rb.exact_error
+            for f in FIELDS:
+                assert np.array_equal(a.download(f), b.download(f)), (inner, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()
