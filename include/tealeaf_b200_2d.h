@@ -259,6 +259,14 @@ void tl2d_set_temporal_blocking(Chunk* chunk, int on);
  * results are bit-identical) or by per-thread loads (0). */
 void tl2d_set_tma(Chunk* chunk, int on);
 
+/* No counterpart in the reference. Runs every operation the suite has
+ * deferred for this chunk (a CG p update, halo updates, queued PPCG inner
+ * steps), as every run_* call that touches device data does first. Call it
+ * before reading the chunk's device fields by other means (own kernels, or
+ * an allocation-free entry point given a field pointer). Asynchronous on the
+ * chunk's stream. */
+void tl2d_flush(Chunk* chunk);
+
 /* Per-kernel device-time profile (CUDA events around every launch on the
  * chunk's stream, resolved at the next synchronisation): enable/disable,
  * reset, and read entry `index` (returns 0 past the last entry). */

@@ -256,6 +256,11 @@ long long tl3d_launch_count(Chunk* chunk);
  * TMA tile loads (1, the default, where the halo depth and row length are
  * even; results are bit-identical) or by per-thread asynchronous copies (0). */
 void tl3d_set_tma(Chunk* chunk, int on);
+/* No counterpart in the reference. Runs every operation the suite has
+ * deferred for this chunk (a CG p update, halo updates), as every run_* call
+ * that touches device data does first; call it before reading the chunk's
+ * device fields by other means. Asynchronous on the chunk's stream. */
+void tl3d_flush(Chunk* chunk);
 
 /* Field ids for the host-buffer staging calls (x*y*z values each). */
 #define TL3D_DENSITY0 0

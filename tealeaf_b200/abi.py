@@ -208,6 +208,10 @@ def load(dims: int) -> C.CDLL:
         f = getattr(lib, pre + "refine_solve_step")
         f.argtypes = head + [_i, _d, _i, C.POINTER(RefineStats)]
         f.restype = _i
+    if hasattr(lib, pre + "flush"):
+        f = getattr(lib, pre + "flush")
+        f.argtypes = [C.POINTER(chunk_t)]
+        f.restype = None
     if hasattr(lib, pre + "set_tma"):  # 2D and 3D
         f = getattr(lib, pre + "set_tma")
         f.argtypes = [C.POINTER(chunk_t), _i]

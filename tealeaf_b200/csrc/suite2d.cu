@@ -205,6 +205,7 @@ void tl2d_set_tma(Chunk* chunk, int on)
     TlSuite2D* s = suite_of(chunk);
     if (s) s->tma = on != 0;
 }
+void tl2d_flush(Chunk* chunk) { ready(chunk); }
 
 void tl2d_profile_enable(Chunk* chunk, int on)
 {

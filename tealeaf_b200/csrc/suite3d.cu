@@ -156,6 +156,7 @@ void tl3d_set_tma(Chunk* chunk, int on)
     TlSuite3D* s = suite_of(chunk);
     if (s) s->tma = on != 0;
 }
+void tl3d_flush(Chunk* chunk) { ready(chunk); }
 long long tl3d_launch_count(Chunk* chunk)
 {
     TlSuite3D* s = suite_of(chunk);
