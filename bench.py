@@ -124,7 +124,7 @@ class ClockSampler:
 
 def cpu_reference_sample(tea_in: str, steps: int, cap: int, threads: int, dims: int = 2):
     """Reference omp3 program (stock flags) on this host: per-step (iterations, seconds)."""
-    from oracle.oracle import run_reference  # checker/baseline only
+    from oracle.oracle import run_reference  # the CPU baseline leg only
     res = run_reference(tea_in, dims=dims, suite="omp3", threads=threads, fast=True, max_iters=cap)
     out = []
     for s in res[:steps]:
@@ -588,7 +588,7 @@ def bench_adjoint(args) -> dict:
             Jg, gg, _ = hs.adjoint_gradient(steps, every, box, tol)
         finally:
             hs.finalise()
-        from oracle.oracle import OracleLib  # checker only
+        from oracle.oracle import OracleLib  # the CPU adjoint comparison only
         cfg, states = read_config(small.tea_in(), 3)
         t0 = time.time()
         Jc, gc = OracleLib().adjoint3d(cfg, states, box, tol)

@@ -1,5 +1,5 @@
 """Pins the CPU adjoint of the oracle (oracle_adjoint3d in oracle/tl_oracle.c)
-before it is trusted as the checker of the B200 adjoint.
+before the B200 adjoint is compared with it.
 
 The reference has no adjoint, so the pin is the reference's own forward
 timestep (the oracle's restatement of 3d/c_kernels/omp3/cg_solver.c, itself
