@@ -6,7 +6,7 @@ dt 0.004 (tealeaf_b200.problems.dropin_2d). A "step" is one implicit
 timestep (solve(), 2d/diffuse.c:22-80) of that problem.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--size 4096] [--solver cg|cheby|ppcg]
+                  [--size 4096] [--solver cg|cheby|ppcg] [--workload ...]
 
 B200 arm: value = solver iterations/s of the whole job (independent replicas
 on N GPUs: the path does not shard), fields resident in HBM, timesteps run by
@@ -15,9 +15,15 @@ through the C ABI with the step's inputs copied from pinned host buffers and
 the energy field copied back every step; e2e_kernel_interface = the same,
 with the timestep driven through the run_* kernel interface the way the
 reference drivers call it.
+At N=1 the line also carries the other configurations, each driver-measured
+in the same run: `refine` (FP32 storage + FP64 refinement against FP64 at
+8192^2), `dropin_8192` and `dropin_3d_256` (the FP64 CG drop-in at 8192^2 and
+at 256^3), `adjoint` (the 3D adjoint at 256^3 with the 64^3 CPU-adjoint
+check) and `batch` (64 uneven problems in one launch against 64 sequential
+FP64 solves).
 Reference arm (--impl reference): the reference omp3 CPU program on this
-host's cores, bounded samples of the same workload (each step capped at a
-fixed iteration count).
+host's cores, bounded samples of the same workload: each timed timestep
+capped at --cpu-cap CG iterations, warm-up timesteps at --warm-cap.
 """
 from __future__ import annotations
 
@@ -122,12 +128,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_sample(tea_in: str, steps: int, cap: int, threads: int, dims: int = 2):
-    """Reference omp3 program (stock flags) on this host: per-step (iterations, seconds)."""
+def cpu_reference_sample(tea_in: str, steps: int, cap: int, threads: int, dims: int = 2, warm_steps: int = 0,
+                         warm_cap: int = 20):
+    """Reference omp3 program (stock flags) on this host: per timed step
+    (iterations, seconds). The deck must hold warm_steps + steps timesteps; the
+    first warm_steps run capped at warm_cap iterations and are not returned,
+    the others are capped at `cap`."""
     from oracle.oracle import run_reference  # the CPU baseline leg only
-    res = run_reference(tea_in, dims=dims, suite="omp3", threads=threads, fast=True, max_iters=cap)
+    res = run_reference(tea_in, dims=dims, suite="omp3", threads=threads, fast=True, max_iters=cap,
+                        warm=(warm_steps, warm_cap) if warm_steps > 0 else None)
     out = []
-    for s in res[:steps]:
+    for s in res[warm_steps:warm_steps + steps]:
         it = sum(s.iterations.values())
         out.append((it, s.seconds))
     return out
@@ -140,6 +151,45 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def cpu_info() -> dict:
+    """The host CPU as lscpu reports it: model name and physical cores."""
+    info = {"cpu_model": None, "physical_cores": None, "logical_cpus": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=20).stdout
+        kv = {}
+        for line in out.splitlines():
+            if ":" in line:
+                k, v = line.split(":", 1)
+                kv.setdefault(k.strip(), v.strip())
+        info["cpu_model"] = kv.get("Model name")
+        cores, sockets = int(kv.get("Core(s) per socket", "0")), int(kv.get("Socket(s)", "0"))
+        if cores and sockets:
+            info["physical_cores"] = cores * sockets
+    except Exception:
+        pass
+    return info
+
+
+def workload_config(args) -> dict:
+    """`config` of the drop-in line, identical on both arms."""
+    n = args.size
+    return {"workload": "dropin_2d_%d_%s" % (n, args.solver), "cells": n * n, "solver": args.solver,
+            "eps": 1e-15, "dt": 0.004, "parallelism": "replicas",
+            "l2": l2_note(8 * (n + 4) ** 2 * 8)}
+
+
+def l2_note(working_set_bytes: float) -> str:
+    if working_set_bytes > 126e6:
+        return "no flush: working set %.2f GB > 126 MB L2" % (working_set_bytes / 1e9)
+    return "no flush: working set %.1f MB fits in the 126 MB L2 (timings include L2 reuse)" % (working_set_bytes / 1e6)
+
+
+def cpu_baseline_record(value, threads, sample) -> dict:
+    d = {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference", "sample": sample}
+    d.update(cpu_info())
+    return d
+
+
 def bench_reference(args, rank, world):
     from tealeaf_b200 import problems
     if rank != 0:
@@ -147,24 +197,24 @@ def bench_reference(args, rank, world):
     prob = problems.dropin_2d(args.size, seed=2, steps=args.warmup + args.steps, solver=args.solver)
     threads = host_threads()
     t0 = time.time()
-    samples = cpu_reference_sample(prob.tea_in(), args.warmup + args.steps, args.cpu_cap, threads)
-    timed = samples[args.warmup:]
+    timed = cpu_reference_sample(prob.tea_in(), args.steps, args.cpu_cap, threads, warm_steps=args.warmup,
+                                 warm_cap=args.warm_cap)
     iters = sum(i for i, _ in timed)
     secs = sum(t for _, t in timed)
     value = iters / secs if secs > 0 else 0.0
     cells = args.size * args.size
+    sample = ("reference omp3 (oracle/_ref/harness2d_omp3_fast, stock flags, OMP_NUM_THREADS=%d): %d timed "
+              "timesteps of the same deck, each capped at %d CG iterations, after %d warm-up timesteps capped "
+              "at %d" % (threads, len(timed), args.cpu_cap, args.warmup, args.warm_cap))
     line = {
         "metric": "solver_iterations_per_s", "value": value, "unit": "iter/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(1, len(timed)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded tea.in generator)", "impl": "reference",
-        "config": {"workload": "dropin_2d_%d_%s" % (args.size, args.solver), "cells": cells,
-                   "solver": args.solver, "eps": 1e-15, "dt": 0.004, "parallelism": "replicas"},
+        "data": "synthetic (seeded tea.in generator, dropin_2d seed 2)", "impl": "reference",
+        "config": workload_config(args),
+        "driver": "reference host, drivers and omp3 kernels (timestep loop of oracle/ref_harness.c)",
         "cells_iterations_per_s": value * cells,
-        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
-                         "sample": "reference omp3 (oracle/_ref/harness2d_omp3_fast, OMP_NUM_THREADS=%d), "
-                                   "%d timesteps capped at %d CG iterations each"
-                                   % (threads, len(timed), args.cpu_cap)},
+        "cpu_baseline": cpu_baseline_record(value, threads, sample),
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(time.time() - t0, 2),
     }
@@ -220,7 +270,7 @@ def bench_b200(args, rank, world, local_rank):
         its = 0
         n0 = h.lib.tl2d_launch_count(C.byref(h.chunk))
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(min(args.steps, args.profile_steps) if profile else args.steps):
             r = step(tt)
             its += sum(r.iterations.values())
             tt += 1
@@ -303,7 +353,7 @@ def bench_b200(args, rank, world, local_rank):
                         "bytes_per_launch": bpc * interior_launch_cells, "avg_launch_ms": kms_tot / kcalls,
                         "timing": "CUDA events around every launch on the suite stream, over a second timed "
                                   "pass of %d steps (%.1f iter/s with the events in place)"
-                                  % (args.steps, iters_prof / (ms_prof / 1000.0)),
+                                  % (min(args.steps, args.profile_steps), iters_prof / (ms_prof / 1000.0)),
                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                         else "fallback 6650 GB/s"}
     total_kernel_ms = sum(v[1] for v in prof.values())
@@ -313,11 +363,9 @@ def bench_b200(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded tea.in generator, dropin_2d seed 2)",
-        "config": {"workload": "dropin_2d_%d_%s" % (args.size, args.solver), "cells": cells,
-                   "solver": args.solver, "eps": 1e-15, "dt": 0.004, "parallelism": "replicas",
-                   "l2": "no flush: working set %.2f GB > 126 MB L2" % (8 * (args.size + 4) ** 2 * 8 / 1e9),
-                   "driver": "device-resident solver loop (tl2d_solve_step)" if args.driver == "device"
-                   else "host mirror of the reference drivers over run_*"},
+        "config": workload_config(args),
+        "driver": "device-resident solver loop (tl2d_solve_step)" if args.driver == "device"
+        else "host mirror of the reference drivers over run_*",
         "cells_iterations_per_s": value * cells,
         "hbm_effective_gbs_per_gpu": eff_gbs,
         "hbm_effective_frac_per_gpu": eff_gbs / peak,
@@ -340,14 +388,67 @@ def bench_b200(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         try:
             threads = host_threads()
-            samples = cpu_reference_sample(prob.tea_in(), 2, args.cpu_cap, threads)
+            sprob = problems.dropin_2d(args.size, seed=2, steps=3, solver=args.solver)
+            samples = cpu_reference_sample(sprob.tea_in(), 2, args.cpu_cap, threads, warm_steps=1,
+                                           warm_cap=args.warm_cap)
             it_s = sum(i for i, _ in samples) / sum(t for _, t in samples)
-            line["cpu_baseline"] = {"value": it_s, "unit": "iter/s", "cores": threads, "kind": "reference",
-                                    "sample": "reference omp3 (stock flags) on this host, 2 timesteps of the "
-                                              "same workload capped at %d CG iterations each" % args.cpu_cap}
+            line["cpu_baseline"] = cpu_baseline_record(
+                it_s, threads, "reference omp3 (stock flags) on this host: 2 timesteps of the same workload, "
+                               "each capped at %d CG iterations, after 1 warm-up timestep" % args.cpu_cap)
         except Exception as exc:  # baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    if world == 1 and not args.no_extras:
+        line["dropin_8192"] = extra_dropin(8192, 2, peak)
+        line["dropin_3d_256"] = extra_dropin(256, 3, peak)
+        line["adjoint"] = adjoint_object(256, fd_cells=0, cpu_size=args.adjoint_cpu_size)
+        line["batch"] = bench_batch(args)
     return line
+
+
+def extra_dropin(n: int, dims: int, peak: float, steps: int = 2, warm_cap: int = 50) -> dict:
+    """The FP64 CG drop-in at another size (2D: the 8 rectangle + 4 circle
+    deck; 3D: the 6-box deck of the adjoint configuration): one warm-up
+    timestep capped at `warm_cap` iterations, then `steps` full timesteps of
+    the device-resident loop to eps 1e-15, timed with CUDA events on the
+    suite stream; the fraction counts 96 (2D) / 104 (3D) algorithmic bytes
+    per cell and iteration."""
+    import ctypes as C
+
+    import torch
+
+    from tealeaf_b200 import problems
+    from tealeaf_b200.host import Host
+    prob = (problems.dropin_2d(n, seed=2, steps=steps + 1, solver="cg") if dims == 2
+            else problems.adjoint_3d(n, seed=4, steps=steps + 1))
+    h = Host(prob.tea_in(), dims=dims)
+    per_step = []
+    try:
+        stream = torch.cuda.ExternalStream(getattr(h.lib, "tl%dd_stream" % dims)(C.byref(h.chunk)))
+        full = h.settings.max_iters
+        h.settings.max_iters = warm_cap
+        h.solve_device(0, summary=False)
+        h.settings.max_iters = full
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(0)
+        with sampler:
+            e0.record(stream)
+            for tt in range(1, steps + 1):
+                per_step.append(sum(h.solve_device(tt, summary=False).iterations.values()))
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+    finally:
+        h.finalise()
+    cells = n ** dims
+    value = sum(per_step) / (ms / 1000.0)
+    bpc = CG_BYTES_PER_CELL_ITER if dims == 2 else 104
+    gbs = bpc * cells * value / 1e9
+    return {"metric": "solver_iterations_per_s", "value": value, "unit": "iter/s", "dtype": "f64",
+            "workload": "dropin_%dd_%d_cg" % (dims, n), "cells": cells, "eps": prob.eps, "steps": steps,
+            "iterations_per_step": per_step, "ms_per_step": ms / steps, "cells_iterations_per_s": value * cells,
+            "bytes_per_cell_iteration": bpc, "hbm_effective_gbs": gbs, "frac_of_measured_hbm": gbs / peak,
+            "warmup": "1 timestep capped at %d iterations" % warm_cap, "clocks": sampler.summary()}
 
 
 def bench_dropin3d(args) -> dict:
@@ -461,11 +562,13 @@ def bench_dropin3d(args) -> dict:
     if not args.no_cpu_baseline:
         try:
             threads = host_threads()
-            samples = cpu_reference_sample(prob.tea_in(), 2, args.cpu_cap, threads, dims=3)
+            sprob = prob.with_(end_step=3)
+            samples = cpu_reference_sample(sprob.tea_in(), 2, args.cpu_cap, threads, dims=3, warm_steps=1,
+                                           warm_cap=args.warm_cap)
             it_s = sum(i for i, _ in samples) / sum(t for _, t in samples)
-            line["cpu_baseline"] = {"value": it_s, "unit": "iter/s", "cores": threads, "kind": "reference",
-                                    "sample": "reference omp3 3D (stock flags), 2 timesteps of the same workload "
-                                              "capped at %d iterations each" % args.cpu_cap}
+            line["cpu_baseline"] = cpu_baseline_record(
+                it_s, threads, "reference omp3 3D (stock flags): 2 timesteps of the same workload, each capped "
+                               "at %d iterations, after 1 warm-up timestep" % args.cpu_cap)
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     return line
@@ -520,17 +623,22 @@ def bench_refine(n: int, peak: float) -> dict:
 
 
 def bench_adjoint(args) -> dict:
+    """The 3D adjoint form at `--size`^3 (see adjoint_object)."""
+    return adjoint_object(args.size, args.fd_cells, args.adjoint_cpu_size)
+
+
+def adjoint_object(n: int, fd_cells: int, cpu_size: int) -> dict:
     """The 3D adjoint form: dJ/dlog(density) for J = sum over [6,9]^3 of
     volume*density*u after 20 CG timesteps (checkpoints every 5) on the seeded
     adjoint case, timed on the device; checked against central differences
-    (h = 1e-6) at `--fd-cells` seeded cells of the same mesh and against the
-    oracle's FP64 CPU adjoint at `--adjoint-cpu-size`^3."""
+    (h = 1e-6) at `fd_cells` seeded cells of the same mesh and against the
+    oracle's FP64 CPU adjoint at `cpu_size`^3."""
     import numpy as np
 
     from tealeaf_b200 import problems
     from tealeaf_b200.config import read_config
     from tealeaf_b200.host import Host
-    n, steps, every, tol, h = args.size, 20, 5, 1e-12, 1e-6
+    steps, every, tol, h = 20, 5, 1e-12, 1e-6
     box = [6.0, 9.0, 6.0, 9.0, 6.0, 9.0]
     prob = problems.adjoint_3d(n, seed=4, steps=steps)
     host = Host(prob.tea_in(), dims=3)
@@ -563,11 +671,11 @@ def bench_adjoint(args) -> dict:
         m = inb[:, None, None] & inb[None, :, None] & inb[None, None, :]
         return float(np.sum((v[sl] * d[sl] * u[sl])[m]))
 
-    if args.fd_cells > 0:
+    if fd_cells > 0:
         rng = np.random.default_rng(4)
         top = np.argsort(-np.abs(gf))[: max(1, gf.size // 100)]
-        cells = list(rng.choice(top, args.fd_cells // 2, replace=False)) + \
-            list(rng.integers(0, gf.size, args.fd_cells - args.fd_cells // 2))
+        cells = list(rng.choice(top, fd_cells // 2, replace=False)) + \
+            list(rng.integers(0, gf.size, fd_cells - fd_cells // 2))
         noise = 8.0 * np.finfo(float).eps * abs(J) / (2 * h)
         rows = []
         for c in cells:
@@ -580,8 +688,8 @@ def bench_adjoint(args) -> dict:
                             "max_abs_err_over_noise": max(abs(r[2] - r[1]) / noise for r in rows),
                             "per_cell": [{"cell": r[0], "adjoint": r[1], "fd": r[2], "rel": r[3]} for r in rows]}
     host.finalise()
-    if args.adjoint_cpu_size > 0:
-        m = args.adjoint_cpu_size
+    if cpu_size > 0:
+        m = cpu_size
         small = problems.adjoint_3d(m, seed=4, steps=steps)
         hs = Host(small.tea_in(), dims=3)
         try:
@@ -651,6 +759,76 @@ def bench_batch(args) -> dict:
             "temp_max_rel_diff_vs_sequential": worst}
 
 
+def precond_object(n: int, peak: float, steps: int = 1, warm_cap: int = 50) -> dict:
+    """The Jacobi preconditioners of the device-resident CG against plain CG
+    on the drop-in deck at n^2: per variant, one warm-up timestep capped at
+    `warm_cap` iterations, then `steps` full timesteps to eps 1e-15 timed with
+    CUDA events on the suite stream (iterations, ms per timestep)."""
+    import ctypes as C
+
+    import torch
+
+    from tealeaf_b200 import problems
+    from tealeaf_b200.host import Host
+    out = {"workload": "dropin_2d_%d_cg, preconditioner none / jac_diag / jac_block" % n, "cells": n * n,
+           "bytes_per_cell_iteration": {"none": 96, "jac_diag": 120, "jac_block": 120}}
+    for pc in ("none", "jac_diag", "jac_block"):
+        prob = problems.dropin_2d(n, seed=2, steps=steps + 1, solver="cg").with_(preconditioner=pc)
+        h = Host(prob.tea_in(), dims=2)
+        try:
+            stream = torch.cuda.ExternalStream(h.lib.tl2d_stream(C.byref(h.chunk)))
+            full = h.settings.max_iters
+            h.settings.max_iters = warm_cap
+            h.solve_device(0, summary=False)
+            h.settings.max_iters = full
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            its = []
+            e0.record(stream)
+            for tt in range(1, steps + 1):
+                its.append(h.solve_device(tt, summary=False).iterations["CG"])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            temp = h.field_summary()[3]
+        finally:
+            h.finalise()
+        bpc = out["bytes_per_cell_iteration"][pc]
+        out[pc] = {"ms_per_step": ms, "iterations_per_step": its, "temp": temp,
+                   "hbm_effective_gbs": bpc * n * n * sum(its) / steps / (ms / 1000.0) / 1e9}
+    for pc in ("jac_diag", "jac_block"):
+        out[pc]["time_ratio_vs_none"] = out[pc]["ms_per_step"] / out["none"]["ms_per_step"]
+        out[pc]["iteration_ratio_vs_none"] = sum(out[pc]["iterations_per_step"]) / sum(out["none"]["iterations_per_step"])
+    return out
+
+
+def bench_refine_case(args) -> dict:
+    """One refinement timestep of the mixed-precision deck (16 rectangles,
+    seed 3) at `--size`, solved to the FP64 relative residual 1e-10 in
+    `--precision` 32 or 64, with `--solver` cg or ppcg (`--errswitch`: the
+    switch after 21 CG trips, epslim 1e30) and an optional `--max-iters` cap.
+    The case the refinement profiles are captured on."""
+    from tealeaf_b200 import problems
+    from tealeaf_b200.host import Host
+    prob = problems.mixed_2d(args.size, seed=3, steps=1).with_(solver=args.solver)
+    if args.errswitch:
+        prob = prob.with_(error_switch=True, eps_lim=1e30)
+    if args.max_iters > 0:
+        prob = prob.with_(max_iters=args.max_iters)
+    h = Host(prob.tea_in(), dims=2)
+    try:
+        r = h.refine_step(0, 1e-10, args.precision)
+    finally:
+        h.finalise()
+    return {"metric": "refine_timestep_ms", "value": r.device_ms, "unit": "ms", "higher_is_better": False,
+            "n_gpus": 1, "dtype": "f%d storage, f64 reductions/solution" % args.precision,
+            "data": "synthetic (seeded tea.in generator, mixed_2d seed 3)",
+            "config": {"workload": "mixed_2d_%d_%s%s" % (args.size, args.solver, "_errswitch" if args.errswitch else ""),
+                       "rel_tol": 1e-10, "max_iters": prob.max_iters, "precision": args.precision},
+            "iterations": r.iterations, "cg_trips": r.cg_trips, "residual_updates": r.residual_updates,
+            "rel_residual": r.rel_residual, "converged": r.converged}
+
+
 def traffic_per_launch(kernel: str, cells: int):
     """DRAM bytes per launch from the committed ncu summary (scaled per cell), if any."""
     p = REPO / "profiles" / "ncu_traffic.json"
@@ -673,14 +851,25 @@ def main():
     ap.add_argument("--size", type=int, default=4096)
     ap.add_argument("--solver", default="cg", choices=["cg", "cheby", "ppcg"])
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-cap", type=int, default=200)
+    ap.add_argument("--cpu-cap", type=int, default=1000,
+                    help="reference CPU samples: CG iterations per timed timestep")
+    ap.add_argument("--warm-cap", type=int, default=20,
+                    help="reference CPU samples: CG iterations per warm-up timestep")
+    ap.add_argument("--profile-steps", type=int, default=5,
+                    help="timesteps of the second pass with per-launch events (kernel shares, roofline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without the 8192^2 / 3D 256^3 drop-in, adjoint and batch objects")
     ap.add_argument("--refine-size", type=int, default=8192,
                     help="mesh of the FP32-refinement vs FP64 comparison (0: skip)")
     ap.add_argument("--driver", default="device", choices=["device", "run"])
-    ap.add_argument("--workload", default="dropin", choices=["dropin", "dropin3d", "adjoint", "batch"],
+    ap.add_argument("--workload", default="dropin", choices=["dropin", "dropin3d", "adjoint", "batch", "refine", "precond"],
                     help="dropin: the 2D FP64 drop-in line (default); adjoint: the 3D adjoint form; "
-                         "batch: the batched form")
+                         "batch: the batched form; refine: one refinement timestep (--precision, --errswitch); "
+                         "precond: plain CG against the Jacobi-preconditioned CGs")
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--errswitch", action="store_true")
+    ap.add_argument("--max-iters", type=int, default=0)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--tune-iters", type=int, default=30)
     ap.add_argument("--fd-cells", type=int, default=32)
@@ -697,6 +886,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batch":
         line = bench_batch(args) if rank == 0 else None
+    elif args.workload == "refine":
+        line = bench_refine_case(args) if rank == 0 else None
+    elif args.workload == "precond":
+        line = precond_object(args.size, measured_peaks()[0], steps=args.steps) if rank == 0 else None
     elif args.workload == "dropin3d":
         if args.size == 4096:
             args.size = 256

@@ -247,12 +247,26 @@ void tl2d_set_device(int device);
 /* The cudaStream_t every kernel of this chunk is issued on (as void*). */
 void* tl2d_stream(Chunk* chunk);
 
-/* Device-resident driver (tl2d_solve_step): run Chebyshev trips and PPCG
- * inner steps temporally blocked in shared memory (1, the default; results
- * are bit-identical) or one launch per step (0). The same switch selects the
+/* No counterpart in the reference. Run Chebyshev trips and PPCG inner steps
+ * temporally blocked in shared memory (1, the default; results are
+ * bit-identical) or one launch per step (0): in the device-resident driver
+ * (tl2d_solve_step), and through the kernel interface, where consecutive
+ * run_cheby_iterate / run_ppcg_inner_iteration calls (each preceded only by
+ * the drivers' depth-1 halo update) are deferred and run as blocked launches
+ * when the next other entry point is called. The same switch selects the
  * blocked preconditioner of the refinement form's PPCG (tl2d_refine_solve_step;
  * its fields are bit-identical, its r.z is summed over another partition). */
 void tl2d_set_temporal_blocking(Chunk* chunk, int on);
+
+/* Jacobi preconditioner of the device-resident CG (tl2d_solve_step with the
+ * CG solver): 0 none, 1 jac_diag, 2 jac_block (tridiagonal blocks of 4 rows
+ * along y). The reference documents both as tl_preconditioner_type
+ * (README.md:127-133) but its C kernels ignore `preconditioner_on`; here
+ * settings->preconditioner at run_kernel_initialise selects jac_diag and
+ * this call any of the three. The stop test stays r.r < eps. The run_*
+ * kernel interface is unpreconditioned, as in the reference. Returns 0, or
+ * 37 for another type. */
+int tl2d_set_preconditioner(Chunk* chunk, int type);
 
 /* No counterpart in the reference. Feed the CG w sweep's operand rows by TMA
  * tile loads (1, the default, where the halo depth and row length are even;
@@ -319,21 +333,37 @@ typedef struct TlStepStats
 /* Allocation-free 2-norm: no counterpart in the reference. Adds the sum of
  * squares of the interior of `field` (a device array of x*y values, halo
  * included, index k + j*x) to the device double *norm_dev, like
- * run_calculate_2norm does for a host double, with the same launch shape and
- * summation order. For callers that cannot allocate device memory, or cannot
+ * run_calculate_2norm does for a host double; the sum equals that entry
+ * point's up to rounding (the block partials are added in another tree).
+ * For callers that cannot allocate device memory, or cannot
  * take the device-wide synchronisation a cudaMalloc/cudaFree implies (e.g. a
  * host whose memory is held by its own pool allocator): the reduction scratch
  * is a static device array of 65536 block partials (about 512 KiB) that every
  * GPU loading the library holds until exit, so this call allocates nothing.
  * Interiors needing more than 65536 blocks of 128 x 8 cells (beyond about
  * 8192 x 8192) are rejected with an error before any launch. Asynchronous on
- * `stream` (a cudaStream_t, NULL for the default stream). The first call on
- * a device looks up the array's address (cudaGetSymbolAddress) and caches it;
- * make that first call before any stream capture. All calls share the one
+ * `stream` (a cudaStream_t, NULL for the default stream). The array's address
+ * is looked up once per device (cudaGetSymbolAddress) and cached; under CUDA's
+ * lazy module loading that look-up is also when the driver reserves the
+ * array. run_kernel_initialise does it, so a host that initialises a chunk
+ * first has the array in place; a caller without a chunk should make its
+ * first call before it gives the rest of device memory to its pool and
+ * before any stream capture, or set CUDA_MODULE_LOADING=EAGER. All calls share the one
  * array: calls that overlap on the GPU race and must be serialised. Returns 0,
  * or an error code with the message available from tl2d_get_error. */
 int tl2d_calculate_2norm_noalloc(const double* field, int x, int y, int halo_depth,
         double* norm_dev, void* stream);
+
+/* Drives the bounded barrier wait that every TMA-fed sweep uses to expiry,
+ * without a GPU fault: one block waits on a shared-memory barrier that no copy
+ * and no thread completes, gives up after `polls` polls (1 .. 2^26) and
+ * records that in the chunk's wait-error word, as a sweep whose tile load
+ * never completed would. Returns 35 with the message from tl2d_get_error
+ * (set tl2d_set_error_mode(1) first, or the error exits like die()); every
+ * later solve on the chunk then reports error 35 as well, until the chunk is
+ * finalised. No counterpart in the reference: its failures are die() calls
+ * (2d/shared.c:97-111); this exists to test the error path of the waits. */
+int tl2d_check_bounded_wait(Chunk* chunk, long long polls);
 
 /* The four field-summary totals from a parallel tree reduction: one sweep at
  * full bandwidth instead of run_field_summary's serial reference order, so
@@ -410,6 +440,12 @@ int tl2d_batch_step(TlBatch* batch, TlBatchStats* stats);
 /* Per problem of the last step: CG iterations, FP64 r.r, converged flag
  * (arrays of count; any may be NULL). */
 int tl2d_batch_results(TlBatch* batch, int* iterations, double* rr, int* converged);
+/* How many SM clocks a grid-barrier wait of the persistent kernel may take
+ * before it gives up (cycles <= 0: the default, about 2 s). A wait that gives
+ * up makes every block return and tl2d_batch_step report error 63; the
+ * batch's fields are then invalid until the next step. No counterpart in the
+ * reference (its MPI barriers do not time out). */
+int tl2d_batch_set_wait_limit(TlBatch* batch, long long cycles);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

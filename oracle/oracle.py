@@ -37,7 +37,8 @@ class OSettings(C.Structure):
                 ("dt_init", C.c_double), ("eps", C.c_double), ("eps_lim", C.c_double),
                 ("max_iters", C.c_int), ("end_step", C.c_int), ("solver", C.c_int),
                 ("coefficient", C.c_int), ("presteps", C.c_int), ("ppcg_inner_steps", C.c_int),
-                ("error_switch", C.c_int), ("check_result", C.c_int), ("summary_frequency", C.c_int)]
+                ("error_switch", C.c_int), ("check_result", C.c_int), ("summary_frequency", C.c_int),
+                ("preconditioner", C.c_int)]
 
 
 class OState(C.Structure):
@@ -111,6 +112,7 @@ class OracleLib:
         s.coefficient, s.presteps, s.ppcg_inner_steps = config.coefficient, config.presteps, config.ppcg_inner_steps
         s.error_switch, s.check_result = int(config.error_switch), int(config.check_result)
         s.summary_frequency = config.summary_frequency
+        s.preconditioner = config.preconditioner_type
         return s
 
     @staticmethod
@@ -202,8 +204,10 @@ def harness_path(dims: int, suite: str = "omp3", fast: bool = False) -> Path:
 
 def run_reference(tea_in_text: str, dims: int = 2, suite: str = "omp3", threads: Optional[int] = None,
                   fast: bool = False, max_iters: Optional[int] = None, timeout: float = 3600.0,
-                  env_extra: Optional[dict] = None) -> List[StepResult]:
-    """Run a reference-host harness in a scratch directory and parse its output."""
+                  env_extra: Optional[dict] = None, warm: Optional[tuple] = None) -> List[StepResult]:
+    """Run a reference-host harness in a scratch directory and parse its output.
+    `max_iters` caps every timestep's solve; `warm` = (steps, cap) gives the
+    first `steps` timesteps a cap of their own (warm-up steps)."""
     exe = harness_path(dims, suite, fast)
     if not exe.exists():
         raise FileNotFoundError("%s is missing (build with oracle/build_ref.py)" % exe)
@@ -215,6 +219,8 @@ def run_reference(tea_in_text: str, dims: int = 2, suite: str = "omp3", threads:
     with tempfile.TemporaryDirectory(prefix="tl_ref_") as tmp:
         Path(tmp, "tea.in").write_text(tea_in_text)
         cmd = [str(exe), "tea.in"] + ([str(max_iters)] if max_iters is not None else [])
+        if warm is not None and max_iters is not None:
+            cmd += [str(int(warm[0])), str(int(warm[1]))]
         r = subprocess.run(cmd, cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError("%s failed (%d):\n%s\n%s" % (exe.name, r.returncode, r.stdout[-4000:], r.stderr[-4000:]))

@@ -16,7 +16,7 @@
  * with %.17e values, one line per timestep, and a final
  *   TLDONE <total solve seconds>
  *
- * Build: oracle/Makefile (TL3D selects the 3D host).
+ * Build: oracle/build_ref.py (-DTL3D selects the 3D host).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -43,7 +43,7 @@ static double now_seconds(void)
 int main(int argc, char** argv)
 {
     if (argc < 2) {
-        fprintf(stderr, "usage: %s tea.in [max_iters_override]\n", argv[0]);
+        fprintf(stderr, "usage: %s tea.in [max_iters_override [warm_steps warm_cap]]\n", argv[0]);
         return 2;
     }
 
@@ -58,14 +58,23 @@ int main(int argc, char** argv)
     Chunk* chunks = NULL;
     initialise_application(&chunks, settings);
 
-    /* Optional cap used for the bounded CPU-baseline samples. */
+    /* Optional cap used for the bounded CPU-baseline samples; the first
+     * warm_steps timesteps (warm-up, not timed by the caller) may use a
+     * smaller cap of their own. */
+    int cap = settings->max_iters, warm_steps = 0, warm_cap = 0;
     if (argc >= 3) {
-        settings->max_iters = atoi(argv[2]);
+        cap = atoi(argv[2]);
     }
+    if (argc >= 5) {
+        warm_steps = atoi(argv[3]);
+        warm_cap = atoi(argv[4]);
+    }
+    settings->max_iters = cap;
 
     double wallclock_prev = 0.0;
     double total = 0.0;
     for (int tt = 0; tt < settings->end_step; ++tt) {
+        settings->max_iters = (tt < warm_steps && warm_cap > 0) ? warm_cap : cap;
         double t0 = now_seconds();
         solve(chunks, settings, tt, &wallclock_prev);
         double t1 = now_seconds();

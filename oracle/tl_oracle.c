@@ -620,6 +620,7 @@ typedef struct {
     double dt_init, eps, eps_lim;
     int max_iters, end_step, solver, coefficient, presteps, ppcg_inner_steps;
     int error_switch, check_result, summary_frequency;
+    int preconditioner;     /* CG only: 0 none, 1 jac_diag, 2 jac_block (2D) */
 } OSettings;
 
 typedef struct {
@@ -632,7 +633,7 @@ typedef struct {
 typedef struct {
     int dims, x, y, z, hd;
     long n;
-    double *density, *energy0, *energy, *u, *u0, *p, *r, *w, *kx, *ky, *kz, *sd, *volume;
+    double *density, *energy0, *energy, *u, *u0, *p, *r, *w, *kx, *ky, *kz, *sd, *mi, *volume;
     double *vx, *vy, *vz, *cx, *cy, *cz, *xa, *ya, *za;
     double *cg_alphas, *cg_betas, *cheby_alphas, *cheby_betas;
     double theta, eigmin, eigmax;
@@ -725,6 +726,97 @@ static int oc_cg(OChunk* c, const OSettings* s, double rx, double ry, double rz,
         oc_cg_main_step(c, tt, &rro, error);
         oc_halo(c, 1);
         oc_post_trip(c, error);
+        if (fabs(*error) < s->eps) break;
+    }
+    st->cg_iters = tt;
+    st->total_iters = tt;
+    return 0;
+}
+
+/* Jacobi preconditioners of CG (2D). The reference C ports only parse
+ * preconditioner_on (2d/parse_config.c:136-138) and their kernels ignore it;
+ * the README documents jac_diag and jac_block with a block size of 4
+ * (README.md:127-133), and the reference's cuda 3D kernel forms the diagonal
+ * one as mi = 1 / diag(A), z = mi r (3d/c_kernels/cuda/cg_solver.cuknl:93-100).
+ * z = M^-1 r on the interior. jac_block: M is the tridiagonal part of A
+ * within blocks of 4 rows along y that start at the first interior row (the
+ * last block of a column may be shorter), solved by Thomas' algorithm:
+ * diagonal d = 1 + (kx_i+1 + kx_i) + (ky_i+x + ky_i), coupling -ky_i between
+ * rows i-x and i. */
+void o2_precond(int x, int y, int hd, int type, const double* kx, const double* ky, const double* r, double* z)
+{
+    const int bs = type == 2 ? 4 : 1;
+    for (int k = hd; k < x - hd; ++k) {
+        for (int jb = hd; jb < y - hd; jb += bs) {
+            const int m = (y - hd - jb) < bs ? (y - hd - jb) : bs;
+            double cp[4], dp[4];
+            for (int q = 0; q < m; ++q) {
+                const long i = k + (long)(jb + q) * x;
+                const double d = 1.0 + (kx[i + 1] + kx[i]) + (ky[i + x] + ky[i]);
+                if (type == 1) {
+                    const double mi = 1.0 / d;
+                    z[i] = mi * r[i];
+                    continue;
+                }
+                if (q == 0) {
+                    cp[0] = -ky[i + x] / d;
+                    dp[0] = r[i] / d;
+                } else {
+                    const double den = d + ky[i] * cp[q - 1];
+                    cp[q] = -ky[i + x] / den;
+                    dp[q] = (r[i] + ky[i] * dp[q - 1]) / den;
+                }
+            }
+            if (type == 1) continue;
+            double zn = dp[m - 1];
+            z[k + (long)(jb + m - 1) * x] = zn;
+            for (int q = m - 2; q >= 0; --q) {
+                zn = dp[q] - cp[q] * zn;
+                z[k + (long)(jb + q) * x] = zn;
+            }
+        }
+    }
+}
+
+static double o2_dot_interior(int x, int y, int hd, const double* a, const double* b)
+{
+    double s = 0.0;
+    for (int j = hd; j < y - hd; ++j)
+        for (int k = hd; k < x - hd; ++k) s += a[k + (long)j * x] * b[k + (long)j * x];
+    return s;
+}
+
+/* Preconditioned CG (2D): cg_driver.c's loop with z = M^-1 r (held in the
+ * chunk's mi field, which the reference allocates for its preconditioner):
+ * after cg_init, z = M^-1 r, p = z (depth-1 reflective halo), rro = r.z; per
+ * trip pw = p.w, alpha = rro / pw, u += alpha p, r -= alpha w, z = M^-1 r,
+ * beta = r.z / rro, p = beta p + z, rro = r.z; the stop test is on r.r, the
+ * error of the unpreconditioned CG, so eps means the same for both. */
+static int oc_pcg(OChunk* c, const OSettings* s, double rx, double ry, double rz, double* error, OStep* st)
+{
+    if (c->dims != 2) return -4;
+    oc_cg_init_driver(c, s, rx, ry, rz);
+    o2_precond(c->x, c->y, c->hd, s->preconditioner, c->kx, c->ky, c->r, c->mi);
+    for (int j = c->hd; j < c->y - c->hd; ++j)
+        for (int k = c->hd; k < c->x - c->hd; ++k) c->p[k + (long)j * c->x] = c->mi[k + (long)j * c->x];
+    oc_reset_flags(c);
+    c->flags[3] = c->flags[4] = true;
+    oc_halo(c, 1);
+    double rro = o2_dot_interior(c->x, c->y, c->hd, c->r, c->mi);
+    int tt;
+    for (tt = 0; tt < s->max_iters; ++tt) {
+        const double pw = oc_calc_w(c);
+        const double alpha = rro / pw;
+        c->cg_alphas[tt] = alpha;
+        const double rrn = oc_calc_ur(c, alpha);
+        o2_precond(c->x, c->y, c->hd, s->preconditioner, c->kx, c->ky, c->r, c->mi);
+        const double rzn = o2_dot_interior(c->x, c->y, c->hd, c->r, c->mi);
+        const double beta = rzn / rro;
+        c->cg_betas[tt] = beta;
+        o2_cg_calc_p(c->x, c->y, c->hd, beta, c->p, c->mi);
+        rro = rzn;
+        *error = rrn;
+        oc_halo(c, 1);
         if (fabs(*error) < s->eps) break;
     }
     st->cg_iters = tt;
@@ -894,7 +986,7 @@ static void oc_setup(OChunk* c, const OSettings* s, const OState* states, int nu
     for (int f = 0; f < 6; ++f) c->nb[f] = -1;
     c->density = zalloc(c->n); c->energy0 = zalloc(c->n); c->energy = zalloc(c->n); c->u = zalloc(c->n);
     c->u0 = zalloc(c->n); c->p = zalloc(c->n); c->r = zalloc(c->n); c->w = zalloc(c->n); c->kx = zalloc(c->n);
-    c->ky = zalloc(c->n); c->kz = zalloc(c->n); c->sd = zalloc(c->n); c->volume = zalloc(c->n);
+    c->ky = zalloc(c->n); c->kz = zalloc(c->n); c->sd = zalloc(c->n); c->mi = zalloc(c->n); c->volume = zalloc(c->n);
     c->xa = zalloc(c->n + c->y * c->z); c->ya = zalloc(c->n + c->x * c->z); c->za = zalloc(c->n + c->x * c->y);
     c->vx = zalloc(c->x + 1); c->vy = zalloc(c->y + 1); c->vz = zalloc(c->z + 1);
     c->cx = zalloc(c->x); c->cy = zalloc(c->y); c->cz = zalloc(c->z);
@@ -923,7 +1015,7 @@ static void oc_setup(OChunk* c, const OSettings* s, const OState* states, int nu
 static void oc_free(OChunk* c)
 {
     double* f[] = {c->density, c->energy0, c->energy, c->u, c->u0, c->p, c->r, c->w, c->kx, c->ky, c->kz,
-                   c->sd, c->volume, c->xa, c->ya, c->za, c->vx, c->vy, c->vz, c->cx, c->cy, c->cz,
+                   c->sd, c->mi, c->volume, c->xa, c->ya, c->za, c->vx, c->vy, c->vz, c->cx, c->cy, c->cz,
                    c->cg_alphas, c->cg_betas, c->cheby_alphas, c->cheby_betas};
     for (size_t k = 0; k < sizeof(f) / sizeof(f[0]); ++k) free(f[k]);
 }
@@ -942,7 +1034,7 @@ static int oc_step(OChunk* c, const OSettings* s, const double* dxyz, OStep* st)
     int rc;
     switch (s->solver) {
         case O_JACOBI: rc = oc_jacobi(c, s, rx, ry, rz, &error, st); break;
-        case O_CG: rc = oc_cg(c, s, rx, ry, rz, &error, st); break;
+        case O_CG: rc = s->preconditioner ? oc_pcg(c, s, rx, ry, rz, &error, st) : oc_cg(c, s, rx, ry, rz, &error, st); break;
         case O_CHEBY: rc = oc_cheby(c, s, rx, ry, rz, &error, st); break;
         case O_PPCG: rc = oc_ppcg(c, s, rx, ry, rz, &error, st); break;
         default: rc = -3;

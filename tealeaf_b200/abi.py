@@ -233,6 +233,16 @@ def load(dims: int) -> C.CDLL:
         lib.tl2d_batch_step.restype = _i
         lib.tl2d_batch_results.argtypes = [_p, _p, _p, _p]
         lib.tl2d_batch_results.restype = _i
+        lib.tl2d_batch_set_wait_limit.argtypes = [_p, C.c_longlong]
+        lib.tl2d_batch_set_wait_limit.restype = _i
+    if hasattr(lib, pre + "set_preconditioner"):
+        f = getattr(lib, pre + "set_preconditioner")
+        f.argtypes = [C.POINTER(chunk_t), _i]
+        f.restype = _i
+    if hasattr(lib, pre + "check_bounded_wait"):
+        f = getattr(lib, pre + "check_bounded_wait")
+        f.argtypes = [C.POINTER(chunk_t), C.c_longlong]
+        f.restype = _i
     if hasattr(lib, pre + "adjoint_gradient"):
         f = getattr(lib, pre + "adjoint_gradient")
         f.argtypes = head + [_i, _i, C.POINTER(_d), _d, _p, C.POINTER(AdjointStats)]

@@ -55,6 +55,13 @@ class Batch:
             raise DriverError("tl2d_batch_step returned %d" % rc)
         return st
 
+    def set_wait_limit(self, cycles: int) -> None:
+        """SM clocks a grid-barrier wait may take before it gives up (<= 0: the default)."""
+        rc = self.lib.tl2d_batch_set_wait_limit(self.handle, cycles)
+        abi.check(self.lib, 2)
+        if rc:
+            raise DriverError("tl2d_batch_set_wait_limit returned %d" % rc)
+
     def results(self):
         n = self.count
         it = np.zeros(n, dtype=np.int32)

@@ -5,9 +5,10 @@ Each library is a plain C-ABI ``.so`` (no torch types) compiled for sm_100a:
 * ``libtealeaf_b200_2d.so`` -- the 2D suite (reference 2d/kernel_interface.h)
 * ``libtealeaf_b200_3d.so`` -- the 3D suite (reference 3d/kernel_interface.h)
 
-FP64 drop-in sources are compiled with ``-fmad=false`` (each multiply and add
-rounded separately, in the reference's expression order); sources listed in
-``FMAD_SOURCES`` (the FP32 mixed-precision kernels) keep contraction.
+Every source is compiled with ``-fmad=false``: each multiply and add of the
+FP64 drop-in rounds separately, in the reference's expression order, and the
+FP32 kernels of the precision form contract only where they call fma
+explicitly (``fma_t`` in refine2d.cuh).
 The CUDA runtime is linked statically so the libraries load in any process
 (a C host, ctypes) without a matching libcudart on the library path.
 """
@@ -30,7 +31,6 @@ INCLUDE = REPO / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
               "--expt-relaxed-constexpr", "-I%s" % INCLUDE, "-I%s" % CSRC]
-FMAD_SOURCES = set()   # filled as FP32 sources are added
 
 LIBS = {
     "tealeaf_b200_2d": ["suite2d.cu", "driver2d.cu", "noalloc2d.cu", "mixed2d.cu", "batch2d.cu"],
@@ -77,8 +77,7 @@ def build(verbose: bool = False, force: bool = False):
         for src in srcs:
             obj = OBJ_DIR / (Path(src).stem + ".o")
             if force or _stale(obj, [CSRC / src] + _deps()):
-                fmad = [] if src in FMAD_SOURCES else ["-fmad=false"]
-                jobs.append([nvcc()] + cc + ARCH + NVCC_FLAGS + fmad + ["-c", CSRC / src, "-o", obj])
+                jobs.append([nvcc()] + cc + ARCH + NVCC_FLAGS + ["-fmad=false", "-c", CSRC / src, "-o", obj])
     with cf.ThreadPoolExecutor(max_workers=4) as ex:
         for out in ex.map(_run, jobs):
             if verbose and out.strip():

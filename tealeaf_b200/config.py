@@ -55,6 +55,12 @@ class Config:
     check_result: bool = True
     ppcg_inner_steps: int = 10
     preconditioner: bool = False
+    # Jacobi preconditioner of the device-resident CG: 0 none, 1 jac_diag,
+    # 2 jac_block. The reference C parser only reads `preconditioner_on`
+    # (2d/parse_config.c:136-138), which selects jac_diag here;
+    # `preconditioner_type = jac_diag | jac_block | none` is the reference
+    # README's tl_preconditioner_type (README.md:127-133).
+    preconditioner_type: int = 0
     num_chunks_per_rank: int = 1
     halo_depth: int = 2
     kernel_language: Optional[int] = None   # never defaulted by the reference
@@ -181,6 +187,11 @@ def read_config(text: str, dims: int = 2) -> Tuple[Config, List[StateDef]]:
                 break
         if hit:
             continue
+        if _starts_with("preconditioner_type", line):
+            v = _read_value(line, "preconditioner_type").strip().lower()
+            c.preconditioner_type = {"jac_diag": 1, "jac_block": 2}.get(v, 0)
+            c.preconditioner = c.preconditioner_type != 0
+            continue
         if _starts_with("use_fortran_kernels", line):
             c.kernel_language = 1
             continue
@@ -239,6 +250,8 @@ def read_config(text: str, dims: int = 2) -> Tuple[Config, List[StateDef]]:
             elif geom == "point":
                 st.geometry = POINT
         states[sn - 1] = st
+    if c.preconditioner and c.preconditioner_type == 0:
+        c.preconditioner_type = 1   # preconditioner_on alone: jac_diag
     return c, [s if s is not None else StateDef(0.0, 0.0, defined=False) for s in states]
 
 

@@ -40,7 +40,7 @@ using namespace tl2d::rf;
 namespace {
 
 constexpr int kBatchMinB = 8;                    // resident blocks per SM of the persistent kernel
-constexpr long long kBarrierLimit = 4000000000LL;   // SM clocks a barrier wait may take (~2 s)
+constexpr long long kBarrierLimit = 4000000000LL;   // default: SM clocks a barrier wait may take (~2 s)
 
 enum { BF_KX = 0, BF_KY, BF_P0, BF_P1, BF_W, BF_R, BF_XS, BF_COUNT };
 
@@ -63,6 +63,7 @@ struct BCtl {
     int upd_iter;     // last iteration in which some problem asked for a residual replacement
     int ndone;        // problems finished
     int iters;        // iterations the kernel ran
+    long long limit;  // SM clocks a barrier wait may take before it gives up (kept across steps)
 };
 
 __device__ bool grid_barrier(BCtl* c)
@@ -81,7 +82,7 @@ __device__ bool grid_barrier(BCtl* c)
             const long long t0 = clock64();
             while (*vgen == g) {
                 if (*(volatile int*)&c->err) break;
-                if (clock64() - t0 > kBarrierLimit) {
+                if (clock64() - t0 > c->limit) {
                     atomicExch(&c->err, 1);
                     break;
                 }
@@ -206,9 +207,12 @@ __global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __rest
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = max_iters;
 }
 
-// Counts problems already converged by the setup (done before any iteration).
-__global__ void k_batch_count_done(const MxState* st, int np, BCtl* ctl)
+// Counts problems already converged by the setup (done before any iteration)
+// and clears the per-problem tile tickets (a step whose barrier wait gave up
+// may have left some mid-phase).
+__global__ void k_batch_count_done(const MxState* st, int np, BCtl* ctl, unsigned* tickets)
 {
+    for (int b = threadIdx.x; b < np; b += blockDim.x) tickets[b] = 0u;
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int n = 0;
     for (int b = 0; b < np; ++b) n += st[b].done ? 1 : 0;
@@ -357,7 +361,7 @@ void issue_step(TlBatch* B, int iter_cap, bool finish)
             s->g.x, s->g.hd, B->lay[b], c->r, c->u0, c->kx, c->ky, f[BF_KX], f[BF_KY], f[BF_R], f[BF_P0], f[BF_P1],
             f[BF_W], f[BF_XS], B->rs, FinMxInit{&B->d_st[b], 0.0, st->eps, st->max_iters, nullptr});
     }
-    k_batch_count_done<<<1, 32, 0, B->stream>>>(B->d_st, B->count, B->d_ctl);
+    k_batch_count_done<<<1, 32, 0, B->stream>>>(B->d_st, B->count, B->d_ctl, B->d_tickets);
     void* args[] = {&B->d_prob, &B->count, &B->d_tile_prob, &B->ntiles, &B->d_st, &B->d_tickets, &B->d_partials,
                     &B->d_ctl, &iter_cap};
     cudaLaunchConfig_t cfg{};
@@ -475,6 +479,8 @@ TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int t
     TL_CUDA(cudaMemsetAsync(B->rs.ticket, 0, 256, B->stream));
     TL_CUDA(cudaMemsetAsync(B->d_tickets, 0, sizeof(unsigned) * count, B->stream));
     TL_CUDA(cudaMemsetAsync(B->d_ctl, 0, sizeof(BCtl), B->stream));
+    static const long long default_limit = kBarrierLimit;
+    TL_CUDA(cudaMemcpyAsync(&B->d_ctl->limit, &default_limit, sizeof(long long), cudaMemcpyHostToDevice, B->stream));
     int per_sm = 0;
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, BX, 0));
     B->max_grid = std::max(1, per_sm) * B->sm_count;
@@ -611,6 +617,22 @@ int tl2d_batch_step(TlBatch* B, TlBatchStats* stats)
     out->graph = B->exec ? 1 : 0;
     out->device_ms = ms;
     return tl::failed() ? tl::error_state().code : 0;
+}
+
+// How long (SM clocks) a grid-barrier wait of the persistent kernel may take
+// before it gives up; cycles <= 0 restores the default (about 2 s). The
+// limit lives in device memory, so captured graphs pick it up.
+int tl2d_batch_set_wait_limit(TlBatch* B, long long cycles)
+{
+    if (!B) {
+        tl::fail(64, "tl2d_batch_set_wait_limit: null batch");
+        return 64;
+    }
+    const long long v = cycles > 0 ? cycles : kBarrierLimit;
+    if (!TL_CUDA(cudaMemcpyAsync(&B->d_ctl->limit, &v, sizeof(long long), cudaMemcpyHostToDevice, B->stream)) ||
+        !TL_CUDA(cudaStreamSynchronize(B->stream)))
+        return tl::error_state().code;
+    return 0;
 }
 
 // Per-problem CG iterations and final FP64 residual r.r of the last step.

@@ -20,6 +20,8 @@
 //
 // Chebyshev (MODE 0), carried fields A = u, B = p, state (u_{n-1}, p_{n-1})
 // with the add pending:   A += B ;  B = a_n B + b_n (u0 - A A)
+// (or, with add_end, state (u_n, p_n):   B = a B + b (u0 - A A) ;  A += B,
+// the order of run_cheby_iterate, cheby.c:57-85)
 // PPCG (MODE 1), A = sd, B = r, fold index pp:
 //   A = pp == 0 ? B / theta : a_{pp-1} A + b_{pp-1} B ;  B -= A A ;  u += A
 #pragma once
@@ -46,6 +48,8 @@ struct BlockedArgs {
     double theta;       // PPCG fold of pp == 0
     const double* alphas;
     const double* betas;
+    int add_end;        // Chebyshev: each trip ends with its u += p (the kernel-interface calls'
+                        // order) instead of starting with the previous trip's
 };
 
 // Thread (cx, cy) holds column cx of the region, rows cy * kTSeg .. + kTSeg,
@@ -119,6 +123,9 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, Blocked
                     av[k] = bv[k] / a.theta;
                     As[(r0 + k) * kTW + cx] = av[k];
                 }
+            } else if (MODE == 0 && a.add_end && i == 0) {
+#pragma unroll
+                for (int k = 0; k < kTSeg; ++k) As[(r0 + k) * kTW + cx] = av[k];
             } else {
 #pragma unroll
                 for (int k = 0; k < kTSeg; ++k) {
@@ -170,6 +177,11 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, Blocked
         };
         if (touches) pass_b(std::true_type());
         else pass_b(std::false_type());
+    }
+    // the last trip's u += p when each trip ends with its add
+    if (MODE == 0 && a.add_end && H > 0) {
+#pragma unroll
+        for (int k = 0; k < kTSeg; ++k) av[k] = av[k] + bv[k];
     }
     // write the tile: A (u, resp. sd) with its reflective depth-1 halo, B (p, resp. r)
     if (colin && mxc == 0) {

@@ -19,6 +19,7 @@
 // diffuse_overload (2d/application.h:9-11) runs every timestep this way.
 #include "blocked2d.cuh"
 #include "host_maths.hpp"
+#include "pcg2d.cuh"
 #include "suite2d_impl.hpp"
 
 #include <cfloat>
@@ -137,22 +138,34 @@ struct Run {
     // pending). Closes the phase: last p update and the halo of u and p.
     DevState cg_phase(int from, bool fresh)
     {
+        FinCgUr fin_ur{s->d_state, s->d_cg_betas, prm, s->d_mirror};
+        const Scalar alpha{0.0, &s->d_state->alpha};
+        return cg_trips(from, fresh, chunk->r, [&](double* p) {
+            launch_cg_ur2(s, gi, alpha, chunk->u, p, chunk->r, chunk->w, done(), fin_ur);
+        });
+    }
+
+    // The CG loop with `fold` the field of the p update p = beta p + fold (r
+    // for CG, z for the preconditioned CG) and ur(p) launching the second
+    // sweep of a trip on the current p buffer.
+    template <typename Ur>
+    DevState cg_trips(int from, bool fresh, const double* fold, Ur&& ur)
+    {
         double* buf[2] = {chunk->p, s->alt[ALT_P]};
         FinCgW fin_w{s->d_state, s->d_cg_alphas};
-        FinCgUr fin_ur{s->d_state, s->d_cg_betas, prm, s->d_mirror};
-        const Scalar beta{0.0, &s->d_state->beta}, alpha{0.0, &s->d_state->alpha};
+        const Scalar beta{0.0, &s->d_state->beta};
         // parity of the current p buffer: trip t (t > from or !fresh) writes buf[(t - from + base) & 1]
         int cur = 0;
         auto trip = [&](int t) {
             if (fresh && t == from) {
-                launch_cg_w2<false, false>(s, chunk, gh, fc, beta, buf[cur], buf[cur], chunk->r, chunk->w, nullptr,
+                launch_cg_w2<false, false>(s, chunk, gh, fc, beta, buf[cur], buf[cur], fold, chunk->w, nullptr,
                                            0, done(), fin_w);
             } else {
-                launch_cg_w2<true, true>(s, chunk, gh, fc, beta, buf[cur], buf[cur ^ 1], chunk->r, chunk->w,
+                launch_cg_w2<true, true>(s, chunk, gh, fc, beta, buf[cur], buf[cur ^ 1], fold, chunk->w,
                                          nullptr, 0, done(), fin_w);
                 cur ^= 1;
             }
-            launch_cg_ur2(s, gi, alpha, chunk->u, buf[cur], chunk->r, chunk->w, done(), fin_ur);
+            ur(buf[cur]);
         };
         DevState st = loop(from, trip);
         // Trips from..st.trip-1 ran; the fused ones flipped the current buffer.
@@ -160,7 +173,7 @@ struct Run {
         const int flips = fresh ? std::max(0, ran - 1) : ran;
         double* pcur = buf[flips & 1];
         if (pcur != chunk->p) swap_alt(s, chunk, ALT_P);
-        TL_LAUNCH(s, "k_cg_close", (k_cg_close<<<gi, BX, 0, s->stream>>>(s->g, fc, beta, 1, chunk->p, chunk->r,
+        TL_LAUNCH(s, "k_cg_close", (k_cg_close<<<gi, BX, 0, s->stream>>>(s->g, fc, beta, 1, chunk->p, fold,
                                                                            chunk->u)));
         // host copies of the CG coefficients (the reference drivers keep them on the host)
         if (st.trip > 0) {
@@ -171,6 +184,30 @@ struct Run {
         }
         TL_CUDA(cudaStreamSynchronize(s->stream));
         return st;
+    }
+
+    // ------------------------------------------------- preconditioned CG
+    // After cg_init, the halo of u and p and copy_u: z = M^-1 r, p = z,
+    // rro = r.z, then the CG loop with z folded into p and the u/r/z sweep
+    // (pcg2d.cuh). z is held in the chunk's mi field.
+    template <int BS>
+    DevState pcg_phase()
+    {
+        Geo gb = s->g;
+        gb.rows = (gb.rows + BS - 1) / BS * BS;   // strips of whole blocks
+        const dim3 gbi = interior_grid(gb);
+        double* z = chunk->mi;
+        TL_LAUNCH(s, "k_pcg_init", (k_pcg_init<BS><<<gbi, BX, 0, s->stream>>>(
+                                       gb, fc, chunk->r, chunk->kx, chunk->ky, z, chunk->p, s->rs,
+                                       FinCgInit{s->d_state, s->d_mirror})));
+        read_state();
+        FinPcgUr fin_ur{s->d_state, s->d_cg_betas, prm, s->d_mirror};
+        const Scalar alpha{0.0, &s->d_state->alpha};
+        return cg_trips(0, true, z, [&](double* p) {
+            TL_LAUNCH(s, "k_pcg_ur", (k_pcg_ur<BS><<<gbi, BX, 0, s->stream>>>(gb, alpha, chunk->u, p, chunk->r,
+                                                                              chunk->w, chunk->kx, chunk->ky, z,
+                                                                              s->rs, done(), fin_ur)));
+        });
     }
 
     double norm(const double* b)
@@ -500,7 +537,9 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
     TL_LAUNCH(s, "k_copy_u", k_copy_u<<<R.gi, BX, 0, s->stream>>>(s->g, chunk->u0, chunk->u));
     R.read_state();
 
-    st = R.cg_phase(0, true);
+    if (settings->solver == TL_CG_SOLVER && s->precond == kPrecondDiag) st = R.pcg_phase<1>();
+    else if (settings->solver == TL_CG_SOLVER && s->precond == kPrecondBlock) st = R.pcg_phase<4>();
+    else st = R.cg_phase(0, true);
     error = st.error;
     if (st.reason == 2 && settings->solver == TL_CHEBY_SOLVER) {
         const int tt_sw = st.trip;

@@ -7,9 +7,19 @@
 // handed (nearly) all device memory to its own pool allocator and must not
 // fail with out-of-memory in the middle of a solve, or latency-sensitive code
 // that must not take the device-wide synchronisation cudaFree implies. For
-// them tl2d_calculate_2norm_noalloc computes the same sum with its scratch
-// in a fixed static device array that the driver reserves when the library
-// is loaded, so the call itself allocates nothing.
+// them tl2d_calculate_2norm_noalloc computes the same sum (equal to
+// run_calculate_2norm's up to rounding: its blocks cover 8 rows where the
+// regular sweep's cover a per-mesh row count, so the partials are added in
+// another tree) with its scratch in a fixed static device array.
+//
+// When the array is reserved: under CUDA's lazy module loading (the default
+// since CUDA 12.2) the driver loads this file's module, and with it the
+// array, the first time its address is looked up. run_kernel_initialise does
+// that look-up (tl_noalloc_prepare below), so a host that calls it, as every
+// TeaLeaf host does, has the array in place before it hands the rest of the
+// device memory to its pool. A caller that uses this entry point without
+// run_kernel_initialise should make its first call before that hand-over, or
+// run with CUDA_MODULE_LOADING=EAGER, which loads the array with the library.
 //
 // The limit: the array holds kMaxBlocks block partials, one per block of the
 // interior sweep (128 columns x 8 rows per block), which covers interior
@@ -24,11 +34,11 @@
 #include "tealeaf_b200_2d.h"
 
 #include <cuda_runtime.h>
+#include <atomic>
 
 namespace {
 
-// Launch shape of the regular 2-norm sweep; the same shape gives the same
-// per-block partials and the same summation tree, hence the same result.
+// Launch shape: 128 columns x 8 rows per block (one partial per block).
 constexpr int kBX = 128;
 constexpr int kRows = 8;
 constexpr long kMaxBlocks = 65536;
@@ -41,8 +51,9 @@ constexpr long kTicketOffset = kMaxBlocks;
 constexpr long kResultOffset = kMaxBlocks + 32;
 static __device__ __align__(256) double g_norm_scratch[kMaxBlocks + 64];
 
-// Host-side cache of the scratch array's device address, per device.
-double* g_scratch_addr[kMaxDevices] = {nullptr};
+// Host-side cache of the scratch array's device address, per device. Two
+// host threads making their first call at once both store the same address.
+std::atomic<double*> g_scratch_addr[kMaxDevices];
 
 struct AccumulateInto {
     double* out;
@@ -65,7 +76,32 @@ __global__ void __launch_bounds__(kBX) k_norm2_noalloc(int x, int y, int hd, con
                          AccumulateInto{norm_dev});
 }
 
+// The scratch array's device address on the current device (looked up once,
+// which loads the module under lazy loading); nullptr after a recorded error.
+double* scratch_on_current_device(int code)
+{
+    int dev = 0;
+    if (!TL_CUDA(cudaGetDevice(&dev))) return nullptr;
+    if (dev < 0 || dev >= kMaxDevices) {
+        tl::fail(code, "tl2d_calculate_2norm_noalloc: device %d out of range", dev);
+        return nullptr;
+    }
+    double* addr = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!addr) {
+        if (!TL_CUDA(cudaGetSymbolAddress((void**)&addr, g_norm_scratch))) return nullptr;
+        g_scratch_addr[dev].store(addr, std::memory_order_release);
+    }
+    return addr;
+}
+
 }  // namespace
+
+// Called by run_kernel_initialise with the chunk's device current, so the
+// static scratch is in place before the host's solve starts.
+bool tl_noalloc_prepare()
+{
+    return scratch_on_current_device(24) != nullptr;
+}
 
 extern "C" int tl2d_calculate_2norm_noalloc(const double* field, int x, int y, int halo_depth, double* norm_dev,
                                             void* stream)
@@ -89,18 +125,8 @@ extern "C" int tl2d_calculate_2norm_noalloc(const double* field, int x, int y, i
         return 22;
     }
     // 2. Once per device, with that device current: the scratch array's address.
-    int dev = 0;
-    if (!TL_CUDA(cudaGetDevice(&dev))) return 23;
-    if (dev < 0 || dev >= kMaxDevices) {
-        tl::fail(24, "tl2d_calculate_2norm_noalloc: device %d out of range", dev);
-        return 24;
-    }
-    if (!g_scratch_addr[dev]) {
-        double* addr = nullptr;
-        if (!TL_CUDA(cudaGetSymbolAddress((void**)&addr, g_norm_scratch))) return 25;
-        g_scratch_addr[dev] = addr;
-    }
-    double* scratch = g_scratch_addr[dev];
+    double* scratch = scratch_on_current_device(24);
+    if (!scratch) return 25;
     cudaStream_t st = (cudaStream_t)stream;
     tl::ReduceSlots rs;
     rs.partials = scratch;

@@ -114,6 +114,22 @@ struct FinCgUr {           // beta = rrn / rro; rro = error = rrn  (cg_driver.c:
     }
 };
 
+struct FinPcgUr {          // preconditioned CG: t = (r.r, r.z); beta = r.z / rro, rro = r.z, error = r.r
+    DevState* st;
+    double* cg_betas;
+    DevParams prm;
+    int* host_mirror;
+    __device__ void operator()(const double* t) const
+    {
+        const double b = t[1] / st->rro;
+        st->beta = b;
+        cg_betas[st->trip] = b;
+        st->rro = t[1];
+        st->rrn = t[0];
+        end_of_trip(st, prm, t[0], host_mirror);
+    }
+};
+
 __device__ __forceinline__ bool gate_closed(const int* done) { return done && *(volatile const int*)done; }
 
 // Chebyshev coefficients of the current trip: host values, or the device

@@ -34,6 +34,8 @@
 using namespace tl2d;
 using tl::ReduceSlots;
 
+bool tl_noalloc_prepare();   // noalloc2d.cu: reserves the allocation-free 2-norm's static scratch
+
 
 
 // ================================================================= helpers
@@ -142,9 +144,50 @@ static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
     s->pq.b.clear();
 }
 
-void flush(TlSuite2D* s, Chunk* chunk)
+// Runs the deferred Chebyshev trips (cheby.c:57-85 as the reference drivers
+// call them: per trip w = A u, r = u0 - w, p = alpha p + beta r, u += p, then
+// a depth-1 halo of u): temporally blocked launches of up to kTB trips, each
+// ending with its u += p, u reflected on the fly and its halo written; the
+// last trip also writes w and r. The same results as one launch per call.
+static void run_cheby_queue(TlSuite2D* s, Chunk* chunk)
+{
+    s->cq.active = false;
+    const int n = (int)s->cq.a.size();
+    if (n == 0) return;
+    TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, s->cq.a.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                            s->stream));
+    TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, s->cq.b.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                            s->stream));
+    const size_t smem = blocked_smem<0>();
+    TL_CUDA(cudaFuncSetAttribute(k_blocked<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // As for the PPCG queue: an odd number of launches gets a closing
+    // zero-step launch, so u and p end in the buffers the chunk pointed at.
+    const int launches = (n + kTB - 1) / kTB;
+    for (int q = 0; q < launches + (launches & 1); ++q) {
+        const int first = std::min(q * kTB, n);
+        const int steps = std::max(0, std::min(kTB, n - first));
+        const BlockedArgs a{steps, first, steps > 0 && first + steps == n ? 1 : 0, 0.0,
+                            s->d_cheby_alphas, s->d_cheby_betas, 1};
+        TL_LAUNCH(s, "k_blocked<cheby>", (k_blocked<0><<<blocked_grid(s->g), kTBThreads, smem, s->stream>>>(
+                                             s->g, a, chunk->u, chunk->p, s->alt[ALT_U], s->alt[ALT_P], chunk->u0,
+                                             nullptr, chunk->w, chunk->r, chunk->kx, chunk->ky, nullptr)));
+        swap_alt(s, chunk, ALT_U);
+        swap_alt(s, chunk, ALT_P);
+    }
+    s->cq.a.clear();
+    s->cq.b.clear();
+}
+
+// Runs whichever deferred queue is open.
+static void run_queues(TlSuite2D* s, Chunk* chunk)
 {
     if (s->pq.active) run_ppcg_queue(s, chunk);
+    if (s->cq.active) run_cheby_queue(s, chunk);
+}
+
+void flush(TlSuite2D* s, Chunk* chunk)
+{
+    run_queues(s, chunk);
     if (s->pend.calc_p) {
         TL_LAUNCH(s, "k_cg_calc_p",
                   k_cg_calc_p<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, s->pend.beta, chunk->p, chunk->r));
@@ -180,6 +223,21 @@ TlSuite2D* ready(Chunk* chunk)
 
 }  // namespace
 
+// The bounded barrier wait of the TMA-fed sweeps, on a barrier that nothing
+// completes: no copy is issued and nothing arrives, so the wait runs out
+// after `polls` polls, and the give-up is recorded in `err` exactly as a
+// sweep records it. Thread 0 waits; the block holds no copy in flight.
+__global__ void k_bounded_wait_check(long polls, int* err)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        tl::mbar_init(&bar, 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) tl::mbar_wait_limited(&bar, 0u, err, polls);
+}
+
 // The reference host's logger (2d/shared.c:25-51), used when the host provides it.
 extern "C" void print_and_log(Settings* settings, const char* format, ...) __attribute__((weak));
 
@@ -207,6 +265,18 @@ void tl2d_set_tma(Chunk* chunk, int on)
 }
 void tl2d_flush(Chunk* chunk) { ready(chunk); }
 
+int tl2d_set_preconditioner(Chunk* chunk, int type)
+{
+    TlSuite2D* s = suite_of(chunk);
+    if (!s) return tl::error_state().code;
+    if (type < 0 || type > 2) {
+        tl::fail(37, "tl2d_set_preconditioner: type %d is not 0 (none), 1 (jac_diag) or 2 (jac_block)", type);
+        return 37;
+    }
+    s->precond = type;
+    return 0;
+}
+
 void tl2d_profile_enable(Chunk* chunk, int on)
 {
     TlSuite2D* s = suite_of(chunk);
@@ -219,6 +289,24 @@ void tl2d_profile_reset(Chunk* chunk)
 {
     TlSuite2D* s = suite_of(chunk);
     if (s) s->prof.reset();
+}
+
+int tl2d_check_bounded_wait(Chunk* chunk, long long polls)
+{
+    TlSuite2D* s = ready(chunk);
+    if (!s) return tl::error_state().code;
+    if (polls < 1 || polls > tl::kTmaSpinLimit) {
+        tl::fail(36, "tl2d_check_bounded_wait: polls must be in [1, %ld]", tl::kTmaSpinLimit);
+        return 36;
+    }
+    k_bounded_wait_check<<<1, 32, 0, s->stream>>>((long)polls, s->d_mirror + kTmaErrWord2);
+    if (!TL_LAUNCHED("k_bounded_wait_check") || !TL_CUDA(cudaStreamSynchronize(s->stream))) return tl::error_state().code;
+    if (tma_failed(s)) {
+        tl::fail(35, "a bounded barrier wait gave up after %lld polls (wait check on a barrier nothing completes)",
+                 polls);
+        return 35;
+    }
+    return 0;
 }
 
 long long tl2d_launch_count(Chunk* chunk)
@@ -255,6 +343,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     if (!TL_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) return;
     s->g = Geo{chunk->x, chunk->y, settings->halo_depth};
     s->g.rows = choose_rows(chunk->x - 2 * settings->halo_depth, chunk->y - 2 * settings->halo_depth, s->sm_count);
+    s->precond = settings->preconditioner ? 1 : 0;
     const long x = chunk->x, y = chunk->y, n = x * y;
     const long mi = settings->max_iters > 0 ? settings->max_iters : 1;
 
@@ -309,6 +398,7 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     chunk->cheby_alphas = (double*)calloc((size_t)mi, sizeof(double));
     chunk->cheby_betas = (double*)calloc((size_t)mi, sizeof(double));
     TL_CUDA(cudaStreamSynchronize(s->stream));
+    tl_noalloc_prepare();
     if (print_and_log && settings->tea_out_fp)
         print_and_log(settings, "Performing this solve with the B200 (sm_100a) %s solver\n",
                       settings->solver_name ? settings->solver_name : "");
@@ -497,7 +587,7 @@ void run_cg_calc_w(Chunk* chunk, Settings* settings, double* pw)
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
-    if (s->pq.active) run_ppcg_queue(s, chunk);   // deferred PPCG steps precede everything recorded after them
+    run_queues(s, chunk);   // deferred steps precede everything recorded after them
     if (s->pend.halo[TL_FIELD_P] > 1) flush(s, chunk);
     const bool fuse = s->pend.calc_p;
     const bool refl = s->pend.halo[TL_FIELD_P] == 1;
@@ -531,7 +621,7 @@ void run_cg_calc_ur(Chunk* chunk, Settings* settings, double alpha, double* rrn)
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
-    if (s->pq.active) run_ppcg_queue(s, chunk);
+    run_queues(s, chunk);
     if (s->pend.calc_p || s->pend.halo[TL_FIELD_U]) flush(s, chunk);
     launch_cg_ur2(s, interior_grid(s->g), Scalar{alpha, nullptr}, chunk->u, chunk->p, chunk->r, chunk->w, nullptr,
                   tl::NoFinish());
@@ -547,7 +637,7 @@ void run_cg_calc_p(Chunk* chunk, Settings* settings, double beta)
     if (tl::failed()) return;
     TlSuite2D* s = suite_of(chunk);
     if (!s) return;
-    if (s->pq.active) run_ppcg_queue(s, chunk);
+    run_queues(s, chunk);
     if (s->pend.calc_p || s->pend.halo[TL_FIELD_P]) flush(s, chunk);
     s->pend.calc_p = true;
     s->pend.beta = beta;
@@ -567,11 +657,29 @@ void run_cheby_init(Chunk* chunk, Settings* settings)
     TL_LAUNCH(s, "k_add_p", k_add_p<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->u, chunk->p));
 }
 
-// 2d/kernel_interface.h:48 (cheby.c:57-85)
+// 2d/kernel_interface.h:48 (cheby.c:57-85). With temporal blocking on and
+// four external faces, a call preceded by nothing but the depth-1 halo update
+// of u is queued (run_cheby_queue); otherwise it runs at once.
 void run_cheby_iterate(Chunk* chunk, Settings* settings, double alpha, double beta)
 {
     (void)settings;
-    TlSuite2D* s = ready(chunk);
+    if (tl::failed()) return;
+    TlSuite2D* s = suite_of(chunk);
+    if (!s) return;
+    const Faces fc = faces_of(chunk);
+    if (s->temporal_blocking && fc.l && fc.r && fc.b && fc.t && !s->pq.active && !s->pend.calc_p &&
+        s->pend.halo[TL_FIELD_U] <= 1 && (long)s->cq.a.size() < s->table_len) {
+        bool other = false;
+        for (int f = 0; f < TL_NUM_FIELDS; ++f) other |= f != TL_FIELD_U && s->pend.halo[f] != 0;
+        if (!other) {
+            s->pend.halo[TL_FIELD_U] = 0;   // the blocked trips reflect u on the fly and write its halo
+            s->cq.active = true;
+            s->cq.a.push_back(alpha);
+            s->cq.b.push_back(beta);
+            return;
+        }
+    }
+    s = ready(chunk);
     if (!s) return;
     TL_LAUNCH(s, "k_cheby_sweep",
               k_cheby_sweep<false><<<interior_grid(s->g), BX, 0, s->stream>>>(

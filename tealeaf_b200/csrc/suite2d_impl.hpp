@@ -3,11 +3,12 @@
 // (driver2d.cu).
 #pragma once
 
-#include "kernels2d.cuh"
+#include "stream2d.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <vector>
 
 // Buffers that alternate between two slices (fused sweeps read the old values
@@ -55,6 +56,10 @@ struct TlSuite2D {
     // blocked in shared memory (blocked2d.cuh); off = one launch per step.
     bool temporal_blocking = true;
 
+    // Device-resident CG: Jacobi preconditioner (pcg2d.cuh), 0 none,
+    // 1 jac_diag, 2 jac_block; settings->preconditioner selects jac_diag.
+    int precond = 0;
+
     // Kernel-interface PPCG inner steps deferred for the blocked kernel:
     // run_ppcg_init opens the queue, run_ppcg_inner_iteration appends its
     // coefficients (absorbing the depth-1 halo update of sd before it), and
@@ -63,6 +68,15 @@ struct TlSuite2D {
         bool active = false;
         std::vector<double> a, b;
     } pq;
+
+    // Kernel-interface Chebyshev trips deferred for the blocked kernel the
+    // same way: run_cheby_iterate appends its coefficients (absorbing the
+    // depth-1 halo update of u before it), the next other entry point runs
+    // them.
+    struct {
+        bool active = false;
+        std::vector<double> a, b;
+    } cq;
 
     // FP32 buffers of the iterative-refinement form (mixed2d.cu), on first use.
     void* mx_slab = nullptr;
@@ -157,9 +171,9 @@ inline const CUtensorMap* tma_lookup(TlSuite2D* s, const void* ptr, int kind, En
     return &e.map;
 }
 
-// Tensor map of a chunk array for k_cg_w_fused_tma: kind 0 operand rows (box
+// Tensor map of a chunk array for k_cg_w_stream: kind 0 operand rows (box
 // (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT); for
-// k_cg_ur_fused_tma: kind 3 (BX x kRowsU).
+// k_cg_ur_stream: kind 3 (BX x kRowsU).
 inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
 {
     static const unsigned box[4] = {BX + 4, BX + 2, BX, BX};
@@ -174,10 +188,39 @@ inline bool tma_usable(const TlSuite2D* s) { return s->tma && s->g.hd % 2 == 0 &
 
 inline bool tma_failed(const TlSuite2D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord2] != 0; }
 
-// The fused CG w sweep (k_cg_w_fused semantics), by TMA where possible.
-// Internal linkage, like the kernels it launches: each translation unit has
-// its own kernel copies, so each keeps its own record of the raised
-// shared-memory limit.
+// Persistent grid of the streaming sweeps: one block per strip up to
+// kStreamBlocksPerSm blocks per SM.
+inline dim3 stream_grid(const TlSuite2D* s)
+{
+    const dim3 gi = interior_grid(s->g);
+    const long strips = (long)gi.x * gi.y;
+    return dim3((unsigned)std::min<long>(strips, (long)s->sm_count * kStreamBlocksPerSm));
+}
+
+// Launch with programmatic dependent launch allowed (the kernel waits for
+// its predecessor in the stream with griddepcontrol.wait).
+template <typename... Params, typename... Args>
+static cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, size_t smem, cudaStream_t st,
+                                    Args&&... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(BX);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// The fused CG w sweep (k_cg_w_fused semantics): the streaming TMA-fed
+// kernel where the alignment rules allow, else the per-thread-load kernel on
+// `grid` (interior blocks + the halo-duty row). Internal linkage, like the
+// kernels it launches: each translation unit has its own kernel copies, so
+// each keeps its own record of the raised shared-memory limit.
 template <bool F, bool R, typename Finish>
 static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
                   double* p_out, const double* r, double* w, double* u_halo, int uhd, const int* done, Finish fin)
@@ -191,13 +234,14 @@ static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc,
             const Tma2Maps m{*a, *b, *kx, *ky};
             static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
             if (!(attr_set & (1u << (s->device & 31)))) {
-                TL_CUDA(cudaFuncSetAttribute(k_cg_w_fused_tma<F, R, Finish>,
+                TL_CUDA(cudaFuncSetAttribute(k_cg_w_stream<F, R, Finish>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaRowsBytes));
                 attr_set |= 1u << (s->device & 31);
             }
-            TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused_tma<F, R><<<grid, BX, kTmaRowsBytes, s->stream>>>(
-                                             s->g, fc, beta, m, p_in, p_out, r, w, u_halo, uhd, s->rs, done, fin,
-                                             s->d_mirror + kTmaErrWord2)));
+            TL_LAUNCH(s, "k_cg_w_fused",
+                      launch_dependent(k_cg_w_stream<F, R, Finish>, stream_grid(s), kTmaRowsBytes, s->stream, s->g,
+                                       fc, beta, m, p_out, w, u_halo, uhd, s->rs, done, fin,
+                                       s->d_mirror + kTmaErrWord2));
             return;
         }
     }
@@ -206,8 +250,8 @@ static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc,
                                      done, fin)));
 }
 
-// The fused CG u/r update (k_cg_ur_fused semantics), by TMA where possible
-// (internal linkage as launch_cg_w2).
+// The fused CG u/r update (k_cg_ur_fused semantics), streaming and TMA-fed
+// where possible (internal linkage as launch_cg_w2).
 template <typename Finish>
 static void launch_cg_ur2(TlSuite2D* s, dim3 grid, Scalar alpha, double* u, const double* p, double* r, const double* w,
                    const int* done, Finish fin)
@@ -221,12 +265,13 @@ static void launch_cg_ur2(TlSuite2D* s, dim3 grid, Scalar alpha, double* u, cons
             const TmaUrMaps m{*mu, *mp, *mr, *mw};
             static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
             if (!(attr_set & (1u << (s->device & 31)))) {
-                TL_CUDA(cudaFuncSetAttribute(k_cg_ur_fused_tma<Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                TL_CUDA(cudaFuncSetAttribute(k_cg_ur_stream<Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kTmaUrBytes));
                 attr_set |= 1u << (s->device & 31);
             }
-            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused_tma<<<grid, BX, kTmaUrBytes, s->stream>>>(
-                                              s->g, alpha, m, u, r, s->rs, done, fin, s->d_mirror + kTmaErrWord2)));
+            TL_LAUNCH(s, "k_cg_ur_fused",
+                      launch_dependent(k_cg_ur_stream<Finish>, stream_grid(s), kTmaUrBytes, s->stream, s->g, alpha, m,
+                                       u, r, s->rs, done, fin, s->d_mirror + kTmaErrWord2));
             return;
         }
     }

@@ -55,13 +55,18 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 }
 
 // Waits for the phase of `parity` to complete; false (and *err = 1) after
-// kTmaSpinLimit polls.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* err)
+// `limit` polls.
+__device__ __forceinline__ bool mbar_wait_limited(unsigned long long* bar, unsigned parity, int* err, long limit)
 {
-    for (long n = 0; n < kTmaSpinLimit; ++n)
+    for (long n = 0; n < limit; ++n)
         if (mbar_try_wait(bar, parity)) return true;
     if (err) *(volatile int*)err = 1;
     return false;
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* err)
+{
+    return mbar_wait_limited(bar, parity, err, kTmaSpinLimit);
 }
 
 // 3D tile load: box of the map at element coordinates (x, y, z) into dst,

@@ -178,6 +178,9 @@ class Host:
         self._fill_settings()
         self._initialise_chunk()
         self.initialise_application()
+        if dims == 2 and c.preconditioner_type:
+            self.lib.tl2d_set_preconditioner(C.byref(self.chunk), c.preconditioner_type)
+            abi.check(self.lib, dims)
 
     # -- plumbing ------------------------------------------------------------
     def _call(self, name, *args):

@@ -48,6 +48,7 @@ class Problem:
     halo_depth: int = 2
     eps_lim: float = 1e-4
     error_switch: bool = False
+    preconditioner: str = "none"      # CG: none, jac_diag or jac_block
     name: str = ""
     seed: Optional[int] = None
 
@@ -73,6 +74,9 @@ class Problem:
             out.append("check_result")
         if self.error_switch:
             out.append("errswitch")
+        if self.preconditioner != "none":
+            out.append("preconditioner_on")
+            out.append("preconditioner_type = %s" % self.preconditioner)
         out.append("coefficient_" + self.coefficient)
         out.append("")
         out.append("eps = %r" % self.eps)

@@ -3,7 +3,8 @@
 Runs HERE only (it needs the reference sources to build ``oracle/_ref``):
 
     python tests/golden/make_golden.py            # small/medium cases
-    python tests/golden/make_golden.py --big      # 4096^2 drop-in cases (slow)
+    python tests/golden/make_golden.py --big      # configuration-size cases (slow)
+    python tests/golden/make_golden.py --big --only NAME[,NAME]   # regenerate some of them
 
 Writes
   * ``layout_2d.txt`` / ``layout_3d.txt`` -- offsetof/sizeof of the reference
@@ -78,13 +79,43 @@ def small_cases():
 
 
 def big_cases():
+    """The configuration sizes: the 4096^2 drop-in deck with each solver, the
+    3D 256^3 deck of the adjoint configuration, and the reference's own known
+    answers at their full sizes (2d/tea.problems:2-3, 3d/tea.problems:3-4).
+
+    On the 4096^2 deck the reference's Chebyshev and PPCG do not reach eps
+    1e-15 within 20000 iterations per step, and their CG presteps only bring
+    the error below the switch threshold (1) after thousands of iterations.
+    Their runs here use the reference's error switch instead (`errswitch`,
+    epslim 1e30: the switch after CG_ITERS_FOR_EIGENVALUES = 20 CG trips,
+    2d/drivers/cheby_driver.c:30-32) and are capped at max_iters 2000
+    (Chebyshev) and 200 (PPCG), on both sides, so the reference run stays
+    affordable and the comparison covers the CG presteps, the eigenvalue
+    bounds, the Chebyshev coefficients and the capped Chebyshev / PPCG solve."""
     cases = []
-    for solver in ("cg", "cheby", "ppcg"):
-        p = problems.dropin_2d(4096, seed=2, steps=2, solver=solver)
+    p = problems.dropin_2d(4096, seed=2, steps=2, solver="cg")
+    cases.append(dict(name="dropin_2d_4096_cg_2steps", dims=2, tea_in=p.tea_in()))
+    for solver, cap in (("cheby", 2000), ("ppcg", 200)):
+        p = problems.dropin_2d(4096, seed=2, steps=2, solver=solver).with_(max_iters=cap, error_switch=True,
+                                                                          eps_lim=1e30)
         cases.append(dict(name="dropin_2d_4096_%s_2steps" % solver, dims=2, tea_in=p.tea_in()))
-    p = problems.adjoint_3d(64, seed=4, steps=5)
-    cases.append(dict(name="adjoint_3d_64_5steps", dims=3, tea_in=p.tea_in()))
+    p = problems.adjoint_3d(256, seed=4, steps=2)
+    cases.append(dict(name="adjoint_3d_256_cg_2steps", dims=3, tea_in=p.tea_in()))
+    for n, steps in ((4096, 1), (1024, 20)):
+        text, exp = shipped_case(2, n, steps)
+        cases.append(dict(name="shipped_2d_%d_%d" % (n, steps), dims=2, tea_in=text, tea_problems=exp))
+    for n, steps in ((64, 20), (256, 5)):
+        text, exp = shipped_case(3, n, steps)
+        cases.append(dict(name="shipped_3d_%d_%d" % (n, steps), dims=3, tea_in=text, tea_problems=exp))
     return cases
+
+
+def known_answer_cases():
+    """Known answers checked on the GPU only (no reference run is recorded:
+    3d/tea.problems:5 is 256^3 over 20 steps, a long CPU run)."""
+    text, exp = shipped_case(3, 256, 20)
+    return [dict(name="shipped_3d_256_20", dims=3, tea_in=text, tea_problems=exp, steps=None,
+                 generator="3d/tea.problems known answer only")]
 
 
 def run_cases(cases, threads=8):
@@ -107,8 +138,23 @@ def main():
     for dims in (2, 3):
         txt = subprocess.run([str(OUT / ("layout%dd" % dims))], capture_output=True, text=True, check=True).stdout
         (HERE / ("layout_%dd.txt" % dims)).write_text(txt)
+    only = None
+    if "--only" in sys.argv:
+        only = set(sys.argv[sys.argv.index("--only") + 1].split(","))
     if "--big" in sys.argv:
-        (HERE / "ref_runs_big.json").write_text(json.dumps(run_cases(big_cases()), indent=1) + "\n")
+        path = HERE / "ref_runs_big.json"
+        if only:
+            # regenerate the named cases in place, keep the others
+            old = {c["name"]: c for c in json.loads(path.read_text())}
+            for c in run_cases([c for c in big_cases() if c["name"] in only]):
+                old[c["name"]] = c
+            for c in known_answer_cases():
+                old.setdefault(c["name"], c)
+            order = [c["name"] for c in big_cases() + known_answer_cases()]
+            cases = [old[n] for n in order if n in old]
+        else:
+            cases = run_cases(big_cases()) + known_answer_cases()
+        path.write_text(json.dumps(cases, indent=1) + "\n")
     else:
         (HERE / "ref_runs.json").write_text(json.dumps(run_cases(small_cases()), indent=1) + "\n")
 

@@ -1,11 +1,21 @@
 """Batched timesteps (tl2d_batch_*) on the B200.
 
 Every problem of a batch of uneven sizes is stopped by its FP64 residual,
-r.r < eps (1e-12, the reference's 2D stop test); its field summary agrees
-with the same timestep solved alone by the FP64 device driver (whose stop
-test is the recursive residual) within TEMP_RTOL: both residuals are below
-sqrt(eps) = 1e-6 in norm, so the solutions differ by at most that much per
-unit of A's smallest eigenvalue (>= 1), which bounds temp to ~1e-6 relative.
+r.r < eps (1e-12, the reference's 2D stop test). Two checks per problem:
+
+* against the oracle (the reference's CG, 2d/drivers/cg_driver.c, restated
+  in oracle/tl_oracle.c) on the same tea.in: the oracle stops on the
+  recursive residual, the batch on the true FP64 residual of an iteration
+  whose vectors are stored in FP32. Both residual norms are below
+  sqrt(eps) = 1e-6, and A = I + (positive semi-definite diffusion) has
+  smallest eigenvalue >= 1, so the two solutions differ by at most 2e-6 in
+  norm; temp = sum(V rho u) moves by at most that relative to its size
+  (TEMP_RTOL = 1e-6 is checked). FP32 storage costs iterations: the batch
+  needs at most 25 % + 10 more than the oracle (ITER_BAND), and never fewer
+  than 75 % of them;
+* against the same timestep solved alone by the FP64 device driver, with the
+  same bounds.
+
 vol, mass and ie do not depend on the solve and match exactly.
 """
 import numpy as np
@@ -18,6 +28,17 @@ from tealeaf_b200.host import Host
 pytestmark = pytest.mark.gpu
 
 TEMP_RTOL = 1e-6
+
+
+def ITER_BAND(ref_it):
+    return 0.75 * ref_it - 1, 1.25 * ref_it + 10
+
+
+def _oracle(prob, steps):
+    from oracle.oracle import OracleLib
+    from tealeaf_b200.config import read_config
+    cfg, states = read_config(prob.with_(end_step=steps).tea_in(), 2)
+    return OracleLib().run(cfg, states)
 
 
 def _probs(count=6):
@@ -52,6 +73,27 @@ def test_batch_matches_sequential_fp64_solves():
                 assert abs(s[3] / ref[3] - 1.0) < TEMP_RTOL, (k, tt, s[3], ref[3])
                 # FP32 storage costs at most a few extra iterations here
                 assert it[k] <= 1.25 * ref_it + 10, (k, it[k], ref_it)
+    finally:
+        b.close()
+
+
+def test_batch_matches_the_oracle():
+    probs = _probs()
+    want = [_oracle(p, 2) for p in probs]
+    b = Batch([p.tea_in() for p in probs])
+    try:
+        for tt in range(2):
+            st = b.step()
+            assert st.converged == len(probs)
+            it, rr, conv = b.results()
+            assert conv.all() and (rr < 1e-12).all()
+            for k, s in enumerate(b.summaries()):
+                ref = want[k][tt]
+                for a, r in zip(s[:3], ref.summary[:3]):
+                    assert a == pytest.approx(r, rel=1e-15), (k, tt)
+                assert abs(s[3] / ref.summary[3] - 1.0) < TEMP_RTOL, (k, tt, s[3], ref.summary[3])
+                lo, hi = ITER_BAND(ref.iterations["CG"])
+                assert lo <= it[k] <= hi, (k, tt, it[k], ref.iterations["CG"])
     finally:
         b.close()
 

@@ -130,3 +130,31 @@ def test_run_path_ppcg_queue_is_bit_identical(inner):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("cap", [None, 183, 261])
+def test_run_path_cheby_queue_is_bit_identical(cap):
+    """Through run_* (the reference drivers' call sequence), the Chebyshev
+    trips deferred and run temporally blocked (each trip ending with its
+    u += p) give the same iteration counts, summaries and memory state, bit
+    for bit, as one launch per call; capped runs stop the queue at trip counts
+    that split the 5-trip blocks and between norm checks."""
+    prob = problems.seeded(2, (203, 141), 19, 5, 2, solver="cheby", end_step=2, name="cq")
+    if cap:
+        prob = prob.with_(max_iters=cap)
+    text = prob.tea_in()
+    a, b = Host(text, 2), Host(text, 2)
+    try:
+        b.lib.tl2d_set_temporal_blocking(b.chunk, 0)
+        for tt in range(2):
+            ra = a.solve(tt)
+            rb = b.solve(tt)
+            assert ra.iterations == rb.iterations
+            assert ra.iterations.get("Cheby", 0) > 0
+            assert ra.summary == rb.summary
+            assert ra.exact_error == rb.exact_error
+            for f in FIELDS:
+                assert np.array_equal(a.download(f), b.download(f)), (cap, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()

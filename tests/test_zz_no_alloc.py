@@ -4,9 +4,10 @@ It exists for callers that cannot allocate device memory, or cannot afford
 the synchronisation an allocation implies, while a solve is running: its
 reduction scratch is a static device array of fixed size instead of memory
 from cudaMalloc. These tests call it through the C ABI and compare it with the
-regular run_calculate_2norm on the same field, twice in a row (the static
-array keeps the previous call's contents, so the second call checks that the
-entry point resets what must start at zero). The file is named so pytest
+regular run_calculate_2norm on the same field (equal up to rounding: the two
+add their block partials in different trees), twice in a row per field: the
+static array keeps the previous call's contents, and the repeated calls show
+that leftover contents do not change the result. The file is named so pytest
 collects it last.
 """
 import ctypes as C
