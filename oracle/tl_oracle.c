@@ -736,43 +736,59 @@ static int oc_cg(OChunk* c, const OSettings* s, double rx, double ry, double rz,
 /* Jacobi preconditioners of CG (2D). The reference C ports only parse
  * preconditioner_on (2d/parse_config.c:136-138) and their kernels ignore it;
  * the README documents jac_diag and jac_block with a block size of 4
- * (README.md:127-133), and the reference's cuda 3D kernel forms the diagonal
- * one as mi = 1 / diag(A), z = mi r (3d/c_kernels/cuda/cg_solver.cuknl:93-100).
- * z = M^-1 r on the interior. jac_block: M is the tridiagonal part of A
- * within blocks of 4 rows along y that start at the first interior row (the
- * last block of a column may be shorter), solved by Thomas' algorithm:
- * diagonal d = 1 + (kx_i+1 + kx_i) + (ky_i+x + ky_i), coupling -ky_i between
- * rows i-x and i. */
-void o2_precond(int x, int y, int hd, int type, const double* kx, const double* ky, const double* r, double* z)
+ * (README.md:127-133), and the reference's cuda 3D kernel stores the
+ * diagonal one as mi = 1 / diag(A) and applies z = mi r
+ * (3d/c_kernels/cuda/cg_solver.cuknl:93-100).
+ * diag(A) = 1 + (kx_i+1 + kx_i) + (ky_i+x + ky_i). jac_block: M is the
+ * tridiagonal part of A within blocks of 4 rows along y that start at the
+ * first interior row (the last block of a column may be shorter), with
+ * coupling -ky_i between rows i-x and i, solved by Thomas' algorithm; mi
+ * holds the inverse pivots g_q = 1 / (d_q + ky_q c_q-1) (c_q-1 = -ky_q g_q-1,
+ * g_0 = 1 / d_0), so applying M^-1 takes multiplications only:
+ *   forward  y_0 = r_0 g_0,  y_q = (r_q + ky_q y_q-1) g_q
+ *   back     z_m-1 = y_m-1,  z_q = y_q - c_q z_q+1,  c_q = -ky_q+1 g_q.
+ * Factor once per solve (o2_precond_factor), apply per trip (o2_precond). */
+void o2_precond_factor(int x, int y, int hd, int type, const double* kx, const double* ky, double* mi)
 {
     const int bs = type == 2 ? 4 : 1;
     for (int k = hd; k < x - hd; ++k) {
         for (int jb = hd; jb < y - hd; jb += bs) {
             const int m = (y - hd - jb) < bs ? (y - hd - jb) : bs;
-            double cp[4], dp[4];
+            double c = 0.0;
             for (int q = 0; q < m; ++q) {
                 const long i = k + (long)(jb + q) * x;
                 const double d = 1.0 + (kx[i + 1] + kx[i]) + (ky[i + x] + ky[i]);
-                if (type == 1) {
-                    const double mi = 1.0 / d;
-                    z[i] = mi * r[i];
-                    continue;
-                }
-                if (q == 0) {
-                    cp[0] = -ky[i + x] / d;
-                    dp[0] = r[i] / d;
-                } else {
-                    const double den = d + ky[i] * cp[q - 1];
-                    cp[q] = -ky[i + x] / den;
-                    dp[q] = (r[i] + ky[i] * dp[q - 1]) / den;
-                }
+                const double g = q == 0 ? 1.0 / d : 1.0 / (d + ky[i] * c);
+                mi[i] = g;
+                c = -ky[i + x] * g;
             }
-            if (type == 1) continue;
-            double zn = dp[m - 1];
+        }
+    }
+}
+
+void o2_precond(int x, int y, int hd, int type, const double* ky, const double* mi, const double* r, double* z)
+{
+    const int bs = type == 2 ? 4 : 1;
+    for (int k = hd; k < x - hd; ++k) {
+        for (int jb = hd; jb < y - hd; jb += bs) {
+            const int m = (y - hd - jb) < bs ? (y - hd - jb) : bs;
+            if (type == 1) {
+                const long i = k + (long)jb * x;
+                z[i] = mi[i] * r[i];
+                continue;
+            }
+            double yv[4];
+            for (int q = 0; q < m; ++q) {
+                const long i = k + (long)(jb + q) * x;
+                yv[q] = q == 0 ? r[i] * mi[i] : (r[i] + ky[i] * yv[q - 1]) * mi[i];
+            }
+            double zn = yv[m - 1];
             z[k + (long)(jb + m - 1) * x] = zn;
             for (int q = m - 2; q >= 0; --q) {
-                zn = dp[q] - cp[q] * zn;
-                z[k + (long)(jb + q) * x] = zn;
+                const long i = k + (long)(jb + q) * x;
+                const double c = -ky[i + x] * mi[i];
+                zn = yv[q] - c * zn;
+                z[i] = zn;
             }
         }
     }
@@ -786,8 +802,9 @@ static double o2_dot_interior(int x, int y, int hd, const double* a, const doubl
     return s;
 }
 
-/* Preconditioned CG (2D): cg_driver.c's loop with z = M^-1 r (held in the
- * chunk's mi field, which the reference allocates for its preconditioner):
+/* Preconditioned CG (2D): cg_driver.c's loop with z = M^-1 r (M factored
+ * into the chunk's mi field, which the reference allocates for its
+ * preconditioner; z in sd, unused by CG):
  * after cg_init, z = M^-1 r, p = z (depth-1 reflective halo), rro = r.z; per
  * trip pw = p.w, alpha = rro / pw, u += alpha p, r -= alpha w, z = M^-1 r,
  * beta = r.z / rro, p = beta p + z, rro = r.z; the stop test is on r.r, the
@@ -796,24 +813,26 @@ static int oc_pcg(OChunk* c, const OSettings* s, double rx, double ry, double rz
 {
     if (c->dims != 2) return -4;
     oc_cg_init_driver(c, s, rx, ry, rz);
-    o2_precond(c->x, c->y, c->hd, s->preconditioner, c->kx, c->ky, c->r, c->mi);
+    double* z = c->sd;
+    o2_precond_factor(c->x, c->y, c->hd, s->preconditioner, c->kx, c->ky, c->mi);
+    o2_precond(c->x, c->y, c->hd, s->preconditioner, c->ky, c->mi, c->r, z);
     for (int j = c->hd; j < c->y - c->hd; ++j)
-        for (int k = c->hd; k < c->x - c->hd; ++k) c->p[k + (long)j * c->x] = c->mi[k + (long)j * c->x];
+        for (int k = c->hd; k < c->x - c->hd; ++k) c->p[k + (long)j * c->x] = z[k + (long)j * c->x];
     oc_reset_flags(c);
     c->flags[3] = c->flags[4] = true;
     oc_halo(c, 1);
-    double rro = o2_dot_interior(c->x, c->y, c->hd, c->r, c->mi);
+    double rro = o2_dot_interior(c->x, c->y, c->hd, c->r, z);
     int tt;
     for (tt = 0; tt < s->max_iters; ++tt) {
         const double pw = oc_calc_w(c);
         const double alpha = rro / pw;
         c->cg_alphas[tt] = alpha;
         const double rrn = oc_calc_ur(c, alpha);
-        o2_precond(c->x, c->y, c->hd, s->preconditioner, c->kx, c->ky, c->r, c->mi);
-        const double rzn = o2_dot_interior(c->x, c->y, c->hd, c->r, c->mi);
+        o2_precond(c->x, c->y, c->hd, s->preconditioner, c->ky, c->mi, c->r, z);
+        const double rzn = o2_dot_interior(c->x, c->y, c->hd, c->r, z);
         const double beta = rzn / rro;
         c->cg_betas[tt] = beta;
-        o2_cg_calc_p(c->x, c->y, c->hd, beta, c->p, c->mi);
+        o2_cg_calc_p(c->x, c->y, c->hd, beta, c->p, z);
         rro = rzn;
         *error = rrn;
         oc_halo(c, 1);

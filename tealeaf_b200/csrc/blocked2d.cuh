@@ -32,14 +32,20 @@
 
 namespace tl2d {
 
-constexpr int kTB = 5;                  // most steps per launch
+#ifndef TL2D_TB
+#define TL2D_TB 4
+#endif
+constexpr int kTB = TL2D_TB;            // most steps per launch (the region's margin)
 constexpr int kTW = 64;                 // region columns: one per thread of a row group
-constexpr int kTSeg = 16;               // region rows per thread (a column segment in registers)
-constexpr int kTRows = 4;               // row groups
+#ifndef TL2D_TSEG
+#define TL2D_TSEG 16
+#endif
+constexpr int kTSeg = TL2D_TSEG;        // region rows per thread (a column segment in registers)
+constexpr int kTRows = 64 / kTSeg;      // row groups
 constexpr int kTBThreads = kTW * kTRows;   // 256
 constexpr int kTH = kTSeg * kTRows;     // region rows (64)
-constexpr int kTX = kTW - 2 * kTB;      // tile columns (54)
-constexpr int kTY = kTH - 2 * kTB;      // tile rows (54)
+constexpr int kTX = kTW - 2 * kTB;      // tile columns (56)
+constexpr int kTY = kTH - 2 * kTB;      // tile rows (56)
 
 struct BlockedArgs {
     int steps;          // L <= kTB
@@ -52,6 +58,8 @@ struct BlockedArgs {
                         // order) instead of starting with the previous trip's
 };
 
+static_assert(kTX > 0 && kTY > 0 && kTX % 2 == 0, "blocked tiles: an even tile width keeps TMA region starts aligned");
+
 // Thread (cx, cy) holds column cx of the region, rows cy * kTSeg .. + kTSeg,
 // in registers: the two carried fields, u0 (Chebyshev) or u (PPCG, tile cells)
 // and the face coefficients. Each step's stencil field A goes through shared
@@ -61,24 +69,35 @@ struct BlockedArgs {
 // registers. A neighbour outside the interior is the cell itself (the
 // reflective depth-1 halo); cells outside the interior or beyond the loaded
 // margin compute values nothing valid reads.
-template <int MODE>
-static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, BlockedArgs a, const double* __restrict__ A_in,
-                                                                  const double* __restrict__ B_in, double* A_out,
-                                                                  double* __restrict__ B_out,
-                                                                  const double* __restrict__ u0,
-                                                                  double* __restrict__ u, double* __restrict__ w,
-                                                                  double* __restrict__ r,
-                                                                  const double* __restrict__ kx,
-                                                                  const double* __restrict__ ky,
-                                                                  const int* __restrict__ done)
+// The operand region of a tile (kTW x kTH cells from grid column xs =
+// X0 - kTB, row ys = Y0 - kTB): src.a / b / c / kx / ky (gi, ry, cx) give the
+// value of a field at grid index gi, region row ry, region column cx; kxr the
+// face coefficient one column to the right.
+struct GlobalRegion {
+    const double* A;
+    const double* B;
+    const double* C;
+    const double* KX;
+    const double* KY;
+    __device__ __forceinline__ double a(long gi, int, int) const { return A[gi]; }
+    __device__ __forceinline__ double b(long gi, int, int) const { return B[gi]; }
+    __device__ __forceinline__ double c(long gi, int, int) const { return C[gi]; }
+    __device__ __forceinline__ double kx(long gi, int, int) const { return KX[gi]; }
+    __device__ __forceinline__ double kxr(long gi, int, int) const { return KX[gi + 1]; }
+    __device__ __forceinline__ double ky(long gi, int, int) const { return KY[gi]; }
+};
+
+// One tile: L <= kTB steps of MODE on the region given by `src`, then the
+// tile written back. S0, S1: the two kTH x kTW stencil buffers; loaded() runs
+// in every thread once the region is in registers.
+template <int MODE, typename Src, typename Loaded>
+__device__ __forceinline__ void blocked_tile(const Geo& g, const BlockedArgs& a, int X0, int Y0, const Src& src,
+                                             double* A_out, double* __restrict__ B_out, double* __restrict__ u,
+                                             double* __restrict__ w, double* __restrict__ r, double* const S0,
+                                             double* const S1, Loaded loaded)
 {
-    extern __shared__ double tb_smem[];
-    double* const S0 = tb_smem;           // [kTH * kTW]
-    double* const S1 = S0 + kTH * kTW;    // [kTH * kTW]
-    if (gate_closed(done)) return;
     const int x = g.x, hd = g.hd;
     const int ilo = hd, ihi = g.x - hd, jlo = hd, jhi = g.y - hd;   // interior [lo, hi)
-    const int X0 = hd + blockIdx.x * kTX, Y0 = hd + blockIdx.y * kTY;
     const int H = a.steps;
     const int tid = threadIdx.x, cx = tid % kTW, cy = tid / kTW, lane = tid & 31;
     const int gx = X0 - kTB + cx;    // grid column of this thread
@@ -101,15 +120,16 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, Blocked
         const long gi = gx + (long)gy * x;
         // ky of rows jlo..jhi: the face above the top interior row is read as the one-step kernels do
         const bool in_ky = colin && gy >= jlo && gy <= jhi && max(mxc, my) <= H + 1;
-        kyc[k] = in_ky ? ky[gi] : 0.0;   // k == kTSeg: ky_u of the segment's top row
+        kyc[k] = in_ky ? src.ky(gi, ry, cx) : 0.0;   // k == kTSeg: ky_u of the segment's top row
         if (k == kTSeg) break;
-        av[k] = in ? A_in[gi] : 0.0;
-        bv[k] = in ? B_in[gi] : 0.0;
-        if (MODE == 0) cv[k] = in ? u0[gi] : 0.0;
-        else cv[k] = (in && mxc == 0 && my == 0) ? u[gi] : 0.0;
-        kxc[k] = in ? kx[gi] : 0.0;
-        kxr[k] = in ? kx[gi + 1] : 0.0;
+        av[k] = in ? src.a(gi, ry, cx) : 0.0;
+        bv[k] = in ? src.b(gi, ry, cx) : 0.0;
+        if (MODE == 0) cv[k] = in ? src.c(gi, ry, cx) : 0.0;
+        else cv[k] = (in && mxc == 0 && my == 0) ? src.c(gi, ry, cx) : 0.0;
+        kxc[k] = in ? src.kx(gi, ry, cx) : 0.0;
+        kxr[k] = in ? src.kxr(gi, ry, cx) : 0.0;
     }
+    loaded();
     for (int i = 0; i < H; ++i) {
         double* const As = (i & 1) ? S1 : S0;
         // pass A, pointwise
@@ -178,27 +198,120 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, Blocked
         if (touches) pass_b(std::true_type());
         else pass_b(std::false_type());
     }
-    // the last trip's u += p when each trip ends with its add
-    if (MODE == 0 && a.add_end && H > 0) {
-#pragma unroll
-        for (int k = 0; k < kTSeg; ++k) av[k] = av[k] + bv[k];
-    }
-    // write the tile: A (u, resp. sd) with its reflective depth-1 halo, B (p, resp. r)
+    // write the tile: A (u, resp. sd) with its reflective depth-1 halo, B (p,
+    // resp. r). With add_end the last trip's u += p is applied here, and the
+    // halo mirrors u before that add: the value a call-by-call sequence
+    // leaves there (its depth-1 halo update comes before each call).
+    const bool add_now = MODE == 0 && a.add_end && H > 0;
     if (colin && mxc == 0) {
 #pragma unroll
         for (int k = 0; k < kTSeg; ++k) {
             const int ry = r0 + k, gy = oy + ry;
             if (ry < kTB || ry >= kTB + kTY || gy >= jhi) continue;
             const long gi = gx + (long)gy * x;
-            const double av_ = av[k];
+            const double hv = av[k];
+            const double av_ = add_now ? av[k] + bv[k] : av[k];
             A_out[gi] = av_;
             B_out[gi] = bv[k];
             if (MODE == 1) u[gi] = cv[k];
-            if (at_l) A_out[gi - 1] = av_;
-            if (at_r) A_out[gi + 1] = av_;
-            if (gy == jlo) A_out[gi - x] = av_;
-            if (gy == jhi - 1) A_out[gi + x] = av_;
+            if (at_l) A_out[gi - 1] = hv;
+            if (at_r) A_out[gi + 1] = hv;
+            if (gy == jlo) A_out[gi - x] = hv;
+            if (gy == jhi - 1) A_out[gi + x] = hv;
         }
+    }
+}
+
+template <int MODE>
+static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, BlockedArgs a, const double* __restrict__ A_in,
+                                                                  const double* __restrict__ B_in, double* A_out,
+                                                                  double* __restrict__ B_out,
+                                                                  const double* __restrict__ u0,
+                                                                  double* __restrict__ u, double* __restrict__ w,
+                                                                  double* __restrict__ r,
+                                                                  const double* __restrict__ kx,
+                                                                  const double* __restrict__ ky,
+                                                                  const int* __restrict__ done)
+{
+    extern __shared__ double tb_smem[];
+    double* const S0 = tb_smem;           // [kTH * kTW]
+    double* const S1 = S0 + kTH * kTW;    // [kTH * kTW]
+    if (gate_closed(done)) return;
+    const GlobalRegion src{A_in, B_in, MODE == 0 ? u0 : u, kx, ky};
+    blocked_tile<MODE>(g, a, g.hd + blockIdx.x * kTX, g.hd + blockIdx.y * kTY, src, A_out, B_out, u, w, r, S0, S1,
+                       [] {});
+}
+
+// ------------------------------------------------------ TMA-staged form --
+// k_blocked as a persistent kernel whose tile regions arrive by TMA: one
+// block per SM walks tiles blockIdx.x, + gridDim.x, ...; one thread issues
+// the five region boxes (kTW x kTH cells of A, B, C = u0 or u, kx, ky, from
+// grid column X0 - kTB, row Y0 - kTB) of the block's NEXT tile into a
+// shared-memory staging area as soon as every thread has taken the current
+// tile's region into registers, so the loads of tile t+1 overlap the steps
+// of tile t. Boxes start on a 16-byte boundary when the halo depth and kTB
+// are even (X0 - kTB = hd - kTB + kTX bx); cells outside the array read as
+// zero and, as in k_blocked, only cells inside the interior and the margin
+// are taken. The two cells the staging lacks (kx one column right of the
+// region, ky one row above it) only feed cells beyond the valid margin.
+// Every wait is bounded (err); every issued region is waited for.
+struct BlockedMaps {
+    CUtensorMap a, b, c, kx, ky;
+};
+constexpr size_t kBlockedFieldDoubles = (size_t)kTH * kTW;
+constexpr size_t kBlockedTmaBytes = sizeof(double) * 7 * kBlockedFieldDoubles + 8 + 128;
+
+struct StagedRegion {
+    const double* s;   // a, b, c, kx, ky: kTH x kTW each
+    __device__ __forceinline__ double at(int f, int ry, int cx) const { return s[(f * kTH + ry) * kTW + cx]; }
+    __device__ __forceinline__ double a(long, int ry, int cx) const { return at(0, ry, cx); }
+    __device__ __forceinline__ double b(long, int ry, int cx) const { return at(1, ry, cx); }
+    __device__ __forceinline__ double c(long, int ry, int cx) const { return at(2, ry, cx); }
+    __device__ __forceinline__ double kx(long, int ry, int cx) const { return at(3, ry, cx); }
+    __device__ __forceinline__ double kxr(long, int ry, int cx) const { return cx + 1 < kTW ? at(3, ry, cx + 1) : 0.0; }
+    __device__ __forceinline__ double ky(long, int ry, int cx) const { return ry < kTH ? at(4, ry, cx) : 0.0; }
+};
+
+template <int MODE>
+static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked_tma(Geo g, BlockedArgs a,
+                                                                      const __grid_constant__ BlockedMaps maps,
+                                                                      double* A_out, double* __restrict__ B_out,
+                                                                      double* __restrict__ u, double* __restrict__ w,
+                                                                      double* __restrict__ r,
+                                                                      const int* __restrict__ done, int* err)
+{
+    extern __shared__ __align__(128) unsigned char tbt_raw[];
+    double* const S0 = reinterpret_cast<double*>(tbt_raw + ((128 - (tl::smem_addr(tbt_raw) & 127)) & 127));
+    double* const S1 = S0 + kBlockedFieldDoubles;
+    double* const stg = S1 + kBlockedFieldDoubles;
+    unsigned long long* const bar = reinterpret_cast<unsigned long long*>(stg + 5 * kBlockedFieldDoubles);
+    if (gate_closed(done)) return;
+    const int ntx = (g.x - 2 * g.hd + kTX - 1) / kTX;
+    const int ntiles = ntx * ((g.y - 2 * g.hd + kTY - 1) / kTY);
+    const int tid = threadIdx.x;
+    auto issue = [&](int t) {
+        const int xs = g.hd + (t % ntx) * kTX - kTB, ys = g.hd + (t / ntx) * kTY - kTB;
+        tl::mbar_expect_tx(bar, (unsigned)(5 * kBlockedFieldDoubles * sizeof(double)));
+        tl::tma_load_3d(stg, &maps.a, xs, ys, 0, bar);
+        tl::tma_load_3d(stg + kBlockedFieldDoubles, &maps.b, xs, ys, 0, bar);
+        tl::tma_load_3d(stg + 2 * kBlockedFieldDoubles, &maps.c, xs, ys, 0, bar);
+        tl::tma_load_3d(stg + 3 * kBlockedFieldDoubles, &maps.kx, xs, ys, 0, bar);
+        tl::tma_load_3d(stg + 4 * kBlockedFieldDoubles, &maps.ky, xs, ys, 0, bar);
+    };
+    if (tid == 0) {
+        tl::mbar_init(bar, 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x);
+    unsigned phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
+        tl::mbar_wait(bar, phase, err);
+        const int X0 = g.hd + (t % ntx) * kTX, Y0 = g.hd + (t / ntx) * kTY;
+        blocked_tile<MODE>(g, a, X0, Y0, StagedRegion{stg}, A_out, B_out, u, w, r, S0, S1, [&] {
+            __syncthreads();   // every thread holds the region: the staging is free for the next tile
+            if (tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
+        });
     }
 }
 

@@ -187,25 +187,26 @@ struct Run {
     }
 
     // ------------------------------------------------- preconditioned CG
-    // After cg_init, the halo of u and p and copy_u: z = M^-1 r, p = z,
-    // rro = r.z, then the CG loop with z folded into p and the u/r/z sweep
-    // (pcg2d.cuh). z is held in the chunk's mi field.
+    // After cg_init, the halo of u and p and copy_u: M factored into the
+    // chunk's mi field, z = M^-1 r, p = z, rro = r.z, then the CG loop with z
+    // folded into p and the u/r/z sweep (pcg2d.cuh). z is held in the suite's
+    // second sd buffer (unused by CG).
     template <int BS>
     DevState pcg_phase()
     {
         Geo gb = s->g;
         gb.rows = (gb.rows + BS - 1) / BS * BS;   // strips of whole blocks
         const dim3 gbi = interior_grid(gb);
-        double* z = chunk->mi;
+        double* z = s->alt[ALT_SD];
         TL_LAUNCH(s, "k_pcg_init", (k_pcg_init<BS><<<gbi, BX, 0, s->stream>>>(
-                                       gb, fc, chunk->r, chunk->kx, chunk->ky, z, chunk->p, s->rs,
+                                       gb, fc, chunk->r, chunk->kx, chunk->ky, chunk->mi, z, chunk->p, s->rs,
                                        FinCgInit{s->d_state, s->d_mirror})));
         read_state();
         FinPcgUr fin_ur{s->d_state, s->d_cg_betas, prm, s->d_mirror};
         const Scalar alpha{0.0, &s->d_state->alpha};
         return cg_trips(0, true, z, [&](double* p) {
             TL_LAUNCH(s, "k_pcg_ur", (k_pcg_ur<BS><<<gbi, BX, 0, s->stream>>>(gb, alpha, chunk->u, p, chunk->r,
-                                                                              chunk->w, chunk->kx, chunk->ky, z,
+                                                                              chunk->w, chunk->ky, chunk->mi, z,
                                                                               s->rs, done(), fin_ur)));
         });
     }
@@ -277,8 +278,6 @@ struct Run {
                 // (FinChebyTrip); a block ends at such a trip, at max_iters or
                 // after kTB trips
                 auto is_norm = [&](int t) { return t - tt + 1 >= est && ((t + 1) % 10) == 0; };
-                const size_t smem = blocked_smem<0>();
-                cudaFuncSetAttribute(k_blocked<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 std::vector<int> starts;
                 st = loop_blocks(tt + 1, [&](int t) {
                     int L = 1;
@@ -287,10 +286,8 @@ struct Run {
                     const int norm = is_norm(last) ? 1 : 0;
                     BlockedArgs a{L, t - tt + 1, (norm || last + 1 >= prm.max_iters) ? 1 : 0, 0.0, s->d_cheby_alphas,
                                   s->d_cheby_betas};
-                    TL_LAUNCH(s, "k_blocked<cheby>", (k_blocked<0><<<blocked_grid(s->g), kTBThreads, smem,
-                                                                      s->stream>>>(
-                                  s->g, a, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->u0, nullptr, chunk->w,
-                                  chunk->r, chunk->kx, chunk->ky, done())));
+                    launch_blocked<0>(s, "k_blocked<cheby>", a, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1],
+                                      chunk->u0, nullptr, chunk->w, chunk->r, chunk->kx, chunk->ky, done());
                     const FinChebyBlock fin{s->d_state, pc, s->d_mirror, L, norm};
                     if (norm)
                         TL_LAUNCH(s, "k_norm2_fin", (k_norm2_fin<<<gi, BX, 0, s->stream>>>(s->g, chunk->r, s->rs,
@@ -347,8 +344,6 @@ struct Run {
         FinPpcgW fin_w{s->d_state};
         FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
         const bool blocked = blocking();
-        const size_t smem = blocked_smem<1>();
-        if (blocked) cudaFuncSetAttribute(k_blocked<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const int inner_flips = blocked ? (ni + kTB - 1) / kTB : ni;   // r/sd buffer flips per outer trip
         auto trip = [&](int t) {
             if (t == tt) {
@@ -365,10 +360,8 @@ struct Run {
                     const int L = std::min(kTB, ni - pp0);
                     const bool last = pp0 + L == ni;
                     BlockedArgs a{L, pp0, 0, chunk->theta, s->d_cheby_alphas, s->d_cheby_betas};
-                    TL_LAUNCH(s, "k_blocked<ppcg>", (k_blocked<1><<<blocked_grid(s->g), kTBThreads, smem,
-                                                                     s->stream>>>(
-                                  s->g, a, sb[sc], rb[rc], sb[sc ^ 1], rb[rc ^ 1], nullptr, chunk->u, nullptr,
-                                  nullptr, chunk->kx, chunk->ky, done())));
+                    launch_blocked<1>(s, "k_blocked<ppcg>", a, sb[sc], rb[rc], sb[sc ^ 1], rb[rc ^ 1], chunk->u,
+                                      chunk->u, nullptr, nullptr, chunk->kx, chunk->ky, done());
                     sc ^= 1;
                     rc ^= 1;
                     if (last)

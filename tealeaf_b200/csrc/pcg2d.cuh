@@ -16,13 +16,18 @@
 // jac_block the tridiagonal part of A inside blocks of 4 rows along y that
 // start at the first interior row (couplings -ky between vertical neighbours;
 // the last block of a column may be shorter), solved per column by Thomas'
-// algorithm from kx and ky on the fly. z lives in the chunk's mi field,
-// which the reference allocates for its preconditioner.
+// algorithm. M is factored once per solve into the chunk's mi field (which
+// the reference allocates for its preconditioner and whose cuda kernel holds
+// 1 / diag(A) there): jac_diag mi = 1 / diag(A), jac_block the inverse pivots
+// g_q = 1 / (d_q + ky_q c_q-1), c_q = -ky_q+1 g_q. Applying M^-1 then takes
+// multiplications only (jac_block: y_q = (r_q + ky_q y_q-1) g_q forward,
+// z_q = y_q - c_q z_q+1 back). z is an internal buffer of the suite.
 //
 // Algorithmic bytes per cell and iteration: the w sweep 48 (z, p_old, kx, ky
-// -> p, w), the u/r/z sweep 72 (u, p, r, w, kx, ky -> u, r, z): 120 against
-// plain CG's 96. The element-wise operations follow the oracle's restatement
-// (oracle/tl_oracle.c, o2_precond) in order, so z is bit-identical to it.
+// -> p, w), the u/r/z sweep 64 for jac_diag (u, p, r, w, mi -> u, r, z) and
+// 72 for jac_block (+ ky): 112 / 120 against plain CG's 96. The element-wise
+// operations follow the oracle's restatement (oracle/tl_oracle.c,
+// o2_precond_factor, o2_precond) in order, so z is bit-identical to it.
 #pragma once
 
 #include "kernels2d.cuh"
@@ -31,54 +36,69 @@ namespace tl2d {
 
 enum { kPrecondNone = 0, kPrecondDiag = 1, kPrecondBlock = 2 };
 
-// z = M^-1 r for rows jb .. jb+m-1 (m <= BS) of the column at i0 = k + jb x,
-// with rv the residual of those rows.
+// Factor of the column block at i0 = k + jb x (rows jb .. jb+m-1, m <= BS)
+// into mi: jac_diag 1 / diag(A), jac_block the inverse pivots.
 template <int BS>
-__device__ __forceinline__ void precond_block(const double* __restrict__ kx, const double* __restrict__ ky, long i0,
+__device__ __forceinline__ void precond_factor(const double* __restrict__ kx, const double* __restrict__ ky,
+                                               double* __restrict__ mi, long i0, int x, int m)
+{
+    double c = 0.0;
+#pragma unroll
+    for (int q = 0; q < BS; ++q) {
+        if (q < m) {
+            const long i = i0 + (long)q * x;
+            const double d = 1.0 + (kx[i + 1] + kx[i]) + (ky[i + x] + ky[i]);
+            const double g = q == 0 ? 1.0 / d : 1.0 / (d + ky[i] * c);
+            mi[i] = g;
+            c = -ky[i + x] * g;
+        }
+    }
+}
+
+// z = M^-1 r for the column block at i0 (rows jb .. jb+m-1), rv its residual.
+template <int BS>
+__device__ __forceinline__ void precond_apply(const double* __restrict__ ky, const double* __restrict__ mi, long i0,
                                               int x, int m, const double (&rv)[BS], double (&zv)[BS])
 {
     if (BS == 1) {
-        const double d = 1.0 + (kx[i0 + 1] + kx[i0]) + (ky[i0 + x] + ky[i0]);
-        const double mi = 1.0 / d;
-        zv[0] = mi * rv[0];
+        zv[0] = mi[i0] * rv[0];
         return;
     }
-    double cp[BS], dp[BS];
+    double g[BS], kyn[BS], yv[BS];
     double kyc = ky[i0];
 #pragma unroll
     for (int q = 0; q < BS; ++q) {
         if (q < m) {
             const long i = i0 + (long)q * x;
-            const double kyu = ky[i + x];
-            const double d = 1.0 + (kx[i + 1] + kx[i]) + (kyu + kyc);
-            if (q == 0) {
-                cp[0] = -kyu / d;
-                dp[0] = rv[0] / d;
-            } else {
-                const double den = d + kyc * cp[q - 1];
-                cp[q] = -kyu / den;
-                dp[q] = (rv[q] + kyc * dp[q - 1]) / den;
-            }
-            kyc = kyu;
+            g[q] = mi[i];
+            kyn[q] = ky[i + x];
+            yv[q] = q == 0 ? rv[0] * g[0] : (rv[q] + kyc * yv[q - 1]) * g[q];
+            kyc = kyn[q];
         }
     }
     double zn = 0.0;
 #pragma unroll
     for (int q = BS - 1; q >= 0; --q) {
         if (q < m) {
-            zn = q == m - 1 ? dp[q] : dp[q] - cp[q] * zn;
+            if (q == m - 1) {
+                zn = yv[q];
+            } else {
+                const double c = -kyn[q] * g[q];
+                zn = yv[q] - c * zn;
+            }
             zv[q] = zn;
         }
     }
 }
 
-// PCG start after cg_init: z = M^-1 r, p = z with its depth-1 reflective
-// halo, sum(r z) -> fin. Strips of g.rows rows (a multiple of BS).
+// PCG start after cg_init: the factor of M into mi, z = M^-1 r, p = z with
+// its depth-1 reflective halo, sum(r z) -> fin. Strips of g.rows rows (a
+// multiple of BS).
 template <int BS, typename Finish>
 static __global__ void __launch_bounds__(BX) k_pcg_init(Geo g, Faces fc, const double* __restrict__ r,
                                                        const double* __restrict__ kx, const double* __restrict__ ky,
-                                                       double* __restrict__ z, double* __restrict__ p, ReduceSlots rs,
-                                                       Finish fin)
+                                                       double* __restrict__ mi, double* __restrict__ z,
+                                                       double* __restrict__ p, ReduceSlots rs, Finish fin)
 {
     Strip s(g);
     double acc[1] = {0.0};
@@ -90,7 +110,8 @@ static __global__ void __launch_bounds__(BX) k_pcg_init(Geo g, Faces fc, const d
             double rv[BS], zv[BS];
 #pragma unroll
             for (int q = 0; q < BS; ++q) rv[q] = q < m ? r[i0 + (long)q * x] : 0.0;
-            precond_block<BS>(kx, ky, i0, x, m, rv, zv);
+            precond_factor<BS>(kx, ky, mi, i0, x, m);
+            precond_apply<BS>(ky, mi, i0, x, m, rv, zv);
 #pragma unroll
             for (int q = 0; q < BS; ++q) {
                 if (q < m) {
@@ -110,8 +131,8 @@ static __global__ void __launch_bounds__(BX) k_pcg_init(Geo g, Faces fc, const d
 template <int BS, typename Finish>
 static __global__ void __launch_bounds__(BX) k_pcg_ur(Geo g, Scalar alpha, double* __restrict__ u,
                                                      const double* __restrict__ p, double* __restrict__ r,
-                                                     const double* __restrict__ w, const double* __restrict__ kx,
-                                                     const double* __restrict__ ky, double* __restrict__ z,
+                                                     const double* __restrict__ w, const double* __restrict__ ky,
+                                                     const double* __restrict__ mi, double* __restrict__ z,
                                                      ReduceSlots rs, const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
@@ -136,7 +157,7 @@ static __global__ void __launch_bounds__(BX) k_pcg_ur(Geo g, Scalar alpha, doubl
                     acc[0] += rn * rn;
                 }
             }
-            precond_block<BS>(kx, ky, i0, x, m, rv, zv);
+            precond_apply<BS>(ky, mi, i0, x, m, rv, zv);
 #pragma unroll
             for (int q = 0; q < BS; ++q) {
                 if (q < m) {

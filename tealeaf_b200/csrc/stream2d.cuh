@@ -41,6 +41,9 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\
 // Allows the next kernel of the stream to be launched.
 __device__ __forceinline__ void pdl_launch_next() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
+#ifndef TL2D_PDL_LATE
+#define TL2D_PDL_LATE 0
+#endif
 constexpr int kStreamBlocksPerSm = 4;
 
 // Strip `sid` of the interior grid (gx strips per row of strips).
@@ -178,7 +181,7 @@ static __global__ void __launch_bounds__(BX, kStreamBlocksPerSm) k_cg_w_stream(
     }
     __syncthreads();
     pdl_wait();
-    pdl_launch_next();
+    if (!TL2D_PDL_LATE) pdl_launch_next();
     if (gate_closed(done)) return;
     const double bt = FUSE_P ? beta.get() : 0.0;
 
@@ -301,6 +304,7 @@ static __global__ void __launch_bounds__(BX, kStreamBlocksPerSm) k_cg_w_stream(
         strip_partial<1>(acc, rs, sid, red);
     }
     // every issued stage was waited for: no copy in flight
+    if (TL2D_PDL_LATE) pdl_launch_next();
     strips_finish<1>(rs, nstrips, fin, red);
 }
 
@@ -342,7 +346,7 @@ static __global__ void __launch_bounds__(BX, kStreamBlocksPerSm) k_cg_ur_stream(
     }
     __syncthreads();
     pdl_wait();
-    pdl_launch_next();
+    if (!TL2D_PDL_LATE) pdl_launch_next();
     if (gate_closed(done)) return;
     const double a = alpha.get();
 
@@ -403,6 +407,7 @@ static __global__ void __launch_bounds__(BX, kStreamBlocksPerSm) k_cg_ur_stream(
         }
         strip_partial<1>(acc, rs, sid, red);
     }
+    if (TL2D_PDL_LATE) pdl_launch_next();
     strips_finish<1>(rs, nstrips, fin, red);
 }
 

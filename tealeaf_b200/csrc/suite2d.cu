@@ -119,8 +119,6 @@ static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
                             s->stream));
     TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, s->pq.b.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
                             s->stream));
-    const size_t smem = blocked_smem<1>();
-    TL_CUDA(cudaFuncSetAttribute(k_blocked<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // An even number of launches leaves r and sd in the buffers the chunk
     // pointed at: the host reads those pointers before its calls (e.g. the r
     // it passes to run_calculate_2norm), so a flush must not move them. An
@@ -132,9 +130,8 @@ static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
         const int pp0 = q * kTB;
         const BlockedArgs a{std::max(0, std::min(kTB, n - pp0)), std::min(pp0, n), 0, chunk->theta,
                             s->d_cheby_alphas, s->d_cheby_betas};
-        TL_LAUNCH(s, "k_blocked<ppcg>", (k_blocked<1><<<blocked_grid(s->g), kTBThreads, smem, s->stream>>>(
-                                            s->g, a, chunk->sd, chunk->r, s->alt[ALT_SD], s->alt[ALT_R], nullptr,
-                                            chunk->u, nullptr, nullptr, chunk->kx, chunk->ky, nullptr)));
+        launch_blocked<1>(s, "k_blocked<ppcg>", a, chunk->sd, chunk->r, s->alt[ALT_SD], s->alt[ALT_R], chunk->u,
+                          chunk->u, nullptr, nullptr, chunk->kx, chunk->ky, nullptr);
         swap_alt(s, chunk, ALT_SD);
         swap_alt(s, chunk, ALT_R);
     }
@@ -145,34 +142,55 @@ static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
 }
 
 // Runs the deferred Chebyshev trips (cheby.c:57-85 as the reference drivers
-// call them: per trip w = A u, r = u0 - w, p = alpha p + beta r, u += p, then
-// a depth-1 halo of u): temporally blocked launches of up to kTB trips, each
-// ending with its u += p, u reflected on the fly and its halo written; the
-// last trip also writes w and r. The same results as one launch per call.
+// call them: per trip a depth-1 halo of u, then w = A u, r = u0 - w,
+// p = alpha p + beta r, u += p): temporally blocked launches of up to kTB
+// trips, each trip ending with its u += p and u reflected on the fly; the
+// last launch also writes w and r, and leaves u's halo as the call-by-call
+// sequence does (mirroring u before the last add). The launches alternate
+// buffers and the host holds the chunk's pointers, so their number is made
+// even (a launch of two or more trips is split); a single trip runs as the
+// one-step kernels. The same results as one launch per call.
 static void run_cheby_queue(TlSuite2D* s, Chunk* chunk)
 {
     s->cq.active = false;
     const int n = (int)s->cq.a.size();
     if (n == 0) return;
-    TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, s->cq.a.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
-                            s->stream));
-    TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, s->cq.b.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
-                            s->stream));
-    const size_t smem = blocked_smem<0>();
-    TL_CUDA(cudaFuncSetAttribute(k_blocked<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    // As for the PPCG queue: an odd number of launches gets a closing
-    // zero-step launch, so u and p end in the buffers the chunk pointed at.
-    const int launches = (n + kTB - 1) / kTB;
-    for (int q = 0; q < launches + (launches & 1); ++q) {
-        const int first = std::min(q * kTB, n);
-        const int steps = std::max(0, std::min(kTB, n - first));
-        const BlockedArgs a{steps, first, steps > 0 && first + steps == n ? 1 : 0, 0.0,
-                            s->d_cheby_alphas, s->d_cheby_betas, 1};
-        TL_LAUNCH(s, "k_blocked<cheby>", (k_blocked<0><<<blocked_grid(s->g), kTBThreads, smem, s->stream>>>(
-                                             s->g, a, chunk->u, chunk->p, s->alt[ALT_U], s->alt[ALT_P], chunk->u0,
-                                             nullptr, chunk->w, chunk->r, chunk->kx, chunk->ky, nullptr)));
-        swap_alt(s, chunk, ALT_U);
-        swap_alt(s, chunk, ALT_P);
+    std::vector<int> sizes;
+    for (int left = n; left > 0; left -= kTB) sizes.push_back(std::min(kTB, left));
+    if (sizes.size() % 2 == 1) {
+        for (int q = (int)sizes.size() - 1; q >= 0; --q) {
+            if (sizes[q] >= 2) {
+                sizes[q] -= 1;
+                sizes.insert(sizes.begin() + q + 1, 1);
+                break;
+            }
+        }
+    }
+    if (sizes.size() % 2 == 1) {   // one trip: the absorbed halo update, then the one-step kernels
+        int which[TL_NUM_FIELDS] = {0};
+        which[TL_FIELD_U] = 1;
+        launch_halos(s, chunk, 1, which);
+        TL_LAUNCH(s, "k_cheby_sweep",
+                  k_cheby_sweep<false><<<interior_grid(s->g), BX, 0, s->stream>>>(
+                      s->g, s->cq.a[0], s->cq.b[0], 0.0, chunk->u, chunk->u0, chunk->p, chunk->r, chunk->w,
+                      chunk->kx, chunk->ky));
+        TL_LAUNCH(s, "k_add_p", k_add_p<<<interior_grid(s->g), BX, 0, s->stream>>>(s->g, chunk->u, chunk->p));
+    } else {
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, s->cq.a.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                                s->stream));
+        TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, s->cq.b.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                                s->stream));
+        int first = 0;
+        for (size_t q = 0; q < sizes.size(); ++q) {
+            const int steps = sizes[q];
+            const BlockedArgs a{steps, first, first + steps == n ? 1 : 0, 0.0, s->d_cheby_alphas,
+                                s->d_cheby_betas, 1};
+            launch_blocked<0>(s, "k_blocked<cheby>", a, chunk->u, chunk->p, s->alt[ALT_U], s->alt[ALT_P], chunk->u0,
+                              nullptr, chunk->w, chunk->r, chunk->kx, chunk->ky, nullptr);
+            swap_alt(s, chunk, ALT_U);
+            swap_alt(s, chunk, ALT_P);
+            first += steps;
+        }
     }
     s->cq.a.clear();
     s->cq.b.clear();

@@ -3,6 +3,7 @@
 // (driver2d.cu).
 #pragma once
 
+#include "blocked2d.cuh"
 #include "stream2d.cuh"
 
 #include <cuda_runtime.h>
@@ -212,7 +213,10 @@ static cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, size_t
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+#ifndef TL2D_PDL
+#define TL2D_PDL 1
+#endif
+    cfg.numAttrs = TL2D_PDL ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
@@ -278,4 +282,57 @@ static void launch_cg_ur2(TlSuite2D* s, dim3 grid, Scalar alpha, double* u, cons
     TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused<<<grid, BX, 0, s->stream>>>(s->g, alpha, u, p, r, w, s->rs, done,
                                                                             fin)));
 }
+// Region boxes (kTW x kTH cells, kind 4) of the TMA-staged blocked kernels.
+inline const CUtensorMap* blocked_map(TlSuite2D* s, const double* ptr)
+{
+    return tma_lookup(s, ptr, 4, [&](CUtensorMap* m) {
+        return tl::tma_encode_3d(m, ptr, s->g.x, s->g.y, 1, kTW, kTH, 1);
+    });
+}
+
+// The region boxes start at X0 - kTB = hd - kTB + kTX bx: an even halo depth
+// minus kTB, an even tile width and an even row length keep them on 16-byte
+// boundaries.
+inline bool blocked_tma_usable(const TlSuite2D* s)
+{
+    return s->tma && (s->g.hd - kTB) % 2 == 0 && kTX % 2 == 0 && s->g.x % 2 == 0;
+}
+
+// One temporally blocked launch of L <= kTB Chebyshev trips (MODE 0, C = u0)
+// or PPCG inner steps (MODE 1, C = u): the persistent TMA-staged kernel where
+// the alignment rules allow, else k_blocked (bit-identical results).
+// Internal linkage as launch_cg_w2.
+template <int MODE>
+static void launch_blocked(TlSuite2D* s, const char* name, const BlockedArgs& a, const double* A_in,
+                           const double* B_in, double* A_out, double* B_out, const double* C, double* u, double* w,
+                           double* r, const double* kx, const double* ky, const int* done)
+{
+    static unsigned attr_set = 0;   // devices on which the shared-memory sizes were raised
+    if (!(attr_set & (1u << (s->device & 31)))) {
+        TL_CUDA(cudaFuncSetAttribute(k_blocked<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)blocked_smem<MODE>()));
+        TL_CUDA(cudaFuncSetAttribute(k_blocked_tma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kBlockedTmaBytes));
+        attr_set |= 1u << (s->device & 31);
+    }
+    const dim3 gb = blocked_grid(s->g);
+    if (blocked_tma_usable(s)) {
+        const CUtensorMap* ma = blocked_map(s, A_in);
+        const CUtensorMap* mb = blocked_map(s, B_in);
+        const CUtensorMap* mc = blocked_map(s, C);
+        const CUtensorMap* mx = blocked_map(s, kx);
+        const CUtensorMap* my = blocked_map(s, ky);
+        if (ma && mb && mc && mx && my) {
+            const BlockedMaps m{*ma, *mb, *mc, *mx, *my};
+            const long tiles = (long)gb.x * gb.y;
+            const unsigned grid = (unsigned)std::min<long>(tiles, s->sm_count);
+            TL_LAUNCH(s, name, (k_blocked_tma<MODE><<<grid, kTBThreads, kBlockedTmaBytes, s->stream>>>(
+                                   s->g, a, m, A_out, B_out, u, w, r, done, s->d_mirror + kTmaErrWord2)));
+            return;
+        }
+    }
+    TL_LAUNCH(s, name, (k_blocked<MODE><<<gb, kTBThreads, blocked_smem<MODE>(), s->stream>>>(
+                           s->g, a, A_in, B_in, A_out, B_out, MODE == 0 ? C : nullptr, u, w, r, kx, ky, done)));
+}
+
 }  // namespace tl2d

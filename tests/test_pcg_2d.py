@@ -1,10 +1,10 @@
 """Jacobi-preconditioned CG (2D): jac_diag and jac_block (blocks of 4 rows).
 
 The reference documents both preconditioners (README.md:127-133) without a C
-implementation, so the oracle's restatement (oracle/tl_oracle.c, o2_precond
-and oc_pcg) is pinned here on its own terms first: its z solves M z = r for
-the stated M exactly (to rounding), and PCG needs fewer iterations than CG on
-the same deck. The GPU tests then hold the device-resident PCG to the oracle:
+implementation, so the oracle's restatement (oracle/tl_oracle.c,
+o2_precond_factor, o2_precond and oc_pcg) is pinned here on its own terms
+first: its z solves M z = r for the stated M exactly (to rounding), and PCG
+needs fewer iterations than CG on the same deck. The GPU tests then hold the device-resident PCG to the oracle:
 per-step iteration counts equal, field summaries within 1e-12 relative.
 """
 import ctypes as C
@@ -38,8 +38,9 @@ def test_oracle_block_solve_satisfies_the_blocks(oracle_lib, ny):
     hd, nx = 2, 9
     x, y = nx + 2 * hd, ny + 2 * hd
     kx, ky, r = _mesh(x, y, ny)
-    z = np.zeros((y, x))
-    oracle_lib.o2_precond(x, y, hd, 2, ptr(kx), ptr(ky), ptr(r), ptr(z))
+    z, mi = np.zeros((y, x)), np.zeros((y, x))
+    oracle_lib.o2_precond_factor(x, y, hd, 2, ptr(kx), ptr(ky), ptr(mi))
+    oracle_lib.o2_precond(x, y, hd, 2, ptr(ky), ptr(mi), ptr(r), ptr(z))
     for k in range(hd, x - hd):
         for jb in range(hd, y - hd, 4):
             m = min(4, y - hd - jb)
@@ -60,10 +61,12 @@ def test_oracle_diag_solve_is_the_diagonal(oracle_lib):
     hd, nx, ny = 2, 7, 6
     x, y = nx + 2 * hd, ny + 2 * hd
     kx, ky, r = _mesh(x, y, 3)
-    z = np.zeros((y, x))
-    oracle_lib.o2_precond(x, y, hd, 1, ptr(kx), ptr(ky), ptr(r), ptr(z))
+    z, mi = np.zeros((y, x)), np.zeros((y, x))
+    oracle_lib.o2_precond_factor(x, y, hd, 1, ptr(kx), ptr(ky), ptr(mi))
+    oracle_lib.o2_precond(x, y, hd, 1, ptr(ky), ptr(mi), ptr(r), ptr(z))
     sl = (slice(hd, y - hd), slice(hd, x - hd))
     d = 1.0 + (kx[hd:y - hd, hd + 1:x - hd + 1] + kx[sl]) + (ky[hd + 1:y - hd + 1, hd:x - hd] + ky[sl])
+    assert np.array_equal(mi[sl], 1.0 / d)      # the reference cuda kernel's mi = 1 / diag(A)
     assert np.array_equal(z[sl], (1.0 / d) * r[sl])
 
 
