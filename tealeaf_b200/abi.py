@@ -233,8 +233,9 @@ def load(dims: int) -> C.CDLL:
         lib.tl2d_batch_step.restype = _i
         lib.tl2d_batch_results.argtypes = [_p, _p, _p, _p]
         lib.tl2d_batch_results.restype = _i
-        lib.tl2d_batch_set_wait_limit.argtypes = [_p, C.c_longlong]
-        lib.tl2d_batch_set_wait_limit.restype = _i
+        if hasattr(lib, "tl2d_batch_set_wait_limit"):
+            lib.tl2d_batch_set_wait_limit.argtypes = [_p, C.c_longlong]
+            lib.tl2d_batch_set_wait_limit.restype = _i
     if hasattr(lib, pre + "set_preconditioner"):
         f = getattr(lib, pre + "set_preconditioner")
         f.argtypes = [C.POINTER(chunk_t), _i]

@@ -38,11 +38,12 @@ namespace tl2d {
 constexpr int kTB = TL2D_TB;            // most steps per launch (the region's margin)
 constexpr int kTW = 64;                 // region columns: one per thread of a row group
 #ifndef TL2D_TSEG
-#define TL2D_TSEG 16
+#define TL2D_TSEG 8
 #endif
-constexpr int kTSeg = TL2D_TSEG;        // region rows per thread (a column segment in registers)
+constexpr int kTSeg = TL2D_TSEG;        // region rows per thread (a column segment in registers; 8: 512
+                                        // threads at 128 registers, 16 warps per SM)
 constexpr int kTRows = 64 / kTSeg;      // row groups
-constexpr int kTBThreads = kTW * kTRows;   // 256
+constexpr int kTBThreads = kTW * kTRows;   // 512
 constexpr int kTH = kTSeg * kTRows;     // region rows (64)
 constexpr int kTX = kTW - 2 * kTB;      // tile columns (56)
 constexpr int kTY = kTH - 2 * kTB;      // tile rows (56)

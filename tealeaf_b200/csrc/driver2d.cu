@@ -204,10 +204,34 @@ struct Run {
         read_state();
         FinPcgUr fin_ur{s->d_state, s->d_cg_betas, prm, s->d_mirror};
         const Scalar alpha{0.0, &s->d_state->alpha};
+        if (tma_usable(s)) {
+            static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
+            if (!(attr_set & (1u << (s->device & 31)))) {
+                TL_CUDA(cudaFuncSetAttribute(k_pcg_ur_tma<BS, FinPcgUr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kPcgTmaBytes));
+                attr_set |= 1u << (s->device & 31);
+            }
+        }
         return cg_trips(0, true, z, [&](double* p) {
-            TL_LAUNCH(s, "k_pcg_ur", (k_pcg_ur<BS><<<gbi, BX, 0, s->stream>>>(gb, alpha, chunk->u, p, chunk->r,
-                                                                              chunk->w, chunk->ky, chunk->mi, z,
-                                                                              s->rs, done(), fin_ur)));
+            const CUtensorMap *mu = nullptr, *mp = nullptr, *mr = nullptr, *mw = nullptr, *mm = nullptr, *my = nullptr;
+            if (tma_usable(s)) {
+                mu = tma_map(s, chunk->u, 3);
+                mp = tma_map(s, p, 3);
+                mr = tma_map(s, chunk->r, 3);
+                mw = tma_map(s, chunk->w, 3);
+                mm = tma_map(s, chunk->mi, 3);
+                my = tma_map(s, chunk->ky, 3);
+            }
+            if (mu && mp && mr && mw && mm && my) {
+                const PcgMaps m{*mu, *mp, *mr, *mw, *mm, *my};
+                TL_LAUNCH(s, "k_pcg_ur", (k_pcg_ur_tma<BS><<<gbi, BX, kPcgTmaBytes, s->stream>>>(
+                                             gb, alpha, m, chunk->u, chunk->r, z, s->rs, done(), fin_ur,
+                                             s->d_mirror + kTmaErrWord2)));
+            } else {
+                TL_LAUNCH(s, "k_pcg_ur", (k_pcg_ur<BS><<<gbi, BX, 0, s->stream>>>(gb, alpha, chunk->u, p, chunk->r,
+                                                                                  chunk->w, chunk->ky, chunk->mi, z,
+                                                                                  s->rs, done(), fin_ur)));
+            }
         });
     }
 

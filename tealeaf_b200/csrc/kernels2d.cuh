@@ -693,6 +693,145 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
+// Rows of the CG w sweep fed by TMA (tma.cuh): kRowsT rows of a block's strip
+// of p and r with a two-column ring on each side (columns k0-2 .. k0+129: the
+// box starts on a 16-byte boundary for an even halo depth), kx with one
+// extra column, ky; each array at a 128-byte aligned offset.
+#ifndef TL2D_TMA_ROWS
+#define TL2D_TMA_ROWS 4
+#endif
+#ifndef TL2D_TMA_STAGES
+#define TL2D_TMA_STAGES 3
+#endif
+constexpr int kRowsT = TL2D_TMA_ROWS;
+constexpr int kStagesT = TL2D_TMA_STAGES;   // rows of stages b and b+1 are read while the rest are in flight
+// TMA alignment: strip starts hd + BX bx and the boxes' widths keep every x
+// start and every box row a multiple of 16 bytes for an even halo depth.
+static_assert((BX * sizeof(double)) % 16 == 0 && ((BX + 4) * sizeof(double)) % 16 == 0 &&
+                  ((BX + 2) * sizeof(double)) % 16 == 0,
+              "TMA boxes of the 2D sweeps must be multiples of 16 bytes wide");
+static_assert(kStagesT >= 3, "row block b reads stages b and b+1 while a later one is in flight");
+struct RowsT {
+    alignas(128) double P[kRowsT][BX + 4];
+    alignas(128) double R[kRowsT][BX + 4];
+    alignas(128) double KX[kRowsT][BX + 2];
+    alignas(128) double KY[kRowsT][BX];
+};
+struct Tma2Maps {
+    CUtensorMap p, r, kx, ky;
+};
+constexpr size_t kTmaRowsBytes = kStagesT * sizeof(RowsT) + kStagesT * 8 + 128;   // + barriers + alignment
+
+// k_cg_w_fused with its operand rows brought in by TMA. The same strips,
+// rows in the same order per thread and the same arithmetic, so the same
+// results (partial sums included). Stage b holds rows j0-1+4b .. j0+2+4b;
+// rows j0+4b .. j0+4b+3 read stages b and b+1. `err`: the bounded barrier
+// waits' flag.
+template <bool FUSE_P, bool REFLECT, typename Finish>
+static __global__ void __launch_bounds__(BX, 4) k_cg_w_fused_tma(Geo g, Faces fc, Scalar beta,
+                                                                      const __grid_constant__ Tma2Maps maps,
+                                                                      const double* __restrict__ p_in, double* p_out,
+                                                                      const double* __restrict__ r,
+                                                                      double* __restrict__ w, double* u_halo,
+                                                                      int uhd, ReduceSlots rs,
+                                                                      const int* __restrict__ done, Finish fin,
+                                                                      int* err)
+{
+    extern __shared__ __align__(128) unsigned char t2_raw[];
+    if (gate_closed(done)) return;
+    double acc[1] = {0.0};
+    const double bt = FUSE_P ? beta.get() : 0.0;
+    auto cur = [&](long idx) { return FUSE_P ? bt * p_in[idx] + r[idx] : p_in[idx]; };
+    if (blockIdx.y + 1 < gridDim.y) {
+        unsigned char* base = t2_raw + ((128 - (tl::smem_addr(t2_raw) & 127)) & 127);
+        RowsT* ring = reinterpret_cast<RowsT*>(base);
+        unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesT * sizeof(RowsT));
+        const StripC s(g);
+        const int x = g.x, tx = threadIdx.x;
+        const int k0 = g.hd + blockIdx.x * BX;
+        const int jb = s.j0 - 1;                              // first row of stage 0
+        const int np = (s.j1 - s.j0 + 2 + kRowsT - 1) / kRowsT;   // stages: rows j0-1 .. j1
+        constexpr unsigned kP = sizeof(double) * kRowsT * (BX + 4);
+        constexpr unsigned kK = sizeof(double) * kRowsT * ((BX + 2) + BX);
+        auto issue = [&](int b) {
+            RowsT& S = ring[b % kStagesT];
+            unsigned long long* bar = &bars[b % kStagesT];
+            const int y0 = jb + b * kRowsT;
+            tl::mbar_expect_tx(bar, kP * (FUSE_P ? 2u : 1u) + kK);
+            tl::tma_load_3d(&S.P[0][0], &maps.p, k0 - 2, y0, 0, bar);
+            if (FUSE_P) tl::tma_load_3d(&S.R[0][0], &maps.r, k0 - 2, y0, 0, bar);
+            tl::tma_load_3d(&S.KX[0][0], &maps.kx, k0, y0, 0, bar);
+            tl::tma_load_3d(&S.KY[0][0], &maps.ky, k0, y0, 0, bar);
+        };
+        if (tx == 0) {
+            for (int q = 0; q < kStagesT; ++q) tl::mbar_init(&bars[q], 1);
+            tl::mbar_fence_init();
+        }
+        __syncthreads();
+        if (tx == 0)
+            for (int b = 0; b < kStagesT - 1 && b < np; ++b) issue(b);
+        // row j of the strip: stage (j - jb) / 4, row (j - jb) % 4
+        auto raw = [&](int j, int dx) -> double {
+            const int t = j - jb;
+            return ring[(t / kRowsT) % kStagesT].P[t % kRowsT][tx + 2 + dx];
+        };
+        auto fused = [&](int j, int dx) -> double {
+            const int t = j - jb;
+            const RowsT& S = ring[(t / kRowsT) % kStagesT];
+            return FUSE_P ? bt * S.P[t % kRowsT][tx + 2 + dx] + S.R[t % kRowsT][tx + 2 + dx]
+                          : S.P[t % kRowsT][tx + 2 + dx];
+        };
+        double pc = 0.0, pd = 0.0, kyc = 0.0;
+        long i = s.kk + (long)s.j0 * x;
+        for (int b = 0; b * kRowsT < s.j1 - s.j0; ++b) {
+            tl::mbar_wait(&bars[b % kStagesT], (unsigned)(b / kStagesT) & 1u, err);
+            if (b + 1 < np) tl::mbar_wait(&bars[(b + 1) % kStagesT], (unsigned)((b + 1) / kStagesT) & 1u, err);
+            __syncthreads();   // every thread is past rows of block b-1: stage b-1 is free
+            if (tx == 0 && b + kStagesT - 1 < np) issue(b + kStagesT - 1);
+            if (b == 0) {
+                pc = fused(s.j0, 0);
+                pd = (s.j0 == g.hd) ? ((REFLECT && fc.b) ? pc : raw(s.j0 - 1, 0)) : fused(s.j0 - 1, 0);
+                kyc = ring[0].KY[1][tx];
+            }
+#pragma unroll
+            for (int u = 0; u < kRowsT; ++u) {
+                const int j = s.j0 + b * kRowsT + u;
+                if (j >= s.j1) break;
+                const int t = j - jb, tu = t + 1;
+                const RowsT& S = ring[(t / kRowsT) % kStagesT];
+                const RowsT& U = ring[(tu / kRowsT) % kStagesT];
+                const bool at_t = j == g.y - g.hd - 1;
+                const double pu = at_t ? ((REFLECT && fc.t) ? pc : raw(j + 1, 0)) : fused(j + 1, 0);
+                const double kyu = U.KY[tu % kRowsT][tx];
+                const double kxc = S.KX[t % kRowsT][tx];
+                double pl = __shfl_up_sync(kFull, pc, 1);
+                double pr = __shfl_down_sync(kFull, pc, 1);
+                double kxr = __shfl_down_sync(kFull, kxc, 1);
+                if (s.at_l) pl = (REFLECT && fc.l) ? pc : raw(j, -1);
+                else if (s.lane == 0) pl = fused(j, -1);
+                if (s.at_r) pr = (REFLECT && fc.r) ? pc : raw(j, 1);
+                else if (s.lane == 31) pr = fused(j, 1);
+                if (s.at_r || s.lane == 31) kxr = S.KX[t % kRowsT][tx + 1];
+                const double v = smvp(kxc, kxr, kyc, kyu, pc, pl, pr, pd, pu);
+                if (s.active) {
+                    w[i] = v;
+                    acc[0] += v * pc;
+                    if (FUSE_P) p_out[i] = pc;
+                }
+                pd = pc;
+                pc = pu;
+                kyc = kyu;
+                i += x;
+            }
+        }
+        // every issued stage was waited for (the last rows read stage np-1): no copy in flight
+    } else {
+        if (REFLECT) halo_duty(g, fc, 1, p_out, cur);
+        if (u_halo) halo_duty(g, fc, uhd, u_halo, [&](long idx) { return u_halo[idx]; });
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
 // CG sweep 2: u += alpha p ; r -= alpha w ; rrn = sum(r*r)  (cg.c:116-143)
 template <typename Finish>
 static __global__ void __launch_bounds__(BX, TL2D_MINB) k_cg_ur_fused(Geo g, Scalar alpha, double* __restrict__ u,
@@ -712,6 +851,80 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
             const double rn = r[i] - a * w[i];
             r[i] = rn;
             acc[0] += rn * rn;
+        }
+    }
+    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
+// k_cg_ur_fused with its operands brought in by TMA: stages of kRowsU rows
+// of the block's strip of u, p, r, w (128-column boxes starting at the strip's
+// first column, even for an even halo depth). Same strips, rows in the same
+// order per thread, same arithmetic: the same results, partial sums included.
+constexpr int kRowsU = 4;
+constexpr int kStagesU = 3;
+struct RowsU {
+    alignas(128) double U[kRowsU][BX];
+    alignas(128) double P[kRowsU][BX];
+    alignas(128) double R[kRowsU][BX];
+    alignas(128) double W[kRowsU][BX];
+};
+struct TmaUrMaps {
+    CUtensorMap u, p, r, w;
+};
+constexpr size_t kTmaUrBytes = kStagesU * sizeof(RowsU) + kStagesU * 8 + 128;
+
+template <typename Finish>
+static __global__ void __launch_bounds__(BX, 4) k_cg_ur_fused_tma(Geo g, Scalar alpha,
+                                                               const __grid_constant__ TmaUrMaps maps,
+                                                               double* __restrict__ u, double* __restrict__ r,
+                                                               ReduceSlots rs, const int* __restrict__ done,
+                                                               Finish fin, int* err)
+{
+    extern __shared__ __align__(128) unsigned char tu_raw[];
+    if (gate_closed(done)) return;
+    unsigned char* base = tu_raw + ((128 - (tl::smem_addr(tu_raw) & 127)) & 127);
+    RowsU* ring = reinterpret_cast<RowsU*>(base);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesU * sizeof(RowsU));
+    Strip s(g);
+    double acc[1] = {0.0};
+    const int tx = threadIdx.x;
+    const int k0 = g.hd + blockIdx.x * BX;
+    const int np = (s.j1 - s.j0 + kRowsU - 1) / kRowsU;
+    auto issue = [&](int b) {
+        RowsU& S = ring[b % kStagesU];
+        unsigned long long* bar = &bars[b % kStagesU];
+        const int y0 = s.j0 + b * kRowsU;
+        tl::mbar_expect_tx(bar, 4u * sizeof(double) * kRowsU * BX);
+        tl::tma_load_3d(&S.U[0][0], &maps.u, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.P[0][0], &maps.p, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.R[0][0], &maps.r, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.W[0][0], &maps.w, k0, y0, 0, bar);
+    };
+    if (tx == 0) {
+        for (int q = 0; q < kStagesU; ++q) tl::mbar_init(&bars[q], 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (tx == 0)
+        for (int b = 0; b < kStagesU - 1 && b < np; ++b) issue(b);
+    const double a = alpha.get();
+    long i = s.k + (long)s.j0 * g.x;
+    for (int b = 0; b < np; ++b) {
+        tl::mbar_wait(&bars[b % kStagesU], (unsigned)(b / kStagesU) & 1u, err);
+        __syncthreads();   // every thread is past stage b-1: its slot is free
+        if (tx == 0 && b + kStagesU - 1 < np) issue(b + kStagesU - 1);
+        const RowsU& S = ring[b % kStagesU];
+#pragma unroll
+        for (int t = 0; t < kRowsU; ++t) {
+            const int j = s.j0 + b * kRowsU + t;
+            if (j >= s.j1) break;
+            if (s.active) {
+                u[i] = S.U[t][tx] + a * S.P[t][tx];
+                const double rn = S.R[t][tx] - a * S.W[t][tx];
+                r[i] = rn;
+                acc[0] += rn * rn;
+            }
+            i += g.x;
         }
     }
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);

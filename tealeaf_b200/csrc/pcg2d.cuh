@@ -170,4 +170,121 @@ static __global__ void __launch_bounds__(BX) k_pcg_ur(Geo g, Scalar alpha, doubl
     tl::grid_sum<2, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
+// k_pcg_ur with its operands brought in by TMA: stages of kPcgRows = 4 rows
+// (one jac_block block, four jac_diag ones) of the strip's u, p, r, w, mi and,
+// for jac_block, ky (BX-column boxes from the strip's first column, 16-byte
+// aligned for an even halo depth), in a 3-stage ring on shared-memory
+// barriers; every wait bounded (err). The same strips, rows, order and
+// arithmetic as k_pcg_ur: the same results, partial sums included.
+constexpr int kPcgRows = 4;
+constexpr int kPcgStages = 3;
+struct PcgRows {
+    alignas(128) double U[kPcgRows][BX];
+    alignas(128) double P[kPcgRows][BX];
+    alignas(128) double R[kPcgRows][BX];
+    alignas(128) double W[kPcgRows][BX];
+    alignas(128) double MI[kPcgRows][BX];
+    alignas(128) double KY[kPcgRows][BX];
+};
+struct PcgMaps {
+    CUtensorMap u, p, r, w, mi, ky;
+};
+constexpr size_t kPcgTmaBytes = kPcgStages * sizeof(PcgRows) + kPcgStages * 8 + 128;
+
+template <int BS, typename Finish>
+static __global__ void __launch_bounds__(BX, 3) k_pcg_ur_tma(Geo g, Scalar alpha, const __grid_constant__ PcgMaps maps,
+                                                            double* __restrict__ u, double* __restrict__ r,
+                                                            double* __restrict__ z, ReduceSlots rs,
+                                                            const int* __restrict__ done, Finish fin, int* err)
+{
+    static_assert(kPcgRows % BS == 0, "a stage holds whole preconditioner blocks");
+    extern __shared__ __align__(128) unsigned char tp_raw[];
+    if (gate_closed(done)) return;
+    unsigned char* base = tp_raw + ((128 - (tl::smem_addr(tp_raw) & 127)) & 127);
+    PcgRows* ring = reinterpret_cast<PcgRows*>(base);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kPcgStages * sizeof(PcgRows));
+    Strip s(g);
+    double acc[2] = {0.0, 0.0};
+    const int tx = threadIdx.x;
+    const int k0 = g.hd + blockIdx.x * BX;
+    const int np = (s.j1 - s.j0 + kPcgRows - 1) / kPcgRows;
+    auto issue = [&](int b) {
+        PcgRows& S = ring[b % kPcgStages];
+        unsigned long long* bar = &bars[b % kPcgStages];
+        const int y0 = s.j0 + b * kPcgRows;
+        tl::mbar_expect_tx(bar, (BS > 1 ? 6u : 5u) * sizeof(double) * kPcgRows * BX);
+        tl::tma_load_3d(&S.U[0][0], &maps.u, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.P[0][0], &maps.p, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.R[0][0], &maps.r, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.W[0][0], &maps.w, k0, y0, 0, bar);
+        tl::tma_load_3d(&S.MI[0][0], &maps.mi, k0, y0, 0, bar);
+        if (BS > 1) tl::tma_load_3d(&S.KY[0][0], &maps.ky, k0, y0, 0, bar);
+    };
+    if (tx == 0) {
+        for (int q = 0; q < kPcgStages; ++q) tl::mbar_init(&bars[q], 1);
+        tl::mbar_fence_init();
+    }
+    __syncthreads();
+    if (tx == 0)
+        for (int b = 0; b < kPcgStages - 1 && b < np; ++b) issue(b);
+    const double a = alpha.get();
+    const int x = g.x;
+    for (int b = 0; b < np; ++b) {
+        tl::mbar_wait(&bars[b % kPcgStages], (unsigned)(b / kPcgStages) & 1u, err);
+        __syncthreads();   // every thread is past stage b-1: its slot is free
+        if (tx == 0 && b + kPcgStages - 1 < np) issue(b + kPcgStages - 1);
+        const PcgRows& S = ring[b % kPcgStages];
+#pragma unroll
+        for (int q0 = 0; q0 < kPcgRows; q0 += BS) {
+            const int jb = s.j0 + b * kPcgRows + q0;
+            if (jb >= s.j1) break;
+            const int m = min(BS, s.j1 - jb);
+            const long i0 = s.k + (long)jb * x;
+            double rv[BS], zv[BS];
+#pragma unroll
+            for (int q = 0; q < BS; ++q) {
+                rv[q] = 0.0;
+                if (q < m && s.active) {
+                    u[i0 + (long)q * x] = S.U[q0 + q][tx] + a * S.P[q0 + q][tx];
+                    const double rn = S.R[q0 + q][tx] - a * S.W[q0 + q][tx];
+                    r[i0 + (long)q * x] = rn;
+                    rv[q] = rn;
+                    acc[0] += rn * rn;
+                }
+            }
+            if (BS == 1) {
+                zv[0] = S.MI[q0][tx] * rv[0];
+            } else {
+                // precond_apply's recurrences on the staged rows (ky of row q+1 is in the block)
+                double yv[BS];
+#pragma unroll
+                for (int q = 0; q < BS; ++q)
+                    if (q < m) yv[q] = q == 0 ? rv[0] * S.MI[q0][tx] : (rv[q] + S.KY[q0 + q][tx] * yv[q - 1]) * S.MI[q0 + q][tx];
+                double zn = 0.0;
+#pragma unroll
+                for (int q = BS - 1; q >= 0; --q) {
+                    if (q < m) {
+                        if (q == m - 1) {
+                            zn = yv[q];
+                        } else {
+                            const double c = -S.KY[q0 + q + 1][tx] * S.MI[q0 + q][tx];
+                            zn = yv[q] - c * zn;
+                        }
+                        zv[q] = zn;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < BS; ++q) {
+                if (q < m && s.active) {
+                    z[i0 + (long)q * x] = zv[q];
+                    acc[1] += rv[q] * zv[q];
+                }
+            }
+        }
+    }
+    // every issued stage was waited for: no copy in flight
+    tl::grid_sum<2, BX>(acc, rs, block_id(), block_count(), fin);
+}
+
 }  // namespace tl2d

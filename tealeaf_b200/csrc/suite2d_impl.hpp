@@ -4,12 +4,10 @@
 #pragma once
 
 #include "blocked2d.cuh"
-#include "stream2d.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <utility>
 #include <vector>
 
 // Buffers that alternate between two slices (fused sweeps read the old values
@@ -172,9 +170,9 @@ inline const CUtensorMap* tma_lookup(TlSuite2D* s, const void* ptr, int kind, En
     return &e.map;
 }
 
-// Tensor map of a chunk array for k_cg_w_stream: kind 0 operand rows (box
+// Tensor map of a chunk array for k_cg_w_fused_tma: kind 0 operand rows (box
 // (BX+4) x kRowsT), 1 kx ((BX+2) x kRowsT), 2 ky (BX x kRowsT); for
-// k_cg_ur_stream: kind 3 (BX x kRowsU).
+// k_cg_ur_fused_tma: kind 3 (BX x kRowsU).
 inline const CUtensorMap* tma_map(TlSuite2D* s, const double* ptr, int kind)
 {
     static const unsigned box[4] = {BX + 4, BX + 2, BX, BX};
@@ -189,42 +187,10 @@ inline bool tma_usable(const TlSuite2D* s) { return s->tma && s->g.hd % 2 == 0 &
 
 inline bool tma_failed(const TlSuite2D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord2] != 0; }
 
-// Persistent grid of the streaming sweeps: one block per strip up to
-// kStreamBlocksPerSm blocks per SM.
-inline dim3 stream_grid(const TlSuite2D* s)
-{
-    const dim3 gi = interior_grid(s->g);
-    const long strips = (long)gi.x * gi.y;
-    return dim3((unsigned)std::min<long>(strips, (long)s->sm_count * kStreamBlocksPerSm));
-}
-
-// Launch with programmatic dependent launch allowed (the kernel waits for
-// its predecessor in the stream with griddepcontrol.wait).
-template <typename... Params, typename... Args>
-static cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, size_t smem, cudaStream_t st,
-                                    Args&&... args)
-{
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = dim3(BX);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-#ifndef TL2D_PDL
-#define TL2D_PDL 1
-#endif
-    cfg.numAttrs = TL2D_PDL ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
-
-// The fused CG w sweep (k_cg_w_fused semantics): the streaming TMA-fed
-// kernel where the alignment rules allow, else the per-thread-load kernel on
-// `grid` (interior blocks + the halo-duty row). Internal linkage, like the
-// kernels it launches: each translation unit has its own kernel copies, so
-// each keeps its own record of the raised shared-memory limit.
+// The fused CG w sweep (k_cg_w_fused semantics), by TMA where possible.
+// Internal linkage, like the kernels it launches: each translation unit has
+// its own kernel copies, so each keeps its own record of the raised
+// shared-memory limit.
 template <bool F, bool R, typename Finish>
 static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc, Scalar beta, const double* p_in,
                   double* p_out, const double* r, double* w, double* u_halo, int uhd, const int* done, Finish fin)
@@ -238,14 +204,13 @@ static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc,
             const Tma2Maps m{*a, *b, *kx, *ky};
             static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
             if (!(attr_set & (1u << (s->device & 31)))) {
-                TL_CUDA(cudaFuncSetAttribute(k_cg_w_stream<F, R, Finish>,
+                TL_CUDA(cudaFuncSetAttribute(k_cg_w_fused_tma<F, R, Finish>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaRowsBytes));
                 attr_set |= 1u << (s->device & 31);
             }
-            TL_LAUNCH(s, "k_cg_w_fused",
-                      launch_dependent(k_cg_w_stream<F, R, Finish>, stream_grid(s), kTmaRowsBytes, s->stream, s->g,
-                                       fc, beta, m, p_out, w, u_halo, uhd, s->rs, done, fin,
-                                       s->d_mirror + kTmaErrWord2));
+            TL_LAUNCH(s, "k_cg_w_fused", (k_cg_w_fused_tma<F, R><<<grid, BX, kTmaRowsBytes, s->stream>>>(
+                                             s->g, fc, beta, m, p_in, p_out, r, w, u_halo, uhd, s->rs, done, fin,
+                                             s->d_mirror + kTmaErrWord2)));
             return;
         }
     }
@@ -254,8 +219,8 @@ static void launch_cg_w2(TlSuite2D* s, Chunk* chunk, dim3 grid, const Faces& fc,
                                      done, fin)));
 }
 
-// The fused CG u/r update (k_cg_ur_fused semantics), streaming and TMA-fed
-// where possible (internal linkage as launch_cg_w2).
+// The fused CG u/r update (k_cg_ur_fused semantics), by TMA where possible
+// (internal linkage as launch_cg_w2).
 template <typename Finish>
 static void launch_cg_ur2(TlSuite2D* s, dim3 grid, Scalar alpha, double* u, const double* p, double* r, const double* w,
                    const int* done, Finish fin)
@@ -269,13 +234,12 @@ static void launch_cg_ur2(TlSuite2D* s, dim3 grid, Scalar alpha, double* u, cons
             const TmaUrMaps m{*mu, *mp, *mr, *mw};
             static unsigned attr_set = 0;   // devices on which the shared-memory size was raised
             if (!(attr_set & (1u << (s->device & 31)))) {
-                TL_CUDA(cudaFuncSetAttribute(k_cg_ur_stream<Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                TL_CUDA(cudaFuncSetAttribute(k_cg_ur_fused_tma<Finish>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kTmaUrBytes));
                 attr_set |= 1u << (s->device & 31);
             }
-            TL_LAUNCH(s, "k_cg_ur_fused",
-                      launch_dependent(k_cg_ur_stream<Finish>, stream_grid(s), kTmaUrBytes, s->stream, s->g, alpha, m,
-                                       u, r, s->rs, done, fin, s->d_mirror + kTmaErrWord2));
+            TL_LAUNCH(s, "k_cg_ur_fused", (k_cg_ur_fused_tma<<<grid, BX, kTmaUrBytes, s->stream>>>(
+                                              s->g, alpha, m, u, r, s->rs, done, fin, s->d_mirror + kTmaErrWord2)));
             return;
         }
     }

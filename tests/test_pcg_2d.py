@@ -121,3 +121,23 @@ def test_preconditioner_setter_rejects_unknown_types():
             abi.check(h.lib, 2)
     finally:
         h.finalise()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pc", ["jac_diag", "jac_block"])
+def test_tma_fed_pcg_sweep_is_bit_identical(pc):
+    """The TMA-fed u/r/z sweep (k_pcg_ur_tma) and the per-thread-load one
+    (k_pcg_ur, tl2d_set_tma(0)) give the same counts, summaries and fields."""
+    from tealeaf_b200.host import Host
+    prob = problems.seeded(2, (300, 170), 33, 4, 2, solver="cg", end_step=2, name="pcgt").with_(preconditioner=pc)
+    a, b = Host(prob.tea_in(), 2), Host(prob.tea_in(), 2)
+    try:
+        b.lib.tl2d_set_tma(C.byref(b.chunk), 0)
+        for tt in range(2):
+            ra, rb = a.solve_device(tt), b.solve_device(tt)
+            assert ra.iterations == rb.iterations and ra.summary == rb.summary
+            for f in ("u", "p", "r", "w", "energy", "mi"):
+                assert np.array_equal(a.download(f), b.download(f)), (pc, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()

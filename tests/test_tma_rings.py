@@ -1,17 +1,8 @@
-"""Host-side check of the TMA ring protocols of the staged sweeps
-(tealeaf_b200/csrc: the streaming 2D CG sweeps k_cg_w_stream and
-k_cg_ur_stream in stream2d.cuh; walkt and k3_cg_ur_tma in kernels3d.cuh;
-k_rf_w_tma and k_rf_ur_tma in rftma2d.cuh; the blocked preconditioner is not
-staged).
-
-Streaming protocol (stream2d.cuh): a persistent block owns several strips
-and their stages form one sequence. Before consuming stage q every thread
-passes a block barrier; then one thread issues stages while fewer than
-q + kStages have been issued (the newest, q + kStages - 1, goes into the slot
-stage q-1 left), then every thread waits for stage q and reads only stage q
-(rows needed later are carried in registers).
-
-Per-strip protocol (the other kernels):
+"""Host-side check of the TMA ring protocol the staged sweeps share
+(tealeaf_b200/csrc: k_cg_w_fused_tma, k_cg_ur_fused_tma in kernels2d.cuh;
+k_pcg_ur_tma in pcg2d.cuh; walkt and k3_cg_ur_tma in kernels3d.cuh;
+k_rf_w_tma and k_rf_ur_tma in rftma2d.cuh), and of the TMA-staged blocked
+kernel (k_blocked_tma in blocked2d.cuh: one barrier, one region in flight).
 
 Each kernel walks its rows (or z-planes) in blocks; before block b it waits
 on the shared-memory barriers of the stages it reads, synchronises the
@@ -79,56 +70,32 @@ def ceil_div(a, b):
     return -(-a // b)
 
 
-def simulate_stream(strip_stage_counts, stages):
-    """Replays one persistent block of the streaming protocol over strips
-    with the given stage counts; returns the stages consumed."""
-    total = sum(strip_stage_counts)
-    slot_of, issued, waited, uses = {}, [], set(), {}
-    done_reading = -1            # every stage <= this one is read no more
-    q = 0
-    for np_ in strip_stage_counts:
-        for _ in range(np_):
-            done_reading = q - 1     # block barrier: stage q-1 was consumed by every thread
-            while len(issued) < total and len(issued) < q + stages:
-                st = len(issued)
-                slot = st % stages
-                prev = slot_of.get(slot)
-                if prev is not None:
-                    assert prev <= done_reading, "slot overwritten while still read"
-                    assert prev in waited, "slot reused before its copy was waited for"
-                slot_of[slot] = st
-                issued.append(st)
-            assert q in issued, "wait on a stage never issued (would hang)"
-            slot = q % stages
-            assert slot_of[slot] == q
-            uses[slot] = uses.get(slot, 0) + 1
-            waited.add(q)
-            assert (q // stages) == uses[slot] - 1     # the wait parity the kernel uses
-            q += 1
-    assert set(issued) == waited, "a copy may still be in flight when the block ends"
-    return q
-
-
-@pytest.mark.parametrize("stages", [3, 4])
-def test_streaming_rings(stages):
-    rows = 4
-    for n in range(1, 70):                     # rows of a full strip
-        for last in (n, max(1, n // 3), 1):    # the grid's last row of strips may be shorter
-            for nstrips in range(1, 6):
-                lens = [n] * (nstrips - 1) + [last]
-                # w sweep: rows j0-1 .. j1 of each strip; u/r update: rows j0 .. j1-1
-                w_counts = [ceil_div(m + 2, rows) for m in lens]
-                assert simulate_stream(w_counts, stages) == sum(w_counts)
-                ur_counts = [ceil_div(m, rows) for m in lens]
-                assert simulate_stream(ur_counts, stages) == sum(ur_counts)
-                # every row a strip needs lies in one of its own stages
-                for m, c in zip(lens, w_counts):
-                    assert c * rows >= m + 2
+def test_blocked_region_prefetch():
+    """k_blocked_tma: one barrier; tile t's region is issued before the loop
+    (t = first) or after every thread has read tile t - G's region (the
+    block barrier in the tile function), and waited for with parity of the
+    tile's ordinal; every issued region is waited for."""
+    for ntiles in range(1, 40):
+        for grid in range(1, 12):
+            for b in range(min(grid, ntiles)):
+                mine = list(range(b, ntiles, grid))
+                issued, waited, reads_done = [mine[0]], [], set()
+                phase = 0
+                for n, t in enumerate(mine):
+                    assert issued[-1] == t, "waiting for a region never issued (would hang)"
+                    assert n % 2 == phase
+                    waited.append(t)
+                    reads_done.add(t)      # registers taken, block barrier passed
+                    if n + 1 < len(mine):
+                        assert t in reads_done   # the staging is free before it is reused
+                        issued.append(mine[n + 1])
+                    phase ^= 1
+                assert issued == waited, "a region copy may still be in flight at exit"
 
 
 @pytest.mark.parametrize("rows,stages", [(4, 3), (4, 4), (8, 3), (2, 5)])
 def test_w_sweep_rings(rows, stages):
-    # the refinement w sweep: stage b holds strip rows
+    # 2D CG w sweep and the refinement w sweep: stage b holds strip rows
     # j0-1+rows*b .. ; row block b (rows j0+rows*b ..) reads stages b and b+1
     for n in range(1, 200):
         def reads(b):
@@ -152,7 +119,8 @@ def test_w_sweep_rings(rows, stages):
 
 @pytest.mark.parametrize("rows,stages", [(4, 3), (2, 3)])
 def test_pointwise_sweep_rings(rows, stages):
-    # 3D / refinement u-r updates: stage b holds units rows*b .. ; trip b reads stage b
+    # 2D / 3D / refinement u-r updates and the PCG u/r/z sweep: stage b holds
+    # units rows*b .. ; trip b reads stage b
     for n in range(1, 200):
         simulate(n, rows, stages,
                  np_fn=lambda n: ceil_div(n, rows),
