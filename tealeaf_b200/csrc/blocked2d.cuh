@@ -3,8 +3,8 @@
 //
 // Between two norm evaluations a Chebyshev trip (cheby.c:57-85) and a PPCG
 // inner step (ppcg.c:29-61) are local stencil updates with no global
-// reduction, so L of them (L <= kTB) run in one launch: a block takes its
-// tile of kTX x kTY cells plus an L-cell halo on chip, each thread holding a
+// reduction, so L of them (L <= Blk::TB) run in one launch: a block takes its
+// tile of Blk::TX x Blk::TY cells plus an L-cell halo on chip, each thread holding a
 // 16-row column segment of the carried fields, u0 (resp. u) and the face
 // coefficients in registers, advances them L times (each step's valid region
 // shrinks by one cell per side; the domain boundary is the depth-1 reflective
@@ -32,10 +32,6 @@
 
 namespace tl2d {
 
-#ifndef TL2D_TB
-#define TL2D_TB 4
-#endif
-constexpr int kTB = TL2D_TB;            // most steps per launch (the region's margin)
 constexpr int kTW = 64;                 // region columns: one per thread of a row group
 #ifndef TL2D_TSEG
 #define TL2D_TSEG 8
@@ -45,11 +41,23 @@ constexpr int kTSeg = TL2D_TSEG;        // region rows per thread (a column segm
 constexpr int kTRows = 64 / kTSeg;      // row groups
 constexpr int kTBThreads = kTW * kTRows;   // 512
 constexpr int kTH = kTSeg * kTRows;     // region rows (64)
-constexpr int kTX = kTW - 2 * kTB;      // tile columns (56)
-constexpr int kTY = kTH - 2 * kTB;      // tile rows (56)
+
+// Tile shape of each mode. The margin TB is the most steps one launch can
+// take (the valid region shrinks by one cell per step); the tile is the
+// region less the margin on each side. Chebyshev (MODE 0): margin 6, whose
+// even value keeps the TMA-staged regions' boxes 16-byte aligned; PPCG
+// (MODE 1): margin 5 with per-thread region loads, which measured faster
+// for it than the staged kernel (bench.py --solver ppcg at 4096^2).
+template <int MODE>
+struct Blk {
+    static constexpr int TB = MODE == 0 ? 6 : 5;
+    static constexpr int TX = kTW - 2 * TB;   // tile columns (52 / 54)
+    static constexpr int TY = kTH - 2 * TB;   // tile rows
+    static_assert(TX > 0 && TY > 0, "the margin must leave a tile");
+};
 
 struct BlockedArgs {
-    int steps;          // L <= kTB
+    int steps;          // L <= the mode's margin (Blk<MODE>::TB)
     int first;          // Chebyshev: coefficient index of the first trip; PPCG: pp of the first step
     int wr_last;        // Chebyshev: write w and r of the last trip
     double theta;       // PPCG fold of pp == 0
@@ -58,8 +66,6 @@ struct BlockedArgs {
     int add_end;        // Chebyshev: each trip ends with its u += p (the kernel-interface calls'
                         // order) instead of starting with the previous trip's
 };
-
-static_assert(kTX > 0 && kTY > 0 && kTX % 2 == 0, "blocked tiles: an even tile width keeps TMA region starts aligned");
 
 // Thread (cx, cy) holds column cx of the region, rows cy * kTSeg .. + kTSeg,
 // in registers: the two carried fields, u0 (Chebyshev) or u (PPCG, tile cells)
@@ -71,7 +77,7 @@ static_assert(kTX > 0 && kTY > 0 && kTX % 2 == 0, "blocked tiles: an even tile w
 // reflective depth-1 halo); cells outside the interior or beyond the loaded
 // margin compute values nothing valid reads.
 // The operand region of a tile (kTW x kTH cells from grid column xs =
-// X0 - kTB, row ys = Y0 - kTB): src.a / b / c / kx / ky (gi, ry, cx) give the
+// X0 - TB, row ys = Y0 - TB): src.a / b / c / kx / ky (gi, ry, cx) give the
 // value of a field at grid index gi, region row ry, region column cx; kxr the
 // face coefficient one column to the right.
 struct GlobalRegion {
@@ -88,7 +94,7 @@ struct GlobalRegion {
     __device__ __forceinline__ double ky(long gi, int, int) const { return KY[gi]; }
 };
 
-// One tile: L <= kTB steps of MODE on the region given by `src`, then the
+// One tile: L <= TB steps of MODE on the region given by `src`, then the
 // tile written back. S0, S1: the two kTH x kTW stencil buffers; loaded() runs
 // in every thread once the region is in registers.
 template <int MODE, typename Src, typename Loaded>
@@ -101,22 +107,22 @@ __device__ __forceinline__ void blocked_tile(const Geo& g, const BlockedArgs& a,
     const int ilo = hd, ihi = g.x - hd, jlo = hd, jhi = g.y - hd;   // interior [lo, hi)
     const int H = a.steps;
     const int tid = threadIdx.x, cx = tid % kTW, cy = tid / kTW, lane = tid & 31;
-    const int gx = X0 - kTB + cx;    // grid column of this thread
-    const int oy = Y0 - kTB;         // grid row of region row 0
+    const int gx = X0 - Blk<MODE>::TB + cx;    // grid column of this thread
+    const int oy = Y0 - Blk<MODE>::TB;         // grid row of region row 0
     const int r0 = cy * kTSeg;       // first region row of this thread
     const bool colin = gx >= ilo && gx < ihi;
-    const int mxc = max(max(kTB - cx, cx - (kTB + kTX - 1)), 0);   // column distance outside the tile
+    const int mxc = max(max(Blk<MODE>::TB - cx, cx - (Blk<MODE>::TB + Blk<MODE>::TX - 1)), 0);   // column distance outside the tile
     const bool at_l = gx == ilo, at_r = gx == ihi - 1;
     const bool hi_half = cx >= 32;
     const int edge_lane = hi_half ? 0 : 31, edge_dx = hi_half ? -1 : 1;
     // does the region reach the domain boundary (then neighbours are reflected)?
-    const bool touches = X0 - kTB <= ilo || X0 - kTB + kTW > ihi - 1 || oy <= jlo || oy + kTH > jhi - 1;
+    const bool touches = X0 - Blk<MODE>::TB <= ilo || X0 - Blk<MODE>::TB + kTW > ihi - 1 || oy <= jlo || oy + kTH > jhi - 1;
 
     double av[kTSeg], bv[kTSeg], cv[kTSeg], kxc[kTSeg], kxr[kTSeg], kyc[kTSeg + 1];
 #pragma unroll
     for (int k = 0; k <= kTSeg; ++k) {
         const int ry = r0 + k, gy = oy + ry;
-        const int my = max(max(kTB - ry, ry - (kTB + kTY - 1)), 0);
+        const int my = max(max(Blk<MODE>::TB - ry, ry - (Blk<MODE>::TB + Blk<MODE>::TY - 1)), 0);
         const bool in = colin && gy >= jlo && gy < jhi && max(mxc, my) <= H;
         const long gi = gx + (long)gy * x;
         // ky of rows jlo..jhi: the face above the top interior row is read as the one-step kernels do
@@ -184,7 +190,7 @@ __device__ __forceinline__ void blocked_tile(const Geo& g, const BlockedArgs& a,
                 if (MODE == 0) {
                     const double res = cv[k] - v;
                     bv[k] = ca * bv[k] + cb * res;
-                    const bool in_tile = colin && mxc == 0 && ry >= kTB && ry < kTB + kTY && gy < jhi;
+                    const bool in_tile = colin && mxc == 0 && ry >= Blk<MODE>::TB && ry < Blk<MODE>::TB + Blk<MODE>::TY && gy < jhi;
                     if (last && in_tile && a.wr_last) {
                         const long gi = gx + (long)gy * x;
                         w[gi] = v;
@@ -208,7 +214,7 @@ __device__ __forceinline__ void blocked_tile(const Geo& g, const BlockedArgs& a,
 #pragma unroll
         for (int k = 0; k < kTSeg; ++k) {
             const int ry = r0 + k, gy = oy + ry;
-            if (ry < kTB || ry >= kTB + kTY || gy >= jhi) continue;
+            if (ry < Blk<MODE>::TB || ry >= Blk<MODE>::TB + Blk<MODE>::TY || gy >= jhi) continue;
             const long gi = gx + (long)gy * x;
             const double hv = av[k];
             const double av_ = add_now ? av[k] + bv[k] : av[k];
@@ -239,7 +245,7 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, Blocked
     double* const S1 = S0 + kTH * kTW;    // [kTH * kTW]
     if (gate_closed(done)) return;
     const GlobalRegion src{A_in, B_in, MODE == 0 ? u0 : u, kx, ky};
-    blocked_tile<MODE>(g, a, g.hd + blockIdx.x * kTX, g.hd + blockIdx.y * kTY, src, A_out, B_out, u, w, r, S0, S1,
+    blocked_tile<MODE>(g, a, g.hd + blockIdx.x * Blk<MODE>::TX, g.hd + blockIdx.y * Blk<MODE>::TY, src, A_out, B_out, u, w, r, S0, S1,
                        [] {});
 }
 
@@ -247,11 +253,11 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked(Geo g, Blocked
 // k_blocked as a persistent kernel whose tile regions arrive by TMA: one
 // block per SM walks tiles blockIdx.x, + gridDim.x, ...; one thread issues
 // the five region boxes (kTW x kTH cells of A, B, C = u0 or u, kx, ky, from
-// grid column X0 - kTB, row Y0 - kTB) of the block's NEXT tile into a
+// grid column X0 - Blk<MODE>::TB, row Y0 - Blk<MODE>::TB) of the block's NEXT tile into a
 // shared-memory staging area as soon as every thread has taken the current
 // tile's region into registers, so the loads of tile t+1 overlap the steps
-// of tile t. Boxes start on a 16-byte boundary when the halo depth and kTB
-// are even (X0 - kTB = hd - kTB + kTX bx); cells outside the array read as
+// of tile t. Boxes start on a 16-byte boundary when the halo depth and Blk<MODE>::TB
+// are even (X0 - Blk<MODE>::TB = hd - Blk<MODE>::TB + Blk<MODE>::TX bx); cells outside the array read as
 // zero and, as in k_blocked, only cells inside the interior and the margin
 // are taken. The two cells the staging lacks (kx one column right of the
 // region, ky one row above it) only feed cells beyond the valid margin.
@@ -287,11 +293,11 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked_tma(Geo g, Blo
     double* const stg = S1 + kBlockedFieldDoubles;
     unsigned long long* const bar = reinterpret_cast<unsigned long long*>(stg + 5 * kBlockedFieldDoubles);
     if (gate_closed(done)) return;
-    const int ntx = (g.x - 2 * g.hd + kTX - 1) / kTX;
-    const int ntiles = ntx * ((g.y - 2 * g.hd + kTY - 1) / kTY);
+    const int ntx = (g.x - 2 * g.hd + Blk<MODE>::TX - 1) / Blk<MODE>::TX;
+    const int ntiles = ntx * ((g.y - 2 * g.hd + Blk<MODE>::TY - 1) / Blk<MODE>::TY);
     const int tid = threadIdx.x;
     auto issue = [&](int t) {
-        const int xs = g.hd + (t % ntx) * kTX - kTB, ys = g.hd + (t / ntx) * kTY - kTB;
+        const int xs = g.hd + (t % ntx) * Blk<MODE>::TX - Blk<MODE>::TB, ys = g.hd + (t / ntx) * Blk<MODE>::TY - Blk<MODE>::TB;
         tl::mbar_expect_tx(bar, (unsigned)(5 * kBlockedFieldDoubles * sizeof(double)));
         tl::tma_load_3d(stg, &maps.a, xs, ys, 0, bar);
         tl::tma_load_3d(stg + kBlockedFieldDoubles, &maps.b, xs, ys, 0, bar);
@@ -308,7 +314,7 @@ static __global__ void __launch_bounds__(kTBThreads, 1) k_blocked_tma(Geo g, Blo
     unsigned phase = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
         tl::mbar_wait(bar, phase, err);
-        const int X0 = g.hd + (t % ntx) * kTX, Y0 = g.hd + (t / ntx) * kTY;
+        const int X0 = g.hd + (t % ntx) * Blk<MODE>::TX, Y0 = g.hd + (t / ntx) * Blk<MODE>::TY;
         blocked_tile<MODE>(g, a, X0, Y0, StagedRegion{stg}, A_out, B_out, u, w, r, S0, S1, [&] {
             __syncthreads();   // every thread holds the region: the staging is free for the next tile
             if (tid == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
@@ -347,9 +353,10 @@ constexpr size_t blocked_smem()
     return sizeof(double) * 2 * kTH * kTW;
 }
 
+template <int MODE>
 inline dim3 blocked_grid(const Geo& g)
 {
-    return dim3(tl::ceil_div(g.x - 2 * g.hd, kTX), tl::ceil_div(g.y - 2 * g.hd, kTY));
+    return dim3(tl::ceil_div(g.x - 2 * g.hd, Blk<MODE>::TX), tl::ceil_div(g.y - 2 * g.hd, Blk<MODE>::TY));
 }
 
 // End of a block of Chebyshev trips: advances the trip and coefficient

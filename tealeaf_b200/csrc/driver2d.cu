@@ -300,12 +300,12 @@ struct Run {
             if (blocking()) {
                 // trip t takes the norm when nch >= est and (t + 1) % 10 == 0
                 // (FinChebyTrip); a block ends at such a trip, at max_iters or
-                // after kTB trips
+                // after Blk<0>::TB trips
                 auto is_norm = [&](int t) { return t - tt + 1 >= est && ((t + 1) % 10) == 0; };
                 std::vector<int> starts;
                 st = loop_blocks(tt + 1, [&](int t) {
                     int L = 1;
-                    while (!(is_norm(t + L - 1) || L == kTB || t + L >= prm.max_iters)) ++L;
+                    while (!(is_norm(t + L - 1) || L == Blk<0>::TB || t + L >= prm.max_iters)) ++L;
                     const int last = t + L - 1;
                     const int norm = is_norm(last) ? 1 : 0;
                     BlockedArgs a{L, t - tt + 1, (norm || last + 1 >= prm.max_iters) ? 1 : 0, 0.0, s->d_cheby_alphas,
@@ -368,7 +368,8 @@ struct Run {
         FinPpcgW fin_w{s->d_state};
         FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
         const bool blocked = blocking();
-        const int inner_flips = blocked ? (ni + kTB - 1) / kTB : ni;   // r/sd buffer flips per outer trip
+        constexpr int TB = Blk<1>::TB;
+        const int inner_flips = blocked ? (ni + TB - 1) / TB : ni;   // r/sd buffer flips per outer trip
         auto trip = [&](int t) {
             if (t == tt) {
                 launch_cg_w2<false, false>(s, chunk, gh, fc, beta, pb[pc], pb[pc], rb[rc], chunk->w, nullptr, 0,
@@ -380,8 +381,8 @@ struct Run {
             }
             launch_cg_ur2(s, gi, alpha, chunk->u, pb[pc], rb[rc], chunk->w, done(), tl::NoFinish());
             if (blocked) {
-                for (int pp0 = 0; pp0 < ni; pp0 += kTB) {
-                    const int L = std::min(kTB, ni - pp0);
+                for (int pp0 = 0; pp0 < ni; pp0 += TB) {
+                    const int L = std::min(TB, ni - pp0);
                     const bool last = pp0 + L == ni;
                     BlockedArgs a{L, pp0, 0, chunk->theta, s->d_cheby_alphas, s->d_cheby_betas};
                     launch_blocked<1>(s, "k_blocked<ppcg>", a, sb[sc], rb[rc], sb[sc ^ 1], rb[rc ^ 1], chunk->u,

@@ -103,7 +103,7 @@ static void launch_halos(TlSuite2D* s, Chunk* chunk, int depth, const int* which
 // Runs the deferred PPCG inner steps (ppcg.c:9-61 as the reference drivers
 // call them: sd = r / theta, then per step a depth-1 halo of sd and
 // r -= A sd, u += sd, sd = a sd + b r): temporally blocked launches of up to
-// kTB steps (the fold of each step at its start, sd reflected on the fly)
+// Blk<1>::TB steps (the fold of each step at its start, sd reflected on the fly)
 // and the last step's sd update, with the same results as one launch per
 // call. With no step queued only sd = r / theta runs.
 static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
@@ -125,10 +125,11 @@ static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
     // odd count gets a closing zero-step launch, which copies the interior of
     // both and writes the depth-1 halo of sd (r's halo is left as the
     // one-step path leaves it: untouched).
-    const int launches = (n + kTB - 1) / kTB;
+    constexpr int TB = Blk<1>::TB;
+    const int launches = (n + TB - 1) / TB;
     for (int q = 0; q < launches + (launches & 1); ++q) {
-        const int pp0 = q * kTB;
-        const BlockedArgs a{std::max(0, std::min(kTB, n - pp0)), std::min(pp0, n), 0, chunk->theta,
+        const int pp0 = q * TB;
+        const BlockedArgs a{std::max(0, std::min(TB, n - pp0)), std::min(pp0, n), 0, chunk->theta,
                             s->d_cheby_alphas, s->d_cheby_betas};
         launch_blocked<1>(s, "k_blocked<ppcg>", a, chunk->sd, chunk->r, s->alt[ALT_SD], s->alt[ALT_R], chunk->u,
                           chunk->u, nullptr, nullptr, chunk->kx, chunk->ky, nullptr);
@@ -143,7 +144,7 @@ static void run_ppcg_queue(TlSuite2D* s, Chunk* chunk)
 
 // Runs the deferred Chebyshev trips (cheby.c:57-85 as the reference drivers
 // call them: per trip a depth-1 halo of u, then w = A u, r = u0 - w,
-// p = alpha p + beta r, u += p): temporally blocked launches of up to kTB
+// p = alpha p + beta r, u += p): temporally blocked launches of up to Blk<0>::TB
 // trips, each trip ending with its u += p and u reflected on the fly; the
 // last launch also writes w and r, and leaves u's halo as the call-by-call
 // sequence does (mirroring u before the last add). The launches alternate
@@ -156,7 +157,8 @@ static void run_cheby_queue(TlSuite2D* s, Chunk* chunk)
     const int n = (int)s->cq.a.size();
     if (n == 0) return;
     std::vector<int> sizes;
-    for (int left = n; left > 0; left -= kTB) sizes.push_back(std::min(kTB, left));
+    constexpr int TB = Blk<0>::TB;
+    for (int left = n; left > 0; left -= TB) sizes.push_back(std::min(TB, left));
     if (sizes.size() % 2 == 1) {
         for (int q = (int)sizes.size() - 1; q >= 0; --q) {
             if (sizes[q] >= 2) {

@@ -254,18 +254,18 @@ inline const CUtensorMap* blocked_map(TlSuite2D* s, const double* ptr)
     });
 }
 
-// The region boxes start at X0 - kTB = hd - kTB + kTX bx: an even halo depth
-// minus kTB, an even tile width and an even row length keep them on 16-byte
-// boundaries.
+// The region boxes of the staged Chebyshev kernel start at X0 - TB =
+// hd - TB + TX bx: an even halo depth minus the margin, an even tile width and
+// an even row length keep them on 16-byte boundaries.
 inline bool blocked_tma_usable(const TlSuite2D* s)
 {
-    return s->tma && (s->g.hd - kTB) % 2 == 0 && kTX % 2 == 0 && s->g.x % 2 == 0;
+    return s->tma && (s->g.hd - Blk<0>::TB) % 2 == 0 && Blk<0>::TX % 2 == 0 && s->g.x % 2 == 0;
 }
 
-// One temporally blocked launch of L <= kTB Chebyshev trips (MODE 0, C = u0)
-// or PPCG inner steps (MODE 1, C = u): the persistent TMA-staged kernel where
-// the alignment rules allow, else k_blocked (bit-identical results).
-// Internal linkage as launch_cg_w2.
+// One temporally blocked launch of L <= TB Chebyshev trips (MODE 0, C = u0)
+// or PPCG inner steps (MODE 1, C = u): for Chebyshev the persistent
+// TMA-staged kernel where the alignment rules allow, else k_blocked
+// (bit-identical results). Internal linkage as launch_cg_w2.
 template <int MODE>
 static void launch_blocked(TlSuite2D* s, const char* name, const BlockedArgs& a, const double* A_in,
                            const double* B_in, double* A_out, double* B_out, const double* C, double* u, double* w,
@@ -275,24 +275,27 @@ static void launch_blocked(TlSuite2D* s, const char* name, const BlockedArgs& a,
     if (!(attr_set & (1u << (s->device & 31)))) {
         TL_CUDA(cudaFuncSetAttribute(k_blocked<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)blocked_smem<MODE>()));
-        TL_CUDA(cudaFuncSetAttribute(k_blocked_tma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kBlockedTmaBytes));
+        if constexpr (MODE == 0)
+            TL_CUDA(cudaFuncSetAttribute(k_blocked_tma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kBlockedTmaBytes));
         attr_set |= 1u << (s->device & 31);
     }
-    const dim3 gb = blocked_grid(s->g);
-    if (blocked_tma_usable(s)) {
-        const CUtensorMap* ma = blocked_map(s, A_in);
-        const CUtensorMap* mb = blocked_map(s, B_in);
-        const CUtensorMap* mc = blocked_map(s, C);
-        const CUtensorMap* mx = blocked_map(s, kx);
-        const CUtensorMap* my = blocked_map(s, ky);
-        if (ma && mb && mc && mx && my) {
-            const BlockedMaps m{*ma, *mb, *mc, *mx, *my};
-            const long tiles = (long)gb.x * gb.y;
-            const unsigned grid = (unsigned)std::min<long>(tiles, s->sm_count);
-            TL_LAUNCH(s, name, (k_blocked_tma<MODE><<<grid, kTBThreads, kBlockedTmaBytes, s->stream>>>(
-                                   s->g, a, m, A_out, B_out, u, w, r, done, s->d_mirror + kTmaErrWord2)));
-            return;
+    const dim3 gb = blocked_grid<MODE>(s->g);
+    if constexpr (MODE == 0) {
+        if (blocked_tma_usable(s)) {
+            const CUtensorMap* ma = blocked_map(s, A_in);
+            const CUtensorMap* mb = blocked_map(s, B_in);
+            const CUtensorMap* mc = blocked_map(s, C);
+            const CUtensorMap* mx = blocked_map(s, kx);
+            const CUtensorMap* my = blocked_map(s, ky);
+            if (ma && mb && mc && mx && my) {
+                const BlockedMaps m{*ma, *mb, *mc, *mx, *my};
+                const long tiles = (long)gb.x * gb.y;
+                const unsigned grid = (unsigned)std::min<long>(tiles, s->sm_count);
+                TL_LAUNCH(s, name, (k_blocked_tma<MODE><<<grid, kTBThreads, kBlockedTmaBytes, s->stream>>>(
+                                       s->g, a, m, A_out, B_out, u, w, r, done, s->d_mirror + kTmaErrWord2)));
+                return;
+            }
         }
     }
     TL_LAUNCH(s, name, (k_blocked<MODE><<<gb, kTBThreads, blocked_smem<MODE>(), s->stream>>>(
