@@ -19,8 +19,9 @@ At N=1 the line also carries the other configurations, each driver-measured
 in the same run: `refine` (FP32 storage + FP64 refinement against FP64 at
 8192^2), `dropin_8192` and `dropin_3d_256` (the FP64 CG drop-in at 8192^2 and
 at 256^3), `adjoint` (the 3D adjoint at 256^3 with the 64^3 CPU-adjoint
-check) and `batch` (64 uneven problems in one launch against 64 sequential
-FP64 solves).
+check), `batch` (64 uneven problems in one launch against 64 sequential
+FP64 solves) and `precond` (plain CG against the Jacobi-preconditioned CGs
+at the headline size).
 Reference arm (--impl reference): the reference omp3 CPU program on this
 host's cores, bounded samples of the same workload: each timed timestep
 capped at --cpu-cap CG iterations, warm-up timesteps at --warm-cap.
@@ -398,10 +399,16 @@ def bench_b200(args, rank, world, local_rank):
         except Exception as exc:  # baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     if world == 1 and not args.no_extras:
-        line["dropin_8192"] = extra_dropin(8192, 2, peak)
-        line["dropin_3d_256"] = extra_dropin(256, 3, peak)
-        line["adjoint"] = adjoint_object(256, fd_cells=0, cpu_size=args.adjoint_cpu_size)
-        line["batch"] = bench_batch(args)
+        extras = (("dropin_8192", lambda: extra_dropin(8192, 2, peak)),
+                  ("dropin_3d_256", lambda: extra_dropin(256, 3, peak)),
+                  ("adjoint", lambda: adjoint_object(256, fd_cells=0, cpu_size=args.adjoint_cpu_size)),
+                  ("batch", lambda: bench_batch(args)),
+                  ("precond", lambda: precond_object(args.size, peak)))
+        for key, fn in extras:
+            try:
+                line[key] = fn()
+            except Exception as exc:   # an extra is reported, never required for the headline
+                line[key] = {"error": str(exc)[:300]}
     return line
 
 
