@@ -13,20 +13,24 @@
 //
 // captured once into a CUDA graph and replayed for every timestep.
 //
-// The persistent kernel walks a global list of tiles (BX threads x 2 cells x
-// tile_rows rows, every tile of every problem) with a grid-stride loop, phase
-// by phase: w = A p, then u/r update, then (only when some problem asked for
-// one) the FP64 fold and residual. Phases are separated by a grid barrier
-// whose every wait is bounded (a timeout sets an error word and all blocks
-// return). Per-problem dot products are reduced deterministically: each tile
-// writes its block sum, and the block finishing a problem's last tile of the
-// phase sums that problem's tile partials in a fixed order and runs the CG
-// scalar update (alpha, beta, replacement and stop decisions) for it.
-// Problems that have converged drop out of the tile walk.
+// The persistent kernel gives every problem its own group of blocks, sized
+// by the problem's estimated work (cells x (nx + ny), CG's iteration count
+// growing with the grid's side) and at least one block: the blocks of a
+// group walk that problem's tiles phase by phase -- w = A p, then the u/r
+// update, then (when the problem asked for one) the FP64 fold and residual
+// -- and phases are separated by the group's own barrier (an atomic counter
+// per problem; a group of one block needs none), whose waits are bounded by
+// a clock limit (a timeout sets an error word and every block returns).
+// Problems therefore advance at their own pace: nothing waits for another
+// problem's phase, and a group whose problem has converged leaves. Per-
+// problem dot products are reduced deterministically: each tile writes its
+// block sum, and the block finishing the problem's last tile of the phase
+// sums the problem's tile partials in tile order and runs the CG scalar
+// update (alpha, beta, replacement and stop decisions) for it.
 //
-// tile_rows (and the persistent grid size) come from the autotuner
-// (tl2d_batch_tune): it times a few iterations of the real batch with each
-// candidate and keeps the fastest.
+// tile_rows (and the persistent grid size the groups share) come from the
+// autotuner (tl2d_batch_tune): it times a few iterations of the real batch
+// with each candidate and keeps the fastest.
 #include "refine2d.cuh"
 #include "suite2d_impl.hpp"
 
@@ -48,6 +52,7 @@ struct BProb {
     Lay L;
     int tx, ty;      // tiles per row / column
     int tile0;       // first global tile of this problem
+    int g0, gsize;   // the problem's group: blocks g0 .. g0 + gsize - 1
     int gx, hd;      // FP64 chunk arrays: row length, halo depth
     float* f[BF_COUNT];
     double* u;
@@ -57,27 +62,30 @@ struct BProb {
 };
 
 struct BCtl {
-    unsigned count;   // grid barrier arrivals
-    unsigned gen;     // grid barrier generation
     int err;          // a barrier wait timed out
-    int upd_iter;     // last iteration in which some problem asked for a residual replacement
-    int ndone;        // problems finished
-    int iters;        // iterations the kernel ran
+    int iters;        // most iterations any problem ran
     long long limit;  // SM clocks a barrier wait may take before it gives up (kept across steps)
 };
 
-__device__ bool grid_barrier(BCtl* c)
+// A problem group's barrier state.
+struct PBar {
+    unsigned count;   // arrivals
+    unsigned gen;     // generation
+};
+
+// Barrier of the `size` blocks of one problem group (bounded waits).
+__device__ bool group_barrier(PBar* b, int size, BCtl* c)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = &c->gen;
+        volatile unsigned* vgen = &b->gen;
         const unsigned g = *vgen;
         __threadfence();
-        if (atomicAdd(&c->count, 1u) == gridDim.x - 1) {
-            atomicExch(&c->count, 0u);
+        if (atomicAdd(&b->count, 1u) == (unsigned)size - 1) {
+            atomicExch(&b->count, 0u);
             __threadfence();
-            atomicAdd(&c->gen, 1u);
+            atomicAdd(&b->gen, 1u);
         } else {
             const long long t0 = clock64();
             while (*vgen == g) {
@@ -133,20 +141,22 @@ __device__ bool tile_done(double (&v)[N], int t, const BProb& P, unsigned* ticke
     return true;
 }
 
-__global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __restrict__ P, int np,
-                                                             const int* __restrict__ tile_prob, int ntiles,
-                                                             MxState* st, unsigned* tickets, double* partials,
+__global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __restrict__ P,
+                                                             const int* __restrict__ block_prob, MxState* st,
+                                                             unsigned* tickets, double* partials, PBar* pbar,
                                                              BCtl* ctl, int max_iters)
 {
-    for (int it = 0; it < max_iters; ++it) {
+    const int b = block_prob[blockIdx.x];
+    const BProb& Q = P[b];
+    const int rank = blockIdx.x - Q.g0, G = Q.gsize, nt = Q.tx * Q.ty;
+    int it = 0;
+    for (; it < max_iters; ++it) {
+        if (mx_idle(&st[b])) break;
         // phase 1: [p = beta p + r], w = A p, p.w
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int b = tile_prob[t];
-            if (mx_idle(&st[b])) continue;
-            const BProb& Q = P[b];
-            const int lt = t - Q.tile0, tx = lt % Q.tx, ty = lt / Q.tx;
-            float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
-            float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
+        float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
+        float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
+        for (int lt = rank; lt < nt; lt += G) {
+            const int tx = lt % Q.tx, ty = lt / Q.tx;
             double v[1];
             if (it == 0)
                 v[0] = rf_w_tile<float, false>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W], Q.f[BF_KX],
@@ -155,73 +165,51 @@ __global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __rest
                 v[0] = rf_w_tile<float, true>(Q.L, tx, ty, st[b].beta, pin, pout, Q.f[BF_R], Q.f[BF_W],
                                               Q.f[BF_KX], Q.f[BF_KY]);
             double tot[1];
-            if (tile_done<1>(v, t, Q, &tickets[b], partials, tot) && threadIdx.x == 0) FinMxW{&st[b]}(tot);
+            if (tile_done<1>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0) FinMxW{&st[b]}(tot);
         }
-        if (!grid_barrier(ctl)) return;
+        if (!group_barrier(&pbar[b], G, ctl)) return;
         // phase 2: xs += alpha p, r -= alpha w, r.r; replacement requests
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int b = tile_prob[t];
-            if (mx_idle(&st[b])) continue;
-            const BProb& Q = P[b];
-            const int lt = t - Q.tile0, tx = lt % Q.tx, ty = lt / Q.tx;
-            double v[1] = {rf_ur_tile<float>(Q.L, tx, ty, st[b].alpha, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0],
-                                             Q.f[BF_R], Q.f[BF_W])};
+        for (int lt = rank; lt < nt; lt += G) {
+            double v[1] = {rf_ur_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, st[b].alpha, Q.f[BF_XS],
+                                             Q.f[(it & 1) ? BF_P1 : BF_P0], Q.f[BF_R], Q.f[BF_W])};
             double tot[1];
-            if (tile_done<1>(v, t, Q, &tickets[b], partials, tot) && threadIdx.x == 0) {
+            if (tile_done<1>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0)
                 FinMxUr{&st[b], nullptr}(tot);
-                if (st[b].upd) atomicExch(&ctl->upd_iter, it);
-            }
         }
-        if (!grid_barrier(ctl)) return;
-        if (*(volatile int*)&ctl->upd_iter == it) {
+        if (!group_barrier(&pbar[b], G, ctl)) return;
+        if (vol_read(&st[b].upd)) {
             // phase 3: fold the FP32 correction into the FP64 solution
-            for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-                const int b = tile_prob[t];
-                if (mx_no_update(&st[b])) continue;
-                const BProb& Q = P[b];
-                const int lt = t - Q.tile0;
+            for (int lt = rank; lt < nt; lt += G)
                 rf_fold_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
-            }
-            if (!grid_barrier(ctl)) return;
+            if (!group_barrier(&pbar[b], G, ctl)) return;
             // phase 4: FP64 residual replaces the FP32 one; stop tests
-            for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-                const int b = tile_prob[t];
-                if (mx_no_update(&st[b])) continue;
-                const BProb& Q = P[b];
-                const int lt = t - Q.tile0;
+            for (int lt = rank; lt < nt; lt += G) {
                 double v[2] = {0.0, 0.0};
                 rf_resid_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, Q.gx, Q.hd, Q.u, Q.u0, Q.kx, Q.ky, Q.f[BF_R], v);
                 double tot[2];
-                if (tile_done<2>(v, t, Q, &tickets[b], partials, tot) && threadIdx.x == 0) {
+                if (tile_done<2>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0)
                     FinMxRes{&st[b], nullptr}(tot);
-                    if (st[b].done) atomicAdd(&ctl->ndone, 1);
-                }
             }
-            if (!grid_barrier(ctl)) return;
-        }
-        if (*(volatile int*)&ctl->ndone >= np) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = it + 1;
-            return;
+            if (!group_barrier(&pbar[b], G, ctl)) return;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = max_iters;
+    if (rank == 0 && threadIdx.x == 0) atomicMax(&ctl->iters, it);
 }
 
-// Counts problems already converged by the setup (done before any iteration)
-// and clears the per-problem tile tickets (a step whose barrier wait gave up
-// may have left some mid-phase).
-__global__ void k_batch_count_done(const MxState* st, int np, BCtl* ctl, unsigned* tickets)
+// Clears the per-problem tile tickets and group barriers (a step whose wait
+// gave up may have left them mid-phase) and the step's control words; the
+// clock limit is kept.
+__global__ void k_batch_reset(int np, BCtl* ctl, unsigned* tickets, PBar* pbar)
 {
-    for (int b = threadIdx.x; b < np; b += blockDim.x) tickets[b] = 0u;
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int n = 0;
-    for (int b = 0; b < np; ++b) n += st[b].done ? 1 : 0;
-    ctl->count = 0;
-    ctl->gen = 0;
-    ctl->err = 0;
-    ctl->upd_iter = -1;
-    ctl->ndone = n;
-    ctl->iters = 0;
+    for (int b = threadIdx.x; b < np; b += blockDim.x) {
+        tickets[b] = 0u;
+        pbar[b].count = 0u;
+        pbar[b].gen = 0u;
+    }
+    if (threadIdx.x == 0) {
+        ctl->err = 0;
+        ctl->iters = 0;
+    }
 }
 
 }  // namespace
@@ -242,7 +230,8 @@ struct TlBatch {
     std::vector<size_t> field_off;   // per problem: offset of its first FP32 array
     std::vector<size_t> field_bytes; // per problem: bytes of one FP32 array
     BProb* d_prob = nullptr;
-    int* d_tile_prob = nullptr;
+    int* d_block_prob = nullptr;     // problem of every block of the persistent grid
+    PBar* d_pbar = nullptr;          // group barriers, one per problem
     MxState* d_st = nullptr;
     unsigned* d_tickets = nullptr;
     double* d_partials = nullptr;
@@ -253,7 +242,8 @@ struct TlBatch {
     int max_tiles = 0;               // capacity of the tile tables
     int ntiles = 0;
     int tile_rows = 0;
-    int grid_blocks = 0;
+    int grid_blocks = 0;             // blocks the groups share (co-resident limit at most)
+    int launch_blocks = 0;           // blocks launched: the sum of the group sizes
     int max_grid = 0;
     int max_iters = 0;
     cudaGraph_t graph = nullptr;
@@ -267,7 +257,7 @@ void batch_free(TlBatch* B)
 {
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
-    void* ptrs[] = {B->slab, B->d_prob, B->d_tile_prob, B->d_st, B->d_tickets, B->d_partials, B->d_ctl,
+    void* ptrs[] = {B->slab, B->d_prob, B->d_block_prob, B->d_pbar, B->d_st, B->d_tickets, B->d_partials, B->d_ctl,
                     B->rs.partials, B->rs.ticket, B->rs.out_dev, B->d_scratch_state};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -275,23 +265,65 @@ void batch_free(TlBatch* B)
     delete B;
 }
 
-// Lays out the tiles for tile_rows and uploads the problem and tile tables.
-// tile_rows > 0: that height for every problem; tile_rows == kAdaptiveRows:
-// per problem the height that gives it about one tile per block of the
-// persistent grid (between 8 and 64 rows), so a large problem still fills
-// the grid once the small ones have converged.
+// Splits the grid_blocks blocks into one group per problem, in proportion
+// to the estimated work cells x (nx + ny) (CG's iteration count grows with
+// the grid's side), at least one block and at most one per tile of the
+// problem's finest tiling; lays out the tiles for tile_rows and uploads the
+// problem and block tables. tile_rows > 0: that height for every problem;
+// kAdaptiveRows: per problem the height that gives its group about one tile
+// per block per phase (between 2 and 64 rows).
 constexpr int kAdaptiveRows = -1;
 
 bool batch_layout(TlBatch* B, int tile_rows)
 {
-    std::vector<BProb> P(B->count);
-    std::vector<int> tp;
-    for (int b = 0; b < B->count; ++b) {
+    const int n = B->count;
+    std::vector<double> work(n);
+    std::vector<long> cap(n);
+    double total = 0.0;
+    for (int b = 0; b < n; ++b) {
+        Lay L = B->lay[b];
+        work[b] = (double)L.nx * L.ny * (double)(L.nx + L.ny);
+        total += work[b];
+        L.rows = tile_rows > 0 ? tile_rows : 2;
+        const dim3 t = lay_tiles<float>(L);
+        cap[b] = (long)t.x * t.y;
+    }
+    if (B->grid_blocks < n) {
+        tl::fail(62, "batch: %d problems need at least %d blocks, the grid has %d", n, n, B->grid_blocks);
+        return false;
+    }
+    std::vector<int> size(n);
+    long used = 0;
+    for (int b = 0; b < n; ++b) {
+        size[b] = (int)std::min<long>(cap[b], std::max<long>(1, (long)(B->grid_blocks * work[b] / total)));
+        used += size[b];
+    }
+    while (used > B->grid_blocks) {   // the one-block minimum overshot: trim the largest groups
+        int k = (int)(std::max_element(size.begin(), size.end()) - size.begin());
+        --size[k];
+        --used;
+    }
+    while (used < B->grid_blocks) {   // hand the rest to the most loaded groups per block
+        int k = -1;
+        double best = 0.0;
+        for (int b = 0; b < n; ++b)
+            if (size[b] < cap[b] && work[b] / size[b] > best) {
+                best = work[b] / size[b];
+                k = b;
+            }
+        if (k < 0) break;
+        ++size[k];
+        ++used;
+    }
+    std::vector<BProb> P(n);
+    std::vector<int> bp;
+    int tiles = 0;
+    for (int b = 0; b < n; ++b) {
         Lay L = B->lay[b];
         if (tile_rows == kAdaptiveRows) {
             L.rows = 64;
             const long tx = lay_tiles<float>(L).x;
-            L.rows = (int)std::min<long>(64, std::max<long>(8, (L.ny * tx + B->grid_blocks - 1) / B->grid_blocks));
+            L.rows = (int)std::min<long>(64, std::max<long>(2, (L.ny * tx + size[b] - 1) / size[b]));
         } else {
             L.rows = tile_rows;
         }
@@ -301,7 +333,11 @@ bool batch_layout(TlBatch* B, int tile_rows)
         Q.L = L;
         Q.tx = (int)t.x;
         Q.ty = (int)t.y;
-        Q.tile0 = (int)tp.size();
+        Q.tile0 = tiles;
+        tiles += Q.tx * Q.ty;
+        Q.g0 = (int)bp.size();
+        Q.gsize = std::min(size[b], Q.tx * Q.ty);
+        for (int k = 0; k < Q.gsize; ++k) bp.push_back(b);
         Q.gx = B->suites[b]->g.x;
         Q.hd = B->suites[b]->g.hd;
         char* base = (char*)B->slab + B->field_off[b];
@@ -311,17 +347,17 @@ bool batch_layout(TlBatch* B, int tile_rows)
         Q.u0 = c->u0;
         Q.kx = c->kx;
         Q.ky = c->ky;
-        for (int k = 0; k < Q.tx * Q.ty; ++k) tp.push_back(b);
     }
-    if ((int)tp.size() > B->max_tiles) {
-        tl::fail(62, "batch: %zu tiles exceed the table capacity %d", tp.size(), B->max_tiles);
+    if (tiles > B->max_tiles) {
+        tl::fail(62, "batch: %d tiles exceed the table capacity %d", tiles, B->max_tiles);
         return false;
     }
-    B->ntiles = (int)tp.size();
+    B->ntiles = tiles;
     B->tile_rows = tile_rows;
+    B->launch_blocks = (int)bp.size();
     if (!TL_CUDA(cudaMemcpyAsync(B->d_prob, P.data(), sizeof(BProb) * P.size(), cudaMemcpyHostToDevice, B->stream)))
         return false;
-    if (!TL_CUDA(cudaMemcpyAsync(B->d_tile_prob, tp.data(), sizeof(int) * tp.size(), cudaMemcpyHostToDevice,
+    if (!TL_CUDA(cudaMemcpyAsync(B->d_block_prob, bp.data(), sizeof(int) * bp.size(), cudaMemcpyHostToDevice,
                                  B->stream)))
         return false;
     return TL_CUDA(cudaStreamSynchronize(B->stream));
@@ -361,11 +397,11 @@ void issue_step(TlBatch* B, int iter_cap, bool finish)
             s->g.x, s->g.hd, B->lay[b], c->r, c->u0, c->kx, c->ky, f[BF_KX], f[BF_KY], f[BF_R], f[BF_P0], f[BF_P1],
             f[BF_W], f[BF_XS], B->rs, FinMxInit{&B->d_st[b], 0.0, st->eps, st->max_iters, nullptr});
     }
-    k_batch_count_done<<<1, 32, 0, B->stream>>>(B->d_st, B->count, B->d_ctl, B->d_tickets);
-    void* args[] = {&B->d_prob, &B->count, &B->d_tile_prob, &B->ntiles, &B->d_st, &B->d_tickets, &B->d_partials,
-                    &B->d_ctl, &iter_cap};
+    k_batch_reset<<<1, 128, 0, B->stream>>>(B->count, B->d_ctl, B->d_tickets, B->d_pbar);
+    void* args[] = {&B->d_prob, &B->d_block_prob, &B->d_st, &B->d_tickets, &B->d_partials, &B->d_pbar, &B->d_ctl,
+                    &iter_cap};
     cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(B->grid_blocks);
+    cfg.gridDim = dim3(B->launch_blocks);
     cfg.blockDim = dim3(BX);
     cfg.stream = B->stream;
     cudaLaunchAttribute attr[1];
@@ -389,7 +425,7 @@ bool check_ctl(TlBatch* B, BCtl* out)
     if (!TL_CUDA(cudaMemcpyAsync(&h, B->d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, B->stream))) return false;
     if (!TL_CUDA(cudaStreamSynchronize(B->stream))) return false;
     if (h.err) {
-        tl::fail(63, "batch: a grid barrier of the persistent kernel timed out");
+        tl::fail(63, "batch: a group barrier of the persistent kernel timed out");
         return false;
     }
     if (out) *out = h;
@@ -462,7 +498,7 @@ TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int t
     B->max_tiles = (int)tiles;
     B->rs_capacity = std::max<long>(max_full, B->sm_count) * tl::kMaxSums;
     bool ok = TL_CUDA(cudaMalloc(&B->slab, total)) && TL_CUDA(cudaMalloc(&B->d_prob, sizeof(BProb) * count)) &&
-              TL_CUDA(cudaMalloc(&B->d_tile_prob, sizeof(int) * tiles)) &&
+              TL_CUDA(cudaMalloc(&B->d_pbar, sizeof(PBar) * count)) &&
               TL_CUDA(cudaMalloc(&B->d_st, sizeof(MxState) * count)) &&
               TL_CUDA(cudaMalloc(&B->d_tickets, sizeof(unsigned) * count)) &&
               TL_CUDA(cudaMalloc(&B->d_partials, sizeof(double) * 2 * tiles)) &&
@@ -485,6 +521,10 @@ TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int t
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, BX, 0));
     B->max_grid = std::max(1, per_sm) * B->sm_count;
     B->grid_blocks = grid_blocks > 0 ? std::min(grid_blocks, B->max_grid) : B->max_grid;
+    if (!TL_CUDA(cudaMalloc(&B->d_block_prob, sizeof(int) * B->max_grid))) {
+        batch_free(B);
+        return nullptr;
+    }
     if (!batch_layout(B, tile_rows != 0 ? tile_rows : 16)) {
         batch_free(B);
         return nullptr;
@@ -619,7 +659,7 @@ int tl2d_batch_step(TlBatch* B, TlBatchStats* stats)
     return tl::failed() ? tl::error_state().code : 0;
 }
 
-// How long (SM clocks) a grid-barrier wait of the persistent kernel may take
+// How long (SM clocks) a group-barrier wait of the persistent kernel may take
 // before it gives up; cycles <= 0 restores the default (about 2 s). The
 // limit lives in device memory, so captured graphs pick it up.
 int tl2d_batch_set_wait_limit(TlBatch* B, long long cycles)
