@@ -362,7 +362,11 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     TL_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     if (!TL_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) return;
     s->g = Geo{chunk->x, chunk->y, settings->halo_depth};
-    s->g.rows = choose_rows(chunk->x - 2 * settings->halo_depth, chunk->y - 2 * settings->halo_depth, s->sm_count);
+#ifndef TL2D_ROWS_BLOCKS
+#define TL2D_ROWS_BLOCKS TL2D_MINB
+#endif
+    s->g.rows = choose_rows(chunk->x - 2 * settings->halo_depth, chunk->y - 2 * settings->halo_depth, s->sm_count,
+                            TL2D_ROWS_BLOCKS);
     s->precond = settings->preconditioner ? 1 : 0;
     const long x = chunk->x, y = chunk->y, n = x * y;
     const long mi = settings->max_iters > 0 ? settings->max_iters : 1;

@@ -130,6 +130,9 @@ inline dim3 fused_grid(const Geo& g)
 // wave; the fewest waves whose strips are at most 64 rows (longer strips:
 // fewer boundary re-reads and reduction partials). At least 2 rows.
 // `min_blocks`: resident blocks per SM of the kernels the grid is for.
+#ifndef TL2D_MAX_ROWS
+#define TL2D_MAX_ROWS 64
+#endif
 inline int choose_rows(int nx, int ny, int sm_count, int min_blocks = TL2D_MINB)
 {
     const long slots = (long)sm_count * min_blocks;
@@ -137,7 +140,7 @@ inline int choose_rows(int nx, int ny, int sm_count, int min_blocks = TL2D_MINB)
     for (long waves = 1;; ++waves) {
         const long strips = std::max(1L, waves * slots / bx);   // strips per column band
         const int rows = std::max(2, tl::ceil_div(ny, strips));
-        if (rows <= 64) return rows;
+        if (rows <= TL2D_MAX_ROWS) return rows;
     }
 }
 // Waits for the stream and returns the published sums.

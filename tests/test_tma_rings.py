@@ -97,7 +97,7 @@ def test_blocked_region_prefetch():
 def test_w_sweep_rings(rows, stages):
     # 2D CG w sweep and the refinement w sweep: stage b holds strip rows
     # j0-1+rows*b .. ; row block b (rows j0+rows*b ..) reads stages b and b+1
-    for n in range(1, 200):
+    for n in range(1, 300):
         def reads(b):
             out = set()
             for u in range(rows):
@@ -121,7 +121,7 @@ def test_w_sweep_rings(rows, stages):
 def test_pointwise_sweep_rings(rows, stages):
     # 2D / 3D / refinement u-r updates and the PCG u/r/z sweep: stage b holds
     # units rows*b .. ; trip b reads stage b
-    for n in range(1, 200):
+    for n in range(1, 300):
         simulate(n, rows, stages,
                  np_fn=lambda n: ceil_div(n, rows),
                  loop_fn=lambda n: ceil_div(n, rows),
