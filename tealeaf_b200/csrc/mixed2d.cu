@@ -134,7 +134,7 @@ RfBuffers<T> rf_buffers(TlSuite2D* s, int fields)
     const int nx = s->g.x - 2 * s->g.hd, ny = s->g.y - 2 * s->g.hd;
     // tile rows for whole waves of the TMA sweeps (the default path; the
     // per-thread-load sweeps keep the same tiles so both give the same sums)
-    b.L = make_lay<T>(nx, ny, choose_rows(tl::ceil_div(nx, N), ny, s->sm_count, kRfTmaBlocks));
+    b.L = make_lay<T>(nx, ny, choose_rows(tl::ceil_div(nx, N), ny, s->sm_count, kRfTmaBlocks, 64));
     {
         const dim3 t = lay_tiles<T>(b.L);   // the reduction partials must fit
         if ((long)t.x * t.y * tl::kMaxSums > s->partial_capacity) b.L.rows = s->g.rows;

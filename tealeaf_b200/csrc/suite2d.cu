@@ -362,8 +362,12 @@ void run_kernel_initialise(Chunk* chunk, Settings* settings)
     TL_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     if (!TL_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) return;
     s->g = Geo{chunk->x, chunk->y, settings->halo_depth};
+// Strips are cut for 8 resident blocks per SM: two whole waves of the
+// TMA-fed CG sweeps (4 per SM) at 4096^2 (111-row strips), whose per-wave
+// ring fill and tail then weigh half as much as with one wave of the
+// 16-per-SM per-thread-load sweeps (measured: w sweep 143 against 148 us).
 #ifndef TL2D_ROWS_BLOCKS
-#define TL2D_ROWS_BLOCKS TL2D_MINB
+#define TL2D_ROWS_BLOCKS 8
 #endif
     s->g.rows = choose_rows(chunk->x - 2 * settings->halo_depth, chunk->y - 2 * settings->halo_depth, s->sm_count,
                             TL2D_ROWS_BLOCKS);

@@ -126,21 +126,22 @@ inline dim3 fused_grid(const Geo& g)
     return d;
 }
 // Rows per thread of the interior sweeps: the grid is cut into whole waves
-// of resident blocks (sm_count * TL2D_MINB) so no SM idles in a partial last
-// wave; the fewest waves whose strips are at most 64 rows (longer strips:
-// fewer boundary re-reads and reduction partials). At least 2 rows.
-// `min_blocks`: resident blocks per SM of the kernels the grid is for.
+// of resident blocks (sm_count * min_blocks) so no SM idles in a partial
+// last wave; the fewest waves whose strips are at most TL2D_MAX_ROWS rows
+// (longer strips: fewer per-strip ring fills, boundary re-reads and
+// reduction partials; `max_rows`). At least 2 rows. `min_blocks`: resident
+// blocks per SM of the kernels the grid is cut for.
 #ifndef TL2D_MAX_ROWS
-#define TL2D_MAX_ROWS 64
+#define TL2D_MAX_ROWS 128
 #endif
-inline int choose_rows(int nx, int ny, int sm_count, int min_blocks = TL2D_MINB)
+inline int choose_rows(int nx, int ny, int sm_count, int min_blocks = TL2D_MINB, int max_rows = TL2D_MAX_ROWS)
 {
     const long slots = (long)sm_count * min_blocks;
     const long bx = tl::ceil_div(nx, BX);
     for (long waves = 1;; ++waves) {
         const long strips = std::max(1L, waves * slots / bx);   // strips per column band
         const int rows = std::max(2, tl::ceil_div(ny, strips));
-        if (rows <= TL2D_MAX_ROWS) return rows;
+        if (rows <= max_rows) return rows;
     }
 }
 // Waits for the stream and returns the published sums.
