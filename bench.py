@@ -752,7 +752,19 @@ def bench_batch(args) -> dict:
             worst = max(worst, abs(s[3] / ref[3] - 1.0))
         finally:
             h.finalise()
+    # algorithmic bytes of the FP32 CG sweeps: 24 B per cell in w = A p (r, p, kx, ky -> p, w) and 24 in the
+    # u/r update (xs, p, r, w -> xs, r), per problem over its own iterations; the occasional FP64 fold and
+    # residual replacement are left out, so this is a lower bound on the bytes moved
+    alg = sum(48.0 * p.cells[0] * p.cells[1] * int(n) for p, n in zip(probs, it))
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (st.device_ms * 1e-3) / 1e9
     return {"metric": "batched_timestep_ms", "value": st.device_ms, "unit": "ms", "higher_is_better": False,
+            "roofline": {"bound": "hbm", "kernel": "k_batch_cg", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "algorithmic_bytes": alg,
+                         "bytes_rule": "48 B per cell-iteration (FP32 w and u/r sweeps), per problem over its "
+                                       "own iterations, over the batched step's device time",
+                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s"},
             "n_gpus": 1, "dtype": "f32 vectors, f64 reductions/solution", "data": "synthetic (seeded tea.in "
             "generator, batched_2d seed 5)",
             "config": {"workload": "batched_2d_%d" % len(probs), "problems": len(probs), "cells": cells,
@@ -778,7 +790,7 @@ def precond_object(n: int, peak: float, steps: int = 1, warm_cap: int = 50) -> d
     from tealeaf_b200 import problems
     from tealeaf_b200.host import Host
     out = {"workload": "dropin_2d_%d_cg, preconditioner none / jac_diag / jac_block" % n, "cells": n * n,
-           "bytes_per_cell_iteration": {"none": 96, "jac_diag": 120, "jac_block": 120}}
+           "bytes_per_cell_iteration": {"none": 96, "jac_diag": 112, "jac_block": 120}}
     for pc in ("none", "jac_diag", "jac_block"):
         prob = problems.dropin_2d(n, seed=2, steps=steps + 1, solver="cg").with_(preconditioner=pc)
         h = Host(prob.tea_in(), dims=2)

@@ -440,7 +440,7 @@ int tl2d_batch_step(TlBatch* batch, TlBatchStats* stats);
 /* Per problem of the last step: CG iterations, FP64 r.r, converged flag
  * (arrays of count; any may be NULL). */
 int tl2d_batch_results(TlBatch* batch, int* iterations, double* rr, int* converged);
-/* How many SM clocks a group-barrier wait of the persistent kernel may take
+/* How many SM clocks a phase wait of the persistent kernel may take
  * before it gives up (cycles <= 0: the default, about 2 s). A wait that gives
  * up makes every block return and tl2d_batch_step report error 63; the
  * batch's fields are then invalid until the next step. No counterpart in the

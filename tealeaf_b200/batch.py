@@ -56,7 +56,7 @@ class Batch:
         return st
 
     def set_wait_limit(self, cycles: int) -> None:
-        """SM clocks a group-barrier wait may take before it gives up (<= 0: the default)."""
+        """SM clocks a phase wait of the batch kernel may take before it gives up (<= 0: the default)."""
         rc = self.lib.tl2d_batch_set_wait_limit(self.handle, cycles)
         abi.check(self.lib, 2)
         if rc:

@@ -13,20 +13,21 @@
 //
 // captured once into a CUDA graph and replayed for every timestep.
 //
-// The persistent kernel gives every problem its own group of blocks, sized
-// by the problem's estimated work (cells x (nx + ny), CG's iteration count
-// growing with the grid's side) and at least one block: the blocks of a
-// group walk that problem's tiles phase by phase -- w = A p, then the u/r
-// update, then (when the problem asked for one) the FP64 fold and residual
-// -- and phases are separated by the group's own barrier (an atomic counter
-// per problem; a group of one block needs none), whose waits are bounded by
-// a clock limit (a timeout sets an error word and every block returns).
-// Problems therefore advance at their own pace: nothing waits for another
-// problem's phase, and a group whose problem has converged leaves. Per-
-// problem dot products are reduced deterministically: each tile writes its
-// block sum, and the block finishing the problem's last tile of the phase
-// sums the problem's tile partials in tile order and runs the CG scalar
-// update (alpha, beta, replacement and stop decisions) for it.
+// The persistent kernel starts every problem with its own group of blocks,
+// sized by the problem's estimated work (cells x (nx + ny), CG's iteration
+// count growing with the grid's side) and at least one block. Tiles are
+// handed out per problem by a monotonic counter whose index names both the
+// phase -- w = A p, then the u/r update, then (when the problem asked for
+// one) the FP64 fold and residual -- and the tile; a block whose index lies
+// in a later phase waits (bounded by a clock limit: a timeout sets an error
+// word and every block returns) until the phases before it completed.
+// Problems therefore advance at their own pace, and a block whose problem
+// converged moves to the unfinished problem with the most cells per block
+// working on it, so the long tail of the largest problems gets the whole
+// grid. Per-problem dot products are reduced deterministically: each tile
+// writes its block sum, and the block finishing the problem's last tile of
+// the phase sums the problem's tile partials in tile order and runs the CG
+// scalar update (alpha, beta, replacement and stop decisions) for it.
 //
 // tile_rows (and the persistent grid size the groups share) come from the
 // autotuner (tl2d_batch_tune): it times a few iterations of the real batch
@@ -44,7 +45,7 @@ using namespace tl2d::rf;
 namespace {
 
 constexpr int kBatchMinB = 8;                    // resident blocks per SM of the persistent kernel
-constexpr long long kBarrierLimit = 4000000000LL;   // default: SM clocks a barrier wait may take (~2 s)
+constexpr long long kWaitLimit = 4000000000LL;   // default: SM clocks a phase wait may take (~2 s)
 
 enum { BF_KX = 0, BF_KY, BF_P0, BF_P1, BF_W, BF_R, BF_XS, BF_COUNT };
 
@@ -62,47 +63,26 @@ struct BProb {
 };
 
 struct BCtl {
-    int err;          // a barrier wait timed out
+    int err;          // a phase wait timed out
     int iters;        // most iterations any problem ran
-    long long limit;  // SM clocks a barrier wait may take before it gives up (kept across steps)
+    long long limit;  // SM clocks a phase wait may take before it gives up (kept across steps)
 };
 
-// A problem group's barrier state.
-struct PBar {
-    unsigned count;   // arrivals
-    unsigned gen;     // generation
+// Per-problem schedule of the persistent kernel. Tiles are handed out by a
+// monotonic counter: index t is tile t % nt of phase t / nt, so a block that
+// takes an index knows which phase it belongs to and waits (bounded) until
+// the phases before it have completed; the block that completes a phase's
+// last tile runs the phase's scalar update, sets the next phase's kind and
+// then advances gen.
+enum { PH_W = 0, PH_UR = 1, PH_FOLD = 2, PH_RESID = 3, PH_DONE = 4 };
+struct PCtl {
+    unsigned next;    // tile indices handed out
+    unsigned gen;     // phases completed
+    int kind;         // kind of phase `gen`
+    int it;           // CG iteration of phase `gen`
+    int helpers;      // blocks that have worked on the problem
+    int pad;
 };
-
-// Barrier of the `size` blocks of one problem group (bounded waits).
-__device__ bool group_barrier(PBar* b, int size, BCtl* c)
-{
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* vgen = &b->gen;
-        const unsigned g = *vgen;
-        __threadfence();
-        if (atomicAdd(&b->count, 1u) == (unsigned)size - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*vgen == g) {
-                if (*(volatile int*)&c->err) break;
-                if (clock64() - t0 > c->limit) {
-                    atomicExch(&c->err, 1);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        ok = *(volatile int*)&c->err == 0;
-    }
-    __syncthreads();
-    return ok != 0;
-}
 
 // Block sum of this thread's values; returns true in every thread of the
 // block that completed problem b's last tile of the phase, with the
@@ -141,70 +121,146 @@ __device__ bool tile_done(double (&v)[N], int t, const BProb& P, unsigned* ticke
     return true;
 }
 
-__global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __restrict__ P,
-                                                             const int* __restrict__ block_prob, MxState* st,
-                                                             unsigned* tickets, double* partials, PBar* pbar,
-                                                             BCtl* ctl, int max_iters)
+// The not-converged problem with the most cells per block that has worked
+// on it (warp 0 scans; lane 0 counts itself in and returns it), or -1.
+__device__ int pick_problem(const BProb* __restrict__ P, PCtl* pc, int np)
 {
-    const int b = block_prob[blockIdx.x];
-    const BProb& Q = P[b];
-    const int rank = blockIdx.x - Q.g0, G = Q.gsize, nt = Q.tx * Q.ty;
-    int it = 0;
-    for (; it < max_iters; ++it) {
-        if (mx_idle(&st[b])) break;
-        // phase 1: [p = beta p + r], w = A p, p.w
-        float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
-        float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
-        for (int lt = rank; lt < nt; lt += G) {
-            const int tx = lt % Q.tx, ty = lt / Q.tx;
-            double v[1];
-            if (it == 0)
-                v[0] = rf_w_tile<float, false>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W], Q.f[BF_KX],
-                                               Q.f[BF_KY]);
-            else
-                v[0] = rf_w_tile<float, true>(Q.L, tx, ty, st[b].beta, pin, pout, Q.f[BF_R], Q.f[BF_W],
-                                              Q.f[BF_KX], Q.f[BF_KY]);
-            double tot[1];
-            if (tile_done<1>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0) FinMxW{&st[b]}(tot);
-        }
-        if (!group_barrier(&pbar[b], G, ctl)) return;
-        // phase 2: xs += alpha p, r -= alpha w, r.r; replacement requests
-        for (int lt = rank; lt < nt; lt += G) {
-            double v[1] = {rf_ur_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, st[b].alpha, Q.f[BF_XS],
-                                             Q.f[(it & 1) ? BF_P1 : BF_P0], Q.f[BF_R], Q.f[BF_W])};
-            double tot[1];
-            if (tile_done<1>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0)
-                FinMxUr{&st[b], nullptr}(tot);
-        }
-        if (!group_barrier(&pbar[b], G, ctl)) return;
-        if (vol_read(&st[b].upd)) {
-            // phase 3: fold the FP32 correction into the FP64 solution
-            for (int lt = rank; lt < nt; lt += G)
-                rf_fold_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
-            if (!group_barrier(&pbar[b], G, ctl)) return;
-            // phase 4: FP64 residual replaces the FP32 one; stop tests
-            for (int lt = rank; lt < nt; lt += G) {
-                double v[2] = {0.0, 0.0};
-                rf_resid_tile<float>(Q.L, lt % Q.tx, lt / Q.tx, Q.gx, Q.hd, Q.u, Q.u0, Q.kx, Q.ky, Q.f[BF_R], v);
-                double tot[2];
-                if (tile_done<2>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0)
-                    FinMxRes{&st[b], nullptr}(tot);
-            }
-            if (!group_barrier(&pbar[b], G, ctl)) return;
+    const int lane = threadIdx.x & 31;
+    double best = -1.0;
+    int who = -1;
+    for (int b = lane; b < np; b += 32) {
+        if (vol_read(&pc[b].kind) == PH_DONE) continue;
+        const double score = (double)P[b].L.nx * P[b].L.ny / (double)(vol_read(&pc[b].helpers) + 1);
+        if (score > best) {
+            best = score;
+            who = b;
         }
     }
-    if (rank == 0 && threadIdx.x == 0) atomicMax(&ctl->iters, it);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int ow = __shfl_down_sync(0xffffffffu, who, o);
+        if (ob > best) {
+            best = ob;
+            who = ow;
+        }
+    }
+    if (lane == 0 && who >= 0) atomicAdd(&pc[who].helpers, 1);
+    return who;
 }
 
-// Clears the per-problem tile tickets and group barriers (a step whose wait
-// gave up may have left them mid-phase) and the step's control words; the
-// clock limit is kept.
-__global__ void k_batch_reset(int np, BCtl* ctl, unsigned* tickets, PBar* pbar)
+__global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __restrict__ P, int np,
+                                                             const int* __restrict__ block_prob, MxState* st,
+                                                             unsigned* tickets, double* partials, PCtl* pc,
+                                                             BCtl* ctl, int max_iters)
+{
+    __shared__ int sh_b, sh_go;
+    __shared__ unsigned sh_t;
+    int b = block_prob[blockIdx.x];
+    for (;;) {
+        // a problem to work on: the block's own, then the most loaded one left
+        if (threadIdx.x < 32) {
+            int nb = b;
+            if (vol_read(&pc[b].kind) == PH_DONE) nb = pick_problem(P, pc, np);
+            if (threadIdx.x == 0) sh_b = nb;
+        }
+        __syncthreads();
+        b = sh_b;
+        if (b < 0) return;
+        const BProb& Q = P[b];
+        const unsigned nt = (unsigned)(Q.tx * Q.ty);
+        // take a tile index and wait until its phase is the current one
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(&pc[b].next, 1u);
+            const unsigned phase = t / nt;
+            int go = 1;   // 1: work, 0: the problem ended, -1: error
+            const long long t0 = clock64();
+            while (*(volatile unsigned*)&pc[b].gen < phase) {
+                if (vol_read(&pc[b].kind) == PH_DONE) {
+                    go = 0;
+                    break;
+                }
+                if (vol_read(&ctl->err)) {
+                    go = -1;
+                    break;
+                }
+                if (clock64() - t0 > ctl->limit) {
+                    atomicExch(&ctl->err, 1);
+                    go = -1;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+            if (go == 1 && vol_read(&pc[b].kind) == PH_DONE) go = 0;
+            sh_t = t % nt;
+            sh_go = go;
+        }
+        __syncthreads();
+        const int go = sh_go;
+        const int lt = (int)sh_t;
+        __syncthreads();   // sh_* are rewritten by the next pass
+        if (go < 0) return;
+        if (go == 0) continue;
+        const int tx = lt % Q.tx, ty = lt / Q.tx;
+        const int kind = vol_read(&pc[b].kind), it = vol_read(&pc[b].it);
+        double v[2] = {0.0, 0.0};
+        if (kind == PH_W) {
+            float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
+            float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
+            v[0] = it == 0 ? rf_w_tile<float, false>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W], Q.f[BF_KX],
+                                                      Q.f[BF_KY])
+                           : rf_w_tile<float, true>(Q.L, tx, ty, st[b].beta, pin, pout, Q.f[BF_R], Q.f[BF_W],
+                                                     Q.f[BF_KX], Q.f[BF_KY]);
+        } else if (kind == PH_UR) {
+            v[0] = rf_ur_tile<float>(Q.L, tx, ty, st[b].alpha, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0], Q.f[BF_R],
+                                     Q.f[BF_W]);
+        } else if (kind == PH_FOLD) {
+            rf_fold_tile<float>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
+        } else {
+            rf_resid_tile<float>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.u0, Q.kx, Q.ky, Q.f[BF_R], v);
+        }
+        double tot[2];
+        if (tile_done<2>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0) {
+            // the phase is complete: its scalar update, then the next phase
+            int next = PH_W, nit = it;
+            if (kind == PH_W) {
+                FinMxW{&st[b]}(tot);
+                next = PH_UR;
+            } else if (kind == PH_UR) {
+                FinMxUr{&st[b], nullptr}(tot);
+                if (st[b].upd) next = PH_FOLD;
+                else nit = it + 1;
+            } else if (kind == PH_FOLD) {
+                next = PH_RESID;
+            } else {
+                FinMxRes{&st[b], nullptr}(tot);
+                nit = it + 1;
+                if (st[b].done) next = PH_DONE;
+            }
+            if (next == PH_W && nit >= max_iters) next = PH_DONE;
+            if (next == PH_DONE) atomicMax(&ctl->iters, nit);
+            pc[b].it = nit;
+            pc[b].kind = next;
+            __threadfence();
+            atomicAdd(&pc[b].gen, 1u);
+        }
+    }
+}
+
+// Clears the per-problem tile tickets and schedules (a step whose wait gave
+// up may have left them mid-phase) and the step's control words; the clock
+// limit is kept. A problem the setup already converged starts done.
+__global__ void k_batch_reset(const BProb* __restrict__ P, const MxState* st, int np, BCtl* ctl,
+                              unsigned* tickets, PCtl* pc)
 {
     for (int b = threadIdx.x; b < np; b += blockDim.x) {
         tickets[b] = 0u;
-        pbar[b].count = 0u;
-        pbar[b].gen = 0u;
+        pc[b].next = 0u;
+        pc[b].gen = 0u;
+        pc[b].kind = st[b].done ? PH_DONE : PH_W;
+        pc[b].it = 0;
+        pc[b].helpers = P[b].gsize;
     }
     if (threadIdx.x == 0) {
         ctl->err = 0;
@@ -231,7 +287,7 @@ struct TlBatch {
     std::vector<size_t> field_bytes; // per problem: bytes of one FP32 array
     BProb* d_prob = nullptr;
     int* d_block_prob = nullptr;     // problem of every block of the persistent grid
-    PBar* d_pbar = nullptr;          // group barriers, one per problem
+    PCtl* d_pctl = nullptr;          // per-problem schedules
     MxState* d_st = nullptr;
     unsigned* d_tickets = nullptr;
     double* d_partials = nullptr;
@@ -257,7 +313,7 @@ void batch_free(TlBatch* B)
 {
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
-    void* ptrs[] = {B->slab, B->d_prob, B->d_block_prob, B->d_pbar, B->d_st, B->d_tickets, B->d_partials, B->d_ctl,
+    void* ptrs[] = {B->slab, B->d_prob, B->d_block_prob, B->d_pctl, B->d_st, B->d_tickets, B->d_partials, B->d_ctl,
                     B->rs.partials, B->rs.ticket, B->rs.out_dev, B->d_scratch_state};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -397,9 +453,9 @@ void issue_step(TlBatch* B, int iter_cap, bool finish)
             s->g.x, s->g.hd, B->lay[b], c->r, c->u0, c->kx, c->ky, f[BF_KX], f[BF_KY], f[BF_R], f[BF_P0], f[BF_P1],
             f[BF_W], f[BF_XS], B->rs, FinMxInit{&B->d_st[b], 0.0, st->eps, st->max_iters, nullptr});
     }
-    k_batch_reset<<<1, 128, 0, B->stream>>>(B->count, B->d_ctl, B->d_tickets, B->d_pbar);
-    void* args[] = {&B->d_prob, &B->d_block_prob, &B->d_st, &B->d_tickets, &B->d_partials, &B->d_pbar, &B->d_ctl,
-                    &iter_cap};
+    k_batch_reset<<<1, 128, 0, B->stream>>>(B->d_prob, B->d_st, B->count, B->d_ctl, B->d_tickets, B->d_pctl);
+    void* args[] = {&B->d_prob, &B->count, &B->d_block_prob, &B->d_st, &B->d_tickets, &B->d_partials, &B->d_pctl,
+                    &B->d_ctl, &iter_cap};
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(B->launch_blocks);
     cfg.blockDim = dim3(BX);
@@ -425,7 +481,7 @@ bool check_ctl(TlBatch* B, BCtl* out)
     if (!TL_CUDA(cudaMemcpyAsync(&h, B->d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, B->stream))) return false;
     if (!TL_CUDA(cudaStreamSynchronize(B->stream))) return false;
     if (h.err) {
-        tl::fail(63, "batch: a group barrier of the persistent kernel timed out");
+        tl::fail(63, "batch: a phase wait of the persistent kernel timed out");
         return false;
     }
     if (out) *out = h;
@@ -498,7 +554,7 @@ TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int t
     B->max_tiles = (int)tiles;
     B->rs_capacity = std::max<long>(max_full, B->sm_count) * tl::kMaxSums;
     bool ok = TL_CUDA(cudaMalloc(&B->slab, total)) && TL_CUDA(cudaMalloc(&B->d_prob, sizeof(BProb) * count)) &&
-              TL_CUDA(cudaMalloc(&B->d_pbar, sizeof(PBar) * count)) &&
+              TL_CUDA(cudaMalloc(&B->d_pctl, sizeof(PCtl) * count)) &&
               TL_CUDA(cudaMalloc(&B->d_st, sizeof(MxState) * count)) &&
               TL_CUDA(cudaMalloc(&B->d_tickets, sizeof(unsigned) * count)) &&
               TL_CUDA(cudaMalloc(&B->d_partials, sizeof(double) * 2 * tiles)) &&
@@ -515,7 +571,7 @@ TlBatch* tl2d_batch_create(Chunk** chunks, Settings** settings, int count, int t
     TL_CUDA(cudaMemsetAsync(B->rs.ticket, 0, 256, B->stream));
     TL_CUDA(cudaMemsetAsync(B->d_tickets, 0, sizeof(unsigned) * count, B->stream));
     TL_CUDA(cudaMemsetAsync(B->d_ctl, 0, sizeof(BCtl), B->stream));
-    static const long long default_limit = kBarrierLimit;
+    static const long long default_limit = kWaitLimit;
     TL_CUDA(cudaMemcpyAsync(&B->d_ctl->limit, &default_limit, sizeof(long long), cudaMemcpyHostToDevice, B->stream));
     int per_sm = 0;
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, BX, 0));
@@ -659,7 +715,7 @@ int tl2d_batch_step(TlBatch* B, TlBatchStats* stats)
     return tl::failed() ? tl::error_state().code : 0;
 }
 
-// How long (SM clocks) a group-barrier wait of the persistent kernel may take
+// How long (SM clocks) a phase wait of the persistent kernel may take
 // before it gives up; cycles <= 0 restores the default (about 2 s). The
 // limit lives in device memory, so captured graphs pick it up.
 int tl2d_batch_set_wait_limit(TlBatch* B, long long cycles)
@@ -668,7 +724,7 @@ int tl2d_batch_set_wait_limit(TlBatch* B, long long cycles)
         tl::fail(64, "tl2d_batch_set_wait_limit: null batch");
         return 64;
     }
-    const long long v = cycles > 0 ? cycles : kBarrierLimit;
+    const long long v = cycles > 0 ? cycles : kWaitLimit;
     if (!TL_CUDA(cudaMemcpyAsync(&B->d_ctl->limit, &v, sizeof(long long), cudaMemcpyHostToDevice, B->stream)) ||
         !TL_CUDA(cudaStreamSynchronize(B->stream)))
         return tl::error_state().code;

@@ -7,7 +7,7 @@ These tests drive each failure on purpose and check what is reported:
 
 * a bounded device wait that runs out: the shared-memory barrier wait of the
   TMA-fed sweeps, on a barrier that nothing completes (no copy in flight), and
-  the persistent batch kernel's group barrier with a limit too short to be met;
+  the persistent batch kernel's phase wait with a limit too short to be met;
   the kernel returns, the host reports the error, the context stays usable;
 * host-side errors: max_iters above what the chunk was initialised with
   (error 32), a NaN in the density field, an iteration cap that stops the
@@ -70,12 +70,12 @@ def test_bounded_wait_rejects_a_bad_limit():
         h.finalise()
 
 
-def test_batch_barrier_timeout_is_reported_and_the_batch_recovers():
+def test_batch_phase_wait_timeout_is_reported_and_the_batch_recovers():
     probs = problems.batched_2d(4, seed=11, lo=64, hi=200, steps=2)
     b = Batch([p.tea_in() for p in probs])
     try:
-        b.set_wait_limit(1)          # one SM clock: the first barrier wait runs out
-        with pytest.raises(abi.SuiteError, match="group barrier of the persistent kernel timed out"):
+        b.set_wait_limit(1)          # one SM clock: the first phase wait runs out
+        with pytest.raises(abi.SuiteError, match="phase wait of the persistent kernel timed out"):
             b.step()
         b.set_wait_limit(0)          # back to the default limit
         st = b.step()
