@@ -15,19 +15,21 @@
 //
 // The persistent kernel starts every problem with its own group of blocks,
 // sized by the problem's estimated work (cells x (nx + ny), CG's iteration
-// count growing with the grid's side) and at least one block. Tiles are
-// handed out per problem by a monotonic counter whose index names both the
-// phase -- w = A p, then the u/r update, then (when the problem asked for
-// one) the FP64 fold and residual -- and the tile; a block whose index lies
-// in a later phase waits (bounded by a clock limit: a timeout sets an error
-// word and every block returns) until the phases before it completed.
-// Problems therefore advance at their own pace, and a block whose problem
-// converged moves to the unfinished problem with the most cells per block
-// working on it, so the long tail of the largest problems gets the whole
-// grid. Per-problem dot products are reduced deterministically: each tile
-// writes its block sum, and the block finishing the problem's last tile of
-// the phase sums the problem's tile partials in tile order and runs the CG
-// scalar update (alpha, beta, replacement and stop decisions) for it.
+// count growing with the grid's side) and at least one block. Each problem
+// walks its phases -- w = A p, then the u/r update, then (when the problem
+// asked for one) the FP64 fold and residual -- with its tiles handed out by
+// an atomic counter per problem; a block whose problem has no tile left in
+// its open phase takes one from the problem with the most tiles left, so no
+// block idles at a problem's phase boundary while other problems have work,
+// and the largest problems get the whole grid once the small ones have
+// converged. A block holds at most one tile and never waits while holding
+// it; only a block that finds no tile anywhere polls, bounded by a clock
+// limit (a timeout sets an error word and the blocks return). Per-problem
+// dot products are reduced deterministically: each tile writes its block
+// sum, and the block finishing the problem's last tile of the phase sums
+// the problem's tile partials in tile order and runs the CG scalar update
+// (alpha, beta, replacement and stop decisions) for it, then opens the
+// problem's next phase.
 //
 // tile_rows (and the persistent grid size the groups share) come from the
 // autotuner (tl2d_batch_tune): it times a few iterations of the real batch
@@ -63,26 +65,33 @@ struct BProb {
 };
 
 struct BCtl {
-    int err;          // a phase wait timed out
+    int err;          // a block found no tile to work on for longer than the limit
     int iters;        // most iterations any problem ran
-    long long limit;  // SM clocks a phase wait may take before it gives up (kept across steps)
+    long long limit;  // SM clocks a block may go without a tile before it gives up (kept across steps)
 };
 
-// Per-problem schedule of the persistent kernel. Tiles are handed out by a
-// monotonic counter: index t is tile t % nt of phase t / nt, so a block that
-// takes an index knows which phase it belongs to and waits (bounded) until
-// the phases before it have completed; the block that completes a phase's
-// last tile runs the phase's scalar update, sets the next phase's kind and
-// then advances gen.
+// Per-problem schedule of the persistent kernel. One 64-bit word holds the
+// open phase (high half) and the tiles handed out in it (low half): a block
+// takes tile t with one atomic add and holds a tile of that phase exactly
+// when t < tiles per phase. The block completing the phase's last tile runs
+// the phase's scalar update, writes the next phase's kind and iteration and
+// opens it by swapping in (phase + 1) << 32; a finished problem's low half
+// is kClosed, so every later draw comes back void. A block never waits
+// while it holds a tile: when its problem has no tile left in the open
+// phase it takes one from the problem with the most tiles left, and only
+// when no problem has one does it poll (bounded by the clock limit).
 enum { PH_W = 0, PH_UR = 1, PH_FOLD = 2, PH_RESID = 3, PH_DONE = 4 };
+constexpr unsigned kClosed = 0x40000000u;
 struct PCtl {
-    unsigned next;    // tile indices handed out
-    unsigned gen;     // phases completed
-    int kind;         // kind of phase `gen`
-    int it;           // CG iteration of phase `gen`
-    int helpers;      // blocks that have worked on the problem
-    int pad;
+    unsigned long long word;   // open phase << 32 | tiles handed out in it
+    int kind;                  // kind of the open phase
+    int it;                    // CG iteration of the open phase
 };
+
+__device__ __forceinline__ unsigned long long vol_read64(const unsigned long long* p)
+{
+    return *(volatile const unsigned long long*)p;
+}
 
 // Block sum of this thread's values; returns true in every thread of the
 // block that completed problem b's last tile of the phase, with the
@@ -108,9 +117,20 @@ __device__ bool tile_done(double (&v)[N], int t, const BProb& P, unsigned* ticke
 #pragma unroll
     for (int r = 0; r < N; ++r) s[r] = 0.0;
     const int nt = P.tx * P.ty;
-    for (int k = threadIdx.x; k < nt; k += BX)
+    // partials k = tid, tid + BX, ... added in that order; four loads in flight
+    for (int k0 = threadIdx.x; k0 < nt; k0 += 4 * BX) {
+        double q[4][N];
 #pragma unroll
-        for (int r = 0; r < N; ++r) s[r] += *(volatile double*)&partials[(long)(P.tile0 + k) * 2 + r];
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int r = 0; r < N; ++r)
+                q[u][r] = k0 + u * BX < nt ? __ldcg(&partials[(long)(P.tile0 + k0 + u * BX) * 2 + r]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k0 + u * BX < nt)
+#pragma unroll
+                for (int r = 0; r < N; ++r) s[r] += q[u][r];
+    }
     __syncthreads();
     tl::block_sum<N, BX>(s, smem);
     if (threadIdx.x == 0) {
@@ -121,32 +141,48 @@ __device__ bool tile_done(double (&v)[N], int t, const BProb& P, unsigned* ticke
     return true;
 }
 
-// The not-converged problem with the most cells per block that has worked
-// on it (warp 0 scans; lane 0 counts itself in and returns it), or -1.
-__device__ int pick_problem(const BProb* __restrict__ P, PCtl* pc, int np)
+// Warp 0: the unfinished problem with the most tiles not yet handed out in
+// its open phase (the lowest index among equals); -1 when every problem has
+// finished, -2 when none has a tile to hand out right now.
+__device__ int find_work(const BProb* __restrict__ P, PCtl* pc, int np)
 {
     const int lane = threadIdx.x & 31;
-    double best = -1.0;
-    int who = -1;
+    int best = 0, who = -1;
+    bool live = false;
     for (int b = lane; b < np; b += 32) {
-        if (vol_read(&pc[b].kind) == PH_DONE) continue;
-        const double score = (double)P[b].L.nx * P[b].L.ny / (double)(vol_read(&pc[b].helpers) + 1);
-        if (score > best) {
-            best = score;
+        const unsigned lo = (unsigned)vol_read64(&pc[b].word);
+        if (lo >= kClosed) continue;
+        live = true;
+        const unsigned nt = (unsigned)(P[b].tx * P[b].ty);
+        if (lo < nt && (int)(nt - lo) > best) {
+            best = (int)(nt - lo);
             who = b;
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int ob = __shfl_down_sync(0xffffffffu, best, o);
         const int ow = __shfl_down_sync(0xffffffffu, who, o);
-        if (ob > best) {
+        if (ob > best || (ob == best && ow >= 0 && (who < 0 || ow < who))) {
             best = ob;
             who = ow;
         }
     }
-    if (lane == 0 && who >= 0) atomicAdd(&pc[who].helpers, 1);
-    return who;
+    who = __shfl_sync(0xffffffffu, who, 0);
+    live = __any_sync(0xffffffffu, live);
+    return who >= 0 ? who : (live ? -2 : -1);
+}
+
+// Thread 0: draws a tile of problem b; true with its index in t and the
+// phase in g when one was left in the open phase.
+__device__ __forceinline__ bool draw(const BProb* __restrict__ P, PCtl* pc, int b, int& t, unsigned& g)
+{
+    const unsigned nt = (unsigned)(P[b].tx * P[b].ty);
+    const unsigned long long old = atomicAdd(&pc[b].word, 1ull);
+    if ((unsigned)old >= nt) return false;
+    t = (int)(unsigned)old;
+    g = (unsigned)(old >> 32);
+    return true;
 }
 
 __global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __restrict__ P, int np,
@@ -154,75 +190,82 @@ __global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __rest
                                                              unsigned* tickets, double* partials, PCtl* pc,
                                                              BCtl* ctl, int max_iters)
 {
-    __shared__ int sh_b, sh_go;
-    __shared__ unsigned sh_t;
+    __shared__ int sh_go, sh_b, sh_t, sh_kind, sh_it;
+    __shared__ unsigned sh_g;
+    __shared__ double sh_coef;
     int b = block_prob[blockIdx.x];
+    long long idle0 = clock64();
     for (;;) {
-        // a problem to work on: the block's own, then the most loaded one left
         if (threadIdx.x < 32) {
-            int nb = b;
-            if (vol_read(&pc[b].kind) == PH_DONE) nb = pick_problem(P, pc, np);
-            if (threadIdx.x == 0) sh_b = nb;
-        }
-        __syncthreads();
-        b = sh_b;
-        if (b < 0) return;
-        const BProb& Q = P[b];
-        const unsigned nt = (unsigned)(Q.tx * Q.ty);
-        // take a tile index and wait until its phase is the current one
-        if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(&pc[b].next, 1u);
-            const unsigned phase = t / nt;
-            int go = 1;   // 1: work, 0: the problem ended, -1: error
-            const long long t0 = clock64();
-            while (*(volatile unsigned*)&pc[b].gen < phase) {
-                if (vol_read(&pc[b].kind) == PH_DONE) {
-                    go = 0;
-                    break;
+            int go = 0, t = 0;   // 1: a tile of problem b, 0: none right now, -1: leave
+            unsigned g = 0;
+            if (threadIdx.x == 0 && (unsigned)vol_read64(&pc[b].word) < (unsigned)(P[b].tx * P[b].ty))
+                go = draw(P, pc, b, t, g) ? 1 : 0;
+            go = __shfl_sync(0xffffffffu, go, 0);
+            if (go == 0) {
+                const int nb = find_work(P, pc, np);
+                if (threadIdx.x == 0) {
+                    if (nb == -1) {
+                        go = -1;
+                    } else if (nb >= 0 && draw(P, pc, nb, t, g)) {
+                        go = 1;
+                        b = nb;
+                    }
                 }
-                if (vol_read(&ctl->err)) {
-                    go = -1;
-                    break;
-                }
-                if (clock64() - t0 > ctl->limit) {
-                    atomicExch(&ctl->err, 1);
-                    go = -1;
-                    break;
-                }
-                __nanosleep(64);
             }
-            __threadfence();
-            if (go == 1 && vol_read(&pc[b].kind) == PH_DONE) go = 0;
-            sh_t = t % nt;
-            sh_go = go;
+            if (threadIdx.x == 0) {
+                if (go == 1) {
+                    __threadfence();   // the phase's kind, scalars and fields are those its opener published
+                    idle0 = clock64();
+                    const int kind = vol_read(&pc[b].kind);
+                    sh_kind = kind;
+                    sh_it = vol_read(&pc[b].it);
+                    sh_coef = kind == PH_W ? __ldcg(&st[b].beta) : kind == PH_UR ? __ldcg(&st[b].alpha) : 0.0;
+                } else if (go == 0) {
+                    if (vol_read(&ctl->err)) {
+                        go = -1;
+                    } else if (clock64() - idle0 > ctl->limit) {
+                        atomicExch(&ctl->err, 1);
+                        go = -1;
+                    } else {
+                        __nanosleep(64);
+                    }
+                }
+                sh_go = go;
+                sh_b = b;
+                sh_t = t;
+                sh_g = g;
+            }
         }
         __syncthreads();
-        const int go = sh_go;
-        const int lt = (int)sh_t;
+        const int go = sh_go, lt = sh_t, kind = sh_kind, it = sh_it;
+        const unsigned g = sh_g;
+        const double coef = sh_coef;
+        b = sh_b;
         __syncthreads();   // sh_* are rewritten by the next pass
         if (go < 0) return;
         if (go == 0) continue;
+        const BProb& Q = P[b];
         const int tx = lt % Q.tx, ty = lt / Q.tx;
-        const int kind = vol_read(&pc[b].kind), it = vol_read(&pc[b].it);
         double v[2] = {0.0, 0.0};
         if (kind == PH_W) {
             float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
             float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
-            v[0] = it == 0 ? rf_w_tile<float, false>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W], Q.f[BF_KX],
-                                                      Q.f[BF_KY])
-                           : rf_w_tile<float, true>(Q.L, tx, ty, st[b].beta, pin, pout, Q.f[BF_R], Q.f[BF_W],
-                                                     Q.f[BF_KX], Q.f[BF_KY]);
+            v[0] = it == 0 ? rf_w_tile<float, false, true>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W],
+                                                            Q.f[BF_KX], Q.f[BF_KY])
+                           : rf_w_tile<float, true, true>(Q.L, tx, ty, coef, pin, pout, Q.f[BF_R], Q.f[BF_W],
+                                                           Q.f[BF_KX], Q.f[BF_KY]);
         } else if (kind == PH_UR) {
-            v[0] = rf_ur_tile<float>(Q.L, tx, ty, st[b].alpha, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0], Q.f[BF_R],
-                                     Q.f[BF_W]);
+            v[0] = rf_ur_tile<float, true>(Q.L, tx, ty, coef, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0], Q.f[BF_R],
+                                           Q.f[BF_W]);
         } else if (kind == PH_FOLD) {
-            rf_fold_tile<float>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
+            rf_fold_tile<float, true>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
         } else {
-            rf_resid_tile<float>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.u0, Q.kx, Q.ky, Q.f[BF_R], v);
+            rf_resid_tile<float, true>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.u0, Q.kx, Q.ky, Q.f[BF_R], v);
         }
         double tot[2];
         if (tile_done<2>(v, Q.tile0 + lt, Q, &tickets[b], partials, tot) && threadIdx.x == 0) {
-            // the phase is complete: its scalar update, then the next phase
+            // the phase is complete: its scalar update, then open the next phase
             int next = PH_W, nit = it;
             if (kind == PH_W) {
                 FinMxW{&st[b]}(tot);
@@ -243,24 +286,22 @@ __global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __rest
             pc[b].it = nit;
             pc[b].kind = next;
             __threadfence();
-            atomicAdd(&pc[b].gen, 1u);
+            atomicExch(&pc[b].word, ((unsigned long long)(g + 1u) << 32) | (next == PH_DONE ? kClosed : 0u));
         }
     }
 }
 
-// Clears the per-problem tile tickets and schedules (a step whose wait gave
-// up may have left them mid-phase) and the step's control words; the clock
-// limit is kept. A problem the setup already converged starts done.
-__global__ void k_batch_reset(const BProb* __restrict__ P, const MxState* st, int np, BCtl* ctl,
-                              unsigned* tickets, PCtl* pc)
+// Clears the per-problem tile tickets and schedules (a step that gave up may
+// have left them mid-phase) and the step's control words; the clock limit is
+// kept. A problem the setup already converged starts closed.
+__global__ void k_batch_reset(const MxState* st, int np, BCtl* ctl, unsigned* tickets, PCtl* pc)
 {
     for (int b = threadIdx.x; b < np; b += blockDim.x) {
+        const bool done = st[b].done != 0;
         tickets[b] = 0u;
-        pc[b].next = 0u;
-        pc[b].gen = 0u;
-        pc[b].kind = st[b].done ? PH_DONE : PH_W;
+        pc[b].word = done ? kClosed : 0ull;
+        pc[b].kind = done ? PH_DONE : PH_W;
         pc[b].it = 0;
-        pc[b].helpers = P[b].gsize;
     }
     if (threadIdx.x == 0) {
         ctl->err = 0;
@@ -453,7 +494,7 @@ void issue_step(TlBatch* B, int iter_cap, bool finish)
             s->g.x, s->g.hd, B->lay[b], c->r, c->u0, c->kx, c->ky, f[BF_KX], f[BF_KY], f[BF_R], f[BF_P0], f[BF_P1],
             f[BF_W], f[BF_XS], B->rs, FinMxInit{&B->d_st[b], 0.0, st->eps, st->max_iters, nullptr});
     }
-    k_batch_reset<<<1, 128, 0, B->stream>>>(B->d_prob, B->d_st, B->count, B->d_ctl, B->d_tickets, B->d_pctl);
+    k_batch_reset<<<1, 128, 0, B->stream>>>(B->d_st, B->count, B->d_ctl, B->d_tickets, B->d_pctl);
     void* args[] = {&B->d_prob, &B->count, &B->d_block_prob, &B->d_st, &B->d_tickets, &B->d_partials, &B->d_pctl,
                     &B->d_ctl, &iter_cap};
     cudaLaunchConfig_t cfg{};

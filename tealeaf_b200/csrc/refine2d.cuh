@@ -211,6 +211,22 @@ __device__ __forceinline__ Cells<T> ld(const T* p)
     c.v = *reinterpret_cast<const typename Pack<T>::V*>(p);
     return c;
 }
+// Loads for arrays that other blocks of the same (persistent) launch write
+// between phases: CG = true reads through L2 (ld.global.cg), never from a
+// stale L1 line or the read-only path; false is a plain load.
+template <bool CG, typename T>
+__device__ __forceinline__ Cells<T> ldc(const T* p)
+{
+    if (!CG) return ld(p);
+    Cells<T> c;
+    c.v = __ldcg(reinterpret_cast<const typename Pack<T>::V*>(p));
+    return c;
+}
+template <bool CG, typename T>
+__device__ __forceinline__ T ldc1(const T* p)
+{
+    return CG ? __ldcg(p) : *p;
+}
 template <typename T>
 __device__ __forceinline__ void st8(T* p, const Cells<T>& c)
 {
@@ -300,7 +316,7 @@ __global__ void __launch_bounds__(256) k_rf_init(int gx, int hd, Lay L, const do
 // CG sweep 1 over tile (tx, ty), FP64 arithmetic: [p = beta p + r] (rounded
 // to T as stored), w = A p; returns this thread's share of sum(w p) over the
 // stored values. All threads of the block take part (warp shuffles).
-template <typename T, bool FUSE_P>
+template <typename T, bool FUSE_P, bool CG = false>
 __device__ __forceinline__ double rf_w_tile(const Lay& L, int tx, int ty, double bt, const T* __restrict__ p_in,
                                             T* __restrict__ p_out, const T* __restrict__ r, T* __restrict__ w,
                                             const T* __restrict__ kx, const T* __restrict__ ky)
@@ -309,30 +325,30 @@ __device__ __forceinline__ double rf_w_tile(const Lay& L, int tx, int ty, double
     double acc = 0.0;
     const Span<N> s(L, tx, ty);
     auto cur = [&](long idx) -> Cells<T> {
-        Cells<T> c = ld(p_in + idx);
+        Cells<T> c = ldc<CG>(p_in + idx);
         if (FUSE_P) {
-            const Cells<T> q = ld(r + idx);
+            const Cells<T> q = ldc<CG>(r + idx);
 #pragma unroll
             for (int m = 0; m < N; ++m) c.e[m] = (T)(bt * (double)c.e[m] + (double)q.e[m]);
         }
         return c;
     };
     auto cur1 = [&](long idx) -> T {
-        return FUSE_P ? (T)(bt * (double)p_in[idx] + (double)r[idx]) : p_in[idx];
+        return FUSE_P ? (T)(bt * (double)ldc1<CG>(p_in + idx) + (double)ldc1<CG>(r + idx)) : ldc1<CG>(p_in + idx);
     };
     const long xp = L.xp;
     long i = (long)(s.j0 + 1) * xp + s.cc;
-    Cells<T> pc = cur(i), pd = cur(i - xp), kyc = ld(ky + i);
+    Cells<T> pc = cur(i), pd = cur(i - xp), kyc = ldc<CG>(ky + i);
 TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
     for (int j = s.j0; j < s.j1; ++j, i += xp) {
-        const Cells<T> pu = cur(i + xp), kyu = ld(ky + i + xp), kxc = ld(kx + i);
+        const Cells<T> pu = cur(i + xp), kyu = ldc<CG>(ky + i + xp), kxc = ldc<CG>(kx + i);
         T pl = __shfl_up_sync(kFull, pc.e[N - 1], 1);
         T pr = __shfl_down_sync(kFull, pc.e[0], 1);
         T kxr = __shfl_down_sync(kFull, kxc.e[0], 1);
         if (s.lane == 0) pl = cur1(i - 1);
         if (s.lane == 31) {
             pr = cur1(i + N);
-            kxr = kx[i + N];
+            kxr = ldc1<CG>(kx + i + N);
         }
         Cells<T> wv;
 #pragma unroll
@@ -360,7 +376,7 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
 
 // CG sweep 2 over tile (tx, ty): xs += alpha p ; r -= alpha w ; returns this
 // thread's share of sum(r r).
-template <typename T>
+template <typename T, bool CG = false>
 __device__ __forceinline__ double rf_ur_tile(const Lay& L, int tx, int ty, double a, T* __restrict__ xs,
                                              const T* __restrict__ p, T* __restrict__ r, const T* __restrict__ w)
 {
@@ -371,8 +387,8 @@ __device__ __forceinline__ double rf_ur_tile(const Lay& L, int tx, int ty, doubl
         long i = (long)(s.j0 + 1) * L.xp + s.c0;
 TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
         for (int j = s.j0; j < s.j1; ++j, i += L.xp) {
-            Cells<T> xv = ld(xs + i), rv = ld(r + i);
-            const Cells<T> pv = ld(p + i), wv = ld(w + i);
+            Cells<T> xv = ldc<CG>(xs + i), rv = ldc<CG>(r + i);
+            const Cells<T> pv = ldc<CG>(p + i), wv = ldc<CG>(w + i);
 #pragma unroll
             for (int m = 0; m < N; ++m) {
                 xv.e[m] = (T)((double)xv.e[m] + a * (double)pv.e[m]);
@@ -513,7 +529,7 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
 
 // Reliable update, part 1, tile (tx, ty): u += xs in FP64 (u in the chunk
 // layout: row length gx, halo depth hd), xs = 0.
-template <typename T>
+template <typename T, bool CG = false>
 __device__ __forceinline__ void rf_fold_tile(const Lay& L, int tx, int ty, int gx, int hd, double* __restrict__ u,
                                              T* __restrict__ xs)
 {
@@ -525,7 +541,8 @@ __device__ __forceinline__ void rf_fold_tile(const Lay& L, int tx, int ty, int g
             const int k = s.c0 + m;
             if (k >= L.nx) break;
             const long e = (long)(j + 1) * L.xp + k;
-            u[(long)(hd + k) + (long)(hd + j) * gx] += (double)xs[e];
+            double* ue = u + (long)(hd + k) + (long)(hd + j) * gx;
+            *ue = ldc1<CG>(ue) + (double)ldc1<CG>(xs + e);
             xs[e] = 0;
         }
 }
@@ -533,7 +550,7 @@ __device__ __forceinline__ void rf_fold_tile(const Lay& L, int tx, int ty, int g
 // Reliable update, part 2, tile (tx, ty): r = u0 - A u in FP64 with the FP64
 // coefficients and the reflective boundary (a neighbour outside the interior
 // is the centre value); rT = r; adds r.r and rT.rT to acc.
-template <typename T>
+template <typename T, bool CG = false>
 __device__ __forceinline__ void rf_resid_tile(const Lay& L, int tx, int ty, int gx, int hd,
                                               const double* __restrict__ u, const double* __restrict__ u0,
                                               const double* __restrict__ kx, const double* __restrict__ ky,
@@ -547,11 +564,11 @@ __device__ __forceinline__ void rf_resid_tile(const Lay& L, int tx, int ty, int 
             const int k = s.c0 + m;
             if (k >= L.nx) break;
             const long i = (long)(hd + k) + (long)(hd + j) * gx;
-            const double c = u[i];
-            const double l = k > 0 ? u[i - 1] : c;
-            const double rr = k < L.nx - 1 ? u[i + 1] : c;
-            const double d = j > 0 ? u[i - gx] : c;
-            const double up = j < L.ny - 1 ? u[i + gx] : c;
+            const double c = ldc1<CG>(u + i);
+            const double l = k > 0 ? ldc1<CG>(u + i - 1) : c;
+            const double rr = k < L.nx - 1 ? ldc1<CG>(u + i + 1) : c;
+            const double d = j > 0 ? ldc1<CG>(u + i - gx) : c;
+            const double up = j < L.ny - 1 ? ldc1<CG>(u + i + gx) : c;
             const double rv = u0[i] - smvp(kx[i], kx[i + 1], ky[i], ky[i + gx], c, l, rr, d, up);
             const T rt = (T)rv;
             rT[(long)(j + 1) * L.xp + k] = rt;

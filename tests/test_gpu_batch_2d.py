@@ -113,6 +113,28 @@ def test_autotuner_picks_a_candidate_and_step_still_converges():
         b.close()
 
 
+def test_batch_results_do_not_depend_on_the_grid():
+    """Tiles are handed to whichever block asks first and blocks move between
+    problems, but every dot product is summed from fixed per-tile partials
+    in tile order: the same tile height gives bit-identical results for any
+    grid size and any schedule."""
+    probs = _probs(5)
+    out = []
+    for grid in (148, 0):
+        b = Batch([p.tea_in() for p in probs], tile_rows=8, grid_blocks=grid)
+        try:
+            st = b.step()
+            it, rr, conv = b.results()
+            out.append((st.converged, it.copy(), rr.copy(), [h.download("energy") for h in b.hosts]))
+        finally:
+            b.close()
+    (c0, it0, rr0, e0), (c1, it1, rr1, e1) = out
+    assert c0 == c1 == len(probs)
+    assert np.array_equal(it0, it1) and np.array_equal(rr0, rr1)
+    for a, b_ in zip(e0, e1):
+        assert np.array_equal(a, b_)
+
+
 def test_batch_rejects_an_empty_batch():
     from tealeaf_b200 import abi
     lib = abi.load(2)
