@@ -85,14 +85,26 @@ __device__ __forceinline__ int block_count() { return gridDim.x * gridDim.y; }
 struct Strip {
     int k, j0, j1;
     bool active;
-    __device__ Strip(const Geo& g)
+    __device__ Strip(const Geo& g) : Strip(g, blockIdx.x, blockIdx.y) {}
+    __device__ Strip(const Geo& g, int bx, int by)
     {
-        k = g.hd + blockIdx.x * BX + threadIdx.x;
-        j0 = g.hd + blockIdx.y * g.rows;
+        k = g.hd + bx * BX + threadIdx.x;
+        j0 = g.hd + by * g.rows;
         j1 = min(j0 + g.rows, g.y - g.hd);
         active = k < g.x - g.hd;
     }
 };
+
+// The CG u/r sweep walks the strips in the reverse of the w sweep's order
+// (last strip first, each strip from its last row up), so that it starts on
+// the rows the w sweep touched last, still in L2, and ends on the rows the
+// next w sweep starts on. Each strip's partial sum keeps its slot, so the
+// reduction order over strips is unchanged. 0: forward order.
+#ifndef TL2D_UR_REVERSE
+#define TL2D_UR_REVERSE 1
+#endif
+__device__ __forceinline__ int ur_bx() { return TL2D_UR_REVERSE ? gridDim.x - 1 - blockIdx.x : blockIdx.x; }
+__device__ __forceinline__ int ur_by() { return TL2D_UR_REVERSE ? gridDim.y - 1 - blockIdx.y : blockIdx.y; }
 
 // w = A p and pw = sum(w*p)   (cg.c:88-113)
 static __global__ void __launch_bounds__(BX) k_cg_calc_w(Geo g, const double* __restrict__ p, double* __restrict__ w,
@@ -840,26 +852,30 @@ static __global__ void __launch_bounds__(BX, TL2D_MINB) k_cg_ur_fused(Geo g, Sca
                                                            const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
-    Strip s(g);
+    const int bx = ur_bx(), by = ur_by();
+    Strip s(g, bx, by);
     double acc[1] = {0.0};
     if (s.active) {
         const double a = alpha.get();
-        long i = s.k + (long)s.j0 * g.x;
+        const int j_first = TL2D_UR_REVERSE ? s.j1 - 1 : s.j0;
+        const long step = TL2D_UR_REVERSE ? -(long)g.x : (long)g.x;
+        long i = s.k + (long)j_first * g.x;
 TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
-        for (int j = s.j0; j < s.j1; ++j, i += g.x) {
+        for (int n = 0; n < s.j1 - s.j0; ++n, i += step) {
             u[i] += a * p[i];
             const double rn = r[i] - a * w[i];
             r[i] = rn;
             acc[0] += rn * rn;
         }
     }
-    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+    tl::grid_sum<1, BX>(acc, rs, bx + by * gridDim.x, block_count(), fin);
 }
 
 // k_cg_ur_fused with its operands brought in by TMA: stages of kRowsU rows
 // of the block's strip of u, p, r, w (128-column boxes starting at the strip's
 // first column, even for an even halo depth). Same strips, rows in the same
-// order per thread, same arithmetic: the same results, partial sums included.
+// order per thread (TL2D_UR_REVERSE), same arithmetic: the same results,
+// partial sums included.
 constexpr int kRowsU = 4;
 constexpr int kStagesU = 3;
 struct RowsU {
@@ -885,15 +901,19 @@ static __global__ void __launch_bounds__(BX, 4) k_cg_ur_fused_tma(Geo g, Scalar 
     unsigned char* base = tu_raw + ((128 - (tl::smem_addr(tu_raw) & 127)) & 127);
     RowsU* ring = reinterpret_cast<RowsU*>(base);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesU * sizeof(RowsU));
-    Strip s(g);
+    const int bx = ur_bx(), by = ur_by();
+    Strip s(g, bx, by);
     double acc[1] = {0.0};
     const int tx = threadIdx.x;
-    const int k0 = g.hd + blockIdx.x * BX;
+    const int k0 = g.hd + bx * BX;
     const int np = (s.j1 - s.j0 + kRowsU - 1) / kRowsU;
+    // stage b holds rows y0(b) .. y0(b) + kRowsU - 1 (the last stage of the
+    // strip may run past j1; those rows are loaded and not used)
+    auto stage_y0 = [&](int b) { return s.j0 + (TL2D_UR_REVERSE ? np - 1 - b : b) * kRowsU; };
     auto issue = [&](int b) {
         RowsU& S = ring[b % kStagesU];
         unsigned long long* bar = &bars[b % kStagesU];
-        const int y0 = s.j0 + b * kRowsU;
+        const int y0 = stage_y0(b);
         tl::mbar_expect_tx(bar, 4u * sizeof(double) * kRowsU * BX);
         tl::tma_load_3d(&S.U[0][0], &maps.u, k0, y0, 0, bar);
         tl::tma_load_3d(&S.P[0][0], &maps.p, k0, y0, 0, bar);
@@ -908,26 +928,27 @@ static __global__ void __launch_bounds__(BX, 4) k_cg_ur_fused_tma(Geo g, Scalar 
     if (tx == 0)
         for (int b = 0; b < kStagesU - 1 && b < np; ++b) issue(b);
     const double a = alpha.get();
-    long i = s.k + (long)s.j0 * g.x;
     for (int b = 0; b < np; ++b) {
         tl::mbar_wait(&bars[b % kStagesU], (unsigned)(b / kStagesU) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
         if (tx == 0 && b + kStagesU - 1 < np) issue(b + kStagesU - 1);
         const RowsU& S = ring[b % kStagesU];
+        const int y0 = stage_y0(b);
 #pragma unroll
-        for (int t = 0; t < kRowsU; ++t) {
-            const int j = s.j0 + b * kRowsU + t;
-            if (j >= s.j1) break;
+        for (int q = 0; q < kRowsU; ++q) {
+            const int t = TL2D_UR_REVERSE ? kRowsU - 1 - q : q;   // rows in the order of k_cg_ur_fused
+            const int j = y0 + t;
+            if (j >= s.j1) continue;
             if (s.active) {
+                const long i = s.k + (long)j * g.x;
                 u[i] = S.U[t][tx] + a * S.P[t][tx];
                 const double rn = S.R[t][tx] - a * S.W[t][tx];
                 r[i] = rn;
                 acc[0] += rn * rn;
             }
-            i += g.x;
         }
     }
-    tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
+    tl::grid_sum<1, BX>(acc, rs, bx + by * gridDim.x, block_count(), fin);
 }
 
 // p = beta p + r in place, with the depth-1 halo of p (and of u unless u is
