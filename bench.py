@@ -55,6 +55,8 @@ KERNEL_BYTES_PER_CELL = {
     "k3_cg_ur": 48,          # 3D: reads u, p, r, w; writes u, r
     "k3_cheby_trip": 64,     # 3D: reads u, p, u0, kx, ky, kz; writes u, p
     "k3_ppcg_step": 72,      # 3D: reads sd, r, u, kx, ky, kz; writes sd, r, u
+    "k3_blocked<cheby>": 64,  # 3D, per launch of L Chebyshev trips: reads u, p, u0, kx, ky, kz; writes u, p
+    "k3_blocked<ppcg>": 72,   # 3D, per launch of L PPCG inner steps: reads sd, r, u, kx, ky, kz; writes sd, r, u
     "k_cg_calc_w": 32, "k_cg_calc_ur": 48, "k_cg_calc_p": 24,
     "k_cheby_sweep": 64, "k_add_p": 24, "k_ppcg_inner_a": 56, "k_ppcg_inner_b": 24,
     "k_norm2": 8, "k_residual": 40,
@@ -478,6 +480,8 @@ def bench_dropin3d(args) -> dict:
     lib = h.lib
     if args.no_tma:
         lib.tl3d_set_tma(C.byref(h.chunk), 0)
+    if args.no_temporal_blocking:
+        lib.tl3d_set_temporal_blocking(C.byref(h.chunk), 0)
     stream = torch.cuda.ExternalStream(lib.tl3d_stream(C.byref(h.chunk)))
     tt = 0
     for _ in range(args.warmup):

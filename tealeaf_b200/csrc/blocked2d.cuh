@@ -359,23 +359,4 @@ inline dim3 blocked_grid(const Geo& g)
     return dim3(tl::ceil_div(g.x - 2 * g.hd, Blk<MODE>::TX), tl::ceil_div(g.y - 2 * g.hd, Blk<MODE>::TY));
 }
 
-// End of a block of Chebyshev trips: advances the trip and coefficient
-// counters trip by trip (end_of_trip, as FinChebyTrip does per trip); only
-// the last trip can take the norm (blocks end at norm trips).
-struct FinChebyBlock {
-    DevState* st;
-    DevParams prm;
-    int* host_mirror;
-    int steps;
-    int norm_last;
-    __device__ void operator()(const double* t) const
-    {
-        for (int i = 0; i < steps; ++i) {
-            const bool norm = norm_last && i == steps - 1;
-            st->nch += 1;
-            end_of_trip(st, prm, norm ? t[0] : st->error, host_mirror);
-        }
-    }
-};
-
 }  // namespace tl2d

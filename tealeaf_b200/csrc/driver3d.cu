@@ -8,6 +8,7 @@
 // do not recompute the norm, whose stale error is square-rooted again
 // (3d/drivers/cheby_solver_driver.c:70-71). Jacobi is driven from the host
 // through the suite's own kernel-interface entry points.
+#include "blocked3d.cuh"
 #include "host_maths.hpp"
 #include "suite3d_impl.hpp"
 
@@ -75,6 +76,73 @@ struct Run3 {
         cudaEventDestroy(ev[0]);
         cudaEventDestroy(ev[1]);
         return read_state();
+    }
+
+    // Launches blocks of trips: block(t) launches the block starting at trip t
+    // and returns its length; batches of about kBatch trips, the done word of
+    // the previous batch looked at while the current one runs. Returns the
+    // state read back and, in `starts`, the first trip of every block launched.
+    template <typename F>
+    DevState loop_blocks(int first_trip, F&& block, std::vector<int>& starts)
+    {
+        cudaEvent_t ev[2];
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+        int t = first_trip, batch = 0;
+        bool pending_prev = false;
+        while (t < prm.max_iters && !tl::failed()) {
+            const int end = std::min(prm.max_iters, t + kBatch);
+            while (t < end) {
+                starts.push_back(t);
+                t += block(t);
+            }
+            cudaEventRecord(ev[batch & 1], s->stream);
+            if (pending_prev) {
+                cudaEventSynchronize(ev[(batch + 1) & 1]);
+                if (*(volatile int*)&s->h_mirror[0]) break;
+            }
+            pending_prev = true;
+            ++batch;
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        return read_state();
+    }
+
+    bool blocking() const { return s->temporal_blocking && fc.l && fc.r && fc.b && fc.t && fc.k && fc.f; }
+
+    // Region planes by TMA where the boxes can start on 16-byte boundaries
+    // (even halo depth, margin and row length), else per-thread loads; the
+    // same results either way.
+    template <int MODE>
+    void launch_blocked(const Blocked3Args& a, const double* A_in, const double* B_in, double* A_out, double* B_out,
+                        const double* u0, double* u, double* w, double* r)
+    {
+        const char* name = MODE == 0 ? "k3_blocked<cheby>" : "k3_blocked<ppcg>";
+        if (tma_usable(s) && kTB3 % 2 == 0) {
+            const CUtensorMap* ma = tma_map(s, A_in, 5);
+            const CUtensorMap* mb = tma_map(s, B_in, 5);
+            const CUtensorMap* mc = tma_map(s, MODE == 0 ? u0 : u, 5);
+            const CUtensorMap* mx = tma_map(s, chunk->vec_kx, 5);
+            const CUtensorMap* my = tma_map(s, chunk->vec_ky, 5);
+            const CUtensorMap* mz = tma_map(s, chunk->vec_kz, 5);
+            if (ma && mb && mc && mx && my && mz) {
+                const Blocked3Maps m{*ma, *mb, *mc, *mx, *my, *mz};
+                static unsigned set = 0;   // devices on which the shared-memory size was raised
+                if (!(set & (1u << (s->device & 31)))) {
+                    TL_CUDA(cudaFuncSetAttribute(k3_blocked_tma<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)kBlocked3TmaBytes));
+                    set |= 1u << (s->device & 31);
+                }
+                TL3_LAUNCH(s, name, (k3_blocked_tma<MODE><<<blocked3_grid(s->g), dim3(kRX, kRY), kBlocked3TmaBytes,
+                                                            s->stream>>>(s->g, a, m, A_out, B_out, u, w, r, done(),
+                                                                         s->d_mirror + kTmaErrWord)));
+                return;
+            }
+        }
+        TL3_LAUNCH(s, name, (k3_blocked<MODE><<<blocked3_grid(s->g), dim3(kRX, kRY), 0, s->stream>>>(
+                                s->g, a, A_in, B_in, A_out, B_out, u0, u, w, r, chunk->vec_kx, chunk->vec_ky,
+                                chunk->vec_kz, done())));
     }
 
     double norm(const double* b)
@@ -183,14 +251,43 @@ struct Run3 {
         const double error = s->h_out[0];
         const int est = cheby_est(chunk, error, bb);
         if (stats) stats->est_iters = est;
+        int flips = 1;   // buffer flips of the launches that ran
         if (!st.done) {
             st.est = est;
             write_state(st);
-            st = loop(tt + 1, [&](int t) { trip(t, 0); });
+            if (blocking()) {
+                // trip t takes the norm when nch >= est and (t + 1) % 10 == 0
+                // (FinChebyTrip); a block ends at such a trip, at max_iters or
+                // after kTB3 trips
+                auto is_norm = [&](int t) { return t - tt + 1 >= est && ((t + 1) % 10) == 0; };
+                std::vector<int> starts;
+                st = loop_blocks(tt + 1, [&](int t) {
+                    int L = 1;
+                    while (!(is_norm(t + L - 1) || L == kTB3 || t + L >= prm.max_iters)) ++L;
+                    const int last = t + L - 1;
+                    const int nrm = is_norm(last) ? 1 : 0;
+                    const Blocked3Args a{L, t - tt + 1, (nrm || last + 1 >= prm.max_iters) ? 1 : 0, 0.0,
+                                         s->d_cheby_alphas, s->d_cheby_betas};
+                    launch_blocked<0>(a, ub[cur], pb[cur], ub[cur ^ 1], pb[cur ^ 1], chunk->vec_u0, nullptr,
+                                      chunk->vec_w, chunk->vec_r);
+                    const tl::FinChebyBlock fin{s->d_state, pc, s->d_mirror, L, nrm};
+                    if (nrm)
+                        TL3_LAUNCH(s, "k3_norm2_fin", (k3_norm2_fin<<<gh, bl, 0, s->stream>>>(s->g, chunk->vec_r,
+                                                                                             s->rs, done(), fin)));
+                    else
+                        TL3_LAUNCH(s, "k3_finish_only", (k3_finish_only<<<1, 32, 0, s->stream>>>(done(), fin)));
+                    cur ^= 1;
+                    return L;
+                }, starts);
+                for (int t0 : starts) flips += t0 < st.trip ? 1 : 0;
+            } else {
+                st = loop(tt + 1, [&](int t) { trip(t, 0); });
+                flips = st.nch - 1;
+            }
         }
         const int trips = st.nch - 1;
-        if (ub[trips & 1] != chunk->vec_u) swap_alt(s, chunk, ALT3_U);
-        if (pb[trips & 1] != chunk->vec_p) swap_alt(s, chunk, ALT3_P);
+        if (ub[flips & 1] != chunk->vec_u) swap_alt(s, chunk, ALT3_U);
+        if (pb[flips & 1] != chunk->vec_p) swap_alt(s, chunk, ALT3_P);
         TL3_LAUNCH(s, "k3_add_p<close>", k3_add_p<true><<<gi, bl, 0, s->stream>>>(s->g, fc, chunk->vec_u, chunk->vec_p));
         TL_CUDA(cudaStreamSynchronize(s->stream));
         if (stats) stats->cheby_iters = trips;
@@ -227,6 +324,8 @@ struct Run3 {
         pp_prm.switch_enabled = 0;
         tl::FinPpcgW fin_w{s->d_state};
         tl::FinPpcgNorm fin_n{s->d_state, pp_prm, s->d_mirror};
+        const bool blocked = blocking();
+        const int inner_flips = blocked ? (ni + kTB3 - 1) / kTB3 : ni;   // r/sd buffer flips per outer trip
         auto trip = [&](int t) {
             if (t == tt) {
                 launch_cg_w3<false, false>(s, chunk, gh, fc, beta, pb[pc], pb[pc], rb[rc], chunk->vec_w, nullptr, 0,
@@ -237,6 +336,20 @@ struct Run3 {
                 pc ^= 1;
             }
             launch_cg_ur3(s, gi, alpha, chunk->vec_u, pb[pc], rb[rc], chunk->vec_w, done(), tl::NoFinish());
+            if (blocked) {
+                for (int pp0 = 0; pp0 < ni; pp0 += kTB3) {
+                    const int L = std::min(kTB3, ni - pp0);
+                    const Blocked3Args a{L, pp0, 0, chunk->theta, s->d_cheby_alphas, s->d_cheby_betas};
+                    launch_blocked<1>(a, sb[sc], rb[rc], sb[sc ^ 1], rb[rc ^ 1], nullptr, chunk->vec_u, nullptr,
+                                      nullptr);
+                    sc ^= 1;
+                    rc ^= 1;
+                    if (pp0 + L == ni)
+                        TL3_LAUNCH(s, "k3_norm2_fin", (k3_norm2_fin<<<gh, bl, 0, s->stream>>>(s->g, rb[rc], s->rs,
+                                                                                             done(), fin_n)));
+                }
+                return;
+            }
             for (int pp = 0; pp < ni; ++pp) {
                 const bool last = pp == ni - 1;
 #define STEP3(FOLD, NORM, FIN)                                                                                    \
@@ -269,7 +382,7 @@ struct Run3 {
         st = loop(tt, trip);
         const int outer = st.nch;
         const int pflips = std::max(0, outer - 1);
-        const int rflips = outer * ni;
+        const int rflips = outer * inner_flips;
         if (pb[pflips & 1] != chunk->vec_p) swap_alt(s, chunk, ALT3_P);
         if (rb[rflips & 1] != chunk->vec_r) swap_alt(s, chunk, ALT3_R);
         if (sb[rflips & 1] != chunk->vec_sd) swap_alt(s, chunk, ALT3_SD);

@@ -30,6 +30,7 @@ using tl::FinCgInit;
 using tl::FinCgUr;
 using tl::FinCgW;
 using tl::FinPcgUr;
+using tl::FinChebyBlock;
 using tl::FinChebyTrip;
 using tl::FinPpcgNorm;
 using tl::FinPpcgW;

@@ -24,6 +24,7 @@ using tl::DevState;
 using tl::FinCgInit;
 using tl::FinCgUr;
 using tl::FinCgW;
+using tl::FinChebyBlock;
 using tl::FinChebyTrip;
 using tl::FinPpcgNorm;
 using tl::FinPpcgW;

@@ -165,6 +165,26 @@ struct FinChebyTrip {      // end of one Chebyshev trip of the device-resident l
     }
 };
 
+// End of a block of Chebyshev trips: advances the trip and coefficient
+// counters trip by trip (end_of_trip, as FinChebyTrip does per trip); only
+// the last trip can take the norm (blocks end at norm trips).
+struct FinChebyBlock {
+    DevState* st;
+    DevParams prm;
+    int* host_mirror;
+    int steps;
+    int norm_last;
+    __device__ void operator()(const double* t) const
+    {
+        for (int i = 0; i < steps; ++i) {
+            const bool norm = norm_last && i == steps - 1;
+            st->nch += 1;
+            end_of_trip(st, prm, norm ? t[0] : st->error, host_mirror);
+        }
+    }
+};
+
+
 // PPCG inner-step coefficients: host values or device tables [pp].
 struct PpcgCoef {
     double alpha, beta;

@@ -156,6 +156,11 @@ void tl3d_set_tma(Chunk* chunk, int on)
     TlSuite3D* s = suite_of(chunk);
     if (s) s->tma = on != 0;
 }
+void tl3d_set_temporal_blocking(Chunk* chunk, int on)
+{
+    TlSuite3D* s = suite_of(chunk);
+    if (s) s->temporal_blocking = on != 0;
+}
 void tl3d_flush(Chunk* chunk) { ready(chunk); }
 long long tl3d_launch_count(Chunk* chunk)
 {

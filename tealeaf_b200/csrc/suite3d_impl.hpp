@@ -3,6 +3,7 @@
 // (driver3d.cu). Same design as the 2D suite (suite2d_impl.hpp).
 #pragma once
 
+#include "blocked3d.cuh"
 #include "kernels3d.cuh"
 
 #include <cuda_runtime.h>
@@ -39,12 +40,13 @@ struct TlSuite3D {
     double* d_cheby_betas = nullptr;
     int table_len = 0;
     bool tma = true;   // feed the CG w sweep by TMA where the layout allows (tl3d_set_tma)
+    bool temporal_blocking = true;   // device-driver Chebyshev / PPCG blocks (tl3d_set_temporal_blocking)
     struct TmaEntry {
         const double* ptr;
         int kind;
         CUtensorMap map;
     };
-    TmaEntry tma_cache[24];
+    TmaEntry tma_cache[40];
     int tma_n = 0;
     int tma_next = 0;
 };
@@ -111,7 +113,8 @@ void swap_alt(TlSuite3D* s, Chunk* chunk, AltField3 f);
 
 // Tensor map of a chunk array for walkt: kind 0 operand (box (BX+4) x (BY+2)),
 // 1 kx (BX+2) x BY, 2 ky BX x (BY+1), 3 kz BX x BY; for k3_cg_ur_tma kind 4
-// BX x BY x kPlanesU; encoded once per array.
+// BX x BY x kPlanesU; for k3_blocked_tma kind 5 kRX x kRY; encoded once per
+// array.
 inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
 {
     for (int i = 0; i < s->tma_n; ++i)
@@ -119,8 +122,8 @@ inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
     // a full cache recycles its entries in turn (arrays of released buffers)
     const int cap = (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]));
     const int slot = s->tma_n < cap ? s->tma_n : (s->tma_next++ % cap);
-    static const unsigned box[5][3] = {{BX + 4, BY + 2, 1}, {BX + 2, BY, 1}, {BX, BY + 1, 1}, {BX, BY, 1},
-                                       {BX, BY, kPlanesU}};
+    static const unsigned box[6][3] = {{BX + 4, BY + 2, 1}, {BX + 2, BY, 1}, {BX, BY + 1, 1}, {BX, BY, 1},
+                                       {BX, BY, kPlanesU}, {kRX, kRY, 1}};
     CUtensorMap m;
     if (!tl::tma_encode_3d(&m, ptr, s->g.x, s->g.y, s->g.z, box[kind][0], box[kind][1], box[kind][2]))
         return nullptr;

@@ -277,6 +277,8 @@ def test_3d_tma_sweep_matches_async_copies(solver, path):
     text = prob.tea_in()
     a, b = Host(text, 3), Host(text, 3)
     try:
+        a.lib.tl3d_set_temporal_blocking(a.chunk, 0)   # the one-step sweeps, fed both ways
+        b.lib.tl3d_set_temporal_blocking(b.chunk, 0)
         b.lib.tl3d_set_tma(b.chunk, 0)
         for tt in range(2):
             ra = a.solve_device(tt) if path == "device" else a.solve(tt)
@@ -285,6 +287,43 @@ def test_3d_tma_sweep_matches_async_copies(solver, path):
             assert ra.summary == rb.summary
             for f in FIELDS3:
                 assert np.array_equal(a.download(f), b.download(f)), (path, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()
+
+
+@pytest.mark.parametrize("solver,dims,inner", [
+    ("cheby", (37, 19, 23), 10),
+    ("ppcg", (37, 19, 23), 10),
+    ("ppcg", (37, 19, 23), 7),
+    ("ppcg", (37, 19, 23), 1),
+    ("cheby", (38, 19, 23), 10),
+    ("ppcg", (38, 19, 23), 5),
+    ("cheby", (30, 24, 150), 10),
+    ("ppcg", (30, 24, 150), 4),
+])
+def test_3d_blocked_trips_match_one_step(solver, dims, inner):
+    """The device driver's temporally blocked Chebyshev trips and PPCG inner
+    steps (k3_blocked / k3_blocked_tma: up to two per launch, x-y tiles with
+    a margin, z segments of 64 planes) leave every field and the iteration
+    counts bit-identical to one launch per trip / step, on meshes with
+    ragged tiles in x and y, odd rows (per-thread loads) and even rows (region
+    planes by TMA), one or three z segments, and inner-step counts that fill,
+    split and underfill the blocks."""
+    prob = problems.seeded(3, dims, 31, 3, 1, solver=solver, end_step=2, name="blk3").with_(
+        ppcg_inner_steps=inner)
+    text = prob.tea_in()
+    a, b = Host(text, 3), Host(text, 3)
+    try:
+        b.lib.tl3d_set_temporal_blocking(b.chunk, 0)
+        for tt in range(2):
+            ra = a.solve_device(tt)
+            rb = b.solve_device(tt)
+            assert ra.iterations == rb.iterations
+            assert ra.iterations.get("Cheby" if solver == "cheby" else "PPCG", 0) > 0
+            assert ra.summary == rb.summary
+            for f in FIELDS3:
+                assert np.array_equal(a.download(f), b.download(f)), (solver, dims, tt, f)
     finally:
         a.finalise()
         b.finalise()
