@@ -250,8 +250,9 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked(Geo g, Blocke
 // row length are even; cells outside the array read as zero, and, as in
 // k3_blocked, only cells inside the interior and the margin are used. The
 // ring also stages the plane after the last interior one for its kz (the
-// front face coefficient of the last plane). Every wait is bounded (err);
-// every issued plane is waited for.
+// front face coefficient of the last plane). The launch's step count is a
+// template parameter (HS = a.steps), so the level loop is straight-line
+// code. Every wait is bounded (err); every issued plane is waited for.
 constexpr int kPf3 = 2;                       // planes issued ahead
 constexpr int kRing3 = kTB3 + 1 + kPf3;       // planes s - kTB3 .. s + kPf3
 struct Region3 {
@@ -262,7 +263,7 @@ struct Blocked3Maps {
 };
 constexpr size_t kBlocked3TmaBytes = kRing3 * sizeof(Region3) + kRing3 * 8 + 128;
 
-template <int MODE>
+template <int MODE, int HS>
 static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Blocked3Args a,
                                                                        const __grid_constant__ Blocked3Maps maps,
                                                                        double* A_out, double* __restrict__ B_out,
@@ -280,7 +281,7 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
     const int x = g.x, hd = g.hd;
     const long xy = g.xy();
     const int ilo = hd, ihi = g.x - hd, jlo = hd, jhi = g.y - hd, zlo = hd, zhi = g.z - hd;
-    const int H = a.steps;
+    constexpr int H = HS;   // steps of this launch (a.steps)
     const int cx = threadIdx.x, cy = threadIdx.y;
     const bool leader = cx == 0 && cy == 0;
     const int xs = hd + blockIdx.x * kTX3 - kTB3, ys = hd + blockIdx.y * kTY3 - kTB3;   // region origin
