@@ -83,15 +83,27 @@ __device__ __forceinline__ int block_count() { return gridDim.x * gridDim.y * gr
 struct Pencil {
     int k, j, i0, i1;
     bool active;
-    __device__ Pencil(const Geo& g)
+    __device__ Pencil(const Geo& g) : Pencil(g, blockIdx.x, blockIdx.y, blockIdx.z) {}
+    __device__ Pencil(const Geo& g, int bx, int by, int bz)
     {
-        k = g.hd + blockIdx.x * BX + threadIdx.x;
-        j = g.hd + blockIdx.y * BY + threadIdx.y;
-        i0 = g.hd + blockIdx.z * g.zr;
+        k = g.hd + bx * BX + threadIdx.x;
+        j = g.hd + by * BY + threadIdx.y;
+        i0 = g.hd + bz * g.zr;
         i1 = min(i0 + g.zr, g.z - g.hd);
         active = k < g.x - g.hd && j < g.y - g.hd;
     }
 };
+
+// The CG u/r sweep walks the pencils in the reverse of the w sweep's order
+// (last block first, each pencil from its last plane down), so that it
+// starts on the planes the w sweep touched last, still in L2, and ends on
+// the planes the next w sweep starts on. Each block's partial sum keeps the
+// slot of its pencils, so the reduction order over blocks is unchanged.
+// 0: forward order.
+#ifndef TL3D_UR_REVERSE
+#define TL3D_UR_REVERSE 1
+#endif
+__device__ __forceinline__ int ur3_b(unsigned b, unsigned n) { return TL3D_UR_REVERSE ? (int)(n - 1 - b) : (int)b; }
 
 // Pencil with the cell clamped into the interior for lanes past it (they
 // load valid cells and feed the x-neighbour shuffles, but store nothing).
@@ -481,26 +493,29 @@ static __global__ void __launch_bounds__(NT, 8) k3_cg_ur(Geo g, Scalar alpha, do
                                                                 const int* __restrict__ done, Finish fin)
 {
     if (gate_closed(done)) return;
-    Pencil s(g);
+    const int bx = ur3_b(blockIdx.x, gridDim.x), by = ur3_b(blockIdx.y, gridDim.y), bz = ur3_b(blockIdx.z, gridDim.z);
+    Pencil s(g, bx, by, bz);
     double acc[1] = {0.0};
     if (s.active) {
         const double a = alpha.get();
         const long xy = g.xy();
-        long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
+        const long step = TL3D_UR_REVERSE ? -xy : xy;
+        long i = s.k + (long)s.j * g.x + (long)(TL3D_UR_REVERSE ? s.i1 - 1 : s.i0) * xy;
         TL3D_PRAGMA_UNROLL(TL3D_UNROLL)
-        for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
+        for (int n = 0; n < s.i1 - s.i0; ++n, i += step) {
             u[i] += a * p[i];
             const double rn = r[i] - a * w[i];
             r[i] = rn;
             acc[0] += rn * rn;
         }
     }
-    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+    tl::grid_sum<1, NT>(acc, rs, bx + gridDim.x * (by + gridDim.y * bz), block_count(), fin);
 }
 
 // k3_cg_ur with its operands brought in by TMA: stages of kPlanesU z-planes of
 // the block's 32 x 8 columns of u, p, r, w. Same pencils, planes in the same
-// order per thread, same arithmetic: the same results, partial sums included.
+// order per thread (TL3D_UR_REVERSE), same arithmetic: the same results,
+// partial sums included.
 constexpr int kPlanesU = 2;
 constexpr int kStagesU3 = 3;
 struct PlanesU {
@@ -526,16 +541,20 @@ static __global__ void __launch_bounds__(NT, 4) k3_cg_ur_tma(Geo g, Scalar alpha
     unsigned char* base = u3_raw + ((128 - (tl::smem_addr(u3_raw) & 127)) & 127);
     PlanesU* ring = reinterpret_cast<PlanesU*>(base);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesU3 * sizeof(PlanesU));
-    Pencil s(g);
+    const int bx = ur3_b(blockIdx.x, gridDim.x), by = ur3_b(blockIdx.y, gridDim.y), bz = ur3_b(blockIdx.z, gridDim.z);
+    Pencil s(g, bx, by, bz);
     double acc[1] = {0.0};
     const int tx = threadIdx.x, ty = threadIdx.y;
     const bool leader = tx == 0 && ty == 0;
-    const int kb = g.hd + blockIdx.x * BX, jb = g.hd + blockIdx.y * BY;
+    const int kb = g.hd + bx * BX, jb = g.hd + by * BY;
     const int np = (s.i1 - s.i0 + kPlanesU - 1) / kPlanesU;
+    // stage b holds planes z0(b) .. z0(b) + kPlanesU - 1 (the pencil's last
+    // stage may run past i1; those planes are loaded and not used)
+    auto stage_z0 = [&](int b) { return s.i0 + (TL3D_UR_REVERSE ? np - 1 - b : b) * kPlanesU; };
     auto issue = [&](int b) {
         PlanesU& S = ring[b % kStagesU3];
         unsigned long long* bar = &bars[b % kStagesU3];
-        const int z0 = s.i0 + b * kPlanesU;
+        const int z0 = stage_z0(b);
         tl::mbar_expect_tx(bar, 4u * sizeof(double) * kPlanesU * BY * BX);
         tl::tma_load_3d(&S.U[0][0][0], &maps.u, kb, jb, z0, bar);
         tl::tma_load_3d(&S.P[0][0][0], &maps.p, kb, jb, z0, bar);
@@ -551,25 +570,27 @@ static __global__ void __launch_bounds__(NT, 4) k3_cg_ur_tma(Geo g, Scalar alpha
         for (int b = 0; b < kStagesU3 - 1 && b < np; ++b) issue(b);
     const double a = alpha.get();
     const long xy = g.xy();
-    long i = s.k + (long)s.j * g.x + (long)s.i0 * xy;
     for (int b = 0; b < np; ++b) {
         tl::mbar_wait(&bars[b % kStagesU3], (unsigned)(b / kStagesU3) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
         if (leader && b + kStagesU3 - 1 < np) issue(b + kStagesU3 - 1);
         const PlanesU& S = ring[b % kStagesU3];
+        const int z0 = stage_z0(b);
 #pragma unroll
-        for (int t = 0; t < kPlanesU; ++t) {
-            if (s.i0 + b * kPlanesU + t >= s.i1) break;
+        for (int q = 0; q < kPlanesU; ++q) {
+            const int t = TL3D_UR_REVERSE ? kPlanesU - 1 - q : q;   // planes in the order of k3_cg_ur
+            const int ii = z0 + t;
+            if (ii >= s.i1) continue;
             if (s.active) {
+                const long i = s.k + (long)s.j * g.x + (long)ii * xy;
                 u[i] = S.U[t][ty][tx] + a * S.P[t][ty][tx];
                 const double rn = S.R[t][ty][tx] - a * S.W[t][ty][tx];
                 r[i] = rn;
                 acc[0] += rn * rn;
             }
-            i += xy;
         }
     }
-    tl::grid_sum<1, NT>(acc, rs, block_id(), block_count(), fin);
+    tl::grid_sum<1, NT>(acc, rs, bx + gridDim.x * (by + gridDim.y * bz), block_count(), fin);
 }
 
 // p = beta p + r (APPLY_P) and the depth-1 halos of p and (unless null) u.
