@@ -21,7 +21,11 @@ namespace tl2d {
 namespace rf {
 
 constexpr int kRfRows = 4;
-constexpr int kRfStages = 3;
+constexpr int kRfStages = 3;     // w sweep ring
+#ifndef TL2D_RF_STAGES_U
+#define TL2D_RF_STAGES_U 3
+#endif
+constexpr int kRfStagesU = TL2D_RF_STAGES_U;   // u/r sweep ring
 constexpr int kRfTmaBlocks = 4;   // resident blocks per SM of the TMA sweeps (about 50 KB of shared memory each)
 
 template <typename T>
@@ -67,7 +71,7 @@ constexpr size_t rf_w_tma_bytes()
 template <typename T>
 constexpr size_t rf_u_tma_bytes()
 {
-    return kRfStages * sizeof(RfRowsU<T>) + kRfStages * 8 + 128;
+    return kRfStagesU * sizeof(RfRowsU<T>) + kRfStagesU * 8 + 128;
 }
 
 // k_rf_w by TMA. Stage b holds T-layout rows j0 + 4b .. j0 + 4b + 3 (interior
@@ -209,14 +213,14 @@ __global__ void __launch_bounds__(BX, 4) k_rf_ur_tma(Lay L, const MxState* __res
     if (mx_idle(st)) return;
     unsigned char* base = ru_raw + ((128 - (tl::smem_addr(ru_raw) & 127)) & 127);
     S* ring = reinterpret_cast<S*>(base);
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kRfStages * sizeof(S));
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kRfStagesU * sizeof(S));
     const Span<N> s(L, blockIdx.x, blockIdx.y);
     const int tid = threadIdx.x;
     const int cb = blockIdx.x * W;
     const int np = (s.j1 - s.j0 + kRfRows - 1) / kRfRows;
     auto issue = [&](int b) {
-        S& Q = ring[b % kRfStages];
-        unsigned long long* bar = &bars[b % kRfStages];
+        S& Q = ring[b % kRfStagesU];
+        unsigned long long* bar = &bars[b % kRfStagesU];
         const int y0 = s.j0 + 1 + b * kRfRows;
         tl::mbar_expect_tx(bar, 4u * sizeof(T) * kRfRows * W);
         tl::tma_load_3d(&Q.X[0][0], &m.xs, cb, y0, 0, bar);
@@ -225,20 +229,20 @@ __global__ void __launch_bounds__(BX, 4) k_rf_ur_tma(Lay L, const MxState* __res
         tl::tma_load_3d(&Q.Wv[0][0], &m.w, cb, y0, 0, bar);
     };
     if (tid == 0) {
-        for (int q = 0; q < kRfStages; ++q) tl::mbar_init(&bars[q], 1);
+        for (int q = 0; q < kRfStagesU; ++q) tl::mbar_init(&bars[q], 1);
         tl::mbar_fence_init();
     }
     __syncthreads();
     if (tid == 0)
-        for (int b = 0; b < kRfStages - 1 && b < np; ++b) issue(b);
+        for (int b = 0; b < kRfStagesU - 1 && b < np; ++b) issue(b);
     const double a = st->alpha;
     double acc = 0.0;
     long i = (long)(s.j0 + 1) * L.xp + s.c0;
     for (int b = 0; b < np; ++b) {
-        tl::mbar_wait(&bars[b % kRfStages], (unsigned)(b / kRfStages) & 1u, err);
+        tl::mbar_wait(&bars[b % kRfStagesU], (unsigned)(b / kRfStagesU) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
-        if (tid == 0 && b + kRfStages - 1 < np) issue(b + kRfStages - 1);
-        const S& Q = ring[b % kRfStages];
+        if (tid == 0 && b + kRfStagesU - 1 < np) issue(b + kRfStagesU - 1);
+        const S& Q = ring[b % kRfStagesU];
 #pragma unroll
         for (int u = 0; u < kRfRows; ++u) {
             if (s.j0 + b * kRfRows + u >= s.j1) break;

@@ -117,7 +117,7 @@ def test_w_sweep_rings(rows, stages):
                  waits_fn=lambda b, np_: [b] + ([b + 1] if b + 1 < np_ else []))
 
 
-@pytest.mark.parametrize("rows,stages", [(4, 3), (2, 3)])
+@pytest.mark.parametrize("rows,stages", [(4, 3), (4, 4), (2, 3)])
 def test_pointwise_sweep_rings(rows, stages):
     # 2D / 3D / refinement u-r updates and the PCG u/r/z sweep: stage b holds
     # units rows*b .. ; trip b reads stage b
@@ -140,3 +140,53 @@ def test_walkt_plane_ring():
                  reads_fn=lambda q: {q, q + 1},
                  waits_fn=lambda q, np_: [q, q + 1])
         assert np_ >= 2
+
+
+@pytest.mark.parametrize("steps", [1, 2])
+def test_blocked3d_plane_ring(steps):
+    """The region-plane ring of k3_blocked_tma (blocked3d.cuh): planes
+    s_begin .. load_end - 1 staged kPf3 = 2 ahead into kRing3 = 5 slots (slot
+    (p - s_begin) % 5, one barrier per slot); step s waits for plane s, then
+    (after the barrier) issues plane s + 2, and reads planes s - steps .. s
+    (level l reads plane s - l and, for kz, s - l + 1). Checked for every
+    segment position and length: each read plane was issued and waited for
+    and still holds its slot, each wait uses the slot's use count as parity,
+    every issued plane is waited for."""
+    R, PF, TB = 5, 2, 2
+    for zlo, zhi in [(2, 2 + n) for n in range(1, 140)]:
+        for Z0 in range(zlo, zhi, 64):
+            Z1 = min(Z0 + 64, zhi)
+            H = steps
+            s_begin, s_end = max(Z0 - H, zlo), Z1 + H
+            load_end = min(Z1 + H, zhi + 1)
+            slot_of, uses, issued, waited = {}, [0] * R, set(), set()
+
+            def issue(p):
+                q = (p - s_begin) % R
+                slot_of[q] = p
+                issued.add(p)
+
+            for p in range(s_begin, min(s_begin + PF, load_end)):
+                issue(p)
+            for s_ in range(s_begin, s_end):
+                if s_ < load_end:
+                    q = (s_ - s_begin) % R
+                    assert slot_of.get(q) == s_
+                    assert ((s_ - s_begin) // R) & 1 == uses[q] & 1
+                    uses[q] += 1
+                    waited.add(s_)
+                # after the barrier: the issue two planes ahead
+                if s_ + PF < load_end:
+                    issue(s_ + PF)
+                reads = set()
+                if s_ < min(Z1 + H, zhi):
+                    reads.add(s_)
+                for l in range(1, H + 1):
+                    z = s_ - l
+                    if max(Z0 - H + l, zlo) <= z < min(Z1 + H - l, zhi):
+                        reads |= {z, z + 1}
+                for p in reads:
+                    assert p in waited, (Z0, Z1, s_, p)
+                    assert slot_of[(p - s_begin) % R] == p, (Z0, Z1, s_, p)
+            assert issued == waited
+            assert TB + 1 + PF == R
