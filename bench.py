@@ -836,6 +836,8 @@ def bench_refine_case(args) -> dict:
     `--precision` 32 or 64, with `--solver` cg or ppcg (`--errswitch`: the
     switch after 21 CG trips, epslim 1e30) and an optional `--max-iters` cap.
     The case the refinement profiles are captured on."""
+    import ctypes as C
+
     from tealeaf_b200 import problems
     from tealeaf_b200.host import Host
     prob = problems.mixed_2d(args.size, seed=3, steps=1).with_(solver=args.solver)
@@ -845,6 +847,8 @@ def bench_refine_case(args) -> dict:
         prob = prob.with_(max_iters=args.max_iters)
     h = Host(prob.tea_in(), dims=2)
     try:
+        if args.no_tma:
+            h.lib.tl2d_set_tma(C.byref(h.chunk), 0)
         r = h.refine_step(0, 1e-10, args.precision)
     finally:
         h.finalise()

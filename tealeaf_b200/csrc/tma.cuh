@@ -33,8 +33,22 @@ __device__ __forceinline__ void mbar_fence_init()
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
+// Orders shared-memory accesses of the generic proxy -- this thread's and,
+// after a barrier, the block's -- before the async proxy's next ones.
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// Arms `bar` for `bytes` of TMA transactions. Every arming precedes loads
+// into a buffer the block's threads may have just read (a ring stage or a
+// staging area freed by a barrier), so it first orders those generic reads
+// before the async proxy's writes: without the fence a refill could land
+// under a late read (observed as rare, run-to-run differences of a staged
+// persistent kernel).
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
 {
+    fence_proxy_async();
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
