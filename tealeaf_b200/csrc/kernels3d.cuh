@@ -516,8 +516,14 @@ static __global__ void __launch_bounds__(NT, 8) k3_cg_ur(Geo g, Scalar alpha, do
 // the block's 32 x 8 columns of u, p, r, w. Same pencils, planes in the same
 // order per thread (TL3D_UR_REVERSE), same arithmetic: the same results,
 // partial sums included.
-constexpr int kPlanesU = 2;
-constexpr int kStagesU3 = 3;
+#ifndef TL3D_TMA_PLANES_U
+#define TL3D_TMA_PLANES_U 2
+#endif
+#ifndef TL3D_TMA_STAGES_U
+#define TL3D_TMA_STAGES_U 4   // 4 deep (65.5 KB, 3 blocks per SM): 132.9 against 135.9 us for 3 deep at 256^3
+#endif
+constexpr int kPlanesU = TL3D_TMA_PLANES_U;
+constexpr int kStagesU3 = TL3D_TMA_STAGES_U;
 struct PlanesU {
     alignas(128) double U[kPlanesU][BY][BX];
     alignas(128) double P[kPlanesU][BY][BX];

@@ -117,7 +117,7 @@ def test_w_sweep_rings(rows, stages):
                  waits_fn=lambda b, np_: [b] + ([b + 1] if b + 1 < np_ else []))
 
 
-@pytest.mark.parametrize("rows,stages", [(4, 3), (4, 4), (2, 3)])
+@pytest.mark.parametrize("rows,stages", [(4, 3), (4, 4), (2, 3), (2, 4)])
 def test_pointwise_sweep_rings(rows, stages):
     # 2D / 3D / refinement u-r updates and the PCG u/r/z sweep: stage b holds
     # units rows*b .. ; trip b reads stage b
