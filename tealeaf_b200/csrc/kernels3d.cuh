@@ -292,7 +292,12 @@ struct Tma3Maps {
     CUtensorMap a, b, kx, ky, kz;
 };
 
-constexpr size_t kTmaRingBytes = kStages3 * sizeof(PlaneT) + kStages3 * 8 + 128;   // + barriers + alignment
+#ifndef TL3D_TMA_STAGES
+#define TL3D_TMA_STAGES 4
+#endif
+constexpr int kStagesT3 = TL3D_TMA_STAGES;   // walkt's ring of planes (walkc keeps kStages3)
+static_assert(kStagesT3 >= 3, "plane ii is read with ii+1 while a later one is in flight");
+constexpr size_t kTmaRingBytes = kStagesT3 * sizeof(PlaneT) + kStagesT3 * 8 + 128;   // + barriers + alignment
 // TMA alignment: boxes start at x = hd - 2 + BX bx (operands) or hd + BX bx
 // (coefficients), so BX must keep them even and every box row 16-byte wide.
 static_assert(BX % 2 == 0 && ((BX + 4) * sizeof(double)) % 16 == 0 && ((BX + 2) * sizeof(double)) % 16 == 0 &&
@@ -310,7 +315,7 @@ __device__ __forceinline__ void walkt(const Geo& g, const Faces& fc, const Penci
 {
     unsigned char* base = raw + ((128 - (tl::smem_addr(raw) & 127)) & 127);
     PlaneT* ring = reinterpret_cast<PlaneT*>(base);
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStages3 * sizeof(PlaneT));
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + kStagesT3 * sizeof(PlaneT));
     const int x = g.x;
     const long xy = g.xy();
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -333,25 +338,25 @@ __device__ __forceinline__ void walkt(const Geo& g, const Faces& fc, const Penci
     };
     const int np = s.i1 - s.i0 + 1;   // planes i0 .. i1 (i1: the last plane's front neighbour)
     if (leader) {
-        for (int q = 0; q < kStages3; ++q) tl::mbar_init(&bars[q], 1);
+        for (int q = 0; q < kStagesT3; ++q) tl::mbar_init(&bars[q], 1);
         tl::mbar_fence_init();
     }
     __syncthreads();
     if (leader)
-        for (int q = 0; q < kStages3 - 1 && q < np; ++q) issue(s.i0 + q, q, s.i0 + q < s.i1);
+        for (int q = 0; q < kStagesT3 - 1 && q < np; ++q) issue(s.i0 + q, q, s.i0 + q < s.i1);
     long i = s.k + (long)s.j * x + (long)s.i0 * xy;
     double bk = (s.i0 == g.hd) ? 0.0 : comb(A[i - xy], B ? B[i - xy] : 0.0);
     const bool bk_reflect = s.i0 == g.hd;
 #pragma unroll 1
     for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
         const int q = ii - s.i0;
-        tl::mbar_wait(&bars[q % kStages3], (unsigned)(q / kStages3) & 1u, err);
-        tl::mbar_wait(&bars[(q + 1) % kStages3], (unsigned)((q + 1) / kStages3) & 1u, err);
+        tl::mbar_wait(&bars[q % kStagesT3], (unsigned)(q / kStagesT3) & 1u, err);
+        tl::mbar_wait(&bars[(q + 1) % kStagesT3], (unsigned)((q + 1) / kStagesT3) & 1u, err);
         __syncthreads();   // every thread is past plane ii-1: its slot is free
-        if (leader && q + kStages3 - 1 < np)
-            issue(ii + kStages3 - 1, (q + kStages3 - 1) % kStages3, ii + kStages3 - 1 < s.i1);
-        const PlaneT& P = ring[q % kStages3];
-        const PlaneT& F = ring[(q + 1) % kStages3];
+        if (leader && q + kStagesT3 - 1 < np)
+            issue(ii + kStagesT3 - 1, (q + kStagesT3 - 1) % kStagesT3, ii + kStagesT3 - 1 < s.i1);
+        const PlaneT& P = ring[q % kStagesT3];
+        const PlaneT& F = ring[(q + 1) % kStagesT3];
         const int cx = tx + 2, cy = ty + 1;
         auto cell = [&](const PlaneT& S, int yy, int xx) { return comb(S.A[yy][xx], has_b ? S.B[yy][xx] : 0.0); };
         const double c = cell(P, cy, cx);
