@@ -256,13 +256,17 @@ long long tl3d_launch_count(Chunk* chunk);
  * TMA tile loads (1, the default, where the halo depth and row length are
  * even; results are bit-identical) or by per-thread asynchronous copies (0). */
 void tl3d_set_tma(Chunk* chunk, int on);
-/* No counterpart in the reference. Run the device-resident driver's
- * Chebyshev trips and PPCG inner steps temporally blocked in shared memory
- * (1, the default; results are bit-identical; used when all six faces are
- * external) or one launch per trip / step (0). */
+/* No counterpart in the reference. Run Chebyshev trips and PPCG inner steps
+ * temporally blocked in shared memory (1, the default; results are
+ * bit-identical; used when all six faces are external) or one launch per
+ * trip / step (0): in the device-resident driver, and through
+ * run_cheby_solver_iterate / run_ppcg_inner_iteration, whose calls in the
+ * reference drivers' pattern are deferred and run blocked when another
+ * run_* call needs the device state. */
 void tl3d_set_temporal_blocking(Chunk* chunk, int on);
 /* No counterpart in the reference. Runs every operation the suite has
- * deferred for this chunk (a CG p update, halo updates), as every run_* call
+ * deferred for this chunk (a CG p update, halo updates, queued Chebyshev
+ * trips or PPCG inner steps), as every run_* call
  * that touches device data does first; call it before reading the chunk's
  * device fields by other means. Asynchronous on the chunk's stream. */
 void tl3d_flush(Chunk* chunk);

@@ -28,6 +28,8 @@
 //
 // Chebyshev (MODE 0), carried fields A = u, B = p, state (u_{n-1}, p_{n-1})
 // with the add pending:   S = A + B ;  B = a_n B + b_n (u0 - A S) ;  A = S
+// (or, with add_end, state (u_n, p_n): S = A for the first trip and the last
+// trip's add applied on write-back, the order of run_cheby_solver_iterate)
 // PPCG (MODE 1), A = sd, B = r, fold index pp:
 //   S = pp == 0 ? B / theta : a_{pp-1} A + b_{pp-1} B ;  B -= A S ;  u += S ;  A = S
 #pragma once
@@ -60,6 +62,8 @@ struct Blocked3Args {
     double theta;         // PPCG fold of pp == 0
     const double* alphas;
     const double* betas;
+    int add_end = 0;      // Chebyshev: each trip ends with its u += p (the kernel-interface calls' order)
+                          // instead of starting with the previous trip's
 };
 
 template <int MODE>
@@ -160,7 +164,7 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked(Geo g, Blocke
         }
         // level 0: plane s enters
         {
-            const double sv = MODE == 0 ? av + bv : fold(0, av, bv);
+            const double sv = MODE == 0 ? (a.add_end ? av : av + bv) : fold(0, av, bv);
             if (MODE == 1) uacc[0] = uv + sv;
             win[0][0] = win[0][1];
             win[0][1] = win[0][2];
@@ -226,7 +230,7 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked(Geo g, Blocke
                 sp[l][z & 1][cy][cx] = snew;
             } else if (in_tile && z >= Z0 && z < Z1) {
                 // the tile's plane after H steps: A = S of step H - 1, B, the reflective halo of A
-                A_out[i] = c;
+                A_out[i] = (MODE == 0 && a.add_end) ? c + bnew : c;   // halo: u before the last add
                 B_out[i] = bnew;
                 if (MODE == 1) u[i] = uacc[l];
                 if (at_l) A_out[i - 1] = c;
@@ -363,7 +367,7 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
                 bv = R.f[1][cy][cx];
                 if (MODE == 1 && in_tile && s >= Z0 && s < Z1) uv = R.f[2][cy][cx];
             }
-            const double sv = MODE == 0 ? av + bv : fold(0, av, bv);
+            const double sv = MODE == 0 ? (a.add_end ? av : av + bv) : fold(0, av, bv);
             if (MODE == 1) uacc[0] = uv + sv;
             win[0][0] = win[0][1];
             win[0][1] = win[0][2];
@@ -440,7 +444,7 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
                     bn[l] = bnew;
                     sp[l][z & 1][cy][cx] = snew;
                 } else if (in_tile && z >= Z0 && z < Z1) {
-                    A_out[i] = c;
+                    A_out[i] = (MODE == 0 && a.add_end) ? c + bnew : c;   // halo: u before the last add
                     B_out[i] = bnew;
                     if (MODE == 1) u[i] = uacc[l];
                     if (REFLECT) {

@@ -111,46 +111,11 @@ struct Run3 {
 
     bool blocking() const { return s->temporal_blocking && fc.l && fc.r && fc.b && fc.t && fc.k && fc.f; }
 
-    template <int MODE, int HS>
-    void launch_blocked_tma(const char* name, const Blocked3Args& a, const Blocked3Maps& m, double* A_out,
-                            double* B_out, double* u, double* w, double* r)
-    {
-        static unsigned set = 0;   // devices on which the shared-memory size was raised
-        if (!(set & (1u << (s->device & 31)))) {
-            TL_CUDA(cudaFuncSetAttribute(k3_blocked_tma<MODE, HS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kBlocked3TmaBytes));
-            set |= 1u << (s->device & 31);
-        }
-        TL3_LAUNCH(s, name, (k3_blocked_tma<MODE, HS><<<blocked3_grid(s->g), dim3(kRX, kRY), kBlocked3TmaBytes,
-                                                        s->stream>>>(s->g, a, m, A_out, B_out, u, w, r, done(),
-                                                                     s->d_mirror + kTmaErrWord)));
-    }
-
-    // Region planes by TMA where the boxes can start on 16-byte boundaries
-    // (even halo depth, margin and row length), else per-thread loads; the
-    // same results either way.
     template <int MODE>
     void launch_blocked(const Blocked3Args& a, const double* A_in, const double* B_in, double* A_out, double* B_out,
                         const double* u0, double* u, double* w, double* r)
     {
-        const char* name = MODE == 0 ? "k3_blocked<cheby>" : "k3_blocked<ppcg>";
-        if (tma_usable(s) && kTB3 % 2 == 0) {
-            const CUtensorMap* ma = tma_map(s, A_in, 5);
-            const CUtensorMap* mb = tma_map(s, B_in, 5);
-            const CUtensorMap* mc = tma_map(s, MODE == 0 ? u0 : u, 5);
-            const CUtensorMap* mx = tma_map(s, chunk->vec_kx, 5);
-            const CUtensorMap* my = tma_map(s, chunk->vec_ky, 5);
-            const CUtensorMap* mz = tma_map(s, chunk->vec_kz, 5);
-            if (ma && mb && mc && mx && my && mz && a.steps >= 1 && a.steps <= 2) {
-                const Blocked3Maps m{*ma, *mb, *mc, *mx, *my, *mz};
-                if (a.steps == 1) launch_blocked_tma<MODE, 1>(name, a, m, A_out, B_out, u, w, r);
-                else launch_blocked_tma<MODE, 2>(name, a, m, A_out, B_out, u, w, r);
-                return;
-            }
-        }
-        TL3_LAUNCH(s, name, (k3_blocked<MODE><<<blocked3_grid(s->g), dim3(kRX, kRY), 0, s->stream>>>(
-                                s->g, a, A_in, B_in, A_out, B_out, u0, u, w, r, chunk->vec_kx, chunk->vec_ky,
-                                chunk->vec_kz, done())));
+        launch_blocked3<MODE>(s, chunk, a, A_in, B_in, A_out, B_out, u0, u, w, r, done());
     }
 
     double norm(const double* b)

@@ -12,6 +12,7 @@
 #include "suite3d_impl.hpp"
 
 #include <algorithm>
+#include <vector>
 #include <cstring>
 
 using namespace tl3d;
@@ -80,8 +81,129 @@ static void launch_halos(TlSuite3D* s, Chunk* chunk, int depth, const int* which
                k3_local_halos<<<dim3(tl::ceil_div(per, 256), a.nf), 256, 0, s->stream>>>(g, depth, a));
 }
 
+// Launch sizes of up to kTB3 steps for n queued steps, made an even count
+// (the launches alternate buffers while the host holds the chunk's
+// pointers): a two-step launch is split when the count is odd. n >= 2.
+static std::vector<int> even_blocks(int n)
+{
+    std::vector<int> sizes;
+    for (int left = n; left > 0; left -= kTB3) sizes.push_back(std::min(kTB3, left));
+    if (sizes.size() % 2 == 1) {
+        for (int q = (int)sizes.size() - 1; q >= 0; --q) {
+            if (sizes[q] >= 2) {
+                sizes[q] -= 1;
+                sizes.insert(sizes.begin() + q + 1, 1);
+                break;
+            }
+        }
+    }
+    return sizes;
+}
+
+static void upload_queue(TlSuite3D* s, const TlSuite3D::Queue& q)
+{
+    const size_t n = q.a.size();
+    TL_CUDA(cudaMemcpyAsync(s->d_cheby_alphas, q.a.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+    TL_CUDA(cudaMemcpyAsync(s->d_cheby_betas, q.b.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+}
+
+// Runs the deferred PPCG inner steps (ppcg_solver.c:8-73 as the reference
+// drivers call them: sd = r / theta, then per step a depth-1 halo of sd and
+// r -= A sd, u += sd, sd = a sd + b r): temporally blocked launches (the fold
+// of each step at its start, sd reflected on the fly and its halo written)
+// and the last step's sd update, with the same results as one launch per
+// call; an even number of launches (the sd and r buffers alternate). One
+// step runs as the one-step kernels, and with none queued sd = r / theta
+// alone.
+static void run_ppcg_queue(TlSuite3D* s, Chunk* chunk)
+{
+    s->pq.active = false;
+    const int n = (int)s->pq.a.size();
+    const dim3 gr = interior_grid(s->g), bl = interior_block();
+    if (n <= 1) {
+        TL3_LAUNCH(s, "k3_ppcg_init", k3_ppcg_init<<<gr, bl, 0, s->stream>>>(s->g, chunk->theta, chunk->vec_r,
+                                                                              chunk->vec_sd));
+        if (n == 1) {   // the absorbed halo update, then the step
+            int which[TL3_NUM_FIELDS] = {0};
+            which[TL3_FIELD_SD] = 1;
+            launch_halos(s, chunk, 1, which);
+            TL3_LAUNCH(s, "k3_ppcg_inner_a", k3_ppcg_inner_a<<<gr, bl, 0, s->stream>>>(
+                                                 s->g, chunk->vec_u, chunk->vec_r, chunk->vec_kx, chunk->vec_ky,
+                                                 chunk->vec_kz, chunk->vec_sd));
+            TL3_LAUNCH(s, "k3_ppcg_sd", k3_ppcg_sd<<<gr, bl, 0, s->stream>>>(s->g, s->pq.a[0], s->pq.b[0],
+                                                                              chunk->vec_sd, chunk->vec_r));
+        }
+    } else {
+        upload_queue(s, s->pq);
+        int pp0 = 0;
+        for (int steps : even_blocks(n)) {
+            const Blocked3Args a{steps, pp0, 0, chunk->theta, s->d_cheby_alphas, s->d_cheby_betas};
+            launch_blocked3<1>(s, chunk, a, chunk->vec_sd, chunk->vec_r, s->alt[ALT3_SD], s->alt[ALT3_R], nullptr,
+                               chunk->vec_u, nullptr, nullptr, nullptr);
+            swap_alt(s, chunk, ALT3_SD);
+            swap_alt(s, chunk, ALT3_R);
+            pp0 += steps;
+        }
+        TL3_LAUNCH(s, "k3_ppcg_sd", k3_ppcg_sd<<<gr, bl, 0, s->stream>>>(s->g, s->pq.a[n - 1], s->pq.b[n - 1],
+                                                                          chunk->vec_sd, chunk->vec_r));
+    }
+    s->pq.a.clear();
+    s->pq.b.clear();
+}
+
+// The one-step Chebyshev trip of the run_* path (cheby_solver.c:62-99: w = A u,
+// r = u0 - w, p = alpha p + beta r, then u += p).
+static void cheby_trip_one_step(TlSuite3D* s, Chunk* chunk, double alpha, double beta)
+{
+    const dim3 gf = fused_grid(s->g), gr = interior_grid(s->g), bl = interior_block();
+    const Faces none{0, 0, 0, 0, 0, 0};
+    const tl::ChebyCoef coef{alpha, beta, nullptr, nullptr, nullptr};
+    tl::DevParams prm{};
+    TL3_LAUNCH(s, "k3_cheby_trip",
+               (k3_cheby_trip<false, false, false><<<gf, bl, 0, s->stream>>>(
+                   s->g, none, coef, 0.0, 1, chunk->vec_u, chunk->vec_p, chunk->vec_u, chunk->vec_p, chunk->vec_u0,
+                   chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr,
+                   tl::NoFinish(), prm, Tma3Maps{}, nullptr)));
+    TL3_LAUNCH(s, "k3_add_p", k3_add_p<false><<<gr, bl, 0, s->stream>>>(s->g, none, chunk->vec_u, chunk->vec_p));
+}
+
+// Runs the deferred Chebyshev trips (cheby_solver.c:62-99 as the reference
+// drivers call them: per trip a depth-1 halo of u, then the trip ending with
+// its u += p): temporally blocked launches, each trip's add at its end and u
+// reflected on the fly; the last launch also writes w and r and leaves u's
+// halo as the call-by-call sequence does (mirroring u before the last add).
+// An even number of launches (the u and p buffers alternate); a single trip
+// runs as the one-step kernels. The same results as one launch per call.
+static void run_cheby_queue(TlSuite3D* s, Chunk* chunk)
+{
+    s->cq.active = false;
+    const int n = (int)s->cq.a.size();
+    if (n == 1) {   // the absorbed halo update, then the one-step kernels
+        int which[TL3_NUM_FIELDS] = {0};
+        which[TL3_FIELD_U] = 1;
+        launch_halos(s, chunk, 1, which);
+        cheby_trip_one_step(s, chunk, s->cq.a[0], s->cq.b[0]);
+    } else if (n > 1) {
+        upload_queue(s, s->cq);
+        int first = 0;
+        for (int steps : even_blocks(n)) {
+            const Blocked3Args a{steps, first, first + steps == n ? 1 : 0, 0.0, s->d_cheby_alphas,
+                                 s->d_cheby_betas, 1};
+            launch_blocked3<0>(s, chunk, a, chunk->vec_u, chunk->vec_p, s->alt[ALT3_U], s->alt[ALT3_P],
+                               chunk->vec_u0, nullptr, chunk->vec_w, chunk->vec_r, nullptr);
+            swap_alt(s, chunk, ALT3_U);
+            swap_alt(s, chunk, ALT3_P);
+            first += steps;
+        }
+    }
+    s->cq.a.clear();
+    s->cq.b.clear();
+}
+
 void flush(TlSuite3D* s, Chunk* chunk)
 {
+    if (s->pq.active) run_ppcg_queue(s, chunk);
+    if (s->cq.active) run_cheby_queue(s, chunk);
     if (s->pend.calc_p) {
         TL3_LAUNCH(s, "k3_cg_close",
                    k3_cg_close<<<interior_grid(s->g), interior_block(), 0, s->stream>>>(
@@ -500,21 +622,33 @@ void run_cheby_solver_init(Chunk* chunk, Settings* settings)
 }
 
 // 3d/kernel_interface.h:42 (cheby_solver.c:62-99)
+// With temporal blocking on and all six faces external, trips called in the
+// reference drivers' pattern (a depth-1 halo update of u and nothing else
+// pending before each) are deferred and run temporally blocked when any other
+// run_* call needs the device state (run_cheby_queue); otherwise the trip
+// runs at once.
 void run_cheby_solver_iterate(Chunk* chunk, Settings* settings, double alpha, double beta)
 {
     (void)settings;
-    TlSuite3D* s = ready(chunk);
+    if (tl::failed()) return;
+    TlSuite3D* s = suite_of(chunk);
     if (!s) return;
-    const dim3 gf = fused_grid(s->g), gr = interior_grid(s->g), bl = interior_block();
-    const Faces none{0, 0, 0, 0, 0, 0};
-    const tl::ChebyCoef coef{alpha, beta, nullptr, nullptr, nullptr};
-    tl::DevParams prm{};
-    TL3_LAUNCH(s, "k3_cheby_trip",
-               (k3_cheby_trip<false, false, false><<<gf, bl, 0, s->stream>>>(
-                   s->g, none, coef, 0.0, 1, chunk->vec_u, chunk->vec_p, chunk->vec_u, chunk->vec_p, chunk->vec_u0,
-                   chunk->vec_w, chunk->vec_r, chunk->vec_kx, chunk->vec_ky, chunk->vec_kz, s->rs, nullptr,
-                   tl::NoFinish(), prm, Tma3Maps{}, nullptr)));
-    TL3_LAUNCH(s, "k3_add_p", k3_add_p<false><<<gr, bl, 0, s->stream>>>(s->g, none, chunk->vec_u, chunk->vec_p));
+    const Faces fc = faces_of(chunk);
+    if (s->temporal_blocking && fc.l && fc.r && fc.b && fc.t && fc.k && fc.f && !s->pq.active && !s->pend.calc_p &&
+        s->pend.halo[TL3_FIELD_U] <= 1 && (long)s->cq.a.size() < s->table_len) {
+        bool other = false;
+        for (int f = 0; f < TL3_NUM_FIELDS; ++f) other |= f != TL3_FIELD_U && s->pend.halo[f] != 0;
+        if (!other) {
+            s->pend.halo[TL3_FIELD_U] = 0;   // the blocked trips reflect u on the fly and write its halo
+            s->cq.active = true;
+            s->cq.a.push_back(alpha);
+            s->cq.b.push_back(beta);
+            return;
+        }
+    }
+    s = ready(chunk);
+    if (!s) return;
+    cheby_trip_one_step(s, chunk, alpha, beta);
 }
 
 // 3d/kernel_interface.h:46 (3d/c_kernels/omp3/jacobi_solver.c:9-66)
@@ -554,6 +688,13 @@ void run_ppcg_init(Chunk* chunk, Settings* settings)
     (void)settings;
     TlSuite3D* s = ready(chunk);
     if (!s) return;
+    const Faces fc = faces_of(chunk);
+    if (s->temporal_blocking && fc.l && fc.r && fc.b && fc.t && fc.k && fc.f) {
+        s->pq.active = true;   // sd = r / theta runs with the first queued step
+        s->pq.a.clear();
+        s->pq.b.clear();
+        return;
+    }
     TL3_LAUNCH(s, "k3_ppcg_init", k3_ppcg_init<<<interior_grid(s->g), interior_block(), 0, s->stream>>>(
                                       s->g, chunk->theta, chunk->vec_r, chunk->vec_sd));
 }
@@ -562,7 +703,22 @@ void run_ppcg_init(Chunk* chunk, Settings* settings)
 void run_ppcg_inner_iteration(Chunk* chunk, Settings* settings, double alpha, double beta)
 {
     (void)settings;
-    TlSuite3D* s = ready(chunk);
+    if (tl::failed()) return;
+    TlSuite3D* s = suite_of(chunk);
+    if (!s) return;
+    // queued only in the reference drivers' pattern: a depth-1 halo update of
+    // sd (and nothing else) requested right before the step
+    if (s->pq.active && !s->pend.calc_p && s->pend.halo[TL3_FIELD_SD] == 1 && (long)s->pq.a.size() < s->table_len) {
+        bool other = false;
+        for (int f = 0; f < TL3_NUM_FIELDS; ++f) other |= f != TL3_FIELD_SD && s->pend.halo[f] != 0;
+        if (!other) {
+            s->pend.halo[TL3_FIELD_SD] = 0;   // the blocked steps reflect sd on the fly and write its halo
+            s->pq.a.push_back(alpha);
+            s->pq.b.push_back(beta);
+            return;
+        }
+    }
+    s = ready(chunk);   // runs the queue, if any, and the pending operations
     if (!s) return;
     const dim3 gr = interior_grid(s->g), bl = interior_block();
     TL3_LAUNCH(s, "k3_ppcg_inner_a", k3_ppcg_inner_a<<<gr, bl, 0, s->stream>>>(

@@ -8,6 +8,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 enum AltField3 { ALT3_P = 0, ALT3_U = 1, ALT3_R = 2, ALT3_SD = 3, ALT3_COUNT = 4 };
 
 struct TlSuite3D {
@@ -40,7 +42,14 @@ struct TlSuite3D {
     double* d_cheby_betas = nullptr;
     int table_len = 0;
     bool tma = true;   // feed the CG w sweep by TMA where the layout allows (tl3d_set_tma)
-    bool temporal_blocking = true;   // device-driver Chebyshev / PPCG blocks (tl3d_set_temporal_blocking)
+    bool temporal_blocking = true;   // Chebyshev / PPCG blocks (tl3d_set_temporal_blocking)
+    // Chebyshev trips / PPCG inner steps of the run_* path deferred while the
+    // reference drivers' call pattern holds, then run temporally blocked
+    struct Queue {
+        bool active = false;
+        std::vector<double> a, b;
+    };
+    Queue cq, pq;
     struct TmaEntry {
         const double* ptr;
         int kind;
@@ -140,6 +149,50 @@ inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
 inline bool tma_usable(const TlSuite3D* s) { return s->tma && s->g.hd % 2 == 0 && s->g.x % 2 == 0; }
 
 inline bool tma_failed(const TlSuite3D* s) { return s->h_mirror && s->h_mirror[kTmaErrWord] != 0; }
+
+// One launch of the temporally blocked Chebyshev (MODE 0) / PPCG (MODE 1)
+// steps: region planes by TMA where the boxes can start on 16-byte
+// boundaries (even halo depth, margin and row length), else per-thread
+// loads; the same results either way. Internal linkage, like the kernels.
+template <int MODE, int HS>
+static void launch_blocked3_tma(TlSuite3D* s, const char* name, const Blocked3Args& a, const Blocked3Maps& m,
+                                double* A_out, double* B_out, double* u, double* w, double* r, const int* done)
+{
+    static unsigned set = 0;   // devices on which the shared-memory size was raised
+    if (!(set & (1u << (s->device & 31)))) {
+        TL_CUDA(cudaFuncSetAttribute(k3_blocked_tma<MODE, HS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kBlocked3TmaBytes));
+        set |= 1u << (s->device & 31);
+    }
+    TL3_LAUNCH(s, name, (k3_blocked_tma<MODE, HS><<<blocked3_grid(s->g), dim3(kRX, kRY), kBlocked3TmaBytes,
+                                                    s->stream>>>(s->g, a, m, A_out, B_out, u, w, r, done,
+                                                                 s->d_mirror + kTmaErrWord)));
+}
+
+template <int MODE>
+static void launch_blocked3(TlSuite3D* s, Chunk* chunk, const Blocked3Args& a, const double* A_in,
+                            const double* B_in, double* A_out, double* B_out, const double* u0, double* u, double* w,
+                            double* r, const int* done)
+{
+    const char* name = MODE == 0 ? "k3_blocked<cheby>" : "k3_blocked<ppcg>";
+    if (tma_usable(s) && kTB3 % 2 == 0 && a.steps >= 1 && a.steps <= 2) {
+        const CUtensorMap* ma = tma_map(s, A_in, 5);
+        const CUtensorMap* mb = tma_map(s, B_in, 5);
+        const CUtensorMap* mc = tma_map(s, MODE == 0 ? u0 : u, 5);
+        const CUtensorMap* mx = tma_map(s, chunk->vec_kx, 5);
+        const CUtensorMap* my = tma_map(s, chunk->vec_ky, 5);
+        const CUtensorMap* mz = tma_map(s, chunk->vec_kz, 5);
+        if (ma && mb && mc && mx && my && mz) {
+            const Blocked3Maps m{*ma, *mb, *mc, *mx, *my, *mz};
+            if (a.steps == 1) launch_blocked3_tma<MODE, 1>(s, name, a, m, A_out, B_out, u, w, r, done);
+            else launch_blocked3_tma<MODE, 2>(s, name, a, m, A_out, B_out, u, w, r, done);
+            return;
+        }
+    }
+    TL3_LAUNCH(s, name, (k3_blocked<MODE><<<blocked3_grid(s->g), dim3(kRX, kRY), 0, s->stream>>>(
+                            s->g, a, A_in, B_in, A_out, B_out, u0, u, w, r, chunk->vec_kx, chunk->vec_ky,
+                            chunk->vec_kz, done)));
+}
 
 // The fused CG w sweep (k3_cg_w semantics), by TMA where possible.
 // Internal linkage, like the kernels it launches: each translation unit has

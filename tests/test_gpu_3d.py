@@ -327,3 +327,42 @@ def test_3d_blocked_trips_match_one_step(solver, dims, inner):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("solver,dims,inner,cap", [
+    ("cheby", (37, 19, 23), 10, None),
+    ("cheby", (38, 19, 23), 10, None),
+    ("cheby", (38, 19, 23), 10, 183),
+    ("ppcg", (37, 19, 23), 10, None),
+    ("ppcg", (38, 19, 23), 7, None),
+    ("ppcg", (38, 19, 23), 2, None),
+    ("ppcg", (38, 19, 23), 1, None),
+])
+def test_3d_run_path_queues_are_bit_identical(solver, dims, inner, cap):
+    """Through run_* (the reference drivers' call sequence), the Chebyshev
+    trips and PPCG inner steps deferred and run temporally blocked (each trip
+    ending with its u += p; sd = r / theta with the first step, the last sd
+    update after the blocks) give the same iteration counts, summaries and
+    memory state, bit for bit, as one launch per call; per-thread loads (odd
+    rows) and TMA-staged regions (even rows), an iteration cap that stops
+    the queue between norm checks, and inner-step counts that split, fill
+    and underfill the two-step blocks."""
+    prob = problems.seeded(3, dims, 37, 3, 1, solver=solver, end_step=2, name="q3").with_(ppcg_inner_steps=inner)
+    if cap:
+        prob = prob.with_(max_iters=cap)
+    text = prob.tea_in()
+    a, b = Host(text, 3), Host(text, 3)
+    try:
+        b.lib.tl3d_set_temporal_blocking(b.chunk, 0)
+        for tt in range(2):
+            ra = a.solve(tt)
+            rb = b.solve(tt)
+            assert ra.iterations == rb.iterations
+            assert ra.iterations.get("Cheby" if solver == "cheby" else "PPCG", 0) > 0
+            assert ra.summary == rb.summary
+            assert ra.exact_error == rb.exact_error
+            for f in FIELDS3:
+                assert np.array_equal(a.download(f), b.download(f)), (solver, dims, tt, f)
+    finally:
+        a.finalise()
+        b.finalise()
