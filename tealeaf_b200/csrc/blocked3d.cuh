@@ -245,11 +245,14 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked(Geo g, Blocke
 }
 
 // ------------------------------------------------------ TMA-staged form --
-// k3_blocked with the region planes brought in by TMA: one thread issues the
-// six kRX x kRY boxes of plane p (A, B, C = u0 or u, kx, ky, kz; from grid
-// column hd + bx kTX3 - kTB3, row hd + by kTY3 - kTB3) into a ring of kRing3
-// planes on one shared-memory barrier per slot, kPf3 planes ahead of the
-// plane that enters, so the steps read every operand from shared memory.
+// The same wavefront with the region planes brought in by TMA and two region
+// rows per thread: a block of 32 x 12 threads owns a 32 x 24-column region (a
+// 28 x 20 tile plus the kTB3 margin), thread row t holding rows 2t and 2t+1,
+// whose y-neighbour within the pair comes from registers. One thread issues
+// the six kRX x kRYT boxes of plane p (A, B, C = u0 or u, kx, ky, kz; from
+// grid column hd + bx kTX3 - kTB3, row hd + by kTYT3 - kTB3) into a ring of
+// kRing3 planes on one shared-memory barrier per slot, kPf3 planes ahead of
+// the plane that enters, so the steps read every operand from shared memory.
 // Boxes start on a 16-byte boundary when the halo depth, the margin and the
 // row length are even; cells outside the array read as zero, and, as in
 // k3_blocked, only cells inside the interior and the margin are used. The
@@ -257,26 +260,31 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked(Geo g, Blocke
 // front face coefficient of the last plane). The launch's step count is a
 // template parameter (HS = a.steps), so the level loop is straight-line
 // code. Every wait is bounded (err); every issued plane is waited for.
-constexpr int kPf3 = 2;                       // planes issued ahead
-constexpr int kRing3 = kTB3 + 1 + kPf3;       // planes s - kTB3 .. s + kPf3
+constexpr int kTYT = 12;                  // thread rows of the staged kernel
+constexpr int kRYT = 2 * kTYT;            // region rows: two per thread
+constexpr int kTYT3 = kRYT - 2 * kTB3;    // tile rows
+constexpr int kB3TThreads = kRX * kTYT;   // 384
+constexpr int kPf3 = 2;                   // planes issued ahead
+constexpr int kRing3 = kTB3 + 1 + kPf3;   // planes s - kTB3 .. s + kPf3
 struct Region3 {
-    alignas(128) double f[6][kRY][kRX];       // A, B, C, kx, ky, kz
+    alignas(128) double f[6][kRYT][kRX];   // A, B, C, kx, ky, kz
 };
+static_assert(sizeof(Region3) % 128 == 0, "ring slots start on 128-byte boundaries");
 struct Blocked3Maps {
     CUtensorMap a, b, c, kx, ky, kz;
 };
 constexpr size_t kBlocked3TmaBytes = kRing3 * sizeof(Region3) + kRing3 * 8 + 128;
 
 template <int MODE, int HS>
-static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Blocked3Args a,
-                                                                       const __grid_constant__ Blocked3Maps maps,
-                                                                       double* A_out, double* __restrict__ B_out,
-                                                                       double* __restrict__ u,
-                                                                       double* __restrict__ w,
-                                                                       double* __restrict__ r,
-                                                                       const int* __restrict__ done, int* err)
+static __global__ void __launch_bounds__(kB3TThreads, 1) k3_blocked_tma(Geo g, Blocked3Args a,
+                                                                        const __grid_constant__ Blocked3Maps maps,
+                                                                        double* A_out, double* __restrict__ B_out,
+                                                                        double* __restrict__ u,
+                                                                        double* __restrict__ w,
+                                                                        double* __restrict__ r,
+                                                                        const int* __restrict__ done, int* err)
 {
-    __shared__ double sp[kTB3][2][kRY][kRX];   // level l's stencil field, plane parity, region
+    __shared__ double sp[kTB3][2][kRYT][kRX];   // level l's stencil field, plane parity, region
     extern __shared__ __align__(128) unsigned char b3_raw[];
     if (gate_closed(done)) return;
     unsigned char* base = b3_raw + ((128 - (tl::smem_addr(b3_raw) & 127)) & 127);
@@ -286,27 +294,39 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
     const long xy = g.xy();
     const int ilo = hd, ihi = g.x - hd, jlo = hd, jhi = g.y - hd, zlo = hd, zhi = g.z - hd;
     constexpr int H = HS;   // steps of this launch (a.steps)
-    const int cx = threadIdx.x, cy = threadIdx.y;
-    const bool leader = cx == 0 && cy == 0;
-    const int xs = hd + blockIdx.x * kTX3 - kTB3, ys = hd + blockIdx.y * kTY3 - kTB3;   // region origin
-    const int gx = xs + cx, gy = ys + cy;
-    const bool colin = gx >= ilo && gx < ihi && gy >= jlo && gy < jhi;
+    const int cx = threadIdx.x, ty = threadIdx.y;
+    const bool leader = cx == 0 && ty == 0;
+    const int xs = hd + blockIdx.x * kTX3 - kTB3, ys = hd + blockIdx.y * kTYT3 - kTB3;   // region origin
+    const int gx = xs + cx;
     const int mx = max(max(kTB3 - cx, cx - (kTB3 + kTX3 - 1)), 0);
-    const int my = max(max(kTB3 - cy, cy - (kTB3 + kTY3 - 1)), 0);
-    const bool in_tile = colin && mx == 0 && my == 0;
-    const bool at_l = gx == ilo, at_r = gx == ihi - 1, at_b = gy == jlo, at_t = gy == jhi - 1;
-    const int Z0 = zlo + blockIdx.z * kBZ3, Z1 = min(Z0 + kBZ3, zhi);
-    const long col = gx + (long)gy * x;
-
-    double win[kTB3][3], bp[kTB3], bn[kTB3];
-    double uacc[kTB3 + 1];
+    const bool at_l = gx == ilo, at_r = gx == ihi - 1;
+    bool colin[2], in_tile[2], at_b[2], at_t[2];
+    long col[2];
 #pragma unroll
-    for (int l = 0; l < kTB3; ++l) {
-        win[l][0] = win[l][1] = win[l][2] = 0.0;
-        bp[l] = bn[l] = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        const int ry = 2 * ty + k, gy = ys + ry;
+        const int my = max(max(kTB3 - ry, ry - (kTB3 + kTYT3 - 1)), 0);
+        colin[k] = gx >= ilo && gx < ihi && gy >= jlo && gy < jhi;
+        in_tile[k] = colin[k] && mx == 0 && my == 0;
+        at_b[k] = gy == jlo;
+        at_t[k] = gy == jhi - 1;
+        col[k] = gx + (long)gy * x;
     }
+    const int Z0 = zlo + blockIdx.z * kBZ3, Z1 = min(Z0 + kBZ3, zhi);
+
+    // per level l < kTB3 and row k: stencil field of the three planes around
+    // the plane level l + 1 advances next; B of that plane (bp) and the newest (bn)
+    double win[kTB3][3][2], bp[kTB3][2], bn[kTB3][2];
+    double uacc[kTB3 + 1][2];   // PPCG: u of the tile plane at level l (plane s - l), its adds so far
 #pragma unroll
-    for (int q = 0; q <= kTB3; ++q) uacc[q] = 0.0;
+    for (int l = 0; l < kTB3; ++l)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            win[l][0][k] = win[l][1][k] = win[l][2][k] = 0.0;
+            bp[l][k] = bn[l][k] = 0.0;
+        }
+#pragma unroll
+    for (int q = 0; q <= kTB3; ++q) uacc[q][0] = uacc[q][1] = 0.0;
     double ca[kTB3], cb[kTB3];
 #pragma unroll
     for (int l = 0; l < kTB3; ++l) {
@@ -325,10 +345,10 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
     const int s_begin = max(Z0 - H, zlo);
     const int s_end = Z1 + H;
     const int load_end = min(Z1 + H, zhi + 1);   // planes staged: s_begin .. load_end - 1
-    auto slot = [&](int p) { return (p - s_begin) % kRing3; };
     auto issue = [&](int p) {
-        Region3& R = ring[slot(p)];
-        unsigned long long* bar = &bars[slot(p)];
+        const int q = (p - s_begin) % kRing3;
+        Region3& R = ring[q];
+        unsigned long long* bar = &bars[q];
         tl::mbar_expect_tx(bar, (unsigned)sizeof(Region3));
         tl::tma_load_3d(&R.f[0][0][0], &maps.a, xs, ys, p, bar);
         tl::tma_load_3d(&R.f[1][0][0], &maps.b, xs, ys, p, bar);
@@ -346,35 +366,42 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
         for (int p = s_begin; p < s_begin + kPf3 && p < load_end; ++p) issue(p);
 
     // does the region reach a domain face in x or y (then neighbours there are reflected)?
-    const bool touches = xs <= ilo || xs + kRX > ihi - 1 || ys <= jlo || ys + kRY > jhi - 1;
+    const bool touches = xs <= ilo || xs + kRX > ihi - 1 || ys <= jlo || ys + kRYT > jhi - 1;
     int qs = 0;          // ring slot of plane s
     unsigned ph = 0;     // barrier phase of that slot's current use
     for (int s = s_begin; s < s_end; ++s) {
         if (s < load_end) tl::mbar_wait(&bars[qs], ph, err);
         __syncthreads();   // the previous step's planes are read: the slot of plane s - kTB3 - 1 is free
         if (leader && s + kPf3 < load_end) issue(s + kPf3);
-        if (MODE == 1) {
+        if (MODE == 1) {   // every plane in flight moves up one level
 #pragma unroll
-            for (int l = kTB3; l > 0; --l) uacc[l] = uacc[l - 1];
+            for (int l = kTB3; l > 0; --l) {
+                uacc[l][0] = uacc[l - 1][0];
+                uacc[l][1] = uacc[l - 1][1];
+            }
         }
         // level 0: plane s enters
         {
             const bool act0 = s < min(Z1 + H, zhi);
-            double av = 0.0, bv = 0.0, uv = 0.0;
-            if (act0 && colin) {
-                const Region3& R = ring[qs];
-                av = R.f[0][cy][cx];
-                bv = R.f[1][cy][cx];
-                if (MODE == 1 && in_tile && s >= Z0 && s < Z1) uv = R.f[2][cy][cx];
+            const Region3& R = ring[qs];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int ry = 2 * ty + k;
+                double av = 0.0, bv = 0.0, uv = 0.0;
+                if (act0 && colin[k]) {
+                    av = R.f[0][ry][cx];
+                    bv = R.f[1][ry][cx];
+                    if (MODE == 1 && in_tile[k] && s >= Z0 && s < Z1) uv = R.f[2][ry][cx];
+                }
+                const double sv = MODE == 0 ? (a.add_end ? av : av + bv) : fold(0, av, bv);
+                if (MODE == 1) uacc[0][k] = uv + sv;
+                win[0][0][k] = win[0][1][k];
+                win[0][1][k] = win[0][2][k];
+                win[0][2][k] = sv;
+                bp[0][k] = bn[0][k];
+                bn[0][k] = bv;
+                if (act0) sp[0][s & 1][ry][cx] = sv;
             }
-            const double sv = MODE == 0 ? (a.add_end ? av : av + bv) : fold(0, av, bv);
-            if (MODE == 1) uacc[0] = uv + sv;
-            win[0][0] = win[0][1];
-            win[0][1] = win[0][2];
-            win[0][2] = sv;
-            bp[0] = bn[0];
-            bn[0] = bv;
-            if (act0) sp[0][s & 1][cy][cx] = sv;
         }
         auto levels = [&](auto reflect) {
             constexpr bool REFLECT = decltype(reflect)::value;
@@ -385,11 +412,14 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
                 const bool act = z >= max(Z0 - H + l, zlo) && z < min(Z1 + H - l, zhi);
                 if (!act) {
                     if (l < H) {
-                        win[l][0] = win[l][1];
-                        win[l][1] = win[l][2];
-                        win[l][2] = 0.0;
-                        bp[l] = bn[l];
-                        bn[l] = 0.0;
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            win[l][0][k] = win[l][1][k];
+                            win[l][1][k] = win[l][2][k];
+                            win[l][2][k] = 0.0;
+                            bp[l][k] = bn[l][k];
+                            bn[l][k] = 0.0;
+                        }
                     }
                     continue;
                 }
@@ -397,64 +427,75 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
                 const int qf = qs - l + 1 < 0 ? qs - l + 1 + kRing3 : qs - l + 1;  // slot of plane z + 1
                 const Region3& R = ring[qz];
                 const Region3& F = ring[qf];
-                const double* W = win[l - 1];
-                const double c = W[1];
-                double lf = __shfl_up_sync(kFull3, c, 1);
-                double rt = __shfl_down_sync(kFull3, c, 1);
-                double dn = cy > 0 ? sp[l - 1][z & 1][cy - 1][cx] : 0.0;
-                double up = cy < kRY - 1 ? sp[l - 1][z & 1][cy + 1][cx] : 0.0;
-                double bk = W[0], fr = W[2];
-                if (REFLECT) {
-                    if (at_l) lf = c;
-                    if (at_r) rt = c;
-                    if (at_b) dn = c;
-                    if (at_t) up = c;
-                }
-                if (z == zlo) bk = c;
-                if (z == zhi - 1) fr = c;
-                const double kxc = R.f[3][cy][cx];
-                const double kxr = cx + 1 < kRX ? R.f[3][cy][cx + 1] : 0.0;
-                const double kyc = R.f[4][cy][cx];
-                const double kyu = cy + 1 < kRY ? R.f[4][cy + 1][cx] : 0.0;
-                const double kzc = R.f[5][cy][cx];
-                const double kzf = F.f[5][cy][cx];
-                const double cc = MODE == 0 ? R.f[2][cy][cx] : 0.0;
-                const double v = smvp(kxc, kxr, kyc, kyu, kzc, kzf, c, lf, rt, dn, up, bk, fr);
-                const double bz = bp[l - 1];
-                const long i = col + (long)z * xy;
-                double bnew, snew = 0.0;
-                if (MODE == 0) {
-                    const double res = cc - v;
-                    bnew = ca[l - 1] * bz + cb[l - 1] * res;
-                    if (l == H && a.wr_last && in_tile && z >= Z0 && z < Z1) {
-                        w[i] = v;
-                        r[i] = res;
-                    }
-                    if (l < H) snew = c + bnew;
-                } else {
-                    bnew = bz - v;
-                    if (l < H) snew = fold(l, c, bnew);
-                    if (l < H) uacc[l] += snew;
-                }
-                if (l < H) {
-                    win[l][0] = win[l][1];
-                    win[l][1] = win[l][2];
-                    win[l][2] = snew;
-                    bp[l] = bn[l];
-                    bn[l] = bnew;
-                    sp[l][z & 1][cy][cx] = snew;
-                } else if (in_tile && z >= Z0 && z < Z1) {
-                    A_out[i] = (MODE == 0 && a.add_end) ? c + bnew : c;   // halo: u before the last add
-                    B_out[i] = bnew;
-                    if (MODE == 1) u[i] = uacc[l];
+                const double c0 = win[l - 1][1][0], c1 = win[l - 1][1][1];
+                double snew[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int ry = 2 * ty + k;
+                    const double c = k == 0 ? c0 : c1;
+                    double lf = __shfl_up_sync(kFull3, c, 1);
+                    double rt = __shfl_down_sync(kFull3, c, 1);
+                    double dn = k == 1 ? c0 : (ry > 0 ? sp[l - 1][z & 1][ry - 1][cx] : 0.0);
+                    double up = k == 0 ? c1 : (ry < kRYT - 1 ? sp[l - 1][z & 1][ry + 1][cx] : 0.0);
+                    double bk = win[l - 1][0][k], fr = win[l - 1][2][k];
                     if (REFLECT) {
-                        if (at_l) A_out[i - 1] = c;
-                        if (at_r) A_out[i + 1] = c;
-                        if (at_b) A_out[i - x] = c;
-                        if (at_t) A_out[i + x] = c;
+                        if (at_l) lf = c;
+                        if (at_r) rt = c;
+                        if (at_b[k]) dn = c;
+                        if (at_t[k]) up = c;
                     }
-                    if (z == zlo) A_out[i - xy] = c;
-                    if (z == zhi - 1) A_out[i + xy] = c;
+                    if (z == zlo) bk = c;
+                    if (z == zhi - 1) fr = c;
+                    const double kxc = R.f[3][ry][cx];
+                    const double kxr = cx + 1 < kRX ? R.f[3][ry][cx + 1] : 0.0;
+                    const double kyc = R.f[4][ry][cx];
+                    const double kyu = ry + 1 < kRYT ? R.f[4][ry + 1][cx] : 0.0;
+                    const double kzc = R.f[5][ry][cx];
+                    const double kzf = F.f[5][ry][cx];
+                    const double cc = MODE == 0 ? R.f[2][ry][cx] : 0.0;
+                    const double v = smvp(kxc, kxr, kyc, kyu, kzc, kzf, c, lf, rt, dn, up, bk, fr);
+                    const double bz = bp[l - 1][k];
+                    const long i = col[k] + (long)z * xy;
+                    double bnew;
+                    snew[k] = 0.0;
+                    if (MODE == 0) {
+                        const double res = cc - v;
+                        bnew = ca[l - 1] * bz + cb[l - 1] * res;
+                        if (l == H && a.wr_last && in_tile[k] && z >= Z0 && z < Z1) {
+                            w[i] = v;
+                            r[i] = res;
+                        }
+                        if (l < H) snew[k] = c + bnew;
+                    } else {
+                        bnew = bz - v;
+                        if (l < H) snew[k] = fold(l, c, bnew);
+                        if (l < H) uacc[l][k] += snew[k];
+                    }
+                    if (l < H) {
+                        bp[l][k] = bn[l][k];
+                        bn[l][k] = bnew;
+                        sp[l][z & 1][ry][cx] = snew[k];
+                    } else if (in_tile[k] && z >= Z0 && z < Z1) {
+                        A_out[i] = (MODE == 0 && a.add_end) ? c + bnew : c;   // halo: u before the last add
+                        B_out[i] = bnew;
+                        if (MODE == 1) u[i] = uacc[l][k];
+                        if (REFLECT) {
+                            if (at_l) A_out[i - 1] = c;
+                            if (at_r) A_out[i + 1] = c;
+                            if (at_b[k]) A_out[i - x] = c;
+                            if (at_t[k]) A_out[i + x] = c;
+                        }
+                        if (z == zlo) A_out[i - xy] = c;
+                        if (z == zhi - 1) A_out[i + xy] = c;
+                    }
+                }
+                if (l < H) {   // the window moves after both rows used level l - 1's planes
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        win[l][0][k] = win[l][1][k];
+                        win[l][1][k] = win[l][2][k];
+                        win[l][2][k] = snew[k];
+                    }
                 }
             }
         };
@@ -466,6 +507,12 @@ static __global__ void __launch_bounds__(kB3Threads, 1) k3_blocked_tma(Geo g, Bl
         }
     }
     // every issued plane was waited for (planes s_begin .. load_end - 1 at their steps)
+}
+
+inline dim3 blocked3_tma_grid(const Geo& g)
+{
+    return dim3(tl::ceil_div(g.x - 2 * g.hd, kTX3), tl::ceil_div(g.y - 2 * g.hd, kTYT3),
+                tl::ceil_div(g.z - 2 * g.hd, kBZ3));
 }
 
 // sum(b^2) over the interior with the partition and order of the one-step

@@ -122,7 +122,7 @@ void swap_alt(TlSuite3D* s, Chunk* chunk, AltField3 f);
 
 // Tensor map of a chunk array for walkt: kind 0 operand (box (BX+4) x (BY+2)),
 // 1 kx (BX+2) x BY, 2 ky BX x (BY+1), 3 kz BX x BY; for k3_cg_ur_tma kind 4
-// BX x BY x kPlanesU; for k3_blocked_tma kind 5 kRX x kRY; encoded once per
+// BX x BY x kPlanesU; for k3_blocked_tma kind 5 kRX x kRYT; encoded once per
 // array.
 inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
 {
@@ -132,7 +132,7 @@ inline const CUtensorMap* tma_map(TlSuite3D* s, const double* ptr, int kind)
     const int cap = (int)(sizeof(s->tma_cache) / sizeof(s->tma_cache[0]));
     const int slot = s->tma_n < cap ? s->tma_n : (s->tma_next++ % cap);
     static const unsigned box[6][3] = {{BX + 4, BY + 2, 1}, {BX + 2, BY, 1}, {BX, BY + 1, 1}, {BX, BY, 1},
-                                       {BX, BY, kPlanesU}, {kRX, kRY, 1}};
+                                       {BX, BY, kPlanesU}, {kRX, kRYT, 1}};
     CUtensorMap m;
     if (!tl::tma_encode_3d(&m, ptr, s->g.x, s->g.y, s->g.z, box[kind][0], box[kind][1], box[kind][2]))
         return nullptr;
@@ -164,7 +164,7 @@ static void launch_blocked3_tma(TlSuite3D* s, const char* name, const Blocked3Ar
                                      (int)kBlocked3TmaBytes));
         set |= 1u << (s->device & 31);
     }
-    TL3_LAUNCH(s, name, (k3_blocked_tma<MODE, HS><<<blocked3_grid(s->g), dim3(kRX, kRY), kBlocked3TmaBytes,
+    TL3_LAUNCH(s, name, (k3_blocked_tma<MODE, HS><<<blocked3_tma_grid(s->g), dim3(kRX, kTYT), kBlocked3TmaBytes,
                                                     s->stream>>>(s->g, a, m, A_out, B_out, u, w, r, done,
                                                                  s->d_mirror + kTmaErrWord)));
 }
