@@ -389,9 +389,10 @@ typedef struct TlRefineStats
  * timestep of solve() (2d/diffuse.c:22-80: halos, cg_init, u0 = u, solve,
  * finalise) with the solve run to the relative FP64 residual
  * ||u0 - A u||_2 / ||u0||_2 <= rel_tol. precision 32: vectors and operator
- * coefficients stored in FP32, FP64 arithmetic and FP64 dot products, the
- * solution accumulated in FP64 with the residual recomputed in FP64 (reliable
- * updates); precision 64: the same iteration with FP64 storage. The solve is
+ * coefficients stored in FP32, the stencil and vector updates in FP32
+ * arithmetic, FP64 dot products and scalars, the solution accumulated in FP64
+ * with the residual recomputed in FP64 (reliable updates); precision 64: the
+ * same iteration with FP64 storage and arithmetic. The solve is
  * CG, or PPCG when settings->solver is TL_PPCG_SOLVER (2d/drivers/ppcg_driver.c:
  * CG trips to the reference's switch test, Lanczos eigenvalue bounds and
  * Chebyshev coefficients in FP64 from the FP64 CG scalars, outer steps with

@@ -3,8 +3,9 @@
 // tl2d_refine_solve_step solves one timestep's system A u = u0 (the operator
 // of 2d/c_kernels/omp3/cg.c:9-85 with the reflective boundary) to a stated
 // relative residual ||u0 - A u||_2 / ||u0||_2 <= rel_tol, with one algorithm
-// (refine2d.cuh: CG on T-stored vectors and coefficients, FP64 arithmetic
-// and dot products, FP64 solution with reliable FP64 residual replacement) in
+// (refine2d.cuh: CG on T-stored vectors and coefficients, arithmetic in T,
+// FP64 dot products and scalars, FP64 solution with reliable FP64 residual
+// replacement) in
 // two storage precisions on identical inputs: T = float (48 B per cell per
 // iteration) and T = double (96 B).
 //
@@ -38,7 +39,8 @@ __global__ void __launch_bounds__(BX, Pack<T>::MINB) k_rf_w(Lay L, const MxState
 {
     if (mx_idle(st)) return;
     const double bt = FUSE_P ? st->beta : 0.0;
-    double acc[1] = {rf_w_tile<T, FUSE_P>(L, blockIdx.x, blockIdx.y, bt, p_in, p_out, r, w, kx, ky)};
+    double acc[1] = {rf_w_tile<T, FUSE_P, false, typename RfMath<T>::M>(L, blockIdx.x, blockIdx.y, bt, p_in, p_out,
+                                                                         r, w, kx, ky)};
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 
@@ -48,7 +50,7 @@ __global__ void __launch_bounds__(BX, Pack<T>::MINB) k_rf_ur(Lay L, const MxStat
                                                              const T* __restrict__ w, ReduceSlots rs, FinMxUr fin)
 {
     if (mx_idle(st)) return;
-    double acc[1] = {rf_ur_tile<T>(L, blockIdx.x, blockIdx.y, st->alpha, xs, p, r, w)};
+    double acc[1] = {rf_ur_tile<T, false, typename RfMath<T>::M>(L, blockIdx.x, blockIdx.y, st->alpha, xs, p, r, w)};
     tl::grid_sum<1, BX>(acc, rs, block_id(), block_count(), fin);
 }
 

@@ -4,9 +4,10 @@
 // (batch2d.cu).
 //
 // CG whose vectors (p, r, w, the solution correction xs) and operator
-// coefficients (kx, ky) are stored in T (float or double). Every sweep
-// computes in FP64 registers and every dot product (p.w, r.r) is accumulated
-// in FP64, so w is the FP64 image of the stored p and only the stores round.
+// coefficients (kx, ky) are stored in T (float or double). The refinement
+// timestep's sweeps compute in T (the stencil and vector updates in FP32 for
+// FP32 storage; RfMath), the batched solver's in FP64 registers; every dot
+// product (p.w, r.r) is accumulated in FP64.
 // The solution is accumulated in FP64 (the chunk's u): when r.r of the stored
 // residual has dropped by kUpdateDelta^2 since the last replacement (or looks
 // converged), xs is folded into u, the residual u0 - A u is recomputed in
@@ -25,6 +26,8 @@
 // stays zero through the iteration (zero coefficients, zero start). A tile is
 // BX threads x N cells (8 bytes of a row per thread) x L.rows rows.
 #pragma once
+
+#include <type_traits>
 
 #include "kernels2d.cuh"
 
@@ -204,6 +207,30 @@ union Cells {
     T e[Pack<T>::N];
 };
 
+// Arithmetic type of the refinement timestep's CG sweeps for storage type T:
+// the storage precision itself (TL2D_RF_MATH_T 1: FP32 arithmetic for FP32
+// storage, measured 9.81 against 10.61 s for the 8192^2 CG timestep to
+// 1e-10 with FP64 arithmetic, same iterations) or FP64 (0). Dot products, the
+// scalars and the FP64 residual stay FP64 either way; the batched solver's
+// sweeps keep FP64 arithmetic (their default M).
+#ifndef TL2D_RF_MATH_T
+#define TL2D_RF_MATH_T 1
+#endif
+template <typename T>
+struct RfMath {
+    using M = double;
+};
+template <>
+struct RfMath<float> {
+    using M = std::conditional_t<TL2D_RF_MATH_T != 0, float, double>;
+};
+// The 5-point operator in type M, in the operand order of smvp.
+template <typename M>
+__device__ __forceinline__ M smvp_m(M kxc, M kxr, M kyc, M kyu, M c, M l, M r, M d, M u)
+{
+    return (M(1) + (kxr + kxc) + (kyu + kyc)) * c - (kxr * r + kxc * l) - (kyu * u + kyc * d);
+}
+
 template <typename T>
 __device__ __forceinline__ Cells<T> ld(const T* p)
 {
@@ -313,28 +340,29 @@ __global__ void __launch_bounds__(256) k_rf_init(int gx, int hd, Lay L, const do
     tl::grid_sum<3, 256>(acc, rs, blockIdx.x, gridDim.x, fin);
 }
 
-// CG sweep 1 over tile (tx, ty), FP64 arithmetic: [p = beta p + r] (rounded
+// CG sweep 1 over tile (tx, ty), arithmetic in M: [p = beta p + r] (rounded
 // to T as stored), w = A p; returns this thread's share of sum(w p) over the
 // stored values. All threads of the block take part (warp shuffles).
-template <typename T, bool FUSE_P, bool CG = false>
-__device__ __forceinline__ double rf_w_tile(const Lay& L, int tx, int ty, double bt, const T* __restrict__ p_in,
+template <typename T, bool FUSE_P, bool CG = false, typename M = double>
+__device__ __forceinline__ double rf_w_tile(const Lay& L, int tx, int ty, double bt_, const T* __restrict__ p_in,
                                             T* __restrict__ p_out, const T* __restrict__ r, T* __restrict__ w,
                                             const T* __restrict__ kx, const T* __restrict__ ky)
 {
     constexpr int N = Pack<T>::N;
     double acc = 0.0;
     const Span<N> s(L, tx, ty);
+    const M bt = (M)bt_;
     auto cur = [&](long idx) -> Cells<T> {
         Cells<T> c = ldc<CG>(p_in + idx);
         if (FUSE_P) {
             const Cells<T> q = ldc<CG>(r + idx);
 #pragma unroll
-            for (int m = 0; m < N; ++m) c.e[m] = (T)(bt * (double)c.e[m] + (double)q.e[m]);
+            for (int m = 0; m < N; ++m) c.e[m] = (T)(bt * (M)c.e[m] + (M)q.e[m]);
         }
         return c;
     };
     auto cur1 = [&](long idx) -> T {
-        return FUSE_P ? (T)(bt * (double)ldc1<CG>(p_in + idx) + (double)ldc1<CG>(r + idx)) : ldc1<CG>(p_in + idx);
+        return FUSE_P ? (T)(bt * (M)ldc1<CG>(p_in + idx) + (M)ldc1<CG>(r + idx)) : ldc1<CG>(p_in + idx);
     };
     const long xp = L.xp;
     long i = (long)(s.j0 + 1) * xp + s.cc;
@@ -353,12 +381,11 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
         Cells<T> wv;
 #pragma unroll
         for (int m = 0; m < N; ++m) {
-            const double c = (double)pc.e[m];
-            const double l = m == 0 ? (double)pl : (double)pc.e[m - 1];
-            const double rr = m == N - 1 ? (double)pr : (double)pc.e[m + 1];
-            const double kr = m == N - 1 ? (double)kxr : (double)kxc.e[m + 1];
-            wv.e[m] = (T)smvp((double)kxc.e[m], kr, (double)kyc.e[m], (double)kyu.e[m], c, l, rr, (double)pd.e[m],
-                              (double)pu.e[m]);
+            const M c = (M)pc.e[m];
+            const M l = m == 0 ? (M)pl : (M)pc.e[m - 1];
+            const M rr = m == N - 1 ? (M)pr : (M)pc.e[m + 1];
+            const M kr = m == N - 1 ? (M)kxr : (M)kxc.e[m + 1];
+            wv.e[m] = (T)smvp_m<M>((M)kxc.e[m], kr, (M)kyc.e[m], (M)kyu.e[m], c, l, rr, (M)pd.e[m], (M)pu.e[m]);
         }
         if (s.any) {
             st8(w + i, wv);
@@ -376,10 +403,11 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
 
 // CG sweep 2 over tile (tx, ty): xs += alpha p ; r -= alpha w ; returns this
 // thread's share of sum(r r).
-template <typename T, bool CG = false>
-__device__ __forceinline__ double rf_ur_tile(const Lay& L, int tx, int ty, double a, T* __restrict__ xs,
+template <typename T, bool CG = false, typename M = double>
+__device__ __forceinline__ double rf_ur_tile(const Lay& L, int tx, int ty, double a_, T* __restrict__ xs,
                                              const T* __restrict__ p, T* __restrict__ r, const T* __restrict__ w)
 {
+    const M a = (M)a_;
     constexpr int N = Pack<T>::N;
     const Span<N> s(L, tx, ty);
     double acc = 0.0;
@@ -391,8 +419,8 @@ TL2D_PRAGMA_UNROLL(TL2D_UNROLL)
             const Cells<T> pv = ldc<CG>(p + i), wv = ldc<CG>(w + i);
 #pragma unroll
             for (int m = 0; m < N; ++m) {
-                xv.e[m] = (T)((double)xv.e[m] + a * (double)pv.e[m]);
-                rv.e[m] = (T)((double)rv.e[m] - a * (double)wv.e[m]);
+                xv.e[m] = (T)((M)xv.e[m] + a * (M)pv.e[m]);
+                rv.e[m] = (T)((M)rv.e[m] - a * (M)wv.e[m]);
                 if (s.c0 + m < L.nx) acc += (double)rv.e[m] * (double)rv.e[m];
             }
             st8(xs + i, xv);

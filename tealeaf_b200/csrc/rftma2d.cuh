@@ -20,13 +20,22 @@
 namespace tl2d {
 namespace rf {
 
-constexpr int kRfRows = 4;
-constexpr int kRfStages = 3;     // w sweep ring
+#ifndef TL2D_RF_ROWS
+#define TL2D_RF_ROWS 4
+#endif
+#ifndef TL2D_RF_STAGES
+#define TL2D_RF_STAGES 3
+#endif
 #ifndef TL2D_RF_STAGES_U
 #define TL2D_RF_STAGES_U 3
 #endif
+#ifndef TL2D_RF_BLOCKS
+#define TL2D_RF_BLOCKS 4
+#endif
+constexpr int kRfRows = TL2D_RF_ROWS;
+constexpr int kRfStages = TL2D_RF_STAGES;      // w sweep ring
 constexpr int kRfStagesU = TL2D_RF_STAGES_U;   // u/r sweep ring
-constexpr int kRfTmaBlocks = 4;   // resident blocks per SM of the TMA sweeps (about 50 KB of shared memory each)
+constexpr int kRfTmaBlocks = TL2D_RF_BLOCKS;   // resident blocks per SM of the TMA sweeps the tiles are cut for
 
 template <typename T>
 struct RfRowsW {
@@ -121,7 +130,9 @@ __global__ void __launch_bounds__(BX, 4) k_rf_w_tma(Lay L, const MxState* __rest
         for (int b = 0; b < kRfStages - 1 && b < np; ++b) issue(b);
     // t: T-layout row - j0
     auto stage = [&](int t) -> const S& { return ring[(t / kRfRows) % kRfStages]; };
-    auto fuse1 = [&](T pv, T rv) -> T { return FUSE_P ? (T)(bt * (double)pv + (double)rv) : pv; };
+    using M = typename RfMath<T>::M;
+    const M btm = (M)bt;
+    auto fuse1 = [&](T pv, T rv) -> T { return FUSE_P ? (T)(btm * (M)pv + (M)rv) : pv; };
     auto cur = [&](int t) -> Cells<T> {
         const S& Q = stage(t);
         Cells<T> c;
@@ -176,12 +187,11 @@ __global__ void __launch_bounds__(BX, 4) k_rf_w_tma(Lay L, const MxState* __rest
             Cells<T> wv;
 #pragma unroll
             for (int k = 0; k < N; ++k) {
-                const double c = (double)pc.e[k];
-                const double l = k == 0 ? (double)pl : (double)pc.e[k - 1];
-                const double rr = k == N - 1 ? (double)pr : (double)pc.e[k + 1];
-                const double kr = k == N - 1 ? (double)kxr : (double)kxc.e[k + 1];
-                wv.e[k] = (T)smvp((double)kxc.e[k], kr, (double)kyc.e[k], (double)kyu.e[k], c, l, rr,
-                                  (double)pd.e[k], (double)pu.e[k]);
+                const M c = (M)pc.e[k];
+                const M l = k == 0 ? (M)pl : (M)pc.e[k - 1];
+                const M rr = k == N - 1 ? (M)pr : (M)pc.e[k + 1];
+                const M kr = k == N - 1 ? (M)kxr : (M)kxc.e[k + 1];
+                wv.e[k] = (T)smvp_m<M>((M)kxc.e[k], kr, (M)kyc.e[k], (M)kyu.e[k], c, l, rr, (M)pd.e[k], (M)pu.e[k]);
             }
             if (s.any) {
                 st8(w + i, wv);
@@ -235,7 +245,8 @@ __global__ void __launch_bounds__(BX, 4) k_rf_ur_tma(Lay L, const MxState* __res
     __syncthreads();
     if (tid == 0)
         for (int b = 0; b < kRfStagesU - 1 && b < np; ++b) issue(b);
-    const double a = st->alpha;
+    using M = typename RfMath<T>::M;
+    const M a = (M)st->alpha;
     double acc = 0.0;
     long i = (long)(s.j0 + 1) * L.xp + s.c0;
     for (int b = 0; b < np; ++b) {
@@ -251,8 +262,8 @@ __global__ void __launch_bounds__(BX, 4) k_rf_ur_tma(Lay L, const MxState* __res
 #pragma unroll
                 for (int k = 0; k < N; ++k) {
                     const int c = tid * N + k;
-                    xv.e[k] = (T)((double)Q.X[u][c] + a * (double)Q.P[u][c]);
-                    rv.e[k] = (T)((double)Q.R[u][c] - a * (double)Q.Wv[u][c]);
+                    xv.e[k] = (T)((M)Q.X[u][c] + a * (M)Q.P[u][c]);
+                    rv.e[k] = (T)((M)Q.R[u][c] - a * (M)Q.Wv[u][c]);
                     if (s.c0 + k < L.nx) acc += (double)rv.e[k] * (double)rv.e[k];
                 }
                 st8(xs + i, xv);
