@@ -407,8 +407,8 @@ int tl2d_refine_solve_step(Chunk* chunk, Settings* settings, int tt, double rel_
  * with its own settings). tl2d_batch_step runs one solve() of every problem
  * (halos, cg_init, u0 = u, the solve, finalise, energy halo) with the CG
  * solve of all problems in one persistent cooperative kernel: FP32 vectors
- * and coefficients, FP64 arithmetic, dot products and solution, FP64
- * residual replacement, each problem stopped when its FP64 residual gives
+ * and coefficients, FP32 arithmetic in the sweeps, FP64 dot products,
+ * scalars and solution, FP64 residual replacement, each problem stopped when its FP64 residual gives
  * r.r < its settings->eps (the reference's 2D stop test). The whole timestep
  * is captured once into a CUDA graph and replayed. */
 typedef struct TlBatch TlBatch;

@@ -3,8 +3,9 @@
 // A batch holds `count` initialised chunks of different sizes (each with its
 // own tea.in settings). One batched timestep runs, for every problem, the
 // reference's solve() (2d/diffuse.c:22-80) with the CG solve replaced by the
-// refinement CG of refine2d.cuh (FP32 vectors and coefficients, FP64
-// arithmetic, dot products and solution, FP64 residual replacement) stopped
+// refinement CG of refine2d.cuh (FP32 vectors and coefficients, FP32
+// arithmetic in the sweeps, FP64 dot products, scalars and solution, FP64
+// residual replacement) stopped
 // when the FP64 residual satisfies the problem's own r.r < eps:
 //
 //   per problem: energy/density halos, cg_init, u0 = u, T-layout setup
@@ -39,12 +40,21 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 using namespace tl2d;
 using namespace tl2d::rf;
 
 namespace {
+
+// Arithmetic of the batch's FP32 sweeps (dot products and scalars are FP64
+// either way): FP32 (TL2D_BATCH_MATH_F32 1; 785 against 846 ms for the
+// 64-problem step, the same iterations) or FP64 on the FP32 values (0).
+#ifndef TL2D_BATCH_MATH_F32
+#define TL2D_BATCH_MATH_F32 1
+#endif
+using BatchM = std::conditional_t<TL2D_BATCH_MATH_F32 != 0, float, double>;
 
 constexpr int kBatchMinB = 8;                    // resident blocks per SM of the persistent kernel
 constexpr long long kWaitLimit = 4000000000LL;   // default: SM clocks a phase wait may take (~2 s)
@@ -251,13 +261,13 @@ __global__ void __launch_bounds__(BX, kBatchMinB) k_batch_cg(const BProb* __rest
         if (kind == PH_W) {
             float* pin = Q.f[it == 0 ? BF_P0 : (((it - 1) & 1) ? BF_P1 : BF_P0)];
             float* pout = Q.f[(it & 1) ? BF_P1 : BF_P0];
-            v[0] = it == 0 ? rf_w_tile<float, false, true>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R], Q.f[BF_W],
-                                                            Q.f[BF_KX], Q.f[BF_KY])
-                           : rf_w_tile<float, true, true>(Q.L, tx, ty, coef, pin, pout, Q.f[BF_R], Q.f[BF_W],
-                                                           Q.f[BF_KX], Q.f[BF_KY]);
+            v[0] = it == 0 ? rf_w_tile<float, false, true, BatchM>(Q.L, tx, ty, 0.0, pin, pin, Q.f[BF_R],
+                                                                    Q.f[BF_W], Q.f[BF_KX], Q.f[BF_KY])
+                           : rf_w_tile<float, true, true, BatchM>(Q.L, tx, ty, coef, pin, pout, Q.f[BF_R],
+                                                                   Q.f[BF_W], Q.f[BF_KX], Q.f[BF_KY]);
         } else if (kind == PH_UR) {
-            v[0] = rf_ur_tile<float, true>(Q.L, tx, ty, coef, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0], Q.f[BF_R],
-                                           Q.f[BF_W]);
+            v[0] = rf_ur_tile<float, true, BatchM>(Q.L, tx, ty, coef, Q.f[BF_XS], Q.f[(it & 1) ? BF_P1 : BF_P0],
+                                                   Q.f[BF_R], Q.f[BF_W]);
         } else if (kind == PH_FOLD) {
             rf_fold_tile<float, true>(Q.L, tx, ty, Q.gx, Q.hd, Q.u, Q.f[BF_XS]);
         } else {

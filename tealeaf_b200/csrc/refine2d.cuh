@@ -5,8 +5,8 @@
 //
 // CG whose vectors (p, r, w, the solution correction xs) and operator
 // coefficients (kx, ky) are stored in T (float or double). The refinement
-// timestep's sweeps compute in T (the stencil and vector updates in FP32 for
-// FP32 storage; RfMath), the batched solver's in FP64 registers; every dot
+// timestep's and the batched solver's sweeps compute in T (the stencil and
+// vector updates in FP32 for FP32 storage; RfMath, BatchM); every dot
 // product (p.w, r.r) is accumulated in FP64.
 // The solution is accumulated in FP64 (the chunk's u): when r.r of the stored
 // residual has dropped by kUpdateDelta^2 since the last replacement (or looks
@@ -211,8 +211,8 @@ union Cells {
 // the storage precision itself (TL2D_RF_MATH_T 1: FP32 arithmetic for FP32
 // storage, measured 9.81 against 10.61 s for the 8192^2 CG timestep to
 // 1e-10 with FP64 arithmetic, same iterations) or FP64 (0). Dot products, the
-// scalars and the FP64 residual stay FP64 either way; the batched solver's
-// sweeps keep FP64 arithmetic (their default M).
+// scalars and the FP64 residual stay FP64 either way. The tile functions'
+// M defaults to double; the batched solver picks its own (BatchM).
 #ifndef TL2D_RF_MATH_T
 #define TL2D_RF_MATH_T 1
 #endif
