@@ -797,10 +797,10 @@ static __global__ void __launch_bounds__(BX, 4) k_cg_w_fused_tma(Geo g, Faces fc
         double pc = 0.0, pd = 0.0, kyc = 0.0;
         long i = s.kk + (long)s.j0 * x;
         for (int b = 0; b * kRowsT < s.j1 - s.j0; ++b) {
-            tl::mbar_wait(&bars[b % kStagesT], (unsigned)(b / kStagesT) & 1u, err);
-            if (b + 1 < np) tl::mbar_wait(&bars[(b + 1) % kStagesT], (unsigned)((b + 1) / kStagesT) & 1u, err);
             __syncthreads();   // every thread is past rows of block b-1: stage b-1 is free
             if (tx == 0 && b + kStagesT - 1 < np) issue(b + kStagesT - 1);
+            tl::mbar_wait(&bars[b % kStagesT], (unsigned)(b / kStagesT) & 1u, err);
+            if (b + 1 < np) tl::mbar_wait(&bars[(b + 1) % kStagesT], (unsigned)((b + 1) / kStagesT) & 1u, err);
             if (b == 0) {
                 pc = fused(s.j0, 0);
                 pd = (s.j0 == g.hd) ? ((REFLECT && fc.b) ? pc : raw(s.j0 - 1, 0)) : fused(s.j0 - 1, 0);
@@ -939,9 +939,9 @@ static __global__ void __launch_bounds__(BX, 4) k_cg_ur_fused_tma(Geo g, Scalar 
         for (int b = 0; b < kStagesU - 1 && b < np; ++b) issue(b);
     const double a = alpha.get();
     for (int b = 0; b < np; ++b) {
-        tl::mbar_wait(&bars[b % kStagesU], (unsigned)(b / kStagesU) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
         if (tx == 0 && b + kStagesU - 1 < np) issue(b + kStagesU - 1);
+        tl::mbar_wait(&bars[b % kStagesU], (unsigned)(b / kStagesU) & 1u, err);
         const RowsU& S = ring[b % kStagesU];
         const int y0 = stage_y0(b);
 #pragma unroll

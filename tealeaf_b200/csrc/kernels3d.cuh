@@ -350,11 +350,11 @@ __device__ __forceinline__ void walkt(const Geo& g, const Faces& fc, const Penci
 #pragma unroll 1
     for (int ii = s.i0; ii < s.i1; ++ii, i += xy) {
         const int q = ii - s.i0;
-        tl::mbar_wait(&bars[q % kStagesT3], (unsigned)(q / kStagesT3) & 1u, err);
-        tl::mbar_wait(&bars[(q + 1) % kStagesT3], (unsigned)((q + 1) / kStagesT3) & 1u, err);
         __syncthreads();   // every thread is past plane ii-1: its slot is free
         if (leader && q + kStagesT3 - 1 < np)
             issue(ii + kStagesT3 - 1, (q + kStagesT3 - 1) % kStagesT3, ii + kStagesT3 - 1 < s.i1);
+        tl::mbar_wait(&bars[q % kStagesT3], (unsigned)(q / kStagesT3) & 1u, err);
+        tl::mbar_wait(&bars[(q + 1) % kStagesT3], (unsigned)((q + 1) / kStagesT3) & 1u, err);
         const PlaneT& P = ring[q % kStagesT3];
         const PlaneT& F = ring[(q + 1) % kStagesT3];
         const int cx = tx + 2, cy = ty + 1;
@@ -582,9 +582,9 @@ static __global__ void __launch_bounds__(NT, 4) k3_cg_ur_tma(Geo g, Scalar alpha
     const double a = alpha.get();
     const long xy = g.xy();
     for (int b = 0; b < np; ++b) {
-        tl::mbar_wait(&bars[b % kStagesU3], (unsigned)(b / kStagesU3) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
         if (leader && b + kStagesU3 - 1 < np) issue(b + kStagesU3 - 1);
+        tl::mbar_wait(&bars[b % kStagesU3], (unsigned)(b / kStagesU3) & 1u, err);
         const PlanesU& S = ring[b % kStagesU3];
         const int z0 = stage_z0(b);
 #pragma unroll

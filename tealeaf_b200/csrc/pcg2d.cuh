@@ -230,9 +230,9 @@ static __global__ void __launch_bounds__(BX, 3) k_pcg_ur_tma(Geo g, Scalar alpha
     const double a = alpha.get();
     const int x = g.x;
     for (int b = 0; b < np; ++b) {
-        tl::mbar_wait(&bars[b % kPcgStages], (unsigned)(b / kPcgStages) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
         if (tx == 0 && b + kPcgStages - 1 < np) issue(b + kPcgStages - 1);
+        tl::mbar_wait(&bars[b % kPcgStages], (unsigned)(b / kPcgStages) & 1u, err);
         const PcgRows& S = ring[b % kPcgStages];
 #pragma unroll
         for (int q0 = 0; q0 < kPcgRows; q0 += BS) {

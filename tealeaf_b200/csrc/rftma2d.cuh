@@ -160,10 +160,10 @@ __global__ void __launch_bounds__(BX, 4) k_rf_w_tma(Lay L, const MxState* __rest
     Cells<T> pc, pd, kyc;
     long i = (long)(s.j0 + 1) * L.xp + s.cc;
     for (int b = 0; b * kRfRows < s.j1 - s.j0; ++b) {
-        tl::mbar_wait(&bars[b % kRfStages], (unsigned)(b / kRfStages) & 1u, err);
-        if (b + 1 < np) tl::mbar_wait(&bars[(b + 1) % kRfStages], (unsigned)((b + 1) / kRfStages) & 1u, err);
         __syncthreads();   // every thread is past the rows of block b-1: stage b-1 is free
         if (tid == 0 && b + kRfStages - 1 < np) issue(b + kRfStages - 1);
+        tl::mbar_wait(&bars[b % kRfStages], (unsigned)(b / kRfStages) & 1u, err);
+        if (b + 1 < np) tl::mbar_wait(&bars[(b + 1) % kRfStages], (unsigned)((b + 1) / kRfStages) & 1u, err);
         if (b == 0) {
             pc = cur(1);
             pd = cur(0);
@@ -250,9 +250,9 @@ __global__ void __launch_bounds__(BX, 4) k_rf_ur_tma(Lay L, const MxState* __res
     double acc = 0.0;
     long i = (long)(s.j0 + 1) * L.xp + s.c0;
     for (int b = 0; b < np; ++b) {
-        tl::mbar_wait(&bars[b % kRfStagesU], (unsigned)(b / kRfStagesU) & 1u, err);
         __syncthreads();   // every thread is past stage b-1: its slot is free
         if (tid == 0 && b + kRfStagesU - 1 < np) issue(b + kRfStagesU - 1);
+        tl::mbar_wait(&bars[b % kRfStagesU], (unsigned)(b / kRfStagesU) & 1u, err);
         const S& Q = ring[b % kRfStagesU];
 #pragma unroll
         for (int u = 0; u < kRfRows; ++u) {

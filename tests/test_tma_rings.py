@@ -4,10 +4,10 @@ k_pcg_ur_tma in pcg2d.cuh; walkt and k3_cg_ur_tma in kernels3d.cuh;
 k_rf_w_tma and k_rf_ur_tma in rftma2d.cuh), and of the TMA-staged blocked
 kernel (k_blocked_tma in blocked2d.cuh: one barrier, one region in flight).
 
-Each kernel walks its rows (or z-planes) in blocks; before block b it waits
-on the shared-memory barriers of the stages it reads, synchronises the
-block, and one thread issues the stage kStages - 1 ahead into the slot the
-previous occupant left. The simulation below replays that schedule for every
+Each kernel walks its rows (or z-planes) in blocks; before block b it
+synchronises the block, one thread issues the stage kStages - 1 ahead into
+the slot the previous occupant left, and every thread then waits on the
+shared-memory barriers of the stages it reads. The simulation below replays that schedule for every
 strip length the kernels can see and checks, without a GPU, that:
 
 * a stage is issued once, only after every read of the slot's previous
@@ -45,6 +45,10 @@ def simulate(n_units, rows, stages, np_fn, loop_fn, reads_fn, waits_fn):
     for b in range(min(stages - 1, np_)):
         issue(b, -1)
     for b in range(loop_fn(n_units)):
+        # __syncthreads(); the issue of the stage stages - 1 ahead; the waits
+        nxt = b + stages - 1
+        if nxt < np_:
+            issue(nxt, b)
         for s in waits_fn(b, np_):
             assert s in issued, "wait on a stage never issued (would hang)"
             slot = s % stages
@@ -54,10 +58,6 @@ def simulate(n_units, rows, stages, np_fn, loop_fn, reads_fn, waits_fn):
                 waited.add(s)
             # the kernel waits with parity (s // stages) & 1 on the slot's barrier
             assert (s // stages) == uses[slot] - 1
-        # __syncthreads(); then the issue of the stage stages - 1 ahead
-        nxt = b + stages - 1
-        if nxt < np_:
-            issue(nxt, b)
         for s in reads_fn(b):
             assert s in waited, "read of a stage not waited for"
             assert slot_of[s % stages] == s, "read of a slot already reissued"
