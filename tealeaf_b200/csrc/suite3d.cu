@@ -200,10 +200,16 @@ static void run_cheby_queue(TlSuite3D* s, Chunk* chunk)
     s->cq.b.clear();
 }
 
-void flush(TlSuite3D* s, Chunk* chunk)
+// Runs whichever deferred queue is open.
+static void run_queues(TlSuite3D* s, Chunk* chunk)
 {
     if (s->pq.active) run_ppcg_queue(s, chunk);
     if (s->cq.active) run_cheby_queue(s, chunk);
+}
+
+void flush(TlSuite3D* s, Chunk* chunk)
+{
+    run_queues(s, chunk);
     if (s->pend.calc_p) {
         TL3_LAUNCH(s, "k3_cg_close",
                    k3_cg_close<<<interior_grid(s->g), interior_block(), 0, s->stream>>>(
@@ -551,6 +557,7 @@ void run_cg_solver_calc_w(Chunk* chunk, Settings* settings, double* pw)
     if (tl::failed()) return;
     TlSuite3D* s = suite_of(chunk);
     if (!s) return;
+    run_queues(s, chunk);   // deferred steps precede everything recorded after them
     if (s->pend.halo[TL3_FIELD_P] > 1) flush(s, chunk);
     const bool fuse = s->pend.calc_p;
     const bool refl = s->pend.halo[TL3_FIELD_P] == 1;
@@ -584,6 +591,7 @@ void run_cg_solver_calc_ur(Chunk* chunk, Settings* settings, double alpha, doubl
     if (tl::failed()) return;
     TlSuite3D* s = suite_of(chunk);
     if (!s) return;
+    run_queues(s, chunk);
     if (s->pend.calc_p || s->pend.halo[TL3_FIELD_U]) flush(s, chunk);
     launch_cg_ur3(s, interior_grid(s->g), Scalar{alpha, nullptr}, chunk->vec_u, chunk->vec_p, chunk->vec_r,
                   chunk->vec_w, nullptr, tl::NoFinish());
@@ -598,6 +606,7 @@ void run_cg_solver_calc_p(Chunk* chunk, Settings* settings, double beta)
     if (tl::failed()) return;
     TlSuite3D* s = suite_of(chunk);
     if (!s) return;
+    run_queues(s, chunk);
     if (s->pend.calc_p || s->pend.halo[TL3_FIELD_P]) flush(s, chunk);
     s->pend.calc_p = true;
     s->pend.beta = beta;

@@ -366,3 +366,22 @@ def test_3d_run_path_queues_are_bit_identical(solver, dims, inner, cap):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("dims,trips", [((37, 19, 23), 1), ((38, 19, 23), 4), ((38, 19, 23), 5)])
+def test_3d_cg_sweeps_run_the_deferred_trips_first(dims, trips, cheby_then_cg_sweeps):
+    """Chebyshev trips still queued when run_cg_solver_calc_w, _calc_ur and
+    _calc_p are called run before them: the sweeps' dot products and the
+    memory state match, bit for bit, a chunk that ran every trip at once."""
+    text = problems.seeded(3, dims, 41, 3, 1, solver="cheby", end_step=1, name="qcg3").tea_in()
+    a, b = Host(text, 3), Host(text, 3)
+    try:
+        b.lib.tl3d_set_temporal_blocking(b.chunk, 0)
+        ra = cheby_then_cg_sweeps(a, trips)
+        rb = cheby_then_cg_sweeps(b, trips)
+        assert ra == rb
+        for f in FIELDS3:
+            assert np.array_equal(a.download(f), b.download(f)), (dims, trips, f)
+    finally:
+        a.finalise()
+        b.finalise()

@@ -158,3 +158,23 @@ def test_run_path_cheby_queue_is_bit_identical(cap):
     finally:
         a.finalise()
         b.finalise()
+
+
+@pytest.mark.parametrize("dims,trips", [((203, 141), 1), ((203, 141), 5), ((204, 142), 7)])
+def test_cg_sweeps_run_the_deferred_trips_first(dims, trips, cheby_then_cg_sweeps):
+    """Chebyshev trips still queued when run_cg_calc_w, run_cg_calc_ur and
+    run_cg_calc_p are called run before them: the sweeps' dot products and
+    the memory state match, bit for bit, a chunk that ran every trip at
+    once."""
+    text = problems.seeded(2, dims, 43, 5, 2, solver="cheby", end_step=1, name="qcg2").tea_in()
+    a, b = Host(text, 2), Host(text, 2)
+    try:
+        b.lib.tl2d_set_temporal_blocking(b.chunk, 0)
+        ra = cheby_then_cg_sweeps(a, trips)
+        rb = cheby_then_cg_sweeps(b, trips)
+        assert ra == rb
+        for f in FIELDS:
+            assert np.array_equal(a.download(f), b.download(f)), (dims, trips, f)
+    finally:
+        a.finalise()
+        b.finalise()
