@@ -9,7 +9,9 @@
 // are filled with zeros. Every wait is bounded: a barrier that has not
 // completed after kTmaSpinLimit polls sets *err (a plain store: the word may
 // be mapped host memory) and the caller goes on (its results are then
-// invalid and the host reports the error).
+// invalid and the host reports the error). A wait still polling after each
+// kTmaErrPoll polls reads *err and gives up at once if another wait already
+// did, so the remaining waits of a failed launch end quickly.
 #pragma once
 
 #include <cuda.h>
@@ -18,6 +20,7 @@
 namespace tl {
 
 constexpr long kTmaSpinLimit = 1L << 26;
+constexpr long kTmaErrPoll = 1L << 20;   // power of two; far beyond any wait of a working copy
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -72,8 +75,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 // `limit` polls.
 __device__ __forceinline__ bool mbar_wait_limited(unsigned long long* bar, unsigned parity, int* err, long limit)
 {
-    for (long n = 0; n < limit; ++n)
+    for (long n = 0; n < limit; ++n) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((n & (kTmaErrPoll - 1)) == kTmaErrPoll - 1 && err && *(volatile int*)err) break;
+    }
     if (err) *(volatile int*)err = 1;
     return false;
 }
