@@ -503,6 +503,12 @@ void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stat
                  settings->num_chunks_per_rank);
         return;
     }
+    const Faces fc = faces_of(chunk);
+    if (!(fc.l && fc.r && fc.b && fc.t)) {   // no remote halo exchange inside the device loop
+        tl::fail(34, "the device-resident driver solves a chunk whose four faces are external (a decomposed mesh "
+                     "runs through run_*)");
+        return;
+    }
     flush(s, chunk);
     TlStepStats local{};
     TlStepStats* st_out = stats ? stats : &local;

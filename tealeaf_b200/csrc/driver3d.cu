@@ -438,6 +438,12 @@ void tl3d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats3* sta
                  settings->num_chunks_per_rank);
         return;
     }
+    const Faces fc = faces_of(chunk);
+    if (!(fc.l && fc.r && fc.b && fc.t && fc.k && fc.f)) {   // no remote halo exchange inside the device loop
+        tl::fail(34, "the device-resident driver solves a chunk whose six faces are external (a decomposed mesh "
+                     "runs through run_*)");
+        return;
+    }
     flush(s, chunk);
     TlStepStats3 local{};
     TlStepStats3* st_out = stats ? stats : &local;

@@ -167,7 +167,7 @@ class Host:
 
     def __init__(self, tea_in: str, dims: int = 2):
         self.dims = dims
-        self.lib = abi.load(dims)
+        self.lib = self._load_lib()
         self.cfg, self.states = read_config(tea_in, dims)
         c = self.cfg
         if c.kernel_language not in (None, 0):
@@ -183,6 +183,9 @@ class Host:
             abi.check(self.lib, dims)
 
     # -- plumbing ------------------------------------------------------------
+    def _load_lib(self):
+        return abi.load(self.dims)
+
     def _call(self, name, *args):
         if self.dims == 3:
             name = _NAMES3.get(name, name)
@@ -280,10 +283,15 @@ class Host:
         self._call(name, *args, C.byref(v))
         return v.value
 
+    def _sum(self, value: float) -> float:
+        """sum_over_ranks (2d/comms.c:55-61), called where the reference
+        drivers call it; on one rank the value itself."""
+        return value
+
     def field_summary(self):
         v = [C.c_double(0.0) for _ in range(4)]
         self._call("run_field_summary", *[C.byref(x) for x in v])
-        return [x.value for x in v]
+        return [self._sum(x.value) for x in v]
 
     def norm(self, which: str) -> float:
         ptr = getattr(self.chunk, which if self.dims == 2 else "vec_" + which)
@@ -295,7 +303,7 @@ class Host:
     # -- CG (2d/drivers/cg_driver.c) --------------------------------------------
     def cg_init_driver(self, rx, ry, rz):
         args = (rx, ry) if self.dims == 2 else (rx, ry, rz)
-        rro = self._acc("run_cg_init", *args)
+        rro = self._sum(self._acc("run_cg_init", *args))
         self.reset_fields_to_exchange()
         self.flags[FIELD_U] = self.flags[FIELD_P] = True
         self.halo_update(1)
@@ -303,10 +311,10 @@ class Host:
         return rro
 
     def cg_main_step(self, tt, rro):
-        pw = self._acc("run_cg_calc_w")
+        pw = self._sum(self._acc("run_cg_calc_w"))
         alpha = rro / pw
         self.chunk.cg_alphas[tt] = alpha
-        rrn = self._acc("run_cg_calc_ur", alpha)
+        rrn = self._sum(self._acc("run_cg_calc_ur", alpha))
         beta = rrn / rro
         self.chunk.cg_betas[tt] = beta
         self._call("run_cg_calc_p", beta)
@@ -365,19 +373,19 @@ class Host:
                 if nch == 1:
                     self._eigenvalues(tt)
                     self._cheby_coefs(self.cfg.max_iters - tt)
-                    bb = self.norm("u0")
+                    bb = self._sum(self.norm("u0"))
                     self._call("run_cheby_init")
                     self.reset_fields_to_exchange()
                     self.flags[FIELD_U] = True
                     self.halo_update(1)
                     self._call("run_cheby_iterate", ch.cheby_alphas[nch], ch.cheby_betas[nch])
-                    error = self.norm("r")
+                    error = self._sum(self.norm("r"))
                     est = cheby_est_iterations(ch.eigmin, ch.eigmax, error, bb)
                 else:
                     calc_norm = nch >= est and (tt + 1) % 10 == 0
                     self._call("run_cheby_iterate", ch.cheby_alphas[nch], ch.cheby_betas[nch])
                     if calc_norm:
-                        error = self.norm("r")
+                        error = self._sum(self.norm("r"))
             self.halo_update(1)
             error = self._post_trip(error)
             if abs(error) < self.cfg.eps:
@@ -407,7 +415,7 @@ class Host:
                     self.reset_fields_to_exchange()
                     self.flags[FIELD_P] = True
                     self.halo_update(1)
-                pw = self._acc("run_cg_calc_w")
+                pw = self._sum(self._acc("run_cg_calc_w"))
                 alpha = rro / pw
                 self._acc("run_cg_calc_ur", alpha)
                 self._call("run_ppcg_init")
@@ -418,7 +426,7 @@ class Host:
                     self._call("run_ppcg_inner_iteration", ch.cheby_alphas[pp], ch.cheby_betas[pp])
                 self.reset_fields_to_exchange()
                 self.flags[FIELD_P] = True
-                rrn = self.norm("r")
+                rrn = self._sum(self.norm("r"))
                 beta = rrn / rro
                 self._call("run_cg_calc_p", beta)
                 error = rrn
@@ -450,6 +458,7 @@ class Host:
                 self.halo_update(1)
                 self._call("run_calculate_residual")
                 error += self.norm("r")
+            error = self._sum(error)
             self.halo_update(1)
             error = self._post_trip(error)
             if abs(error) < self.cfg.eps:
@@ -475,7 +484,7 @@ class Host:
         # solve_finished_driver (2d/drivers/solve_finished_driver.c:7-43)
         if c.check_result:
             self._call("run_calculate_residual")
-            res.exact_error = self.norm("r")
+            res.exact_error = self._sum(self.norm("r"))
         self._call("run_finalise")
         self.flags[FIELD_ENERGY1] = True
         self.halo_update(1)

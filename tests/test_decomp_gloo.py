@@ -1,0 +1,252 @@
+"""The decomposed mesh (tealeaf_b200.decomp) on the CPU, gloo ranks over
+127.0.0.1.
+
+* decompose: chunk counts by the reference's search and metric
+  (decompose_field, 2d/initialise.c:34-134, 3d/initialise.c:34-174), chunks
+  that tile the mesh once, remainders to the first chunks, neighbours that
+  face each other.
+* FaceExchange: after one exchange every halo layer on an internal face
+  holds the neighbour's interior cells, for 2D and 3D meshes and 2 to 4
+  ranks, several fields per message; external faces and corners untouched.
+* DistHost: whole timesteps of the reference drivers' sequence through
+  run_*, each rank's kernels computed by the oracle's restatement of the
+  reference kernels (tests/oracle_suite2d.py); one rank reproduces the
+  oracle's own run bit for bit, and 2, 3 and 4 ranks reproduce it to the
+  rounding of their split sums (per-rank partial sums added across ranks).
+"""
+import datetime
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from tealeaf_b200 import decomp, problems
+from tealeaf_b200.config import read_config
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _init(rank, world, port):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    return dist
+
+
+def _run(target, world, args, timeout=300):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=target, args=(r, world, port, q) + tuple(args)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        out = [q.get(timeout=timeout) for _ in range(world)]
+    finally:
+        for p in procs:
+            p.join(timeout=timeout)
+            if p.is_alive():
+                p.kill()
+    for r, payload in out:
+        if isinstance(payload, str):
+            pytest.fail("rank %d: %s" % (r, payload))
+    return [payload for _, payload in sorted(out, key=lambda t: t[0])]
+
+
+# -- decompose -------------------------------------------------------------------------
+
+def test_chunk_counts_follow_the_reference_search():
+    assert decomp.chunk_counts((100, 100), 1) == (1, 1)
+    assert decomp.chunk_counts((100, 100), 4) == (2, 2)
+    assert decomp.chunk_counts((100, 100), 2) == (1, 2)     # a tie keeps the first factorisation
+    assert decomp.chunk_counts((200, 100), 2) == (2, 1)
+    assert decomp.chunk_counts((100, 200), 2) == (1, 2)
+    assert decomp.chunk_counts((70, 10), 7) == (7, 1)
+    assert decomp.chunk_counts((64, 32, 16), 8) == (4, 2, 1)
+    assert decomp.chunk_counts((30, 30, 30), 8) == (2, 2, 2)
+    assert decomp.chunk_counts((30, 30, 30), 2) == (1, 1, 2)
+
+
+@pytest.mark.parametrize("cells,n", [((10, 7), 4), ((37, 23), 6), ((41, 3), 5), ((9, 8, 7), 12),
+                                     ((40, 30, 20), 8), ((5, 5), 1), ((17, 13, 11), 3)])
+def test_chunks_tile_the_mesh_and_face_each_other(cells, n):
+    boxes = decomp.decompose(cells, n)
+    counts = decomp.chunk_counts(cells, n)
+    assert len(boxes) == n
+    cover = np.zeros(cells[::-1], dtype=int)
+    for b in boxes:
+        cover[tuple(slice(l, h) for l, h in zip(b.lo[::-1], b.hi[::-1]))] += 1
+        for f, nb in enumerate(b.neighbours):
+            axis = f // 2
+            if nb == decomp.EXTERNAL_FACE:
+                assert b.lo[axis] == 0 if f % 2 == 0 else b.hi[axis] == cells[axis]
+                continue
+            o = boxes[nb]
+            assert o.neighbours[f ^ 1] == b.index
+            assert o.hi[axis] == b.lo[axis] if f % 2 == 0 else o.lo[axis] == b.hi[axis]
+            for a in range(len(cells)):
+                if a != axis:
+                    assert (o.lo[a], o.hi[a]) == (b.lo[a], b.hi[a])
+    assert (cover == 1).all()
+    for a, (cnt, c) in enumerate(zip(counts, cells)):
+        spans = sorted({(b.lo[a], b.cells[a]) for b in boxes})
+        assert len(spans) == cnt
+        widths = [w for _, w in spans]   # the first c % cnt chunks take one cell more
+        assert widths == [c // cnt + 1] * (c % cnt) + [c // cnt] * (cnt - c % cnt)
+        assert [l for l, _ in spans] == [sum(widths[:k]) for k in range(cnt)]
+
+
+def test_more_chunks_than_cells_is_an_error():
+    with pytest.raises(ValueError):
+        decomp.decompose((3, 3), 16)
+    with pytest.raises(ValueError):
+        decomp.chunk_counts((8, 8), 0)
+
+
+# -- FaceExchange -----------------------------------------------------------------------
+
+def _tag(field, gz, gy, gx):
+    return field * 0.5 + gx + 1000.0 * gy + 1.0e6 * gz
+
+
+def _slabs(shape, hd, depth, face):
+    """(pack slab, unpack slab) index tuples of one face, array order z, y, x."""
+    dims = len(shape)
+    axis = dims - 1 - face // 2
+    n = shape[axis]
+    inner = [slice(hd, s - hd) for s in shape]
+    lo = face % 2 == 0
+    pack, unpack = list(inner), list(inner)
+    pack[axis] = slice(hd, hd + depth) if lo else slice(n - hd - depth, n - hd)
+    unpack[axis] = slice(hd - depth, hd) if lo else slice(n - hd, n - hd + depth)
+    return tuple(pack), tuple(unpack)
+
+
+def _exchange_worker(rank, world, port, q, cells, hd, depth):
+    try:
+        import ctypes as C
+        dist = _init(rank, world, port)
+        box = decomp.decompose(cells, world)[rank]
+        dims = len(cells)
+        shape = tuple(c + 2 * hd for c in box.cells[::-1])
+        fields = []
+        for f in range(3):
+            a = np.full(shape, np.nan)
+            idx = np.indices(box.cells[::-1])
+            g = [idx[k] + box.lo[::-1][k] for k in range(dims)]
+            gz, gy, gx = ([np.zeros_like(g[0])] + g) if dims == 2 else g
+            a[(slice(hd, -hd),) * dims] = _tag(f, gz, gy, gx)
+            fields.append(a)
+
+        def pack(face, d, field, address, is_pack):
+            src, dst = _slabs(field.shape, hd, d, face)
+            view = field[src] if is_pack else field[dst]
+            buf = np.ctypeslib.as_array(C.cast(address, C.POINTER(C.c_double)), shape=(view.size,))
+            if is_pack:
+                buf[:] = view.ravel()
+            else:
+                field[dst] = buf.reshape(view.shape)
+
+        ex = decomp.FaceExchange(box)
+        assert ex.face_len(0, depth) == depth * int(np.prod(box.cells[1:]))
+        ex.run(depth, fields, pack)
+        bad = []
+        for f, a in enumerate(fields):
+            for face, nb in enumerate(box.neighbours):
+                _, dst = _slabs(shape, hd, depth, face)
+                got = a[dst]
+                if nb == decomp.EXTERNAL_FACE:
+                    if not np.isnan(got).all():
+                        bad.append(("external face written", f, face))
+                    continue
+                coords = np.indices(shape)[(slice(None),) + dst]
+                g = [coords[k] - hd + box.lo[::-1][k] for k in range(dims)]
+                gz, gy, gx = ([np.zeros_like(g[0])] + g) if dims == 2 else g
+                if not np.array_equal(got, _tag(f, gz, gy, gx)):
+                    bad.append(("wrong halo", f, face))
+            inside = np.zeros(shape, dtype=bool)   # the interior and the face slabs
+            inside[(slice(hd, -hd),) * dims] = True
+            for face in range(2 * dims):
+                inside[_slabs(shape, hd, depth, face)[1]] = True
+            if not np.isnan(a[~inside]).all():
+                bad.append(("cells outside the face slabs written", f))
+        q.put((rank, bad))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as exc:   # reported to the test, not swallowed
+        q.put((rank, "%s: %s" % (type(exc).__name__, exc)))
+
+
+@pytest.mark.parametrize("cells,world,hd,depth", [((12, 9), 2, 2, 1), ((12, 9), 4, 2, 2), ((13, 11), 3, 2, 2),
+                                                  ((8, 7, 6), 2, 2, 2), ((8, 7, 6), 4, 2, 1)])
+def test_face_exchange_fills_internal_halos(cells, world, hd, depth):
+    for bad in _run(_exchange_worker, world, (cells, hd, depth)):
+        assert bad == []
+
+
+# -- DistHost ---------------------------------------------------------------------------
+
+def _solve_worker(rank, world, port, q, text, steps):
+    try:
+        dist = _init(rank, world, port)
+        from oracle_suite2d import OracleSuite2D
+        h = decomp.DistHost(text, 2, lib=OracleSuite2D())
+        out = []
+        for tt in range(steps):
+            r = h.solve(tt)
+            out.append((dict(r.iterations), list(r.summary), r.error))
+        u = h.gather_interior("u")
+        q.put((rank, (h.box, out, u)))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as exc:
+        q.put((rank, "%s: %s" % (type(exc).__name__, exc)))
+
+
+CASES = {
+    "cg": problems.seeded(2, (48, 40), 51, 3, 1, solver="cg", end_step=2, name="d_cg").tea_in(),
+    "cheby": problems.seeded(2, (48, 40), 52, 3, 1, solver="cheby", end_step=2, name="d_cheby").tea_in(),
+    "ppcg": problems.seeded(2, (48, 40), 53, 3, 1, solver="ppcg", end_step=2, name="d_ppcg").tea_in(),
+    "jacobi": problems.seeded(2, (24, 20), 54, 2, 1, solver="jacobi", end_step=1, name="d_jac").with_(
+        max_iters=400).tea_in(),
+}
+
+
+@pytest.mark.parametrize("solver", ["cg", "cheby", "ppcg", "jacobi"])
+def test_one_rank_reproduces_the_oracle_run(solver, oracle_lib):
+    text = CASES[solver]
+    cfg, states = read_config(text, 2)
+    ref = oracle_lib.run(cfg, states)
+    (box, out, _), = _run(_solve_worker, 1, (text, cfg.end_step))
+    assert box.neighbours == (-1, -1, -1, -1)
+    for (its, summary, _), r in zip(out, ref):
+        assert its == r.iterations
+        assert summary == r.summary
+
+
+@pytest.mark.parametrize("solver,world", [("cg", 2), ("cg", 4), ("cg", 3), ("cheby", 2), ("ppcg", 4),
+                                          ("jacobi", 2)])
+def test_ranks_reproduce_the_one_rank_solve(solver, world):
+    """Split sums differ from the one-rank sums by rounding only: iteration
+    counts equal and summaries and the solution within 1e-11."""
+    text = CASES[solver]
+    cfg, _ = read_config(text, 2)
+    (_, one, u1), = _run(_solve_worker, 1, (text, cfg.end_step))
+    res = _run(_solve_worker, world, (text, cfg.end_step))
+    boxes = [b for b, _, _ in res]
+    assert sorted(b.index for b in boxes) == list(range(world))
+    for _, out, u in res:
+        assert np.allclose(u, u1, rtol=1e-11, atol=0.0)
+        for (its, summary, err), (its1, summary1, err1) in zip(out, one):
+            assert its == its1
+            assert summary == pytest.approx(summary1, rel=1e-11)
+    # every rank holds the same reduced figures
+    for _, out, _ in res[1:]:
+        assert out == res[0][1]

@@ -1,0 +1,86 @@
+"""The decomposed mesh through the B200 suite (tealeaf_b200.decomp.DistHost).
+
+Two ranks run as processes sharing cuda:0: their kernels never wait on each
+other, the faces cross as host buffers over gloo between timesteps'
+run_* calls. Against the undivided solve of the same deck on the same GPU
+through the same drivers: iteration counts within one (the ranks' split sums
+differ from the one-chunk sums by rounding), summaries and the solution
+within 1e-10. The device-resident timestep refuses the decomposed chunk.
+"""
+import datetime
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from tealeaf_b200 import problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, q, text, steps):
+    try:
+        import torch.distributed as dist
+        from tealeaf_b200 import abi, decomp
+        from tealeaf_b200.host import Host
+        dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=60))
+        h = decomp.DistHost(text, 2)
+        out = [h.solve(tt) for tt in range(steps)]
+        u = h.gather_interior("u")
+        refused = None
+        if world > 1:   # the library's own check, past DistHost's
+            try:
+                Host.solve_device(h, steps)
+            except abi.SuiteError as exc:
+                refused = str(exc)
+        q.put((rank, ([(dict(r.iterations), list(r.summary)) for r in out], u, refused)))
+        h.finalise()
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as exc:
+        q.put((rank, "%s: %s" % (type(exc).__name__, exc)))
+
+
+def _run(world, text, steps, timeout=240):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, text, steps)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        out = [q.get(timeout=timeout) for _ in range(world)]
+    finally:
+        for p in procs:
+            p.join(timeout=timeout)
+            if p.is_alive():
+                p.kill()
+    for r, payload in out:
+        if isinstance(payload, str):
+            pytest.fail("rank %d: %s" % (r, payload))
+    return [payload for _, payload in sorted(out, key=lambda t: t[0])]
+
+
+@pytest.mark.parametrize("solver", ["cg", "ppcg"])
+def test_two_ranks_on_one_gpu_match_the_undivided_solve(solver):
+    text = problems.seeded(2, (160, 128), 61, 3, 1, solver=solver, end_step=2, name="dg_" + solver).tea_in()
+    (one, u1, _), = _run(1, text, 2)
+    res = _run(2, text, 2)
+    for out, u, refused in res:
+        assert refused is not None and "error 34" in refused and "four faces are external" in refused
+        assert np.allclose(u, u1, rtol=1e-10, atol=0.0)
+        for (its, summary), (its1, summary1) in zip(out, one):
+            assert its.keys() == its1.keys()
+            assert all(abs(its[k] - its1[k]) <= 1 for k in its)
+            assert summary == pytest.approx(summary1, rel=1e-10)
+    assert res[0][0] == res[1][0]
