@@ -187,9 +187,13 @@ class DistHost(Host):
 
     Needs an initialised torch.distributed process group (`group`, default
     the world); rank r owns chunk r. Messages and the rank sums use `device`:
-    by default the current CUDA device under NCCL, the host otherwise."""
+    by default the current CUDA device under NCCL, the host otherwise. The
+    suite library (its own statically linked CUDA runtime) is pointed at
+    `gpu`: by default the message device's index under NCCL, else the
+    library's default device."""
 
-    def __init__(self, tea_in: str, dims: int = 2, group=None, device: Optional[torch.device] = None, lib=None):
+    def __init__(self, tea_in: str, dims: int = 2, group=None, device: Optional[torch.device] = None,
+                 gpu: Optional[int] = None, lib=None):
         if not dist.is_available() or not dist.is_initialized():
             raise DriverError("DistHost needs an initialised torch.distributed process group")
         self.group = group
@@ -199,12 +203,18 @@ class DistHost(Host):
             device = (torch.device("cuda", torch.cuda.current_device())
                       if dist.get_backend(group) == "nccl" else torch.device("cpu"))
         self.device = device
+        self.gpu = gpu if gpu is not None else (device.index if device.type == "cuda" else None)
         self._lib_override = lib
         super().__init__(tea_in, dims)
 
     # -- chunk and settings (2d/initialise.c:34-134 for this rank) -------------------
     def _load_lib(self):
-        return self._lib_override if self._lib_override is not None else super()._load_lib()
+        if self._lib_override is not None:
+            return self._lib_override
+        lib = super()._load_lib()
+        if self.gpu is not None:
+            getattr(lib, "tl%dd_set_device" % self.dims)(self.gpu)
+        return lib
 
     def _fill_settings(self):
         super()._fill_settings()
