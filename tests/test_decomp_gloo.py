@@ -10,7 +10,7 @@
   ranks, several fields per message; external faces and corners untouched.
 * DistHost: whole timesteps of the reference drivers' sequence through
   run_*, each rank's kernels computed by the oracle's restatement of the
-  reference kernels (tests/oracle_suite2d.py); one rank reproduces the
+  reference kernels (tests/oracle_suites.py); one rank reproduces the
   oracle's own run bit for bit, and 2, 3 and 4 ranks reproduce it to the
   rounding of their split sums (per-rank partial sums added across ranks).
 """
@@ -193,11 +193,11 @@ def test_face_exchange_fills_internal_halos(cells, world, hd, depth):
 
 # -- DistHost ---------------------------------------------------------------------------
 
-def _solve_worker(rank, world, port, q, text, steps):
+def _solve_worker(rank, world, port, q, text, dims, steps):
     try:
         dist = _init(rank, world, port)
-        from oracle_suite2d import OracleSuite2D
-        h = decomp.DistHost(text, 2, lib=OracleSuite2D())
+        from oracle_suites import OracleSuite2D, OracleSuite3D
+        h = decomp.DistHost(text, dims, lib=OracleSuite2D() if dims == 2 else OracleSuite3D())
         out = []
         for tt in range(steps):
             r = h.solve(tt)
@@ -211,37 +211,55 @@ def _solve_worker(rank, world, port, q, text, steps):
 
 
 CASES = {
-    "cg": problems.seeded(2, (48, 40), 51, 3, 1, solver="cg", end_step=2, name="d_cg").tea_in(),
-    "cheby": problems.seeded(2, (48, 40), 52, 3, 1, solver="cheby", end_step=2, name="d_cheby").tea_in(),
-    "ppcg": problems.seeded(2, (48, 40), 53, 3, 1, solver="ppcg", end_step=2, name="d_ppcg").tea_in(),
-    "jacobi": problems.seeded(2, (24, 20), 54, 2, 1, solver="jacobi", end_step=1, name="d_jac").with_(
+    (2, "cg"): problems.seeded(2, (48, 40), 51, 3, 1, solver="cg", end_step=2, name="d_cg").tea_in(),
+    (2, "cheby"): problems.seeded(2, (48, 40), 52, 3, 1, solver="cheby", end_step=2, name="d_cheby").tea_in(),
+    (2, "ppcg"): problems.seeded(2, (48, 40), 53, 3, 1, solver="ppcg", end_step=2, name="d_ppcg").tea_in(),
+    (2, "jacobi"): problems.seeded(2, (24, 20), 54, 2, 1, solver="jacobi", end_step=1, name="d_jac").with_(
         max_iters=400).tea_in(),
+    (3, "cg"): problems.seeded(3, (20, 16, 14), 55, 3, 1, solver="cg", end_step=2, name="d3_cg").tea_in(),
+    (3, "cheby"): problems.seeded(3, (20, 16, 14), 56, 3, 1, solver="cheby", end_step=1, name="d3_ch").tea_in(),
+    (3, "ppcg"): problems.seeded(3, (20, 16, 14), 57, 3, 1, solver="ppcg", end_step=1, name="d3_pp").tea_in(),
 }
 
 
-@pytest.mark.parametrize("solver", ["cg", "cheby", "ppcg", "jacobi"])
-def test_one_rank_reproduces_the_oracle_run(solver, oracle_lib):
-    text = CASES[solver]
-    cfg, states = read_config(text, 2)
+_ONE_RANK = {}
+
+
+def _one_rank(dims, solver):
+    """The one-rank solve of a deck, run once per test session."""
+    if (dims, solver) not in _ONE_RANK:
+        text = CASES[(dims, solver)]
+        cfg, _ = read_config(text, dims)
+        _ONE_RANK[(dims, solver)], = _run(_solve_worker, 1, (text, dims, cfg.end_step))
+    return _ONE_RANK[(dims, solver)]
+
+
+@pytest.mark.parametrize("dims,solver", [(2, "cg"), (2, "cheby"), (2, "ppcg"), (2, "jacobi"), (3, "cg"),
+                                         (3, "cheby"), (3, "ppcg")])
+def test_one_rank_reproduces_the_oracle_run(dims, solver, oracle_lib):
+    text = CASES[(dims, solver)]
+    cfg, states = read_config(text, dims)
     ref = oracle_lib.run(cfg, states)
-    (box, out, _), = _run(_solve_worker, 1, (text, cfg.end_step))
-    assert box.neighbours == (-1, -1, -1, -1)
+    box, out, _ = _one_rank(dims, solver)
+    assert box.neighbours == (-1,) * (2 * dims)
     for (its, summary, _), r in zip(out, ref):
         assert its == r.iterations
         assert summary == r.summary
 
 
-@pytest.mark.parametrize("solver,world", [("cg", 2), ("cg", 4), ("cg", 3), ("cheby", 2), ("ppcg", 4),
-                                          ("jacobi", 2)])
-def test_ranks_reproduce_the_one_rank_solve(solver, world):
+@pytest.mark.parametrize("dims,solver,world", [(2, "cg", 2), (2, "cg", 4), (2, "cg", 3), (2, "cheby", 2),
+                                               (2, "ppcg", 4), (2, "jacobi", 2), (3, "cg", 2), (3, "cg", 4),
+                                               (3, "ppcg", 3)])
+def test_ranks_reproduce_the_one_rank_solve(dims, solver, world):
     """Split sums differ from the one-rank sums by rounding only: iteration
     counts equal and summaries and the solution within 1e-11."""
-    text = CASES[solver]
-    cfg, _ = read_config(text, 2)
-    (_, one, u1), = _run(_solve_worker, 1, (text, cfg.end_step))
-    res = _run(_solve_worker, world, (text, cfg.end_step))
+    text = CASES[(dims, solver)]
+    cfg, _ = read_config(text, dims)
+    _, one, u1 = _one_rank(dims, solver)
+    res = _run(_solve_worker, world, (text, dims, cfg.end_step))
     boxes = [b for b, _, _ in res]
     assert sorted(b.index for b in boxes) == list(range(world))
+    assert sum(int(np.prod(b.cells)) for b in boxes) == u1.size
     for _, out, u in res:
         assert np.allclose(u, u1, rtol=1e-11, atol=0.0)
         for (its, summary, err), (its1, summary1, err1) in zip(out, one):
