@@ -205,6 +205,9 @@ class DistHost(Host):
         self.device = device
         self.gpu = gpu if gpu is not None else (device.index if device.type == "cuda" else None)
         self._lib_override = lib
+        # every rank takes part in the group's first operation (NCCL creates its
+        # communicator there; a first point-to-point batch must involve all ranks)
+        dist.all_reduce(torch.zeros(1, dtype=torch.float64, device=device), group=group)
         super().__init__(tea_in, dims)
 
     # -- chunk and settings (2d/initialise.c:34-134 for this rank) -------------------
