@@ -143,6 +143,14 @@ class FaceExchange:
         self.box = box
         self.group = group
         self.device = device if device is not None else torch.device("cpu")
+        self._buffers = {}   # (face, doubles) -> (send, recv); free again once run() returns
+
+    def _pair(self, face: int, count: int):
+        key = (face, count)
+        if key not in self._buffers:
+            send = torch.empty(count, dtype=torch.float64, device=self.device)
+            self._buffers[key] = (send, torch.empty_like(send))
+        return self._buffers[key]
 
     def face_len(self, face: int, depth: int) -> int:
         n = depth
@@ -164,8 +172,7 @@ class FaceExchange:
                 if nb == EXTERNAL_FACE:
                     continue
                 n = self.face_len(face, depth)
-                send = torch.empty(n * len(fields), dtype=torch.float64, device=self.device)
-                recv = torch.empty_like(send)
+                send, recv = self._pair(face, n * len(fields))
                 for k, f in enumerate(fields):
                     pack(face, depth, f, send.data_ptr() + 8 * k * n, True)
                 peer = self._peer(nb)
