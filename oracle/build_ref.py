@@ -20,6 +20,9 @@ Products in ``oracle/_ref`` (``D`` = 2d or 3d, ``F`` = flavour):
                              shared library: the drop-in proof.
 * ``layout{D}``           -- prints ``offsetof``/``sizeof`` of the reference
                              ``Chunk``/``Settings``/``State`` structs.
+* ``decompose{D}``        -- ``oracle/decompose_probe.c`` + reference host and
+                             omp3 objects: the reference's ``decompose_field``
+                             for every rank of an N-rank run.
 
 Compiler flags follow the reference GNU flags (2d/make.flags:10: -O3
 -funroll-loops -std=gnu99, plus -fopenmp) with ``-DNO_MPI -DENABLE_PROFILING``.
@@ -154,7 +157,9 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
             plan[flav] = (host, omp3, harness)
         layout = _Job(HERE / "layout_probe.c", OUT / "obj" / ("%s_layout.o" % dim),
                       [_ext_include_dir(dim, "omp3"), REF / dim], CFLAGS_STOCK + d_flags)
-        jobs.append(layout)
+        probe = _Job(HERE / "decompose_probe.c", OUT / "obj" / ("%s_decompose.o" % dim),
+                     [_ext_include_dir(dim, "omp3"), REF / dim], CFLAGS_STOCK + d_flags)
+        jobs += [layout, probe]
         if with_b200:
             host_b200 = [j for j in _host_jobs(dim, "b200", "") if j.src.name != "main.c"]
             harness_b200 = _Job(HERE / "ref_harness.c", OUT / "obj" / ("%s_harness_b200.o" % dim),
@@ -170,6 +175,9 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
             _link(OUT / ("tealeaf%s_omp3%s" % (dim, flav)), host_objs + k_objs)
             _link(OUT / ("harness%s_omp3%s" % (dim, flav)), [harness.obj] + no_main + k_objs)
         _link(OUT / ("layout%s" % dim), [layout.obj])
+        host, omp3, _ = plan[""]
+        _link(OUT / ("decompose%s" % dim), [probe.obj] + [j.obj for j in host if j.src.name != "main.c"]
+              + [j.obj for j in omp3])
         if with_b200:
             lib = LIB_DIR / ("lib%s.so" % LIB_NAME[dim])
             if not lib.exists():

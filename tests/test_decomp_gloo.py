@@ -1,10 +1,10 @@
 """The decomposed mesh (tealeaf_b200.decomp) on the CPU, gloo ranks over
 127.0.0.1.
 
-* decompose: chunk counts by the reference's search and metric
-  (decompose_field, 2d/initialise.c:34-134, 3d/initialise.c:34-174), chunks
-  that tile the mesh once, remainders to the first chunks, neighbours that
-  face each other.
+* decompose: every chunk as the reference's own decompose_field
+  (2d/initialise.c:34-134, 3d/initialise.c:34-174, compiled from its sources)
+  places it for 28 meshes; chunks that tile the mesh once, remainders to the
+  first chunks, neighbours that face each other.
 * FaceExchange: after one exchange every halo layer on an internal face
   holds the neighbour's interior cells, for 2D and 3D meshes and 2 to 4
   ranks, several fields per message; external faces and corners untouched.
@@ -101,6 +101,20 @@ def test_chunks_tile_the_mesh_and_face_each_other(cells, n):
         widths = [w for _, w in spans]   # the first c % cnt chunks take one cell more
         assert widths == [c // cnt + 1] * (c % cnt) + [c // cnt] * (cnt - c % cnt)
         assert [l for l, _ in spans] == [sum(widths[:k]) for k in range(cnt)]
+
+
+def test_decompose_matches_the_reference_decompose_field(golden_dir):
+    """Every chunk of 28 meshes (2D and 3D, 1 to 27 ranks) as the reference's
+    own decompose_field placed it (tests/golden/decompose_ref.json, made by
+    tests/golden/make_decompose_golden.py from the reference sources)."""
+    import json
+    cases = json.loads((golden_dir / "decompose_ref.json").read_text())
+    assert len(cases) == 28
+    for c in cases:
+        boxes = decomp.decompose(c["cells"], c["ranks"])
+        got = [{"rank": b.index, "lo": list(b.lo), "cells": list(b.cells), "neighbours": list(b.neighbours)}
+               for b in boxes]
+        assert got == c["chunks"], (c["cells"], c["ranks"])
 
 
 def test_more_chunks_than_cells_is_an_error():
