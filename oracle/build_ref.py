@@ -23,6 +23,12 @@ Products in ``oracle/_ref`` (``D`` = 2d or 3d, ``F`` = flavour):
 * ``decompose{D}``        -- ``oracle/decompose_probe.c`` + reference host and
                              omp3 objects: the reference's ``decompose_field``
                              for every rank of an N-rank run.
+* ``harness{D}_omp3_mpi`` -- the parity harness with the reference host built
+                             for several ranks (no ``-DNO_MPI``) over
+                             ``oracle/minimpi`` (the MPI calls of ``comms.c``
+                             on Unix sockets between processes): the reference's
+                             own multi-rank runs, launched by
+                             ``oracle.oracle.run_reference_ranks``.
 
 Compiler flags follow the reference GNU flags (2d/make.flags:10: -O3
 -funroll-loops -std=gnu99, plus -fopenmp) with ``-DNO_MPI -DENABLE_PROFILING``.
@@ -52,6 +58,8 @@ CC = os.environ.get("TL_CC", "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() els
 CFLAGS_STOCK = ["-O3", "-march=x86-64-v3", "-funroll-loops", "-std=gnu99", "-fopenmp",
                 "-DNO_MPI", "-DENABLE_PROFILING", "-w"]
 FLAVOURS = {"": ["-ffp-contract=off"], "_fast": []}
+
+MPI_DIR = HERE / "minimpi"
 
 SUITE_DIR = {"2d": REPO / "tealeaf_b200" / "suite" / "2d",
              "3d": REPO / "tealeaf_b200" / "suite" / "3d"}
@@ -166,6 +174,15 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
                                 [_ext_include_dir(dim, "b200"), REF / dim],
                                 CFLAGS_STOCK + FLAVOURS[""] + d_flags)
             jobs += host_b200 + [harness_b200]
+        mpi_flags = [f for f in CFLAGS_STOCK if f != "-DNO_MPI"] + FLAVOURS[""] + d_flags
+        host_mpi = [_Job(j.src, OUT / "obj" / ("%s_host_omp3_mpi" % dim) / j.obj.name, j.incs + [MPI_DIR],
+                         [f for f in j.flags if f != "-DNO_MPI"])
+                    for j in _host_jobs(dim, "omp3", "") if j.src.name != "main.c"]
+        harness_mpi = _Job(HERE / "ref_harness.c", OUT / "obj" / ("%s_harness_omp3_mpi.o" % dim),
+                           [_ext_include_dir(dim, "omp3"), REF / dim, MPI_DIR], mpi_flags)
+        minimpi = _Job(MPI_DIR / "minimpi.c", OUT / "obj" / ("%s_minimpi.o" % dim), [MPI_DIR],
+                       ["-O2", "-std=gnu99", "-D_POSIX_C_SOURCE=200809L"])
+        jobs += host_mpi + [harness_mpi, minimpi]
         _compile_all(jobs, parallel)
 
         for flav, (host, omp3, harness) in plan.items():
@@ -178,6 +195,8 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
         host, omp3, _ = plan[""]
         _link(OUT / ("decompose%s" % dim), [probe.obj] + [j.obj for j in host if j.src.name != "main.c"]
               + [j.obj for j in omp3])
+        _link(OUT / ("harness%s_omp3_mpi" % dim), [harness_mpi.obj] + [j.obj for j in host_mpi]
+              + [j.obj for j in omp3] + [minimpi.obj])
         if with_b200:
             lib = LIB_DIR / ("lib%s.so" % LIB_NAME[dim])
             if not lib.exists():

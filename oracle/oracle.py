@@ -225,3 +225,39 @@ def run_reference(tea_in_text: str, dims: int = 2, suite: str = "omp3", threads:
         if r.returncode != 0:
             raise RuntimeError("%s failed (%d):\n%s\n%s" % (exe.name, r.returncode, r.stdout[-4000:], r.stderr[-4000:]))
         return parse_harness_output(r.stdout)
+
+
+def run_reference_ranks(tea_in_text: str, dims: int, ranks: int, threads: int = 1,
+                        timeout: float = 600.0) -> List[StepResult]:
+    """The reference program's own multi-rank run: `ranks` processes of the
+    parity harness built over oracle/minimpi, each in a scratch directory of
+    its own (the reference writes its log there), connected through sockets
+    in a shared one; the master rank's per-step iteration counts and summed
+    field summaries. Every rank must exit 0."""
+    exe = REF_DIR / ("harness%dd_omp3_mpi" % dims)
+    if not exe.exists():
+        raise FileNotFoundError("%s is missing (build with oracle/build_ref.py)" % exe)
+    with tempfile.TemporaryDirectory(prefix="tlm", dir="/tmp") as tmp:
+        deck = Path(tmp, "tea.in")
+        deck.write_text(tea_in_text)
+        procs = []
+        for r in range(ranks):
+            cwd = Path(tmp, "r%d" % r)
+            cwd.mkdir()
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads), MINIMPI_RANK=str(r), MINIMPI_SIZE=str(ranks),
+                       MINIMPI_DIR=tmp, MINIMPI_TIMEOUT=str(int(timeout)))
+            procs.append(subprocess.Popen([str(exe), str(deck)], cwd=cwd, env=env, stdout=subprocess.PIPE,
+                                          stderr=subprocess.PIPE, text=True))
+        outs = []
+        try:
+            for p in procs:
+                outs.append(p.communicate(timeout=timeout))
+        finally:
+            for p in procs:
+                if p.poll() is None:
+                    p.kill()
+        for r, (p, (out, err)) in enumerate(zip(procs, outs)):
+            if p.returncode != 0:
+                raise RuntimeError("%s rank %d failed (%d):\n%s\n%s" % (exe.name, r, p.returncode, out[-4000:],
+                                                                       err[-4000:]))
+        return parse_harness_output(outs[0][0])

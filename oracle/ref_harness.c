@@ -11,9 +11,9 @@
  * reference omp3 suite (the oracle) or the B200 suite (to prove the B200
  * library is a drop-in behind the unchanged `kernel_interface.h`).
  *
- * Output (stdout), besides the reference's own log lines:
+ * Output (stdout, the master rank), besides the reference's own log lines:
  *   TLSTEP <step> <vol> <mass> <ie> <temp> <seconds>
- * with %.17e values, one line per timestep, and a final
+ * with %.17e values (summed over ranks), one line per timestep, and a final
  *   TLDONE <total solve seconds>
  *
  * Build: oracle/build_ref.py (-DTL3D selects the 3D host).
@@ -82,12 +82,21 @@ int main(int argc, char** argv)
 
         double vol = 0.0, mass = 0.0, ie = 0.0, temp = 0.0;
         run_field_summary(&chunks[0], settings, &vol, &mass, &ie, &temp);
-        printf("TLSTEP %d %.17e %.17e %.17e %.17e %.9f\n",
-               tt + 1, vol, mass, ie, temp, t1 - t0);
+        /* the mesh's summary on several ranks (field_summary_driver.c:28-31) */
+        sum_over_ranks(settings, &vol);
+        sum_over_ranks(settings, &mass);
+        sum_over_ranks(settings, &ie);
+        sum_over_ranks(settings, &temp);
+        if (settings->rank == MASTER) {
+            printf("TLSTEP %d %.17e %.17e %.17e %.17e %.9f\n",
+                   tt + 1, vol, mass, ie, temp, t1 - t0);
+            fflush(stdout);
+        }
+    }
+    if (settings->rank == MASTER) {
+        printf("TLDONE %.9f\n", total);
         fflush(stdout);
     }
-    printf("TLDONE %.9f\n", total);
-    fflush(stdout);
 
 #ifndef TL3D
     kernel_finalise_driver(chunks, settings);

@@ -19,8 +19,9 @@ fields being updated between neighbouring chunks before the local halos
   between host processes), and each received message is unpacked on the face
   it came through; the next axis starts once the previous one is unpacked.
 * `DistHost` is tealeaf_b200.host.Host over that chunk: the reference
-  drivers' call sequence, the remote faces before the local halos, and an
-  all-reduce of one double wherever the drivers call sum_over_ranks.
+  drivers' call sequence, the remote faces before the local halos, and,
+  wherever the drivers call sum_over_ranks, the ranks' values gathered and
+  added in rank order.
 
 The device-resident entry points (tl2d_solve_step, tl3d_solve_step, the
 refinement and adjoint forms) hold no exchange and refuse a chunk with an
@@ -274,9 +275,18 @@ class DistHost(Host):
 
     # -- sum_over_ranks (2d/comms.c:55-61) ----------------------------------------------
     def _sum(self, value: float) -> float:
+        """The ranks' values added in rank order, ((v0 + v1) + v2) + ..., on
+        every rank: the same rounding whatever the backend's reduction
+        algorithm, and the order of the MPI stand-in the reference's own
+        multi-rank runs are checked with."""
         t = torch.tensor([value], dtype=torch.float64, device=self.device)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
-        return float(t.item())
+        parts = [torch.empty_like(t) for _ in range(self.world)]
+        dist.all_gather(parts, t, group=self.group)
+        vals = [float(v.item()) for v in parts]
+        acc = vals[0]
+        for v in vals[1:]:
+            acc += v
+        return acc
 
     # -- the device-resident forms hold no exchange -------------------------------------
     def _one_chunk_only(self, what):

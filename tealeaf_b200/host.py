@@ -415,6 +415,10 @@ class Host:
                     self.reset_fields_to_exchange()
                     self.flags[FIELD_P] = True
                     self.halo_update(1)
+                    # ppcg_init_driver sums rro over the ranks once more, although
+                    # it already is the mesh's sum (2d/drivers/ppcg_driver.c:83,
+                    # 3d/drivers/ppcg_solver_driver.c:84): N ranks scale it by N
+                    rro = self._sum(rro)
                 pw = self._sum(self._acc("run_cg_calc_w"))
                 alpha = rro / pw
                 self._acc("run_cg_calc_ur", alpha)
