@@ -1,14 +1,21 @@
 """The decomposed mesh through the B200 suite (tealeaf_b200.decomp.DistHost).
 
 Two ranks run as processes sharing cuda:0: their kernels never wait on each
-other, the faces cross as host buffers over gloo between timesteps'
-run_* calls. Against the undivided solve of the same deck on the same GPU
-through the same drivers: iteration counts within one (the ranks' split sums
-differ from the one-chunk sums by rounding), summaries and the solution
-within 1e-10. The device-resident timestep refuses the decomposed chunk.
+other, the faces cross as host buffers over gloo between run_* calls.
+
+* Against the reference program's own two-rank runs (tests/golden/
+  ref_ranks.json: its host built for several ranks, omp3 kernels): CG,
+  Chebyshev, PPCG and Jacobi, iteration counts within one and summaries
+  within 1e-10 (the GPU's per-chunk sums differ from the serial ones by
+  rounding).
+* Against the undivided solve of the same CG deck on the same GPU: the
+  solution within 1e-10.
+* The device-resident timestep refuses the decomposed chunk.
 """
 import datetime
+import json
 import socket
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -71,13 +78,29 @@ def _run(world, text, steps, timeout=240):
     return [payload for _, payload in sorted(out, key=lambda t: t[0])]
 
 
-@pytest.mark.parametrize("solver", ["cg", "ppcg"])
-def test_two_ranks_on_one_gpu_match_the_undivided_solve(solver):
-    text = problems.seeded(2, (160, 128), 61, 3, 1, solver=solver, end_step=2, name="dg_" + solver).tea_in()
+def _two_rank_cases():
+    cases = json.loads((Path(__file__).resolve().parent / "golden" / "ref_ranks.json").read_text())
+    return [c for c in cases if c["dims"] == 2 and c["ranks"] == 2]
+
+
+@pytest.mark.parametrize("case", _two_rank_cases(), ids=lambda c: c["name"])
+def test_two_ranks_on_one_gpu_match_the_reference_two_rank_run(case):
+    res = _run(2, case["tea_in"], len(case["steps"]))
+    for out, _, refused in res:
+        assert refused is not None and "error 34" in refused and "four faces are external" in refused
+        assert len(out) == len(case["steps"])
+        for (its, summary), ref in zip(out, case["steps"]):
+            assert its.keys() == ref["iterations"].keys()
+            assert all(abs(its[k] - ref["iterations"][k]) <= 1 for k in its)
+            assert summary == pytest.approx(ref["summary"], rel=1e-10)
+    assert res[0][0] == res[1][0]
+
+
+def test_two_ranks_on_one_gpu_match_the_undivided_solve():
+    text = problems.seeded(2, (160, 128), 61, 3, 1, solver="cg", end_step=2, name="dg_cg").tea_in()
     (one, u1, _), = _run(1, text, 2)
     res = _run(2, text, 2)
-    for out, u, refused in res:
-        assert refused is not None and "error 34" in refused and "four faces are external" in refused
+    for out, u, _ in res:
         assert np.allclose(u, u1, rtol=1e-10, atol=0.0)
         for (its, summary), (its1, summary1) in zip(out, one):
             assert its.keys() == its1.keys()
