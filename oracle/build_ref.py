@@ -29,6 +29,8 @@ Products in ``oracle/_ref`` (``D`` = 2d or 3d, ``F`` = flavour):
                              on Unix sockets between processes): the reference's
                              own multi-rank runs, launched by
                              ``oracle.oracle.run_reference_ranks``.
+* ``harness{D}_b200_mpi`` -- the same multi-rank host linked with the B200
+                             library instead of the omp3 suite.
 
 Compiler flags follow the reference GNU flags (2d/make.flags:10: -O3
 -funroll-loops -std=gnu99, plus -fopenmp) with ``-DNO_MPI -DENABLE_PROFILING``.
@@ -154,6 +156,7 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
     OUT.mkdir(parents=True, exist_ok=True)
     for dim in dims:
         d_flags = ["-DTL3D"] if dim == "3d" else []
+        mpi_flags = [f for f in CFLAGS_STOCK if f != "-DNO_MPI"] + FLAVOURS[""] + d_flags
         jobs = []
         plan = {}
         for flav in FLAVOURS:
@@ -173,8 +176,11 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
             harness_b200 = _Job(HERE / "ref_harness.c", OUT / "obj" / ("%s_harness_b200.o" % dim),
                                 [_ext_include_dir(dim, "b200"), REF / dim],
                                 CFLAGS_STOCK + FLAVOURS[""] + d_flags)
-            jobs += host_b200 + [harness_b200]
-        mpi_flags = [f for f in CFLAGS_STOCK if f != "-DNO_MPI"] + FLAVOURS[""] + d_flags
+            host_b200_mpi = [_Job(j.src, OUT / "obj" / ("%s_host_b200_mpi" % dim) / j.obj.name, j.incs + [MPI_DIR],
+                                  [f for f in j.flags if f != "-DNO_MPI"]) for j in host_b200]
+            harness_b200_mpi = _Job(HERE / "ref_harness.c", OUT / "obj" / ("%s_harness_b200_mpi.o" % dim),
+                                    [_ext_include_dir(dim, "b200"), REF / dim, MPI_DIR], mpi_flags)
+            jobs += host_b200 + [harness_b200] + host_b200_mpi + [harness_b200_mpi]
         host_mpi = [_Job(j.src, OUT / "obj" / ("%s_host_omp3_mpi" % dim) / j.obj.name, j.incs + [MPI_DIR],
                          [f for f in j.flags if f != "-DNO_MPI"])
                     for j in _host_jobs(dim, "omp3", "") if j.src.name != "main.c"]
@@ -203,6 +209,8 @@ def build_reference(dims=("2d", "3d"), with_b200=True, parallel=8) -> Path:
                 raise FileNotFoundError("build the B200 library first: %s" % lib)
             _link(OUT / ("harness%s_b200" % dim), [harness_b200.obj] + [j.obj for j in host_b200],
                   [lib, "-Wl,-rpath,$ORIGIN/../../tealeaf_b200/lib"], force=True)
+            _link(OUT / ("harness%s_b200_mpi" % dim), [harness_b200_mpi.obj] + [j.obj for j in host_b200_mpi]
+                  + [minimpi.obj], [lib, "-Wl,-rpath,$ORIGIN/../../tealeaf_b200/lib"], force=True)
     return OUT
 
 

@@ -228,13 +228,14 @@ def run_reference(tea_in_text: str, dims: int = 2, suite: str = "omp3", threads:
 
 
 def run_reference_ranks(tea_in_text: str, dims: int, ranks: int, threads: int = 1,
-                        timeout: float = 600.0) -> List[StepResult]:
+                        timeout: float = 600.0, suite: str = "omp3") -> List[StepResult]:
     """The reference program's own multi-rank run: `ranks` processes of the
     parity harness built over oracle/minimpi, each in a scratch directory of
     its own (the reference writes its log there), connected through sockets
     in a shared one; the master rank's per-step iteration counts and summed
-    field summaries. Every rank must exit 0."""
-    exe = REF_DIR / ("harness%dd_omp3_mpi" % dims)
+    field summaries. Every rank must exit 0. `suite` "b200" runs the same
+    host linked with the B200 library (every rank on the default GPU)."""
+    exe = REF_DIR / ("harness%dd_%s_mpi" % (dims, suite))
     if not exe.exists():
         raise FileNotFoundError("%s is missing (build with oracle/build_ref.py)" % exe)
     with tempfile.TemporaryDirectory(prefix="tlm", dir="/tmp") as tmp:

@@ -11,6 +11,8 @@ other, the faces cross as host buffers over gloo between run_* calls.
 * Against the undivided solve of the same CG deck on the same GPU: the
   solution within 1e-10.
 * The device-resident timestep refuses the decomposed chunk.
+* The reference's own multi-rank host linked with the B200 library against
+  the same host's omp3 two-rank runs.
 """
 import datetime
 import json
@@ -107,3 +109,19 @@ def test_two_ranks_on_one_gpu_match_the_undivided_solve():
             assert all(abs(its[k] - its1[k]) <= 1 for k in its)
             assert summary == pytest.approx(summary1, rel=1e-10)
     assert res[0][0] == res[1][0]
+
+
+@pytest.mark.parametrize("case", _two_rank_cases(), ids=lambda c: c["name"])
+def test_reference_multi_rank_host_on_the_b200_library(case):
+    """The reference's own host built for several ranks (its comms over the
+    MPI stand-in oracle/minimpi), linked with the B200 library instead of the
+    omp3 suite: its remote_halo_driver packs into its own host buffers through
+    run_pack_or_unpack. Two ranks sharing cuda:0 against the same host's omp3
+    two-rank run: iteration counts within one, summaries within 1e-10."""
+    from oracle.oracle import run_reference_ranks
+    steps = run_reference_ranks(case["tea_in"], 2, 2, suite="b200", timeout=240)
+    assert len(steps) == len(case["steps"])
+    for s, ref in zip(steps, case["steps"]):
+        assert s.iterations.keys() == ref["iterations"].keys()
+        assert all(abs(s.iterations[k] - ref["iterations"][k]) <= 1 for k in s.iterations)
+        assert s.summary == pytest.approx(ref["summary"], rel=1e-10)
