@@ -277,6 +277,18 @@ def _reference_ranks():
     return json.loads((Path(__file__).resolve().parent / "golden" / "ref_ranks.json").read_text())
 
 
+@pytest.mark.parametrize("name", ["r2_cg_odd_5ranks", "r3_ppcg_4ranks"])
+def test_reference_multi_rank_harness_reproduces_its_fixture(name):
+    """The MPI stand-in and its build, live: the reference's multi-rank
+    harness rerun on a fixture's deck gives the fixture again."""
+    from oracle.oracle import REF_DIR, run_reference_ranks
+    case = next(c for c in _reference_ranks() if c["name"] == name)
+    if not (REF_DIR / ("harness%dd_omp3_mpi" % case["dims"])).exists():
+        pytest.skip("reference harnesses not built here")
+    steps = run_reference_ranks(case["tea_in"], case["dims"], case["ranks"], timeout=120)
+    assert [(s.iterations, s.summary) for s in steps] == [(r["iterations"], r["summary"]) for r in case["steps"]]
+
+
 @pytest.mark.parametrize("world", sorted({c["ranks"] for c in _reference_ranks()}))
 def test_ranks_reproduce_the_reference_multi_rank_run(world):
     """Bit for bit against the reference program run as the same number of
