@@ -282,7 +282,7 @@ class DistHost(Host):
         t = torch.tensor([value], dtype=torch.float64, device=self.device)
         parts = [torch.empty_like(t) for _ in range(self.world)]
         dist.all_gather(parts, t, group=self.group)
-        vals = [float(v.item()) for v in parts]
+        vals = torch.cat(parts).tolist()
         acc = vals[0]
         for v in vals[1:]:
             acc += v
