@@ -327,3 +327,40 @@ def test_ranks_reproduce_the_one_rank_solve(dims, solver, world):
     # every rank holds the same reduced figures
     for _, out, _ in res[1:]:
         assert out == res[0][1]
+
+
+def _group_worker(rank, world, port, q, jobs):
+    """Ranks {0,1} and {2,3} form two process groups; each solves its job
+    (deck, dims, steps) on its own group."""
+    try:
+        dist = _init(rank, world, port)
+        from oracle_suites import OracleSuite2D, OracleSuite3D
+        groups = [dist.new_group([0, 1]), dist.new_group([2, 3])]
+        mine = rank // 2
+        text, dims, steps = jobs[mine]
+        h = decomp.DistHost(text, dims, group=groups[mine],
+                            lib=OracleSuite2D() if dims == 2 else OracleSuite3D())
+        out = []
+        for tt in range(steps):
+            r = h.solve(tt)
+            out.append((dict(r.iterations), list(r.summary)))
+        q.put((rank, (mine, h.rank, h.box.index, out)))
+        h.finalise()
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as exc:
+        q.put((rank, "%s: %s" % (type(exc).__name__, exc)))
+
+
+def test_ranks_of_a_process_group_solve_on_their_own():
+    """DistHost on a process group: group ranks own the chunks, faces go to
+    the peers' global ranks, sums stay inside the group; two groups of two
+    solving different decks at once each reproduce the reference's two-rank
+    run of their deck bit for bit."""
+    cases = [c for c in _reference_ranks() if c["name"] in ("r2_cg_2ranks", "r3_cg_2ranks")]
+    assert len(cases) == 2
+    res = _run(_group_worker, 4, ([(c["tea_in"], c["dims"], len(c["steps"])) for c in cases],))
+    for rank, (mine, group_rank, chunk, out) in enumerate(res):
+        assert mine == rank // 2 and group_rank == rank % 2 and chunk == group_rank
+        ref = cases[mine]["steps"]
+        assert [(o[0], o[1]) for o in out] == [(r["iterations"], r["summary"]) for r in ref]
