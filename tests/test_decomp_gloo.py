@@ -364,3 +364,47 @@ def test_ranks_of_a_process_group_solve_on_their_own():
         assert mine == rank // 2 and group_rank == rank % 2 and chunk == group_rank
         ref = cases[mine]["steps"]
         assert [(o[0], o[1]) for o in out] == [(r["iterations"], r["summary"]) for r in ref]
+
+
+def _leaver_worker(rank, world, port, q, text):
+    """Rank 1 leaves after set-up; rank 0 starts a timestep, whose first face
+    exchange has no peer."""
+    import datetime as dt
+    import time
+    import torch.distributed as dist
+    try:
+        dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                                timeout=dt.timedelta(seconds=5))
+        from oracle_suites import OracleSuite2D
+        h = decomp.DistHost(text, 2, lib=OracleSuite2D())
+        if rank == 1:
+            q.put((rank, "left"))
+            return
+        t0 = time.monotonic()
+        try:
+            h.solve(0)
+            q.put((rank, "completed"))
+        except Exception as exc:   # the peer is gone: an error, not a hang
+            q.put((rank, ("error", type(exc).__name__, time.monotonic() - t0)))
+    except Exception as exc:
+        q.put((rank, "%s: %s" % (type(exc).__name__, exc)))
+
+
+def test_a_rank_that_leaves_ends_the_others_with_an_error():
+    text = _reference_ranks()[0]["tea_in"]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaver_worker, args=(r, 2, port, q, text)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        out = dict(q.get(timeout=120) for _ in range(2))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert out[1] == "left"
+    kind, _, seconds = out[0]
+    assert kind == "error" and seconds < 60
