@@ -371,7 +371,9 @@ int tl2d_check_bounded_wait(Chunk* chunk, long long polls);
 void tl2d_field_summary_fast(Chunk* chunk, Settings* settings,
         double* vol, double* mass, double* ie, double* temp);
 
-/* One timestep of solve() (2d/diffuse.c:22-80) on the device-resident path. */
+/* One timestep of solve() (2d/diffuse.c:22-80) on the device-resident path.
+ * The chunk must be undivided (four external faces: the loop holds no remote
+ * halo exchange); a chunk with a neighbour reports error 34. */
 void tl2d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats* stats);
 
 /* Statistics of one iterative-refinement timestep. */

@@ -313,7 +313,9 @@ typedef struct TlStepStats3
 void tl3d_field_summary_fast(Chunk* chunk, Settings* settings,
         double* vol, double* mass, double* ie, double* temp);
 
-/* One timestep of solve() (3d/diffuse.c:21-81) on the device-resident path. */
+/* One timestep of solve() (3d/diffuse.c:21-81) on the device-resident path.
+ * The chunk must be undivided (six external faces: the loop holds no remote
+ * halo exchange); a chunk with a neighbour reports error 34. */
 void tl3d_solve_step(Chunk* chunk, Settings* settings, int tt, TlStepStats3* stats);
 
 /* Adjoint of the implicit CG timestep: no counterpart in the reference.
